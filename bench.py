@@ -1,0 +1,345 @@
+"""Benchmark of the grid-block evaluator on the 740-function workload.
+
+Workload (one "step"): rho, grad rho, lap rho, tau and ELF of the total
+density of a seeded C12N4O4H20 molecule (740 spherical AOs, 76 doubly
+occupied MOs, written as FCHK) on a 128^3 grid at 0.2 bohr centred on the
+atoms (2,097,152 points), AUTO backend (AO-MO), block 128, screening 1e-12.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl kumo|reference]
+
+value: grid points/s of the mixed-precision form with the molecule resident
+and outputs left in HBM (device API), max over ranks; `fp64` holds the same
+for the FP64 form.  e2e: the same metric through the host C-ABI call
+(kumo_evaluate_grid, host output arrays, device-to-host copies inside the
+timed region).  Under torchrun each rank evaluates its own copy of the
+workload (independent requests, weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "chem-kumo_b200"))
+
+WORKLOAD = "organic_740"
+METRIC = "grid pts/s (ρ,∇ρ,∇²ρ,τ,ELF) mixed vs FP64 on B200 @≤1e-7 rel; serve p50/p99 ms"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def _props(K):
+    P = K.PropertyKind
+    return [K.density(P.Density), K.density(P.Gradient), K.density(P.Laplacian), K.density(P.Tau), K.density(P.Elf)]
+
+
+def _synth_dir() -> str:
+    d = os.environ.get("KUMO_SYNTH_CACHE") or os.path.join(tempfile.gettempdir(), "kumo_b200_synth")
+    os.makedirs(d, exist_ok=True)
+    return d
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p, "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(tempfile.gettempdir(), f"kumo_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        loaded = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_baseline(fchk: str, grid, nblocks_sample: int, threads: int = 0):
+    """Oracle restatement of the reference's CPU path on a bounded sample of the
+    workload's 128-point blocks (evenly spaced over the grid), all host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    o = O.OracleMolecule.from_fchk(fchk)
+    pts = grid.points()
+    nb = (len(pts) + 127) // 128
+    pick = np.unique(np.linspace(0, nb - 1, nblocks_sample).astype(int))
+    sample = np.concatenate([pts[b * 128:(b + 1) * 128] for b in pick])
+    props = [(0, 0, 0, 0), (1, 0, 0, 0), (3, 0, 0, 0), (4, 0, 0, 0), (6, 0, 0, 0)]
+    o.evaluate(props, points=sample[:256], threads=threads)  # warm-up
+    t0 = time.perf_counter()
+    o.evaluate(props, points=sample, threads=threads)
+    dt = time.perf_counter() - t0
+    cores = O.lib().ko_max_threads()
+    return {"value": len(sample) / dt, "unit": "grid pts/s", "cores": cores, "kind": "port",
+            "sample": f"{len(pick)} evenly spaced 128-point blocks ({len(sample)} points) of the 128^3 grid, "
+                      f"{dt:.1f} s"}
+
+
+def run_reference(args, rank: int) -> None:
+    """--impl reference: the CPU restatement of the reference path (oracle port),
+    all host threads, each step a bounded sample of the workload."""
+    if rank != 0:
+        return
+    import kumo_b200.synth as synth
+    from kumo_b200 import Grid
+
+    fchk = synth.workload_fchk(WORKLOAD, _synth_dir())
+    rec = synth.read_fchk(fchk)
+    coords = np.asarray(rec["Current cartesian coordinates"]).reshape(-1, 3)
+    origin, steps, counts = synth.workload_grid(WORKLOAD, coords)
+    grid = Grid(origin, steps, counts)
+    vals = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        info = cpu_baseline(fchk, grid, args.ref_blocks)
+        if i >= args.warmup:
+            vals.append(info["value"])
+    value = float(np.median(vals))
+    line = {"metric": METRIC, "value": value, "unit": "grid pts/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 2097152 / value * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded FCHK)",
+            "config": {"workload": "organic_740 (C12N4O4H20, 740 AOs, 76 occ MOs) rho/grad/lap/tau/ELF on 128^3 @0.2 bohr",
+                       "backend": "AO_MO", "block": 128, "threshold": 1e-12},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "grid pts/s", "cores": info["cores"], "kind": "port",
+                             "sample": info["sample"]},
+            "e2e": {"value": value, "unit": "grid pts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="kumo", choices=["kumo", "reference"])
+    ap.add_argument("--ref-blocks", type=int, default=96)
+    ap.add_argument("--cpu-blocks", type=int, default=96)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    import kumo_b200 as K
+    import kumo_b200.synth as synth
+
+    torch.cuda.set_device(local)
+    K.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    d = _synth_dir()
+    if rank == 0:
+        fchk = synth.workload_fchk(WORKLOAD, d)
+    if world > 1:
+        dist.barrier()
+    fchk = synth.workload_fchk(WORKLOAD, d)
+    m = K.Molecule.from_fchk(fchk)
+    _, _, xyz = m.atoms()
+    origin, steps, counts = synth.workload_grid(WORKLOAD, xyz)
+    grid = K.Grid(origin, steps, counts)
+    n = grid.npoints
+    props = _props(K)
+    nchan = sum(K.channels(p.kind) for p in props)
+    out = torch.empty(nchan * n, dtype=torch.float64, device="cuda")
+    ptrs, off = [], 0
+    for p in props:
+        ptrs.append(out.data_ptr() + 8 * off)
+        off += K.channels(p.kind) * n
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    ev = {"mixed": K.Evaluator(m, precision=K.Precision.Mixed), "fp64": K.Evaluator(m)}
+
+    def step(name):
+        used = ev[name].evaluate_grid_device(grid, props, ptrs, stream.cuda_stream)
+        assert used == 2
+
+    def timed(name, steps_):
+        times = []
+        for _ in range(steps_):
+            flush.zero_()  # L2 flush between timed iterations (not timed)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step(name)
+            e1.record(stream)
+            times.append((e0, e1))
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in times]
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        step("mixed")
+        step("fp64")
+    torch.cuda.synchronize()
+    # FP64 reference output for the accuracy check of the mixed form.
+    step("fp64")
+    torch.cuda.synchronize()
+    ref = out.clone()
+
+    # Timed region: mixed form, with live kernel timing.
+    clocks = ClockSampler(local)
+    K.profile_reset()
+    K.profile_enable(True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_mixed = timed("mixed", args.steps)
+    clk = clocks.stop()
+    prof = K.profile_read()
+    K.profile_enable(False)
+    ms_mixed = max_over_ranks(float(np.mean(t_mixed)))
+    # Accuracy of the last mixed step against FP64 (scaled metric per field).
+    acc = {}
+    off = 0
+    names = ["rho", "grad_rho", "lap_rho", "tau", "elf"]
+    for p, name in zip(props, names):
+        c = K.channels(p.kind) * n
+        a, r = out[off:off + c], ref[off:off + c]
+        acc[name] = float((a - r).abs().max() / max(1.0, float(r.abs().max())))
+        off += c
+
+    if world > 1:
+        dist.barrier()
+    t_f64 = timed("fp64", args.steps)
+    ms_f64 = max_over_ranks(float(np.mean(t_f64)))
+
+    # End to end through the host C ABI (host outputs, D2H inside the timed region).
+    e2e_eval = K.Evaluator(m, precision=K.Precision.Mixed)
+    e2e_eval.evaluate_grid(grid, props)
+    e2e_times = []
+    for _ in range(max(2, args.steps // 2)):
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        e2e_eval.evaluate_grid(grid, props)
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(float(np.median(e2e_times)))
+
+    if rank == 0:
+        peaks, peak_kind = _peaks()
+        # Dominant kernel of the mixed step.
+        kern = max((k for k in prof if prof[k]["launches"]), key=lambda k: prof[k]["ms"])
+        st = prof[kern]
+        if kern.startswith("contract"):
+            achieved = st["flops"] / (st["ms"] * 1e-3) / 1e12
+            peak = peaks["bf16_tflops"]
+            roof = {"bound": "tensor", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak, "traffic": None,
+                    "peak_source": f"{peak_kind} bf16_tflops (burst)",
+                    "algorithmic": "2 * 128 points * 5 panels * 76 MOs per kept AO row of a block"}
+        else:
+            bytes_ = st["kept_rows"] * 5 * 128 * 4
+            achieved = bytes_ / (st["ms"] * 1e-3) / 1e9
+            peak = peaks["hbm_gbs"]
+            roof = {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "traffic": None, "peak_source": f"{peak_kind} hbm_gbs",
+                    "algorithmic": "kept AO rows * 5 panels * 128 points * 4 B written"}
+        total_ms = sum(v["ms"] for v in prof.values())
+        kernels = {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
+                       "share": round(v["ms"] / total_ms, 4) if total_ms else 0.0} for k, v in prof.items()
+                   if v["launches"]}
+        launches = sum(v["launches"] for v in prof.values())
+        launches += 2 * prof["ao_build"]["launches"]  # kept-row counters of the profiler
+        value = world * n / (ms_mixed * 1e-3)
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "grid pts/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_mixed,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "mixed: f32 AO values + f32 products, f64 reductions/fields",
+            "data": "synthetic (seeded FCHK)",
+            "config": {"workload": "organic_740 (C12N4O4H20, 740 AOs, 76 occ MOs) rho/grad/lap/tau/ELF on 128^3 @0.2 bohr",
+                       "points_per_gpu": n, "backend": "AO_MO", "block": 128, "threshold": 1e-12,
+                       "l2": "256 MB buffer written between timed steps (untimed); AO scratch > L2",
+                       "parallelism": f"replicas x{world} (weak)"},
+            "fp64": {"value": world * n / (ms_f64 * 1e-3), "ms_per_step": ms_f64},
+            "mixed_over_fp64": ms_f64 / ms_mixed,
+            "mixed_vs_fp64_scaled_error": acc,
+            "e2e": {"value": world * n / e2e_s, "unit": "grid pts/s", "h2d_bytes_per_step": 108,
+                    "d2h_bytes_per_step": nchan * n * 8},
+            "roofline": roof,
+            "kernels": kernels,
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(fchk, grid, args.cpu_blocks)
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

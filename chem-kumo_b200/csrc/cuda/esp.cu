@@ -1,0 +1,327 @@
+// Electrostatic potential: host setup of the primitive pairs and the FP64
+// device kernel; see esp.cuh.
+#include "esp.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <numbers>
+#include <stdexcept>
+#include <string>
+
+#include "../host/device_state.hpp"
+#include "chem/kumo/density.hpp"
+
+namespace kumo_dev {
+namespace {
+
+constexpr int hermite_count(int s) { return (s + 1) * (s + 2) * (s + 3) / 6; }
+
+struct Triple {
+    int t, u, v;
+};
+
+std::vector<Triple> hermite_triples(int L) {
+    std::vector<Triple> out;
+    for (int sum = 0; sum <= L; ++sum)
+        for (int t = sum; t >= 0; --t)
+            for (int u = sum - t; u >= 0; --u) out.push_back({t, u, sum - t - u});
+    return out;
+}
+
+// Hermite expansion E^{ij}_t of (x-A)^i (x-B)^j exp(-a (x-A)^2 - b (x-B)^2)
+// without the Gaussian prefactor, by the recursions
+// E^{i+1,j}_t = E^{ij}_{t-1}/(2p) + X_PA E^{ij}_t + (t+1) E^{ij}_{t+1} and the
+// same in j with X_PB, stored [(i*(lb+1)+j)*(la+lb+1)+t].
+class Hermite1D {
+public:
+    Hermite1D(int la, int lb, double p, double pa, double pb)
+        : lb_(lb), width_(la + lb + 1), v_(static_cast<std::size_t>((la + 1) * (lb + 1) * (la + lb + 1)), 0.0) {
+        const double h = 0.5 / p;
+        set(0, 0, 0, 1.0);
+        auto step = [&](int si, int sj, int ti, int tj, double shift) {
+            for (int t = 0; t <= ti + tj; ++t) {
+                double value = shift * get(si, sj, t);
+                if (t > 0) value += h * get(si, sj, t - 1);
+                if (t + 1 <= si + sj) value += (t + 1) * get(si, sj, t + 1);
+                set(ti, tj, t, value);
+            }
+        };
+        for (int i = 0; i < la; ++i) step(i, 0, i + 1, 0, pa);
+        for (int i = 0; i <= la; ++i)
+            for (int j = 0; j < lb; ++j) step(i, j, i, j + 1, pb);
+    }
+    double get(int i, int j, int t) const {
+        if (t < 0 || t > i + j) return 0.0;
+        return v_[static_cast<std::size_t>((i * (lb_ + 1) + j) * width_ + t)];
+    }
+
+private:
+    void set(int i, int j, int t, double x) { v_[static_cast<std::size_t>((i * (lb_ + 1) + j) * width_ + t)] = x; }
+    int lb_, width_;
+    std::vector<double> v_;
+};
+
+}  // namespace
+
+std::vector<double> boys_table_host() {
+    std::vector<double> table(static_cast<std::size_t>(kBoysPoints * kBoysOrders));
+    const int top = kBoysOrders - 1;
+    for (int i = 0; i < kBoysPoints; ++i) {
+        const double T = i * 0.05;
+        const double decay = std::exp(-T);
+        double term = 1.0 / (2.0 * top + 1.0);
+        double sum = term;
+        for (int k = 1; k < 10000 && term > 1e-18 * sum; ++k) {
+            term *= 2.0 * T / (2.0 * top + 2.0 * k + 1.0);
+            sum += term;
+        }
+        double* row = table.data() + static_cast<std::size_t>(i * kBoysOrders);
+        row[top] = decay * sum;
+        for (int m = top; m > 0; --m) row[m - 1] = (2.0 * T * row[m] + decay) / (2.0 * m - 1.0);
+    }
+    return table;
+}
+
+void boys_host(const double* table, double T, int n, double* out) {
+    const int top = n - 1;
+    const double decay = std::exp(-T);
+    if (T >= 40.0) {
+        out[0] = 0.5 * std::sqrt(std::numbers::pi / T);
+        for (int m = 0; m < top; ++m) out[m + 1] = ((2.0 * m + 1.0) * out[m] - decay) / (2.0 * T);
+        return;
+    }
+    const int point = static_cast<int>(std::lround(T / 0.05));
+    const double delta = T - point * 0.05;
+    const double* row = table + static_cast<std::size_t>(point * kBoysOrders);
+    double sum = 0.0, factor = 1.0;
+    for (int k = 0; k < kBoysTaylor; ++k) {
+        sum += row[top + k] * factor;
+        factor *= -delta / (k + 1.0);
+    }
+    out[top] = sum;
+    for (int m = top; m > 0; --m) out[m - 1] = (2.0 * T * out[m] + decay) / (2.0 * m - 1.0);
+}
+
+EspDevice::EspDevice(const chem::kumo::Molecule& m, cudaStream_t stream) {
+    using chem::kumo::detail::check_cuda;
+    const auto& blocks = m.blocks();
+    for (const auto& b : blocks)
+        if (2 * b.angular_momentum > kEspMaxL)
+            throw std::invalid_argument("the B200 electrostatic potential supports shells up to l = 4");
+    const chem::kumo::Matrix P = m.density_matrix(chem::kumo::DensityComponent::Total);
+    std::vector<chem::kumo::Matrix> transforms(kMaxL + 1);
+    for (int l = 2; l <= kMaxL; ++l) transforms[static_cast<std::size_t>(l)] = chem::kumo::gaussian_cartesian_to_pure(l);
+    std::vector<EspPair> pairs;
+    std::vector<double> coef;
+    std::vector<double> cart, left, pc;
+    for (std::size_t a = 0; a < blocks.size(); ++a) {
+        const auto& A = blocks[a];
+        for (std::size_t bb = a; bb < blocks.size(); ++bb) {
+            const auto& B = blocks[bb];
+            const std::size_t na = A.powers.size(), nb = B.powers.size();
+            const std::size_t ra = A.count, rb = B.count;
+            // Cartesian block TA^T P(A, B) TB, doubled off the diagonal.
+            left.assign(na * rb, 0.0);
+            for (std::size_t k = 0; k < na; ++k)
+                for (std::size_t j = 0; j < rb; ++j) {
+                    double s = 0.0;
+                    if (A.pure) {
+                        const auto& T = transforms[static_cast<std::size_t>(A.angular_momentum)];
+                        for (std::size_t i = 0; i < ra; ++i) s += T(i, k) * P(A.offset + i, B.offset + j);
+                    } else {
+                        s = P(A.offset + k, B.offset + j);
+                    }
+                    left[k * rb + j] = s;
+                }
+            cart.assign(na * nb, 0.0);
+            for (std::size_t i = 0; i < na; ++i)
+                for (std::size_t k = 0; k < nb; ++k) {
+                    double s = 0.0;
+                    if (B.pure) {
+                        const auto& T = transforms[static_cast<std::size_t>(B.angular_momentum)];
+                        for (std::size_t j = 0; j < rb; ++j) s += left[i * rb + j] * T(j, k);
+                    } else {
+                        s = left[i * rb + k];
+                    }
+                    cart[i * nb + k] = a != bb ? s * 2.0 : s;
+                }
+            if (std::all_of(cart.begin(), cart.end(), [](double x) { return x == 0.0; })) continue;
+            const int la = A.angular_momentum, lb = B.angular_momentum, L = la + lb;
+            const auto list = hermite_triples(L);
+            double ab2 = 0.0;
+            {
+                const double dx = A.origin[0] - B.origin[0], dy = A.origin[1] - B.origin[1],
+                             dz = A.origin[2] - B.origin[2];
+                ab2 = dx * dx + dy * dy + dz * dz;
+            }
+            const std::size_t npa = A.exponents.size(), npb = B.exponents.size();
+            for (std::size_t p = 0; p < npa; ++p)
+                for (std::size_t q = 0; q < npb; ++q) {
+                    const double alpha = A.exponents[p], beta = B.exponents[q];
+                    const double ex = alpha + beta;
+                    double c3[3];
+                    for (int k = 0; k < 3; ++k) c3[k] = (alpha * A.origin[k] + beta * B.origin[k]) / ex;
+                    const double scale = std::exp(-alpha * beta / ex * ab2) * 2.0 * std::numbers::pi / ex;
+                    const Hermite1D hx(la, lb, ex, c3[0] - A.origin[0], c3[0] - B.origin[0]);
+                    const Hermite1D hy(la, lb, ex, c3[1] - A.origin[1], c3[1] - B.origin[1]);
+                    const Hermite1D hz(la, lb, ex, c3[2] - A.origin[2], c3[2] - B.origin[2]);
+                    pc.assign(list.size(), 0.0);
+                    for (std::size_t i = 0; i < na; ++i) {
+                        const auto& pi = A.powers[i];
+                        for (std::size_t j = 0; j < nb; ++j) {
+                            const auto& pj = B.powers[j];
+                            const double w = cart[i * nb + j] * A.weights[i * npa + p] * B.weights[j * npb + q];
+                            if (w == 0.0) continue;
+                            for (std::size_t k = 0; k < list.size(); ++k) {
+                                const Triple& h = list[k];
+                                if (h.t > pi.x + pj.x || h.u > pi.y + pj.y || h.v > pi.z + pj.z) continue;
+                                pc[k] += w * hx.get(pi.x, pj.x, h.t) * hy.get(pi.y, pj.y, h.u) * hz.get(pi.z, pj.z, h.v);
+                            }
+                        }
+                    }
+                    if (std::all_of(pc.begin(), pc.end(), [](double x) { return x == 0.0; })) continue;
+                    pairs.push_back({ex, c3[0], c3[1], c3[2], L, static_cast<int>(coef.size())});
+                    for (double x : pc) coef.push_back(scale * x);
+                }
+        }
+    }
+    // Recursion table of the Hermite triples up to kEspMaxL.
+    const auto all = hermite_triples(kEspMaxL);
+    auto index_of = [&](int t, int u, int v) {
+        for (std::size_t k = 0; k < all.size(); ++k)
+            if (all[k].t == t && all[k].u == u && all[k].v == v) return static_cast<int>(k);
+        return -1;
+    };
+    std::vector<int4> rec(all.size());
+    for (std::size_t k = 0; k < all.size(); ++k) {
+        const Triple& h = all[k];
+        if (h.t > 0)
+            rec[k] = make_int4(0, index_of(h.t - 1, h.u, h.v), h.t > 1 ? index_of(h.t - 2, h.u, h.v) : -1, h.t - 1);
+        else if (h.u > 0)
+            rec[k] = make_int4(1, index_of(h.t, h.u - 1, h.v), h.u > 1 ? index_of(h.t, h.u - 2, h.v) : -1, h.u - 1);
+        else if (h.v > 0)
+            rec[k] = make_int4(2, index_of(h.t, h.u, h.v - 1), h.v > 1 ? index_of(h.t, h.u, h.v - 2) : -1, h.v - 1);
+        else
+            rec[k] = make_int4(-1, -1, -1, 0);
+    }
+    std::vector<double4> atoms;
+    for (const auto& at : m.atoms())
+        atoms.push_back(make_double4(at.position[0], at.position[1], at.position[2], at.nuclear_charge));
+    const auto table = boys_table_host();
+    auto up = [&](const void* src, std::size_t bytes) {
+        void* d = nullptr;
+        check_cuda(cudaMalloc(&d, std::max<std::size_t>(bytes, 16)), "cudaMalloc (potential)");
+        allocs_.push_back(d);
+        if (bytes) check_cuda(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync (potential)");
+        return d;
+    };
+    view_.pairs = static_cast<const EspPair*>(up(pairs.data(), sizeof(EspPair) * pairs.size()));
+    view_.coef = static_cast<const double*>(up(coef.data(), sizeof(double) * coef.size()));
+    view_.npairs = static_cast<long long>(pairs.size());
+    view_.boys_table = static_cast<const double*>(up(table.data(), sizeof(double) * table.size()));
+    view_.atoms = static_cast<const double4*>(up(atoms.data(), sizeof(double4) * atoms.size()));
+    view_.natoms = static_cast<int>(atoms.size());
+    view_.recursion = static_cast<const int4*>(up(rec.data(), sizeof(int4) * rec.size()));
+    check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize (potential setup)");
+}
+
+EspDevice::~EspDevice() {
+    for (void* p : allocs_) cudaFree(p);
+}
+
+__device__ __forceinline__ void boys_device(const double* table, double T, int n, double* out) {
+    const int top = n - 1;
+    const double decay = exp(-T);
+    if (T >= 40.0) {
+        out[0] = 0.5 * sqrt(3.141592653589793 / T);
+        for (int m = 0; m < top; ++m) out[m + 1] = ((2.0 * m + 1.0) * out[m] - decay) / (2.0 * T);
+        return;
+    }
+    const int point = static_cast<int>(llround(T / 0.05));
+    const double delta = T - point * 0.05;
+    const double* row = table + point * kBoysOrders;
+    double sum = 0.0, factor = 1.0;
+#pragma unroll
+    for (int k = 0; k < kBoysTaylor; ++k) {
+        sum += row[top + k] * factor;
+        factor *= -delta / (k + 1.0);
+    }
+    out[top] = sum;
+    for (int m = top; m > 0; --m) out[m - 1] = (2.0 * T * out[m] + decay) / (2.0 * m - 1.0);
+}
+
+// One thread per point; all threads of a CTA walk the pairs in order, so pair
+// data and coefficients are uniform loads.
+__global__ void __launch_bounds__(128) esp_f64_kernel(const __grid_constant__ EspParams prm) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= prm.src.count) return;
+    double x, y, z;
+    point_at(prm.src, q, x, y, z);
+    const EspView& e = prm.esp;
+    double nuclear = 0.0;
+    for (int a = 0; a < e.natoms; ++a) {
+        const double4 at = e.atoms[a];
+        const double dx = at.x - x, dy = at.y - y, dz = at.z - z;
+        const double d = sqrt(dx * dx + dy * dy + dz * dz);
+        if (at.w == 0.0 || d < 1e-8) continue;
+        nuclear += at.w / d;
+    }
+    constexpr int NT = hermite_count(kEspMaxL);
+    double buf0[NT], buf1[NT];
+    double seeds[kEspMaxL + 1];
+    double sum = 0.0;
+    for (long long i = 0; i < e.npairs; ++i) {
+        const EspPair pr = e.pairs[i];
+        const double pcx = pr.qx - x, pcy = pr.qy - y, pcz = pr.qz - z;
+        const int L = pr.order;
+        boys_device(e.boys_table, pr.p * (pcx * pcx + pcy * pcy + pcz * pcz), L + 1, seeds);
+        double power = 1.0;
+        for (int k = 1; k <= L; ++k) {
+            power *= -2.0 * pr.p;
+            seeds[k] *= power;
+        }
+        double* prev = buf0;
+        double* cur = buf1;
+        for (int n = L; n >= 0; --n) {
+            double* t = prev;
+            prev = cur;
+            cur = t;
+            cur[0] = seeds[n];
+            const int entries = hermite_count(L - n);
+            for (int k = 1; k < entries; ++k) {
+                const int4 r = e.recursion[k];
+                const double X = r.x == 0 ? pcx : (r.x == 1 ? pcy : pcz);
+                double value = X * prev[r.y];
+                if (r.z >= 0) value += r.w * prev[r.z];
+                cur[k] = value;
+            }
+        }
+        const double* c = e.coef + pr.first;
+        const int nk = hermite_count(L);
+        double s = 0.0;
+        for (int k = 0; k < nk; ++k) s += c[k] * cur[k];
+        sum += s;
+    }
+    prm.out[q - prm.out_base] = nuclear - sum;
+}
+
+void launch_esp_f64(const EspParams& p, cudaStream_t stream) {
+    const long long n = p.src.count;
+    if (n <= 0) return;
+    esp_f64_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(p);
+}
+
+__global__ void boys_kernel(const double* table, const double* t, long long n, int nvalues, double* out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v[kBoysMaxOrder + 1];
+    boys_device(table, t[i], nvalues, v);
+    for (int m = 0; m < nvalues; ++m) out[i * nvalues + m] = v[m];
+}
+
+void launch_boys_f64(const double* table, const double* t, long long n, int nvalues, double* out, cudaStream_t stream) {
+    if (n <= 0) return;
+    boys_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(table, t, n, nvalues, out);
+}
+
+}  // namespace kumo_dev

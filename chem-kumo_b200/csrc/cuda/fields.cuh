@@ -1,0 +1,233 @@
+// Per-point density-derivative records and the derived fields of
+// src/evaluator.cpp:117-353, evaluated on the device in the epilogue of the
+// contraction kernels.  All of this is FP64, in both precisions.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace kumo_dev {
+
+constexpr int kMaxProps = 40;
+
+// detail::DensityDerivatives (include/chem/kumo/density.hpp:153-160) with the
+// symmetric Hessian stored as xx, xy, xz, yy, yz, zz.
+struct DevDD {
+    double value, grad[3], hess[6], lap, tau, tau_axes[3];
+};
+
+__device__ __forceinline__ void dd_zero(DevDD& d) {
+    d.value = 0;
+    for (int i = 0; i < 3; ++i) d.grad[i] = d.tau_axes[i] = 0;
+    for (int i = 0; i < 6; ++i) d.hess[i] = 0;
+    d.lap = d.tau = 0;
+}
+
+// combine(), src/density.cpp:50-60.  With the full Hessian the Laplacian is
+// its trace; in Laplacian-only mode it is combined like the other terms.
+__device__ __forceinline__ DevDD dd_combine(const DevDD& a, const DevDD& b, double sign, double scale,
+                                            bool full_hessian) {
+    DevDD d;
+    d.value = scale * (a.value + sign * b.value);
+    for (int i = 0; i < 3; ++i) d.grad[i] = scale * (a.grad[i] + sign * b.grad[i]);
+    for (int i = 0; i < 6; ++i) d.hess[i] = scale * (a.hess[i] + sign * b.hess[i]);
+    d.lap = full_hessian ? (d.hess[0] + d.hess[3]) + d.hess[5] : scale * (a.lap + sign * b.lap);
+    d.tau = scale * (a.tau + sign * b.tau);
+    for (int i = 0; i < 3; ++i) d.tau_axes[i] = scale * (a.tau_axes[i] + sign * b.tau_axes[i]);
+    return d;
+}
+
+// One requested property: kind (PropertyKind), component (DensityComponent)
+// and its output, channels(kind) arrays of `stride` doubles.
+struct OutProp {
+    int kind;
+    int component;
+    double* out;
+};
+
+struct FieldSpec {
+    int nprops = 0;
+    long long stride = 0;       // points per output component array
+    long long out_base = 0;     // global index of the point stored at out[0]
+    OutProp props[kMaxProps];
+};
+
+__device__ __forceinline__ double fermi_constant() {
+    // 0.3 (6 pi^2)^(2/3)
+    return 0.3 * pow(6.0 * 3.141592653589793 * 3.141592653589793, 2.0 / 3.0);
+}
+
+__device__ __forceinline__ double sq3(const double* g) { return g[0] * g[0] + g[1] * g[1] + g[2] * g[2]; }
+
+// elf(), src/evaluator.cpp:127-140.
+__device__ inline double dev_elf(const DevDD* const* ch, int n) {
+    const double fermi = fermi_constant();
+    double pauli = 0.0, uniform = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const DevDD* d = ch[i];
+        if (!(d->value > 0.0)) continue;
+        pauli += d->tau - sq3(d->grad) / (8.0 * d->value);
+        uniform += fermi * pow(d->value, 5.0 / 3.0);
+    }
+    if (!(uniform > 0.0)) return 0.0;
+    const double chi = pauli / uniform;
+    return 1.0 / (1.0 + chi * chi);
+}
+
+// lol(), src/evaluator.cpp:168-179.
+__device__ inline double dev_lol(const DevDD* const* ch, int n) {
+    const double fermi = fermi_constant();
+    double tau = 0.0, uniform = 0.0;
+    for (int i = 0; i < n; ++i) {
+        tau += ch[i]->tau;
+        if (ch[i]->value > 0.0) uniform += fermi * pow(ch[i]->value, 5.0 / 3.0);
+    }
+    if (!(uniform > 0.0)) return 0.0;
+    if (!(tau > 0.0)) return 1.0;
+    return uniform / (tau + uniform);
+}
+
+// gradient_expansion_locator(), src/evaluator.cpp:195-215.
+__device__ inline double dev_gradient_expansion(const DevDD* const* ch, int n, bool lol) {
+    const double fermi = fermi_constant();
+    double uniform = 0.0, pauli = 0.0, kinetic = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const DevDD* d = ch[i];
+        if (!(d->value > 0.0)) continue;
+        const double reference = fermi * pow(d->value, 5.0 / 3.0);
+        const double weizsacker = sq3(d->grad) / d->value;
+        uniform += reference;
+        pauli += reference - weizsacker / 9.0 + d->lap / 6.0;
+        kinetic += reference + weizsacker / 72.0 + d->lap / 6.0;
+    }
+    if (!(uniform > 0.0)) return 0.0;
+    if (lol) {
+        const double den = kinetic + uniform;
+        return den != 0.0 ? uniform / den : 0.0;
+    }
+    const double chi = pauli / uniform;
+    return 1.0 / (1.0 + chi * chi);
+}
+
+// reduced_gradient(), src/evaluator.cpp:145-154 (cap 100).
+__device__ inline double dev_reduced_gradient(const DevDD& d) {
+    const double scale = 2.0 * cbrt(3.0 * 3.141592653589793 * 3.141592653589793);
+    if (!(d.value > 0.0)) return 100.0;
+    const double den = scale * pow(d.value, 4.0 / 3.0);
+    const double norm = sqrt(sq3(d.grad));
+    if (!(den > 0.0) || !(norm < 100.0 * den)) return 100.0;
+    return norm / den;
+}
+
+// Middle eigenvalue of the symmetric 3x3 Hessian by cyclic Jacobi rotations
+// (the sign decides sign(lambda2) rho, src/evaluator.cpp:158-161).
+__device__ inline double dev_lambda2(const double* h6) {
+    double a[3][3] = {{h6[0], h6[1], h6[2]}, {h6[1], h6[3], h6[4]}, {h6[2], h6[4], h6[5]}};
+    for (int sweep = 0; sweep < 64; ++sweep) {
+        const double off = fabs(a[0][1]) + fabs(a[0][2]) + fabs(a[1][2]);
+        if (off == 0.0) break;
+        for (int p = 0; p < 2; ++p)
+            for (int q = p + 1; q < 3; ++q) {
+                if (a[p][q] == 0.0) continue;
+                const double theta = (a[q][q] - a[p][p]) / (2.0 * a[p][q]);
+                const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                for (int k = 0; k < 3; ++k) {
+                    const double akp = a[k][p], akq = a[k][q];
+                    a[k][p] = c * akp - s * akq;
+                    a[k][q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    const double apk = a[p][k], aqk = a[q][k];
+                    a[p][k] = c * apk - s * aqk;
+                    a[q][k] = s * apk + c * aqk;
+                }
+            }
+    }
+    const double e0 = a[0][0], e1 = a[1][1], e2 = a[2][2];
+    if ((e0 >= e1 && e0 <= e2) || (e0 <= e1 && e0 >= e2)) return e0;
+    if ((e1 >= e0 && e1 <= e2) || (e1 <= e0 && e1 >= e2)) return e1;
+    return e2;
+}
+
+__device__ inline double dev_iri(const DevDD& d) {
+    if (!(d.value > 0.0)) return 100.0;
+    const double v = sqrt(sq3(d.grad)) / pow(d.value, 1.1);
+    return v < 100.0 ? v : 100.0;
+}
+
+__device__ inline double dev_dori(const DevDD& d) {
+    if (!(d.value > 0.0)) return 0.0;
+    const double q[3] = {d.grad[0] / d.value, d.grad[1] / d.value, d.grad[2] / d.value};
+    const double q2 = sq3(q);
+    if (!(q2 > 0.0)) return 1.0;
+    const double H[3][3] = {{d.hess[0], d.hess[1], d.hess[2]},
+                            {d.hess[1], d.hess[3], d.hess[4]},
+                            {d.hess[2], d.hess[4], d.hess[5]}};
+    double w[3];
+    for (int a = 0; a < 3; ++a) w[a] = (H[a][0] * q[0] + H[a][1] * q[1] + H[a][2] * q[2]) / d.value - q2 * q[a];
+    const double theta = 4.0 * sq3(w) / (q2 * q2 * q2);
+    if (!isfinite(theta)) return 1.0;
+    return theta / (1.0 + theta);
+}
+
+// store_block(), src/evaluator.cpp:248-353, for one point.  comp[c] is the
+// record of DensityComponent c (Total, Alpha, Beta, Difference).
+__device__ inline void store_point(const FieldSpec& spec, const DevDD* comp, long long q) {
+    const long long p = q - spec.out_base;
+    const long long S = spec.stride;
+    for (int i = 0; i < spec.nprops; ++i) {
+        const int kind = spec.props[i].kind;
+        const int cpt = spec.props[i].component;
+        double* out = spec.props[i].out;
+        if ((kind == 6 || kind == 10 || kind == 35 || kind == 36) && cpt == 0) {
+            const DevDD* ch[2] = {&comp[1], &comp[2]};
+            out[p] = kind == 6 ? dev_elf(ch, 2) : kind == 10 ? dev_lol(ch, 2) : dev_gradient_expansion(ch, 2, kind == 36);
+            continue;
+        }
+        if (kind == 16) {
+            const double t = comp[0].value;
+            out[p] = t > 0.0 ? comp[3].value / t : 0.0;
+            continue;
+        }
+        const DevDD& d = comp[cpt];
+        const DevDD* one[1] = {&d};
+        switch (kind) {
+            case 0: out[p] = d.value; break;
+            case 1:
+                for (int a = 0; a < 3; ++a) out[a * S + p] = d.grad[a];
+                break;
+            case 2:
+                for (int h = 0; h < 6; ++h) out[h * S + p] = d.hess[h];
+                break;
+            case 3: out[p] = d.lap; break;
+            case 4: out[p] = d.tau; break;
+            case 6: out[p] = dev_elf(one, 1); break;
+            case 7: out[p] = dev_reduced_gradient(d); break;
+            case 8: out[p] = dev_lambda2(d.hess) < 0.0 ? -d.value : d.value; break;
+            case 10: out[p] = dev_lol(one, 1); break;
+            case 35: out[p] = dev_gradient_expansion(one, 1, false); break;
+            case 36: out[p] = dev_gradient_expansion(one, 1, true); break;
+            case 11: out[p] = dev_iri(d); break;
+            case 12: out[p] = dev_dori(d); break;
+            case 13: out[p] = d.tau - 0.25 * d.lap; break;
+            case 14: out[p] = 0.25 * d.lap - 2.0 * d.tau; break;
+            case 15: out[p] = 0.25 * d.lap - d.tau; break;
+            case 30:
+                for (int a = 0; a < 3; ++a) out[a * S + p] = d.tau_axes[a];
+                break;
+            case 31: {
+                const int diag[3] = {0, 3, 5};
+                for (int a = 0; a < 3; ++a) out[a * S + p] = d.tau_axes[a] - 0.25 * d.hess[diag[a]];
+                break;
+            }
+            case 32: out[p] = d.tau > 0.0 ? fabs(0.25 * d.lap - 2.0 * d.tau) / d.tau : 0.0; break;
+            case 33: out[p] = d.value > 0.0 ? (0.25 * d.lap - d.tau) / d.value : 0.0; break;
+            case 34: out[p] = d.value > 0.0 ? d.tau / d.value : 0.0; break;
+            case 17: out[p] = d.value > 0.0 ? -d.value * log(d.value) : 0.0; break;
+            case 18: out[p] = d.value > 0.0 ? sq3(d.grad) / d.value : 0.0; break;
+            default: break;
+        }
+    }
+}
+
+}  // namespace kumo_dev

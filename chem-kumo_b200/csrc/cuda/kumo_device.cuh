@@ -1,0 +1,111 @@
+// Device-side data layout of a molecule and of the grid-block evaluation.
+//
+// A molecule lives in HBM as structure-of-arrays tables, uploaded once:
+//  - AO blocks (shells after splitting SP shells, src/basis_math.cpp:27-66):
+//    origin + squared cutoff radius, angular momentum, primitive range,
+//    weight range, AO offset, pure flag;
+//  - primitive exponents and weights (contraction coefficient times
+//    primitive normalisation, ncart x nprim per block, row-major);
+//  - occupied MO coefficients transposed to [AO][MO] (MO contiguous, padded
+//    to a multiple of 8) so that a kept AO row is one contiguous load;
+//  - the density matrices P_total / P_spin (n x n).
+// Cartesian-to-pure matrices for l = 2..4 travel in the kernel parameters
+// (constant bank).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace kumo_dev {
+
+constexpr int kBlockPoints = 128;  // points per CTA of the AO build (screening block)
+constexpr int kMaxL = 4;           // largest angular momentum of the device kernels
+constexpr int kMaxPrim = 16;       // largest number of primitives per shell
+constexpr int kMaxBlocksPerWave = 1 << 20;
+
+// Panel sets stored in the AO scratch (mask panels are always those of the
+// reference's AO order: 1, 4 or 10).
+enum PanelMode : int {
+    kPanelsValue = 1,      // value
+    kPanelsGradient = 4,   // value, x, y, z
+    kPanelsLaplacian = 5,  // value, x, y, z, xx + yy + zz
+    kPanelsFull = 10,      // value, x, y, z, xx, xy, xz, yy, yz, zz
+};
+
+struct DevBasis {
+    int nblocks = 0;
+    int nao = 0;
+    int max_l = 0;
+    int max_count = 0;               // largest number of AOs of one block
+    const double4* origin_r2 = nullptr;  // x, y, z, cutoff radius squared
+    const int4* info = nullptr;          // l | pure << 8 | nprim << 16, prim offset, weight offset, ao offset
+    const double* exps = nullptr;
+    const double* weights = nullptr;
+    const float* exps_f = nullptr;
+    const float* weights_f = nullptr;
+};
+
+// Source of the evaluation points: a regular grid (generated in the kernel)
+// or an explicit 3 x N array (x, y, z per point).
+struct PointSource {
+    const double* points = nullptr;  // device, 3 * count, or null for a grid
+    double origin[3] = {0, 0, 0};
+    double steps[9] = {0};           // column a = step vector of axis a
+    long long ny = 1, nz = 1;
+    long long count = 0;
+};
+
+#ifdef __CUDACC__
+__device__ __forceinline__ void point_at(const PointSource& s, long long q, double& x, double& y,
+                                         double& z) {
+    if (s.points) {
+        x = s.points[3 * q];
+        y = s.points[3 * q + 1];
+        z = s.points[3 * q + 2];
+        return;
+    }
+    // src/grid_geometry.hpp:59-68: linear = (i * ny + j) * nz + k.
+    const long long i = q / (s.ny * s.nz);
+    const long long j = (q / s.nz) % s.ny;
+    const long long k = q % s.nz;
+    const double di = (double)i, dj = (double)j, dk = (double)k;
+    x = __dadd_rn(s.origin[0], __dadd_rn(__dadd_rn(__dmul_rn(s.steps[0], di), __dmul_rn(s.steps[3], dj)),
+                                         __dmul_rn(s.steps[6], dk)));
+    y = __dadd_rn(s.origin[1], __dadd_rn(__dadd_rn(__dmul_rn(s.steps[1], di), __dmul_rn(s.steps[4], dj)),
+                                         __dmul_rn(s.steps[7], dk)));
+    z = __dadd_rn(s.origin[2], __dadd_rn(__dadd_rn(__dmul_rn(s.steps[2], di), __dmul_rn(s.steps[5], dj)),
+                                         __dmul_rn(s.steps[8], dk)));
+}
+#endif
+
+// AO scratch of one wave of point blocks.  Block b of the wave holds its
+// kept AO rows, compacted in AO order:
+//   panels[(b * npanel + c) * row_stride + slot) * 128 + j]
+// with kept[b * row_stride + slot] the AO index of the slot and nkept[b]
+// the number of slots.  T is double (FP64 path) or float (mixed path).
+template <typename T>
+struct AoScratch {
+    T* panels = nullptr;
+    int* kept = nullptr;
+    int* nkept = nullptr;
+    int row_stride = 0;   // >= nao
+    int npanel = 0;
+};
+
+// Parameters of the AO build of one wave.
+template <typename T>
+struct AoBuildParams {
+    DevBasis basis;
+    PointSource src;
+    long long first_point = 0;     // first point of the wave
+    long long block_size = 128;    // points per screening block (<= 128)
+    int nblocks = 0;               // blocks in this wave
+    double threshold = 1e-12;      // screening threshold (0 keeps every AO)
+    AoScratch<T> out;
+    T pure[3][135];                // Cartesian-to-pure matrices, l = 2..4, row-major
+};
+
+template <typename T>
+void launch_ao_build(const AoBuildParams<T>& p, int order, int npanel, cudaStream_t stream);
+
+}  // namespace kumo_dev

@@ -1,0 +1,477 @@
+// extern "C" boundary of the B200 grid evaluator (include/kumo_b200.h).
+#include "kumo_b200.h"
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../cuda/esp.cuh"
+#include "chem/kumo/evaluator.hpp"
+#include "device_state.hpp"
+#include "profile.hpp"
+
+struct kumo_molecule {
+    chem::kumo::Molecule mol;
+};
+
+namespace {
+
+using namespace chem::kumo;
+
+void put(char* err, size_t errlen, const std::string& msg) {
+    if (err && errlen) {
+        const size_t n = std::min(errlen - 1, msg.size());
+        std::memcpy(err, msg.data(), n);
+        err[n] = '\0';
+    }
+}
+
+template <typename F>
+int guarded(char* err, size_t errlen, F&& f) {
+    try {
+        f();
+        put(err, errlen, "");
+        return KUMO_OK;
+    } catch (const std::bad_alloc& e) {
+        put(err, errlen, "out of memory");
+        return KUMO_OUT_OF_MEMORY;
+    } catch (const std::out_of_range& e) {
+        put(err, errlen, e.what());
+        return KUMO_OUT_OF_RANGE;
+    } catch (const std::invalid_argument& e) {
+        put(err, errlen, e.what());
+        return KUMO_INVALID_ARGUMENT;
+    } catch (const std::runtime_error& e) {
+        const std::string w = e.what();
+        put(err, errlen, w);
+        return w.rfind("CUDA error", 0) == 0 ? KUMO_CUDA_ERROR : KUMO_RUNTIME_ERROR;
+    } catch (const std::exception& e) {
+        put(err, errlen, e.what());
+        return KUMO_RUNTIME_ERROR;
+    } catch (...) {
+        put(err, errlen, "unknown error");
+        return KUMO_RUNTIME_ERROR;
+    }
+}
+
+EvaluationOptions to_options(const kumo_options* o) {
+    EvaluationOptions e;
+    if (!o) return e;
+    if (o->block_size < 0) throw std::invalid_argument("evaluation block_size must be in [1, 65536]");
+    e.block_size = static_cast<std::size_t>(o->block_size);
+    if (o->backend < 0 || o->backend > 2) throw std::invalid_argument("unknown evaluation backend");
+    e.backend = static_cast<Backend>(o->backend);
+    e.screening_threshold = o->screening_threshold;
+    e.potential_tolerance = o->potential_tolerance;
+    if (o->precision != 0 && o->precision != 1) throw std::invalid_argument("unknown precision");
+    e.precision = o->precision ? Precision::Mixed : Precision::FP64;
+    return e;
+}
+
+Grid to_grid(const kumo_grid* g) {
+    if (!g) throw std::invalid_argument("null grid");
+    Grid r;
+    for (int k = 0; k < 3; ++k) r.origin[k] = g->origin[k];
+    for (int i = 0; i < 9; ++i) r.steps.m[static_cast<std::size_t>(i)] = g->steps[i];
+    for (int k = 0; k < 3; ++k) r.counts[k] = g->counts[k];
+    return r;
+}
+
+Request to_request(const kumo_property* props, int n) {
+    if (n < 0 || (n > 0 && !props)) throw std::invalid_argument("invalid property list");
+    Request r;
+    for (int i = 0; i < n; ++i) {
+        if (props[i].kind < 0 || props[i].kind > static_cast<int>(PropertyKind::LolTsirelsonStash))
+            throw std::invalid_argument("unknown property kind");
+        if (props[i].component < 0 || props[i].component > 3) throw std::invalid_argument("invalid density spin component");
+        if (props[i].channel < 0 || props[i].channel > 1) throw std::invalid_argument("MO spin channel must be alpha or beta");
+        if (props[i].orbital_index < 0) throw std::invalid_argument("orbital indices are one-based");
+        r.add({static_cast<PropertyKind>(props[i].kind), static_cast<DensityComponent>(props[i].component),
+               static_cast<SpinChannel>(props[i].channel), static_cast<std::size_t>(props[i].orbital_index)});
+    }
+    return r;
+}
+
+void copy_results(const Results& res, const Request& req, double* const* outputs, std::size_t n) {
+    const auto& props = req.properties();
+    for (std::size_t i = 0; i < props.size(); ++i) {
+        const auto& f = res.get(props[i]);
+        for (std::size_t c = 0; c < f.components.size(); ++c)
+            std::copy(f.components[c].begin(), f.components[c].end(), outputs[i] + c * n);
+    }
+}
+
+struct DevBuf {
+    void* p = nullptr;
+    explicit DevBuf(std::size_t bytes) { detail::check_cuda(cudaMalloc(&p, std::max<std::size_t>(bytes, 16)), "cudaMalloc"); }
+    ~DevBuf() { cudaFree(p); }
+    template <typename T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+};
+
+template <typename T>
+void run_ao_build(const detail::DeviceMolecule& d, const kumo_dev::PointSource& src, long long block_size, int nblocks,
+                  int order, int npanel, double threshold, kumo_dev::AoScratch<T> out, long long first_point) {
+    kumo_dev::AoBuildParams<T> p{};
+    p.basis = d.basis;
+    p.src = src;
+    p.first_point = first_point;
+    p.block_size = block_size;
+    p.nblocks = nblocks;
+    p.threshold = threshold;
+    p.out = out;
+    for (int l = 0; l < 3; ++l)
+        for (int i = 0; i < 135; ++i) p.pure[l][i] = sizeof(T) == 8 ? static_cast<T>(d.pure_d[l][i]) : static_cast<T>(d.pure_f[l][i]);
+    kumo_dev::launch_ao_build<T>(p, order, npanel, nullptr);
+    detail::check_cuda(cudaGetLastError(), "ao_build launch");
+}
+
+}  // namespace
+
+extern "C" {
+
+void kumo_default_options(kumo_options* opt) {
+    if (!opt) return;
+    opt->block_size = 128;
+    opt->backend = 0;
+    opt->screening_threshold = default_screening_threshold;
+    opt->potential_tolerance = 1e-8;
+    opt->precision = 0;
+}
+
+int kumo_set_device(int device, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] { detail::check_cuda(cudaSetDevice(device), "cudaSetDevice"); });
+}
+
+int kumo_molecule_from_fchk(const char* path, kumo_molecule** out, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!path || !out) throw std::invalid_argument("null argument");
+        *out = new kumo_molecule{Molecule::from_fchk(path)};
+    });
+}
+
+int kumo_molecule_from_arrays(int natoms, const int* z, const double* charges, const double* coords, int nshell,
+                              const int* shell_types, const int* nprim, const int* shell_atom, const double* exponents,
+                              const double* coefs, const double* p_coefs, const double* shell_xyz, int nbasis,
+                              const double* packed_total, const double* packed_spin, int nalpha, int nbeta,
+                              const double* alpha_mos, int nmo_alpha, const double* beta_mos, int nmo_beta,
+                              kumo_molecule** out, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!out || natoms <= 0 || nshell <= 0 || nbasis <= 0 || !z || !coords || !shell_types || !nprim ||
+            !shell_atom || !exponents || !coefs || !shell_xyz || !packed_total)
+            throw std::invalid_argument("invalid molecule arrays");
+        std::vector<Atom> atoms;
+        for (int i = 0; i < natoms; ++i)
+            atoms.push_back({z[i], charges ? charges[i] : static_cast<double>(z[i]),
+                             {coords[3 * i], coords[3 * i + 1], coords[3 * i + 2]}});
+        std::vector<Shell> shells;
+        std::size_t off = 0;
+        for (int s = 0; s < nshell; ++s) {
+            Shell sh;
+            const int t = shell_types[s];
+            if (shell_atom[s] < 1 || shell_atom[s] > natoms) throw std::runtime_error("invalid 1-based shell center in fchk");
+            if (nprim[s] <= 0) throw std::runtime_error("invalid Number of primitives per shell in fchk");
+            sh.center = static_cast<std::size_t>(shell_atom[s] - 1);
+            sh.is_sp = t == -1;
+            sh.angular_momentum = sh.is_sp ? 1 : std::abs(t);
+            sh.representation = (!sh.is_sp && t <= -2) ? ShellRepresentation::Pure : ShellRepresentation::Cartesian;
+            sh.origin = {shell_xyz[3 * s], shell_xyz[3 * s + 1], shell_xyz[3 * s + 2]};
+            sh.exponents.assign(exponents + off, exponents + off + nprim[s]);
+            sh.coefficients.assign(coefs + off, coefs + off + nprim[s]);
+            if (p_coefs)
+                sh.p_coefficients.assign(p_coefs + off, p_coefs + off + nprim[s]);
+            else
+                sh.p_coefficients.assign(static_cast<std::size_t>(nprim[s]), 0.0);
+            if (sh.is_sp && !p_coefs) throw std::runtime_error("missing P(S=P) coefficients for sp shell");
+            off += static_cast<std::size_t>(nprim[s]);
+            shells.push_back(std::move(sh));
+        }
+        BasisSet basis(std::move(shells), static_cast<std::size_t>(nbasis));
+        const std::size_t n = static_cast<std::size_t>(nbasis);
+        auto unpack = [n](const double* packed) {
+            Matrix m(n, n);
+            std::size_t q = 0;
+            for (std::size_t i = 0; i < n; ++i)
+                for (std::size_t j = 0; j <= i; ++j, ++q) m(i, j) = m(j, i) = packed[q];
+            return m;
+        };
+        Matrix total = unpack(packed_total);
+        Matrix spin = packed_spin ? unpack(packed_spin) : Matrix(n, n);
+        Matrix ca, cb;
+        if (alpha_mos && nmo_alpha > 0) {
+            ca = Matrix(n, static_cast<std::size_t>(nmo_alpha));
+            std::copy(alpha_mos, alpha_mos + n * static_cast<std::size_t>(nmo_alpha), ca.data());
+        }
+        if (beta_mos && nmo_beta > 0) {
+            cb = Matrix(n, static_cast<std::size_t>(nmo_beta));
+            std::copy(beta_mos, beta_mos + n * static_cast<std::size_t>(nmo_beta), cb.data());
+        }
+        *out = new kumo_molecule{Molecule::from_parts(std::move(atoms), std::move(basis), std::move(total), std::move(spin),
+                                                      nalpha, nbeta, std::move(ca), std::move(cb), {}, {})};
+    });
+}
+
+void kumo_molecule_destroy(kumo_molecule* m) { delete m; }
+
+int kumo_molecule_info_get(const kumo_molecule* m, kumo_molecule_info* info) {
+    if (!m || !info) return KUMO_INVALID_ARGUMENT;
+    const auto& mol = m->mol;
+    const auto& e = mol.electronic_structure_info();
+    info->natoms = static_cast<int>(mol.atoms().size());
+    info->nbasis = static_cast<int>(mol.basis_size());
+    info->nalpha = static_cast<int>(mol.occupied_count(SpinChannel::Alpha));
+    info->nbeta = static_cast<int>(mol.occupied_count(SpinChannel::Beta));
+    info->nmo_alpha = static_cast<int>(mol.orbital_count(SpinChannel::Alpha));
+    info->nmo_beta = static_cast<int>(mol.orbital_count(SpinChannel::Beta));
+    info->unrestricted = mol.unrestricted() ? 1 : 0;
+    info->ao_mo_eligible = e.ao_mo_eligible() ? 1 : 0;
+    info->check_errors[0] = e.total_absolute_error;
+    info->check_errors[1] = e.total_relative_error;
+    info->check_errors[2] = e.spin_absolute_error;
+    info->check_errors[3] = e.spin_relative_error;
+    info->nblocks = static_cast<int>(mol.blocks().size());
+    info->device_bytes = static_cast<long long>(mol.device_bytes());
+    return KUMO_OK;
+}
+
+int kumo_molecule_atoms(const kumo_molecule* m, int* z, double* charges, double* xyz) {
+    if (!m) return KUMO_INVALID_ARGUMENT;
+    const auto& atoms = m->mol.atoms();
+    for (std::size_t i = 0; i < atoms.size(); ++i) {
+        if (z) z[i] = atoms[i].atomic_number;
+        if (charges) charges[i] = atoms[i].nuclear_charge;
+        if (xyz)
+            for (int k = 0; k < 3; ++k) xyz[3 * i + static_cast<std::size_t>(k)] = atoms[i].position[k];
+    }
+    return KUMO_OK;
+}
+
+int kumo_molecule_block(const kumo_molecule* m, int i, int* l, int* nprim, int* offset, int* count, int* pure,
+                        double* cutoff_r2) {
+    if (!m || i < 0 || static_cast<std::size_t>(i) >= m->mol.blocks().size()) return KUMO_OUT_OF_RANGE;
+    const auto& b = m->mol.blocks()[static_cast<std::size_t>(i)];
+    *l = b.angular_momentum;
+    *nprim = static_cast<int>(b.exponents.size());
+    *offset = static_cast<int>(b.offset);
+    *count = static_cast<int>(b.count);
+    *pure = b.pure ? 1 : 0;
+    *cutoff_r2 = b.cutoff_radius2;
+    return KUMO_OK;
+}
+
+int kumo_evaluate_grid(const kumo_molecule* m, const kumo_options* opt, const kumo_grid* grid, const kumo_property* props,
+                       int nprops, double* const* outputs, int* backend_used, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!m) throw std::invalid_argument("null molecule");
+        const Grid g = to_grid(grid);
+        const Request req = to_request(props, nprops);
+        Evaluator ev(m->mol, to_options(opt));
+        const Results res = ev.evaluate(g, req);
+        if (backend_used) *backend_used = static_cast<int>(res.backend_used());
+        const std::size_t n = static_cast<std::size_t>(g.counts[0]) * g.counts[1] * g.counts[2];
+        copy_results(res, req, outputs, n);
+    });
+}
+
+int kumo_evaluate_points(const kumo_molecule* m, const kumo_options* opt, const double* points, long long npoints,
+                         const kumo_property* props, int nprops, double* const* outputs, int* backend_used, char* err,
+                         size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!m || npoints < 0 || (npoints > 0 && !points)) throw std::invalid_argument("invalid points");
+        const Request req = to_request(props, nprops);
+        Evaluator ev(m->mol, to_options(opt));
+        const Results res = ev.evaluate(Points{points, static_cast<std::size_t>(npoints)}, req);
+        if (backend_used) *backend_used = static_cast<int>(res.backend_used());
+        copy_results(res, req, outputs, static_cast<std::size_t>(npoints));
+    });
+}
+
+int kumo_evaluate_grid_device(const kumo_molecule* m, const kumo_options* opt, const kumo_grid* grid,
+                              const kumo_property* props, int nprops, double* const* outputs, void* stream,
+                              int* backend_used, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!m) throw std::invalid_argument("null molecule");
+        const Grid g = to_grid(grid);
+        const Request req = to_request(props, nprops);
+        Evaluator ev(m->mol, to_options(opt));
+        const Backend b = ev.evaluate_device(g, req, outputs, stream);
+        if (backend_used) *backend_used = static_cast<int>(b);
+    });
+}
+
+int kumo_evaluate_points_device(const kumo_molecule* m, const kumo_options* opt, const double* device_points,
+                                long long npoints, const kumo_property* props, int nprops, double* const* outputs,
+                                void* stream, int* backend_used, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!m || npoints < 0) throw std::invalid_argument("invalid points");
+        const Request req = to_request(props, nprops);
+        Evaluator ev(m->mol, to_options(opt));
+        const Backend b = ev.evaluate_device(Points{device_points, static_cast<std::size_t>(npoints)}, req, outputs, stream);
+        if (backend_used) *backend_used = static_cast<int>(b);
+    });
+}
+
+int kumo_ao_panels(const kumo_molecule* m, const double* points, int npts, int order, int precision, double* out,
+                   char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!m || !points || !out || npts <= 0 || npts > kumo_dev::kBlockPoints)
+            throw std::invalid_argument("kumo_ao_panels needs 1 to 128 points");
+        if (order < 0 || order > 2) throw std::invalid_argument("AO derivative order must be 0, 1 or 2");
+        const auto& d = m->mol.device();
+        const int nao = d.basis.nao;
+        const int npanel = order == 0 ? 1 : (order == 1 ? 4 : 10);
+        DevBuf pts(sizeof(double) * 3 * static_cast<std::size_t>(npts));
+        detail::check_cuda(cudaMemcpy(pts.as<double>(), points, sizeof(double) * 3 * npts, cudaMemcpyHostToDevice), "cudaMemcpy");
+        kumo_dev::PointSource src{};
+        src.points = pts.as<double>();
+        src.count = npts;
+        DevBuf kept(sizeof(int) * nao), nkept(sizeof(int));
+        const std::size_t cells = static_cast<std::size_t>(npanel) * nao * kumo_dev::kBlockPoints;
+        std::vector<double> host(cells);
+        if (precision == 0) {
+            DevBuf panels(sizeof(double) * cells);
+            run_ao_build<double>(d, src, npts, 1, order, npanel, 0.0,
+                                 {panels.as<double>(), kept.as<int>(), nkept.as<int>(), nao, npanel}, 0);
+            detail::check_cuda(cudaMemcpy(host.data(), panels.as<double>(), sizeof(double) * cells, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        } else {
+            DevBuf panels(sizeof(float) * cells);
+            run_ao_build<float>(d, src, npts, 1, order, npanel, 0.0,
+                                {panels.as<float>(), kept.as<int>(), nkept.as<int>(), nao, npanel}, 0);
+            std::vector<float> hf(cells);
+            detail::check_cuda(cudaMemcpy(hf.data(), panels.as<float>(), sizeof(float) * cells, cudaMemcpyDeviceToHost), "cudaMemcpy");
+            std::copy(hf.begin(), hf.end(), host.begin());
+        }
+        // scratch [c][ao][point] -> out column-major nao x (panels * npts)
+        for (int c = 0; c < npanel; ++c)
+            for (int a = 0; a < nao; ++a)
+                for (int j = 0; j < npts; ++j)
+                    out[(static_cast<std::size_t>(c) * npts + j) * nao + a] =
+                        host[(static_cast<std::size_t>(c) * nao + a) * kumo_dev::kBlockPoints + j];
+    });
+}
+
+int kumo_screening_masks(const kumo_molecule* m, const kumo_grid* grid, long long block_size, int ao_order,
+                         double threshold, unsigned char* mask, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!m || !mask) throw std::invalid_argument("null argument");
+        if (block_size <= 0 || block_size > kumo_dev::kBlockPoints)
+            throw std::invalid_argument("block_size must be in [1, 128] for device screening masks");
+        if (ao_order < 0 || ao_order > 2) throw std::invalid_argument("AO derivative order must be 0, 1 or 2");
+        const Grid g = to_grid(grid);
+        const long long n = static_cast<long long>(g.counts[0]) * g.counts[1] * g.counts[2];
+        const auto& d = m->mol.device();
+        const int nao = d.basis.nao;
+        const int npanel = ao_order == 0 ? 1 : (ao_order == 1 ? 4 : 10);
+        kumo_dev::PointSource src{};
+        for (int k = 0; k < 3; ++k) src.origin[k] = g.origin[k];
+        for (int i = 0; i < 9; ++i) src.steps[i] = g.steps.m[static_cast<std::size_t>(i)];
+        src.ny = g.counts[1];
+        src.nz = g.counts[2];
+        src.count = n;
+        const long long nblocks = (n + block_size - 1) / block_size;
+        const int W = static_cast<int>(std::min<long long>(nblocks, 256));
+        DevBuf panels(sizeof(double) * static_cast<std::size_t>(npanel) * nao * kumo_dev::kBlockPoints * W);
+        DevBuf kept(sizeof(int) * static_cast<std::size_t>(nao) * W), nkept(sizeof(int) * W);
+        std::vector<int> hk(static_cast<std::size_t>(nao) * W), hn(W);
+        std::fill(mask, mask + nblocks * nao, 0);
+        for (long long b0 = 0; b0 < nblocks; b0 += W) {
+            const int nb = static_cast<int>(std::min<long long>(W, nblocks - b0));
+            run_ao_build<double>(d, src, block_size, nb, ao_order, npanel, threshold,
+                                 {panels.as<double>(), kept.as<int>(), nkept.as<int>(), nao, npanel}, b0 * block_size);
+            detail::check_cuda(cudaMemcpy(hk.data(), kept.as<int>(), sizeof(int) * nao * nb, cudaMemcpyDeviceToHost), "cudaMemcpy");
+            detail::check_cuda(cudaMemcpy(hn.data(), nkept.as<int>(), sizeof(int) * nb, cudaMemcpyDeviceToHost), "cudaMemcpy");
+            for (int b = 0; b < nb; ++b)
+                for (int s = 0; s < hn[b]; ++s) mask[(b0 + b) * nao + hk[static_cast<std::size_t>(b) * nao + s]] = 1;
+        }
+    });
+}
+
+int kumo_boys(const double* t, long long n, int nvalues, double* out, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (nvalues <= 0 || nvalues > kumo_dev::kBoysMaxOrder + 1) throw std::invalid_argument("unsupported Boys function order");
+        for (long long i = 0; i < n; ++i)
+            if (!std::isfinite(t[i]) || t[i] < 0.0)
+                throw std::invalid_argument("Boys function argument must be finite and nonnegative");
+        if (n == 0) return;
+        const auto table = kumo_dev::boys_table_host();
+        DevBuf dt(sizeof(double) * table.size()), din(sizeof(double) * n), dout(sizeof(double) * n * nvalues);
+        detail::check_cuda(cudaMemcpy(dt.as<double>(), table.data(), sizeof(double) * table.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
+        detail::check_cuda(cudaMemcpy(din.as<double>(), t, sizeof(double) * n, cudaMemcpyHostToDevice), "cudaMemcpy");
+        kumo_dev::launch_boys_f64(dt.as<double>(), din.as<double>(), n, nvalues, dout.as<double>(), nullptr);
+        detail::check_cuda(cudaGetLastError(), "boys launch");
+        detail::check_cuda(cudaMemcpy(out, dout.as<double>(), sizeof(double) * n * nvalues, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    });
+}
+
+int kumo_esp_pair_count(const kumo_molecule* m, long long* count, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!m || !count) throw std::invalid_argument("null argument");
+        kumo_dev::EspDevice e(m->mol, nullptr);
+        *count = e.pair_count();
+    });
+}
+
+int kumo_write_cube(const char* path, const char* comment, const kumo_grid* grid, int natoms, const int* z,
+                    const double* charges, const double* xyz, const double* values, long long orbital_index, char* err,
+                    size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!path || !values || natoms < 0) throw std::invalid_argument("invalid cube arguments");
+        const Grid g = to_grid(grid);
+        std::vector<Atom> atoms;
+        for (int i = 0; i < natoms; ++i) atoms.push_back({z[i], charges[i], {xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]}});
+        const std::size_t n = static_cast<std::size_t>(g.counts[0]) * g.counts[1] * g.counts[2];
+        Field f(g, std::move(atoms), std::vector<double>(values, values + n));
+        if (orbital_index > 0)
+            f.write_orbital_cube(path, static_cast<std::size_t>(orbital_index), comment ? comment : "Molecular orbital amplitude");
+        else
+            f.write_cube(path, comment ? comment : "Electron density");
+    });
+}
+
+int kumo_grid_around(const kumo_molecule* m, double margin, double spacing, kumo_grid* out, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!m || !out) throw std::invalid_argument("null argument");
+        const Grid g = Grid::around(m->mol.atoms(), margin, spacing);
+        for (int k = 0; k < 3; ++k) out->origin[k] = g.origin[k];
+        for (int i = 0; i < 9; ++i) out->steps[i] = g.steps.m[static_cast<std::size_t>(i)];
+        for (int k = 0; k < 3; ++k) out->counts[k] = g.counts[k];
+    });
+}
+
+void kumo_profile_enable(int on) {
+    try {
+        detail::profile_enable(on != 0);
+    } catch (...) {
+    }
+}
+
+void kumo_profile_reset(void) { detail::profile_reset(); }
+
+int kumo_profile_read(kumo_profile_entry* out, int max_entries) {
+    int n = 0;
+    try {
+        for (int k = 0; k < detail::kProfCount && n < max_entries; ++k) {
+            const auto s = detail::profile_read(static_cast<detail::ProfileKernel>(k));
+            kumo_profile_entry& e = out[n++];
+            std::memset(e.name, 0, sizeof e.name);
+            std::strncpy(e.name, detail::profile_name(static_cast<detail::ProfileKernel>(k)), sizeof e.name - 1);
+            e.launches = s.launches;
+            e.ms = s.ms;
+            e.kept_rows = s.kept_rows;
+            e.units = s.units;
+            e.flops = s.flops;
+            e.bytes = s.bytes;
+        }
+    } catch (...) {
+        return -1;
+    }
+    return n;
+}
+
+}  // extern "C"

@@ -1,0 +1,106 @@
+// Upload of a molecule's AO tables, density matrices and MO coefficients.
+#include "device_state.hpp"
+
+#include <algorithm>
+#include <cstring>
+
+namespace chem::kumo::detail {
+
+void throw_cuda(cudaError_t e, const char* what) {
+    throw std::runtime_error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+T* DeviceMolecule::upload(const T* host, std::size_t count) {
+    if (count == 0) count = 1;
+    void* p = nullptr;
+    check_cuda(cudaMalloc(&p, sizeof(T) * count), "cudaMalloc (molecule)");
+    allocations.push_back(p);
+    bytes += sizeof(T) * count;
+    if (host) check_cuda(cudaMemcpy(p, host, sizeof(T) * count, cudaMemcpyHostToDevice), "cudaMemcpy (molecule)");
+    return static_cast<T*>(p);
+}
+
+DeviceMolecule::DeviceMolecule(const Molecule& m) {
+    check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    const auto& blocks = m.blocks();
+    const std::size_t n = m.basis_size();
+    std::vector<double4> origin(blocks.size());
+    std::vector<int4> info(blocks.size());
+    std::vector<double> exps, weights;
+    int max_l = 0, max_count = 0;
+    for (std::size_t i = 0; i < blocks.size(); ++i) {
+        const auto& b = blocks[i];
+        const int l = b.angular_momentum;
+        const int np = static_cast<int>(b.exponents.size());
+        if (l > kumo_dev::kMaxL)
+            throw std::invalid_argument("the B200 evaluator supports shells up to l = 4 (g)");
+        if (np > kumo_dev::kMaxPrim)
+            throw std::invalid_argument("the B200 evaluator supports at most 16 primitives per shell");
+        origin[i] = make_double4(b.origin[0], b.origin[1], b.origin[2], b.cutoff_radius2);
+        info[i] = make_int4(l | (b.pure ? 1 << 8 : 0) | (np << 16), static_cast<int>(exps.size()),
+                            static_cast<int>(weights.size()), static_cast<int>(b.offset));
+        exps.insert(exps.end(), b.exponents.begin(), b.exponents.end());
+        weights.insert(weights.end(), b.weights.begin(), b.weights.end());
+        max_l = std::max(max_l, l);
+        max_count = std::max(max_count, static_cast<int>(b.count));
+    }
+    std::vector<float> exps_f(exps.begin(), exps.end()), weights_f(weights.begin(), weights.end());
+    basis.nblocks = static_cast<int>(blocks.size());
+    basis.nao = static_cast<int>(n);
+    basis.max_l = max_l;
+    basis.max_count = max_count;
+    basis.origin_r2 = upload(origin.data(), origin.size());
+    basis.info = upload(info.data(), info.size());
+    basis.exps = upload(exps.data(), exps.size());
+    basis.weights = upload(weights.data(), weights.size());
+    basis.exps_f = upload(exps_f.data(), exps_f.size());
+    basis.weights_f = upload(weights_f.data(), weights_f.size());
+    for (int l = 2; l <= kumo_dev::kMaxL; ++l) {
+        const Matrix t = gaussian_cartesian_to_pure(l);
+        for (std::size_t r = 0; r < t.rows(); ++r)
+            for (std::size_t c = 0; c < t.cols(); ++c) {
+                pure_d[l - 2][r * t.cols() + c] = t(r, c);
+                pure_f[l - 2][r * t.cols() + c] = static_cast<float>(t(r, c));
+            }
+    }
+    const Matrix pt = m.density_matrix(DensityComponent::Total);
+    const Matrix ps = m.density_matrix(DensityComponent::Difference);
+    p_total = upload(pt.data(), pt.size());
+    p_spin = upload(ps.data(), ps.size());
+    unrestricted = m.unrestricted();
+    const Matrix& ca = m.mo_coefficients(SpinChannel::Alpha);
+    const Matrix& cb = m.mo_coefficients(SpinChannel::Beta);
+    nmo_alpha = static_cast<int>(ca.cols());
+    nmo_beta = static_cast<int>(cb.cols());
+    if (nmo_alpha) c_alpha = upload(ca.data(), ca.size());
+    if (unrestricted && nmo_beta) c_beta = upload(cb.data(), cb.size());
+    if (!unrestricted) c_beta = c_alpha;
+    auto transpose_occ = [&](const Matrix& c, int nocc, int& ld, double*& dst, float*& dst_f) {
+        // Rows padded to a multiple of 4 so that every 16-byte chunk of a row
+        // (2 doubles, 4 floats) lies inside the row.
+        ld = std::max(4, (nocc + 3) / 4 * 4);
+        std::vector<double> t(n * static_cast<std::size_t>(ld), 0.0);
+        for (int o = 0; o < nocc && static_cast<std::size_t>(o) < c.cols(); ++o)
+            for (std::size_t a = 0; a < n; ++a) t[a * static_cast<std::size_t>(ld) + static_cast<std::size_t>(o)] = c(a, static_cast<std::size_t>(o));
+        dst = upload(t.data(), t.size());
+        std::vector<float> tf(t.begin(), t.end());
+        dst_f = upload(tf.data(), tf.size());
+    };
+    nocc_alpha = static_cast<int>(m.occupied_count(SpinChannel::Alpha));
+    nocc_beta = static_cast<int>(m.occupied_count(SpinChannel::Beta));
+    if (nmo_alpha) {
+        transpose_occ(ca, nocc_alpha, ldc_alpha, ct_alpha, ct_alpha_f);
+        transpose_occ(unrestricted ? cb : ca, nocc_beta, ldc_beta, ct_beta, ct_beta_f);
+    }
+}
+
+DeviceMolecule::~DeviceMolecule() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != device) cudaSetDevice(device);
+    for (void* p : allocations) cudaFree(p);
+    if (cur != device && cur >= 0) cudaSetDevice(cur);
+}
+
+}  // namespace chem::kumo::detail

@@ -1,0 +1,55 @@
+#pragma once
+// Device-resident copy of a molecule (internal).
+#include "chem/kumo/density.hpp"
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../cuda/kumo_device.cuh"
+
+namespace chem::kumo::detail {
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what);
+inline void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw_cuda(e, what);
+}
+
+/// AO tables, density matrices and MO coefficients of one molecule in HBM.
+struct DeviceMolecule {
+    int device = -1;
+    kumo_dev::DevBasis basis;
+    double pure_d[3][135] = {};
+    float pure_f[3][135] = {};
+    double* p_total = nullptr;  // n x n
+    double* p_spin = nullptr;
+    // Occupied MOs transposed [AO][MO], rows padded to a multiple of 4.
+    double* ct_alpha = nullptr;
+    int ldc_alpha = 0, nocc_alpha = 0;
+    double* ct_beta = nullptr;
+    int ldc_beta = 0, nocc_beta = 0;
+    // FP32 copies of the occupied MOs for the mixed form.
+    float* ct_alpha_f = nullptr;
+    float* ct_beta_f = nullptr;
+    // All MO coefficients, one MO per column (n x nmo), for amplitudes.
+    double* c_alpha = nullptr;
+    int nmo_alpha = 0;
+    double* c_beta = nullptr;
+    int nmo_beta = 0;
+    bool unrestricted = false;
+    std::size_t bytes = 0;
+    std::vector<void*> allocations;
+
+    explicit DeviceMolecule(const Molecule& m);
+    ~DeviceMolecule();
+    DeviceMolecule(const DeviceMolecule&) = delete;
+    DeviceMolecule& operator=(const DeviceMolecule&) = delete;
+
+    template <typename T>
+    T* upload(const T* host, std::size_t count);
+};
+
+}  // namespace chem::kumo::detail

@@ -1,0 +1,694 @@
+// Evaluator: one evaluation runs the passes of chem-kumo's Evaluator::Run
+// (src/evaluator.cpp:545-615) on the GPU:
+//  - point path: AO panels + screening (ao_build) and the AO-MO or AO-P
+//    contraction with the fused field epilogue, in waves of point blocks;
+//  - electrostatic potential;
+//  - orbital pass / grid-path orbital amplitudes;
+//  - grid-path AO-P densities.
+// The field each property comes from follows src/evaluator.cpp:79-111.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../cuda/contract.cuh"
+#include "../cuda/esp.cuh"
+#include "../cuda/mixed.cuh"
+#include "chem/kumo/evaluator.hpp"
+#include "device_state.hpp"
+#include "grid_geometry.hpp"
+#include "plan.hpp"
+#include "profile.hpp"
+
+namespace chem::kumo {
+
+std::size_t property_channels(PropertyKind k) {
+    switch (k) {
+        case PropertyKind::Gradient:
+        case PropertyKind::OrbitalGradient:
+        case PropertyKind::TauComponents:
+        case PropertyKind::HamiltonianKineticEnergyComponents: return 3;
+        case PropertyKind::Hessian:
+        case PropertyKind::OrbitalHessian: return 6;
+        default: return 1;
+    }
+}
+
+namespace {
+
+using detail::check_cuda;
+
+bool uses_point_path(const detail::ComponentNeeds& c, Backend b, bool grid) {
+    return c.derivatives() || ((b == Backend::AO_MO || !grid) && c.density);
+}
+
+bool on_grid_path(const Property& p, Backend b, bool grid) {
+    return grid && (p.kind == PropertyKind::Orbital || (p.kind == PropertyKind::Density && b == Backend::AO_P));
+}
+
+bool from_point_path(const Property& p, Backend b, bool grid) {
+    return !on_grid_path(p, b, grid) && !detail::is_orbital_kind(p.kind) &&
+           p.kind != PropertyKind::ElectrostaticPotential && !detail::is_orbital_energy_kind(p.kind);
+}
+
+bool needs_full_hessian(PropertyKind k) {
+    return k == PropertyKind::Hessian || k == PropertyKind::SignLambda2Density ||
+           k == PropertyKind::DensityOverlapRegionsIndicator ||
+           k == PropertyKind::HamiltonianKineticEnergyComponents;
+}
+
+// Stream-ordered device allocation, freed when the owner goes out of scope.
+class DeviceAlloc {
+public:
+    DeviceAlloc() = default;
+    DeviceAlloc(std::size_t bytes, cudaStream_t s) : stream_(s) {
+        if (bytes) check_cuda(cudaMallocAsync(&ptr_, bytes, s), "cudaMallocAsync (evaluation scratch)");
+    }
+    DeviceAlloc(const DeviceAlloc&) = delete;
+    DeviceAlloc& operator=(const DeviceAlloc&) = delete;
+    DeviceAlloc(DeviceAlloc&& o) noexcept : ptr_(o.ptr_), stream_(o.stream_) { o.ptr_ = nullptr; }
+    DeviceAlloc& operator=(DeviceAlloc&& o) noexcept {
+        std::swap(ptr_, o.ptr_);
+        std::swap(stream_, o.stream_);
+        return *this;
+    }
+    ~DeviceAlloc() {
+        if (ptr_) cudaFreeAsync(ptr_, stream_);
+    }
+    template <typename T>
+    T* as() const {
+        return static_cast<T*>(ptr_);
+    }
+
+private:
+    void* ptr_ = nullptr;
+    cudaStream_t stream_ = nullptr;
+};
+
+std::size_t scratch_budget() {
+    if (const char* e = std::getenv("KUMO_SCRATCH_MB")) {
+        const long long mb = std::atoll(e);
+        if (mb > 0) return static_cast<std::size_t>(mb) << 20;
+    }
+    return std::size_t(4) << 30;
+}
+
+}  // namespace
+
+Evaluator::Evaluator(const Molecule& molecule, EvaluationOptions options) : molecule_(&molecule), options_(std::move(options)) {
+    if (options_.block_size == 0 || options_.block_size > max_block_size)
+        throw std::invalid_argument("evaluation block_size must be in [1, " + std::to_string(max_block_size) + "]");
+    if (options_.threads < 0) throw std::invalid_argument("invalid evaluation options");
+    if (!std::isfinite(options_.screening_threshold) || options_.screening_threshold < 0.0)
+        throw std::invalid_argument("screening threshold must be finite and nonnegative");
+    if (!std::isfinite(options_.potential_tolerance) || options_.potential_tolerance < 0.0)
+        throw std::invalid_argument("potential tolerance must be finite and nonnegative");
+    if (!std::isfinite(options_.fukui_delta) || options_.fukui_delta <= 0.0)
+        throw std::invalid_argument("fukui_delta must be finite and positive");
+    if (options_.backend != Backend::AUTO && options_.backend != Backend::AO_P && options_.backend != Backend::AO_MO)
+        throw std::invalid_argument("unknown evaluation backend");
+    if (options_.backend == Backend::AO_MO && !molecule.electronic_structure_info().ao_mo_eligible())
+        throw std::invalid_argument("AO_MO backend requested but orbital representation is not eligible");
+    if (options_.threads > 1)
+        throw std::invalid_argument("explicit multi-thread control is not implemented in the API adapter");
+}
+
+// One evaluation on the device.  `outs` pairs each requested property with
+// its device output (channels x n doubles).
+class Evaluator::Run {
+public:
+    Run(const Evaluator& ev, const Grid* grid, const double* device_points, std::size_t n, const Request& request,
+        cudaStream_t stream)
+        : mol_(*ev.molecule_), opt_(ev.options_), grid_(grid), points_(device_points), n_(n), stream_(stream),
+          plan_(detail::Plan::from(request)) {
+        backend_ = detail::choose_backend(opt_.backend, mol_.electronic_structure_info().ao_mo_eligible(), plan_);
+        for (const auto& p : request.properties()) {
+            if (detail::is_orbital_energy_kind(p.kind))
+                throw std::invalid_argument("orbital-energy fields are not evaluated by the B200 grid evaluator");
+            // Orbital requests are checked before any pass (src/evaluator.cpp:623-636).
+            if (detail::is_orbital_kind(p.kind)) {
+                const auto& c = mol_.mo_coefficients(p.channel);
+                if (c.cols() == 0) throw std::runtime_error("FCHK has no MO coefficients");
+                if (p.orbital_index > c.cols()) throw std::out_of_range("MO index outside available coefficient range");
+            }
+        }
+        if (opt_.block_size > static_cast<std::size_t>(kumo_dev::kBlockPoints))
+            throw std::invalid_argument("the B200 evaluator supports block_size up to 128");
+        if (plan_.needs_esp() && opt_.potential_tolerance != 0.0)
+            throw std::invalid_argument(
+                "the B200 evaluator computes the electrostatic potential exactly: set potential_tolerance to 0");
+    }
+
+    Backend backend() const { return backend_; }
+
+    void execute(const std::vector<std::pair<Property, double*>>& outs) {
+        outs_ = outs;
+        if (n_ == 0) return;
+        dev_ = &mol_.device();
+        src_ = kumo_dev::PointSource{};
+        src_.count = static_cast<long long>(n_);
+        if (grid_) {
+            for (int k = 0; k < 3; ++k) src_.origin[k] = grid_->origin[k];
+            for (int i = 0; i < 9; ++i) src_.steps[i] = grid_->steps.m[static_cast<std::size_t>(i)];
+            src_.ny = grid_->counts[1];
+            src_.nz = grid_->counts[2];
+        } else {
+            src_.points = points_;
+        }
+        const bool grid = grid_ != nullptr;
+        bool point_path = false;
+        for (const auto& c : plan_.c) point_path |= uses_point_path(c, backend_, grid);
+        // Progress over all passes, src/evaluator.cpp:599-607.
+        passes_ = (point_path ? 1 : 0) + (plan_.needs_esp() ? 1 : 0);
+        bool orbital_pass = false;
+        bool grid_orbitals[2] = {false, false};
+        std::size_t grid_densities = 0;
+        for (const auto& [key, ptr] : outs_) {
+            if (detail::is_orbital_kind(key.kind)) {
+                if (on_grid_path(key, backend_, grid))
+                    grid_orbitals[key.channel == SpinChannel::Beta ? 1 : 0] = true;
+                else
+                    orbital_pass = true;
+            } else if (on_grid_path(key, backend_, grid)) {
+                ++grid_densities;
+            }
+        }
+        passes_ += (orbital_pass ? 1 : 0) + grid_densities + (grid_orbitals[0] ? 1 : 0) + (grid_orbitals[1] ? 1 : 0);
+
+        if (point_path) point_pass();
+        if (plan_.needs_esp()) potential_pass();
+        if (orbital_pass) orbital_pass_run(false);
+        for (const auto& [key, ptr] : outs_)
+            if (on_grid_path(key, backend_, grid) && key.kind == PropertyKind::Density) grid_density_pass(key, ptr);
+        for (int ch = 0; ch < 2; ++ch)
+            if (grid_orbitals[ch]) orbital_pass_run(true, ch);
+        check_cuda(cudaGetLastError(), "kernel launch");
+    }
+
+private:
+    void report(std::size_t done_in_pass) {
+        if (!opt_.progress) return;
+        check_cuda(cudaStreamSynchronize(stream_), "cudaStreamSynchronize (progress)");
+        opt_.progress(completed_ + done_in_pass, passes_ * n_);
+    }
+
+    std::size_t block_size() const {
+        if (opt_.block_size > static_cast<std::size_t>(kumo_dev::kBlockPoints))
+            throw std::invalid_argument("the B200 evaluator supports block_size up to 128");
+        return opt_.block_size;
+    }
+
+    // Blocks per wave for a scratch of `per_block` bytes per block.
+    static int wave_blocks(std::size_t total_blocks, std::size_t per_block) {
+        std::size_t w = scratch_budget() / std::max<std::size_t>(per_block, 1);
+        w = std::max<std::size_t>(1, std::min(w, total_blocks));
+        w = std::min<std::size_t>(w, kumo_dev::kMaxBlocksPerWave);
+        return static_cast<int>(w);
+    }
+
+    template <typename T>
+    kumo_dev::AoBuildParams<T> build_params(double threshold) const {
+        kumo_dev::AoBuildParams<T> p{};
+        p.basis = dev_->basis;
+        p.src = src_;
+        p.threshold = threshold;
+        for (int l = 0; l < 3; ++l)
+            for (int i = 0; i < 135; ++i)
+                p.pure[l][i] = sizeof(T) == 8 ? static_cast<T>(dev_->pure_d[l][i]) : static_cast<T>(dev_->pure_f[l][i]);
+        return p;
+    }
+
+    kumo_dev::FieldSpec field_spec(bool (*select)(const Property&, Backend, bool)) const {
+        kumo_dev::FieldSpec spec{};
+        spec.stride = static_cast<long long>(n_);
+        spec.out_base = 0;
+        for (const auto& [key, ptr] : outs_) {
+            if (!select(key, backend_, grid_ != nullptr)) continue;
+            if (spec.nprops == kumo_dev::kMaxProps) throw std::invalid_argument("too many properties in one request");
+            spec.props[spec.nprops++] = {static_cast<int>(key.kind), static_cast<int>(key.component), ptr};
+        }
+        return spec;
+    }
+
+    void point_pass() {
+        const bool grid = grid_ != nullptr;
+        std::array<bool, 4> needed{};
+        for (int c = 0; c < 4; ++c) needed[c] = uses_point_path(plan_.c[c], backend_, grid);
+        const int ao_order = grid ? plan_.max_order : std::max(1, plan_.max_order);
+        bool full = false;
+        for (const auto& [key, ptr] : outs_)
+            if (from_point_path(key, backend_, grid) && needs_full_hessian(key.kind)) full = true;
+        int npanel;
+        if (ao_order <= 0)
+            npanel = kumo_dev::kPanelsValue;
+        else if (ao_order == 1)
+            npanel = kumo_dev::kPanelsGradient;
+        else
+            npanel = full ? kumo_dev::kPanelsFull : kumo_dev::kPanelsLaplacian;
+        const kumo_dev::FieldSpec spec = field_spec(&from_point_path);
+        if (backend_ == Backend::AO_MO) {
+            if (opt_.precision == Precision::Mixed)
+                mo_pass_mixed(std::max(0, ao_order), npanel, needed, spec);
+            else
+                mo_pass_f64(std::max(0, ao_order), npanel, needed, spec);
+        } else {
+            p_pass_f64(std::max(1, ao_order), npanel == kumo_dev::kPanelsValue ? kumo_dev::kPanelsGradient : npanel,
+                       needed, spec);
+        }
+        completed_ += n_;
+    }
+
+    // Algorithmic counters of one contraction wave: per kept AO row of a
+    // block, 2 * 128 points * panels * occupied MOs FLOPs (the dense product
+    // C_kept^T Phi_kept of every stored panel), and the AO panel bytes read.
+    void count_contraction(detail::ProfileKernel k, const int* nkept, int nb, int npanel, int nch, int nocc0,
+                           int nocc1, std::size_t elem) const {
+        if (!detail::profiling_enabled()) return;
+        const double mos = static_cast<double>(nocc0) + (nch > 1 ? nocc1 : 0);
+        const double per_row = 2.0 * kumo_dev::kBlockPoints * npanel * mos;
+        detail::profile_count(detail::kProfAoBuild, nkept, nb, 0.0, nb, 0.0, 0.0, stream_);
+        (void)elem;
+        detail::profile_count(k, nkept, nb, per_row, nb, 0.0, 0.0, stream_);
+    }
+
+    // Occupied-MO channels needed by the AO-MO contraction
+    // (src/density.cpp:257-273).
+    int mo_channels(const std::array<bool, 4>& needed, kumo_dev::MoChannel* ch, bool& beta_is_alpha, bool mixed) const {
+        const bool need_a = needed[1] || needed[0] || needed[3];
+        const bool need_b = needed[2] || needed[0] || needed[3];
+        const int na = static_cast<int>(mol_.occupied_count(SpinChannel::Alpha));
+        const int nb = static_cast<int>(mol_.occupied_count(SpinChannel::Beta));
+        beta_is_alpha = need_a && need_b && !mol_.unrestricted() && na == nb;
+        int nch = 0;
+        auto ct = [&](bool beta) -> const double* {
+            if (mixed) return reinterpret_cast<const double*>(beta ? dev_->ct_beta_f : dev_->ct_alpha_f);
+            return beta ? dev_->ct_beta : dev_->ct_alpha;
+        };
+        if (need_a && na > 0) ch[nch++] = {ct(false), dev_->ldc_alpha, na, 1};
+        if (need_b && !beta_is_alpha && nb > 0) ch[nch++] = {ct(true), dev_->ldc_beta, nb, 2};
+        return nch;
+    }
+
+    void mo_pass_f64(int ao_order, int npanel, const std::array<bool, 4>& needed, const kumo_dev::FieldSpec& spec) {
+        const std::size_t bs = block_size();
+        const std::size_t nblocks = (n_ + bs - 1) / bs;
+        const int nao = dev_->basis.nao;
+        const int stride = nao;
+        const std::size_t per_block = sizeof(double) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints +
+                                      sizeof(int) * ((std::size_t)stride + 1);
+        const int W = wave_blocks(nblocks, per_block);
+        DeviceAlloc panels(sizeof(double) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints * W, stream_);
+        DeviceAlloc kept(sizeof(int) * (std::size_t)stride * W, stream_);
+        DeviceAlloc nkept(sizeof(int) * (std::size_t)W, stream_);
+        kumo_dev::AoBuildParams<double> bp = build_params<double>(opt_.screening_threshold);
+        bp.block_size = static_cast<long long>(bs);
+        bp.out = {panels.as<double>(), kept.as<int>(), nkept.as<int>(), stride, npanel};
+        kumo_dev::ContractMoParams cp{};
+        cp.scr = bp.out;
+        cp.block_size = static_cast<long long>(bs);
+        cp.count = static_cast<long long>(n_);
+        bool bia = false;
+        cp.nchannels = mo_channels(needed, cp.ch, bia, false);
+        cp.beta_is_alpha = bia;
+        cp.ao_order = ao_order;
+        cp.spec = spec;
+        for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
+            const int nb = static_cast<int>(std::min<std::size_t>(W, nblocks - b0));
+            bp.first_point = static_cast<long long>(b0 * bs);
+            bp.nblocks = nb;
+            int tok = detail::profile_begin(detail::kProfAoBuild, stream_);
+            kumo_dev::launch_ao_build<double>(bp, ao_order, npanel, stream_);
+            detail::profile_end(tok, stream_);
+            cp.first_point = bp.first_point;
+            cp.nblocks = nb;
+            tok = detail::profile_begin(detail::kProfContractMo, stream_);
+            kumo_dev::launch_contract_mo_f64(cp, npanel, stream_);
+            detail::profile_end(tok, stream_);
+            count_contraction(detail::kProfContractMo, bp.out.nkept, nb, npanel, cp.nchannels, cp.ch[0].nocc,
+                              cp.nchannels > 1 ? cp.ch[1].nocc : 0, sizeof(double));
+            report(std::min(n_, (b0 + nb) * bs));
+        }
+    }
+
+    void mo_pass_mixed(int ao_order, int npanel, const std::array<bool, 4>& needed, const kumo_dev::FieldSpec& spec) {
+        const std::size_t bs = block_size();
+        const std::size_t nblocks = (n_ + bs - 1) / bs;
+        const int nao = dev_->basis.nao;
+        const int stride = (nao + 7) / 8 * 8;
+        const std::size_t per_block = sizeof(float) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints +
+                                      sizeof(int) * ((std::size_t)stride + 1);
+        const int W = wave_blocks(nblocks, per_block);
+        DeviceAlloc panels(sizeof(float) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints * W, stream_);
+        DeviceAlloc kept(sizeof(int) * (std::size_t)stride * W, stream_);
+        DeviceAlloc nkept(sizeof(int) * (std::size_t)W, stream_);
+        kumo_dev::AoBuildParams<float> bp = build_params<float>(opt_.screening_threshold);
+        bp.block_size = static_cast<long long>(bs);
+        bp.out = {panels.as<float>(), kept.as<int>(), nkept.as<int>(), stride, npanel};
+        kumo_dev::ContractMixedParams cp{};
+        cp.scr = bp.out;
+        cp.block_size = static_cast<long long>(bs);
+        cp.count = static_cast<long long>(n_);
+        bool bia = false;
+        kumo_dev::MoChannel ch[2];
+        cp.nchannels = mo_channels(needed, ch, bia, true);
+        for (int i = 0; i < cp.nchannels; ++i)
+            cp.ch[i] = {reinterpret_cast<const float*>(ch[i].ct), ch[i].ldc, ch[i].nocc, ch[i].role};
+        cp.beta_is_alpha = bia;
+        cp.ao_order = ao_order;
+        cp.spec = spec;
+        for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
+            const int nb = static_cast<int>(std::min<std::size_t>(W, nblocks - b0));
+            bp.first_point = static_cast<long long>(b0 * bs);
+            bp.nblocks = nb;
+            int tok = detail::profile_begin(detail::kProfAoBuild, stream_);
+            kumo_dev::launch_ao_build<float>(bp, ao_order, npanel, stream_);
+            detail::profile_end(tok, stream_);
+            cp.first_point = bp.first_point;
+            cp.nblocks = nb;
+            tok = detail::profile_begin(detail::kProfContractMixed, stream_);
+            kumo_dev::launch_contract_mixed(cp, npanel, stream_);
+            detail::profile_end(tok, stream_);
+            count_contraction(detail::kProfContractMixed, bp.out.nkept, nb, npanel, cp.nchannels, cp.ch[0].nocc,
+                              cp.nchannels > 1 ? cp.ch[1].nocc : 0, sizeof(float));
+            report(std::min(n_, (b0 + nb) * bs));
+        }
+    }
+
+    void p_pass_f64(int ao_order, int npanel, const std::array<bool, 4>& needed, const kumo_dev::FieldSpec& spec) {
+        const std::size_t bs = block_size();
+        const std::size_t nblocks = (n_ + bs - 1) / bs;
+        const int nao = dev_->basis.nao;
+        const int stride = nao;
+        const std::size_t per_block = sizeof(double) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints +
+                                      sizeof(int) * ((std::size_t)stride + 1);
+        const int W = wave_blocks(nblocks, per_block);
+        DeviceAlloc panels(sizeof(double) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints * W, stream_);
+        DeviceAlloc kept(sizeof(int) * (std::size_t)stride * W, stream_);
+        DeviceAlloc nkept(sizeof(int) * (std::size_t)W, stream_);
+        kumo_dev::AoBuildParams<double> bp = build_params<double>(opt_.screening_threshold);
+        bp.block_size = static_cast<long long>(bs);
+        bp.out = {panels.as<double>(), kept.as<int>(), nkept.as<int>(), stride, npanel};
+        kumo_dev::ContractPParams cp{};
+        cp.scr = bp.out;
+        cp.block_size = static_cast<long long>(bs);
+        cp.count = static_cast<long long>(n_);
+        cp.nao = nao;
+        cp.total_needed = needed[0] || needed[1] || needed[2];
+        cp.spin_needed = needed[3] || needed[1] || needed[2];
+        cp.p_total = dev_->p_total;
+        cp.p_spin = dev_->p_spin;
+        cp.ao_order = ao_order;
+        cp.spec = spec;
+        for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
+            const int nb = static_cast<int>(std::min<std::size_t>(W, nblocks - b0));
+            bp.first_point = static_cast<long long>(b0 * bs);
+            bp.nblocks = nb;
+            int tok = detail::profile_begin(detail::kProfAoBuild, stream_);
+            kumo_dev::launch_ao_build<double>(bp, ao_order, npanel, stream_);
+            detail::profile_end(tok, stream_);
+            cp.first_point = bp.first_point;
+            cp.nblocks = nb;
+            tok = detail::profile_begin(detail::kProfContractP, stream_);
+            kumo_dev::launch_contract_p_f64(cp, npanel, stream_);
+            detail::profile_end(tok, stream_);
+            report(std::min(n_, (b0 + nb) * bs));
+        }
+    }
+
+    // Molecule::densities_blocked for one component (src/density.cpp:366-444).
+    void grid_density_pass(const Property& key, double* out) {
+        const std::size_t bs = block_size();
+        const std::size_t nblocks = (n_ + bs - 1) / bs;
+        const int nao = dev_->basis.nao;
+        const std::size_t per_block =
+            sizeof(double) * (std::size_t)nao * kumo_dev::kBlockPoints + sizeof(int) * ((std::size_t)nao + 1);
+        const int W = wave_blocks(nblocks, per_block);
+        DeviceAlloc panels(sizeof(double) * (std::size_t)nao * kumo_dev::kBlockPoints * W, stream_);
+        DeviceAlloc kept(sizeof(int) * (std::size_t)nao * W, stream_);
+        DeviceAlloc nkept(sizeof(int) * (std::size_t)W, stream_);
+        kumo_dev::AoBuildParams<double> bp = build_params<double>(opt_.screening_threshold);
+        bp.block_size = static_cast<long long>(bs);
+        bp.out = {panels.as<double>(), kept.as<int>(), nkept.as<int>(), nao, 1};
+        kumo_dev::ContractPParams cp{};
+        cp.scr = bp.out;
+        cp.block_size = static_cast<long long>(bs);
+        cp.count = static_cast<long long>(n_);
+        cp.nao = nao;
+        cp.density_component = static_cast<int>(key.component);
+        cp.p_total = dev_->p_total;
+        cp.p_spin = dev_->p_spin;
+        cp.ao_order = 0;
+        cp.spec.stride = static_cast<long long>(n_);
+        cp.spec.nprops = 1;
+        cp.spec.props[0] = {static_cast<int>(key.kind), static_cast<int>(key.component), out};
+        for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
+            const int nb = static_cast<int>(std::min<std::size_t>(W, nblocks - b0));
+            bp.first_point = static_cast<long long>(b0 * bs);
+            bp.nblocks = nb;
+            kumo_dev::launch_ao_build<double>(bp, 0, 1, stream_);
+            cp.first_point = bp.first_point;
+            cp.nblocks = nb;
+            kumo_dev::launch_density_values_f64(cp, stream_);
+            report(std::min(n_, (b0 + nb) * bs));
+        }
+        completed_ += n_;
+    }
+
+    // Orbital amplitudes and derivatives (src/evaluator.cpp:688-730) or the
+    // grid-path amplitudes of one channel (src/orbitals.cpp:66-102): every AO
+    // kept (no screening), values from evaluate_batch and derivatives from
+    // evaluate_derivatives_batch.
+    void orbital_pass_run(bool grid_path, int channel = 0) {
+        const bool grid = grid_ != nullptr;
+        std::vector<std::pair<Property, double*>> sel;
+        int order = 0;
+        for (const auto& [key, ptr] : outs_) {
+            if (!detail::is_orbital_kind(key.kind)) continue;
+            const bool gp = on_grid_path(key, backend_, grid);
+            if (gp != grid_path) continue;
+            if (grid_path && static_cast<int>(key.channel) != channel) continue;
+            sel.emplace_back(key, ptr);
+            if (key.kind == PropertyKind::OrbitalGradient) order = std::max(order, 1);
+            if (key.kind == PropertyKind::OrbitalHessian) order = 2;
+        }
+        if (sel.empty()) return;
+        const std::size_t bs = grid_path ? 128 : block_size();
+        const std::size_t nblocks = (n_ + bs - 1) / bs;
+        const int nao = dev_->basis.nao;
+        // Values come from the value path (npanel 1); derivatives from the
+        // derivative path with 4 or 10 panels.
+        for (int pass = 0; pass < (order > 0 ? 2 : 1); ++pass) {
+            const int npanel = pass == 0 ? 1 : (order == 1 ? 4 : 10);
+            const int aord = pass == 0 ? 0 : order;
+            const std::size_t per_block = sizeof(double) * npanel * (std::size_t)nao * kumo_dev::kBlockPoints +
+                                          sizeof(int) * ((std::size_t)nao + 1);
+            const int W = wave_blocks(nblocks, per_block);
+            DeviceAlloc panels(sizeof(double) * npanel * (std::size_t)nao * kumo_dev::kBlockPoints * W, stream_);
+            DeviceAlloc kept(sizeof(int) * (std::size_t)nao * W, stream_);
+            DeviceAlloc nkept(sizeof(int) * (std::size_t)W, stream_);
+            kumo_dev::AoBuildParams<double> bp = build_params<double>(0.0);
+            bp.block_size = static_cast<long long>(bs);
+            bp.out = {panels.as<double>(), kept.as<int>(), nkept.as<int>(), nao, npanel};
+            kumo_dev::OrbitalParams op{};
+            op.scr = bp.out;
+            op.block_size = static_cast<long long>(bs);
+            op.count = static_cast<long long>(n_);
+            op.nao = nao;
+            op.npanel = npanel;
+            op.stride = static_cast<long long>(n_);
+            for (const auto& [key, ptr] : sel) {
+                const bool value = key.kind == PropertyKind::Orbital;
+                if ((pass == 0) != value) continue;
+                if (op.nsel == 8) {
+                    run_orbital_waves(bp, op, nblocks, W, bs, aord, npanel);
+                    op.nsel = 0;
+                }
+                const bool beta = key.channel == SpinChannel::Beta;
+                const double* c = beta ? dev_->c_beta : dev_->c_alpha;
+                op.coef[op.nsel] = c + (key.orbital_index - 1) * static_cast<std::size_t>(nao);
+                op.out[op.nsel] = ptr;
+                op.first_channel[op.nsel] = value ? 0 : (key.kind == PropertyKind::OrbitalGradient ? 1 : 4);
+                op.nchan[op.nsel] = static_cast<int>(property_channels(key.kind));
+                ++op.nsel;
+            }
+            if (op.nsel) run_orbital_waves(bp, op, nblocks, W, bs, aord, npanel);
+        }
+        completed_ += n_;
+    }
+
+    void run_orbital_waves(kumo_dev::AoBuildParams<double>& bp, kumo_dev::OrbitalParams& op, std::size_t nblocks, int W,
+                           std::size_t bs, int order, int npanel) {
+        for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
+            const int nb = static_cast<int>(std::min<std::size_t>(W, nblocks - b0));
+            bp.first_point = static_cast<long long>(b0 * bs);
+            bp.nblocks = nb;
+            kumo_dev::launch_ao_build<double>(bp, order, npanel, stream_);
+            op.first_point = bp.first_point;
+            op.nblocks = nb;
+            kumo_dev::launch_orbitals_f64(op, stream_);
+        }
+    }
+
+    void potential_pass() {
+        double* out = nullptr;
+        for (const auto& [key, ptr] : outs_)
+            if (key.kind == PropertyKind::ElectrostaticPotential) out = ptr;
+        if (opt_.potential_tolerance != 0.0)
+            throw std::invalid_argument(
+                "the B200 evaluator computes the electrostatic potential exactly: set potential_tolerance to 0");
+        kumo_dev::EspDevice& esp = esp_state();
+        kumo_dev::EspParams ep{};
+        ep.esp = esp.view();
+        ep.src = src_;
+        ep.out = out;
+        const int tok = detail::profile_begin(detail::kProfEsp, stream_);
+        kumo_dev::launch_esp_f64(ep, stream_);
+        detail::profile_end(tok, stream_);
+        detail::profile_count(detail::kProfEsp, nullptr, 0, 0.0, static_cast<double>(n_) * esp.pair_count(), 0.0, 0.0,
+                              stream_);
+        completed_ += n_;
+        report(0);
+    }
+
+    kumo_dev::EspDevice& esp_state();
+
+    const Molecule& mol_;
+    const EvaluationOptions& opt_;
+    const Grid* grid_;
+    const double* points_;
+    std::size_t n_;
+    cudaStream_t stream_;
+    detail::Plan plan_;
+    Backend backend_ = Backend::AO_P;
+    detail::DeviceMolecule* dev_ = nullptr;
+    kumo_dev::PointSource src_{};
+    std::vector<std::pair<Property, double*>> outs_;
+    std::size_t passes_ = 0, completed_ = 0;
+    std::unique_ptr<kumo_dev::EspDevice> esp_;
+};
+
+kumo_dev::EspDevice& Evaluator::Run::esp_state() {
+    if (!esp_) esp_ = std::make_unique<kumo_dev::EspDevice>(mol_, stream_);
+    return *esp_;
+}
+
+namespace {
+
+std::vector<Property> unique_keys(const Request& request) {
+    std::vector<Property> keys;
+    for (const auto& p : request.properties())
+        if (std::find(keys.begin(), keys.end(), p) == keys.end()) keys.push_back(p);
+    return keys;
+}
+
+}  // namespace
+
+Results Evaluator::evaluate(const Grid& grid, const Request& request) const {
+    const std::size_t n = detail::validated_point_count(grid);
+    Run run(*this, &grid, nullptr, n, request, nullptr);
+    const auto keys = unique_keys(request);
+    std::size_t total = 0;
+    for (const auto& k : keys) total += property_channels(k.kind) * n;
+    DeviceAlloc out(sizeof(double) * std::max<std::size_t>(total, 1), nullptr);
+    std::vector<std::pair<Property, double*>> outs;
+    std::size_t off = 0;
+    for (const auto& k : keys) {
+        outs.emplace_back(k, out.as<double>() + off);
+        off += property_channels(k.kind) * n;
+    }
+    if (total) check_cuda(cudaMemsetAsync(out.as<double>(), 0, sizeof(double) * total, nullptr), "cudaMemsetAsync");
+    run.execute(outs);
+    Results res;
+    res.backend_used_ = run.backend();
+    std::vector<double> host(total);
+    if (total) check_cuda(cudaMemcpy(host.data(), out.as<double>(), sizeof(double) * total, cudaMemcpyDeviceToHost),
+                          "cudaMemcpy (results)");
+    off = 0;
+    for (const auto& k : keys) {
+        PropertyField f;
+        f.points = n;
+        const std::size_t ch = property_channels(k.kind);
+        f.components.resize(ch);
+        for (std::size_t c = 0; c < ch; ++c) {
+            f.components[c].assign(host.begin() + static_cast<std::ptrdiff_t>(off), host.begin() + static_cast<std::ptrdiff_t>(off + n));
+            off += n;
+        }
+        res.fields_.emplace(k, std::move(f));
+    }
+    return res;
+}
+
+Results Evaluator::evaluate(Points points, const Request& request) const {
+    for (std::size_t i = 0; i < 3 * points.count; ++i)
+        if (!std::isfinite(points.data[i])) throw std::invalid_argument("evaluation points must be finite");
+    const std::size_t n = points.count;
+    DeviceAlloc dpts(sizeof(double) * 3 * std::max<std::size_t>(n, 1), nullptr);
+    if (n) check_cuda(cudaMemcpy(dpts.as<double>(), points.data, sizeof(double) * 3 * n, cudaMemcpyHostToDevice),
+                      "cudaMemcpy (points)");
+    Run run(*this, nullptr, dpts.as<double>(), n, request, nullptr);
+    const auto keys = unique_keys(request);
+    std::size_t total = 0;
+    for (const auto& k : keys) total += property_channels(k.kind) * n;
+    DeviceAlloc out(sizeof(double) * std::max<std::size_t>(total, 1), nullptr);
+    std::vector<std::pair<Property, double*>> outs;
+    std::size_t off = 0;
+    for (const auto& k : keys) {
+        outs.emplace_back(k, out.as<double>() + off);
+        off += property_channels(k.kind) * n;
+    }
+    if (total) check_cuda(cudaMemsetAsync(out.as<double>(), 0, sizeof(double) * total, nullptr), "cudaMemsetAsync");
+    run.execute(outs);
+    Results res;
+    res.backend_used_ = run.backend();
+    std::vector<double> host(total);
+    if (total) check_cuda(cudaMemcpy(host.data(), out.as<double>(), sizeof(double) * total, cudaMemcpyDeviceToHost),
+                          "cudaMemcpy (results)");
+    off = 0;
+    for (const auto& k : keys) {
+        PropertyField f;
+        f.points = n;
+        const std::size_t ch = property_channels(k.kind);
+        f.components.resize(ch);
+        for (std::size_t c = 0; c < ch; ++c) {
+            f.components[c].assign(host.begin() + static_cast<std::ptrdiff_t>(off), host.begin() + static_cast<std::ptrdiff_t>(off + n));
+            off += n;
+        }
+        res.fields_.emplace(k, std::move(f));
+    }
+    return res;
+}
+
+Backend Evaluator::evaluate_device(const Grid& grid, const Request& request, double* const* outputs, void* stream) const {
+    const std::size_t n = detail::validated_point_count(grid);
+    Run run(*this, &grid, nullptr, n, request, static_cast<cudaStream_t>(stream));
+    std::vector<std::pair<Property, double*>> outs;
+    for (std::size_t i = 0; i < request.properties().size(); ++i) outs.emplace_back(request.properties()[i], outputs[i]);
+    run.execute(outs);
+    return run.backend();
+}
+
+Backend Evaluator::evaluate_device(Points device_points, const Request& request, double* const* outputs,
+                                   void* stream) const {
+    Run run(*this, nullptr, device_points.data, device_points.count, request, static_cast<cudaStream_t>(stream));
+    std::vector<std::pair<Property, double*>> outs;
+    for (std::size_t i = 0; i < request.properties().size(); ++i) outs.emplace_back(request.properties()[i], outputs[i]);
+    run.execute(outs);
+    return run.backend();
+}
+
+Field Evaluator::field(const Grid& grid, Property property) const {
+    if (property_channels(property.kind) != 1)
+        throw std::invalid_argument(
+            "Evaluator::field needs a one-component property (not a gradient, a Hessian or the Cartesian terms of G "
+            "or K)");
+    const auto results = evaluate(grid, Request().add(property));
+    const auto v = results.get(property).component();
+    return Field(grid, molecule_->atoms(), std::vector<double>(v.begin(), v.end()));
+}
+
+}  // namespace chem::kumo

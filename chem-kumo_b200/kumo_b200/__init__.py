@@ -1,0 +1,471 @@
+"""Python binding of the B200 grid evaluator's C ABI (include/kumo_b200.h).
+
+This module loads chem-kumo_b200/lib/libkumo_b200.so with ctypes and mirrors
+chem-kumo's Evaluator API: ``Molecule.from_fchk``, ``Evaluator.evaluate`` on a
+grid or at points, ``PropertyKind``/``DensityComponent`` values and the Cube
+writer.  There is no CPU fallback: if the library is missing, importing the
+binding raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import os
+from dataclasses import dataclass
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libkumo_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(os.path.dirname(HERE)), "include", "kumo_b200.h")
+
+
+class PropertyKind(enum.IntEnum):
+    """include/chem/kumo/evaluator.hpp:109-153 of chem-kumo."""
+    Density = 0
+    Gradient = 1
+    Hessian = 2
+    Laplacian = 3
+    Tau = 4
+    Orbital = 5
+    Elf = 6
+    ReducedGradient = 7
+    SignLambda2Density = 8
+    ElectrostaticPotential = 9
+    Lol = 10
+    InteractionRegionIndicator = 11
+    DensityOverlapRegionsIndicator = 12
+    HamiltonianKineticEnergy = 13
+    PotentialEnergyDensity = 14
+    EnergyDensity = 15
+    SpinPolarization = 16
+    ShannonEntropyDensity = 17
+    FisherInformationDensity = 18
+    AverageLocalIonizationEnergy = 19
+    LocalElectronAffinity = 20
+    LocalElectronAttachmentEnergy = 21
+    LocalElectronegativity = 22
+    LocalHardness = 23
+    OrbitalGradient = 24
+    OrbitalHessian = 25
+    OrbitalWeightedFukuiPlus = 26
+    OrbitalWeightedFukuiMinus = 27
+    OrbitalWeightedFukuiZero = 28
+    OrbitalWeightedDualDescriptor = 29
+    TauComponents = 30
+    HamiltonianKineticEnergyComponents = 31
+    PotentialKineticRatio = 32
+    EnergyDensityPerElectron = 33
+    KineticEnergyPerElectron = 34
+    ElfTsirelsonStash = 35
+    LolTsirelsonStash = 36
+
+
+class DensityComponent(enum.IntEnum):
+    Total = 0
+    Alpha = 1
+    Beta = 2
+    Difference = 3
+
+
+class SpinChannel(enum.IntEnum):
+    Alpha = 0
+    Beta = 1
+
+
+class Backend(enum.IntEnum):
+    AUTO = 0
+    AO_P = 1
+    AO_MO = 2
+
+
+class Precision(enum.IntEnum):
+    FP64 = 0
+    Mixed = 1
+
+
+def channels(kind: int) -> int:
+    return 3 if kind in (1, 24, 30, 31) else (6 if kind in (2, 25) else 1)
+
+
+@dataclass(frozen=True)
+class Property:
+    kind: int
+    component: int = 0
+    channel: int = 0
+    orbital_index: int = 0
+
+
+def density(kind: PropertyKind, component: DensityComponent = DensityComponent.Total) -> Property:
+    return Property(int(kind), int(component))
+
+
+def orbital(index: int, channel: SpinChannel = SpinChannel.Alpha, kind: PropertyKind = PropertyKind.Orbital) -> Property:
+    return Property(int(kind), 0, int(channel), index)
+
+
+class KumoError(RuntimeError):
+    """Error raised for a non-zero kumo_status; .status holds the code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+class InvalidArgument(KumoError, ValueError):
+    pass
+
+
+class OutOfRange(KumoError, IndexError):
+    pass
+
+
+_EXC = {1: InvalidArgument, 2: OutOfRange}
+
+
+class _Property(C.Structure):
+    _fields_ = [("kind", C.c_int), ("component", C.c_int), ("channel", C.c_int), ("orbital_index", C.c_longlong)]
+
+
+class _Options(C.Structure):
+    _fields_ = [("block_size", C.c_longlong), ("backend", C.c_int), ("screening_threshold", C.c_double),
+                ("potential_tolerance", C.c_double), ("precision", C.c_int)]
+
+
+class _Grid(C.Structure):
+    _fields_ = [("origin", C.c_double * 3), ("steps", C.c_double * 9), ("counts", C.c_int * 3)]
+
+
+class _Info(C.Structure):
+    _fields_ = [("natoms", C.c_int), ("nbasis", C.c_int), ("nalpha", C.c_int), ("nbeta", C.c_int),
+                ("nmo_alpha", C.c_int), ("nmo_beta", C.c_int), ("unrestricted", C.c_int),
+                ("ao_mo_eligible", C.c_int), ("check_errors", C.c_double * 4), ("nblocks", C.c_int),
+                ("device_bytes", C.c_longlong)]
+
+
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+_lib = None
+
+EXPORTS = [
+    "kumo_default_options", "kumo_molecule_from_fchk", "kumo_molecule_from_arrays", "kumo_molecule_destroy",
+    "kumo_molecule_info_get", "kumo_molecule_atoms", "kumo_molecule_block", "kumo_evaluate_grid",
+    "kumo_evaluate_points", "kumo_evaluate_grid_device", "kumo_evaluate_points_device", "kumo_ao_panels",
+    "kumo_screening_masks", "kumo_boys", "kumo_esp_pair_count", "kumo_write_cube", "kumo_grid_around",
+    "kumo_profile_enable", "kumo_profile_reset", "kumo_profile_read", "kumo_set_device",
+]
+
+
+class _ProfileEntry(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_int), ("ms", C.c_double), ("kept_rows", C.c_double),
+                ("units", C.c_double), ("flops", C.c_double), ("bytes", C.c_double)]
+
+
+def lib():
+    """The loaded C library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with chem-kumo_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        eb = [C.c_char_p, C.c_size_t]
+        L.kumo_default_options.argtypes = [C.POINTER(_Options)]
+        L.kumo_molecule_from_fchk.argtypes = [C.c_char_p, C.POINTER(C.c_void_p), *eb]
+        L.kumo_molecule_from_arrays.argtypes = [C.c_int, _I, _D, _D, C.c_int, _I, _I, _I, _D, _D, _D, _D, C.c_int,
+                                                _D, _D, C.c_int, C.c_int, _D, C.c_int, _D, C.c_int,
+                                                C.POINTER(C.c_void_p), *eb]
+        L.kumo_molecule_destroy.argtypes = [C.c_void_p]
+        L.kumo_molecule_info_get.argtypes = [C.c_void_p, C.POINTER(_Info)]
+        L.kumo_molecule_atoms.argtypes = [C.c_void_p, _I, _D, _D]
+        L.kumo_molecule_block.argtypes = [C.c_void_p, C.c_int, _I, _I, _I, _I, _I, _D]
+        L.kumo_evaluate_grid.argtypes = [C.c_void_p, C.POINTER(_Options), C.POINTER(_Grid), C.POINTER(_Property),
+                                         C.c_int, C.POINTER(_D), _I, *eb]
+        L.kumo_evaluate_points.argtypes = [C.c_void_p, C.POINTER(_Options), _D, C.c_longlong, C.POINTER(_Property),
+                                           C.c_int, C.POINTER(_D), _I, *eb]
+        L.kumo_evaluate_grid_device.argtypes = [C.c_void_p, C.POINTER(_Options), C.POINTER(_Grid),
+                                                C.POINTER(_Property), C.c_int, C.POINTER(_D), C.c_void_p, _I, *eb]
+        L.kumo_evaluate_points_device.argtypes = [C.c_void_p, C.POINTER(_Options), _D, C.c_longlong,
+                                                  C.POINTER(_Property), C.c_int, C.POINTER(_D), C.c_void_p, _I, *eb]
+        L.kumo_ao_panels.argtypes = [C.c_void_p, _D, C.c_int, C.c_int, C.c_int, _D, *eb]
+        L.kumo_screening_masks.argtypes = [C.c_void_p, C.POINTER(_Grid), C.c_longlong, C.c_int, C.c_double,
+                                           C.POINTER(C.c_ubyte), *eb]
+        L.kumo_boys.argtypes = [_D, C.c_longlong, C.c_int, _D, *eb]
+        L.kumo_esp_pair_count.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), *eb]
+        L.kumo_write_cube.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(_Grid), C.c_int, _I, _D, _D, _D,
+                                      C.c_longlong, *eb]
+        L.kumo_grid_around.argtypes = [C.c_void_p, C.c_double, C.c_double, C.POINTER(_Grid), *eb]
+        L.kumo_profile_enable.argtypes = [C.c_int]
+        L.kumo_set_device.argtypes = [C.c_int, *eb]
+        L.kumo_profile_read.argtypes = [C.POINTER(_ProfileEntry), C.c_int]
+        _lib = L
+    return _lib
+
+
+def _check(status: int, err) -> None:
+    if status:
+        raise _EXC.get(status, KumoError)(status, err.value.decode(errors="replace"))
+
+
+def _err():
+    return C.create_string_buffer(512)
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(_D)
+
+
+@dataclass
+class Grid:
+    """origin (3,), steps (3, 3) with steps[:, a] the step vector of axis a, counts (3,)."""
+    origin: np.ndarray
+    steps: np.ndarray
+    counts: Tuple[int, int, int]
+
+    @property
+    def npoints(self) -> int:
+        return int(np.prod(self.counts))
+
+    def _c(self) -> _Grid:
+        g = _Grid()
+        for k in range(3):
+            g.origin[k] = float(self.origin[k])
+            g.counts[k] = int(self.counts[k])
+        st = np.asarray(self.steps, dtype=float)
+        for a in range(3):
+            for r in range(3):
+                g.steps[3 * a + r] = float(st[r, a])
+        return g
+
+    def points(self) -> np.ndarray:
+        """Points in Field order (k fastest), shape (N, 3)."""
+        n0, n1, n2 = self.counts
+        i, j, k = np.meshgrid(np.arange(n0), np.arange(n1), np.arange(n2), indexing="ij")
+        ijk = np.stack([i.ravel(), j.ravel(), k.ravel()], 1).astype(float)
+        return self.origin[None, :] + ijk @ np.asarray(self.steps).T
+
+
+def _options(block_size=128, backend=0, threshold=1e-12, potential_tolerance=0.0, precision=0) -> _Options:
+    return _Options(int(block_size), int(backend), float(threshold), float(potential_tolerance), int(precision))
+
+
+def _props(props: Sequence[Property]):
+    arr = (_Property * max(len(props), 1))()
+    for i, p in enumerate(props):
+        arr[i] = _Property(int(p.kind), int(p.component), int(p.channel), int(p.orbital_index))
+    return arr
+
+
+class Molecule:
+    """Molecule::from_fchk with its device-resident copy (created on first use)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def from_fchk(cls, path: str) -> "Molecule":
+        h = C.c_void_p()
+        e = _err()
+        _check(lib().kumo_molecule_from_fchk(path.encode(), C.byref(h), e, 512), e)
+        return cls(h)
+
+    @classmethod
+    def from_records(cls, rec: Dict[str, object]) -> "Molecule":
+        """From FCHK records as returned by kumo_b200.synth.read_fchk."""
+        L = lib()
+        z = np.ascontiguousarray(rec["Atomic numbers"], dtype=np.int32)
+        charges = np.ascontiguousarray(rec.get("Nuclear charges", z.astype(float)), dtype=float)
+        xyz = np.ascontiguousarray(rec["Current cartesian coordinates"], dtype=float)
+        types = np.ascontiguousarray(rec["Shell types"], dtype=np.int32)
+        nprim = np.ascontiguousarray(rec["Number of primitives per shell"], dtype=np.int32)
+        atom = np.ascontiguousarray(rec["Shell to atom map"], dtype=np.int32)
+        ex = np.ascontiguousarray(rec["Primitive exponents"], dtype=float)
+        co = np.ascontiguousarray(rec["Contraction coefficients"], dtype=float)
+        pc = rec.get("P(S=P) Contraction coefficients")
+        pc = None if pc is None else np.ascontiguousarray(pc, dtype=float)
+        sxyz = np.ascontiguousarray(rec["Coordinates of each shell"], dtype=float)
+        n = int(rec["Number of basis functions"])
+        pt = np.ascontiguousarray(rec["Total SCF Density"], dtype=float)
+        ps = rec.get("Spin SCF Density")
+        ps = None if ps is None else np.ascontiguousarray(ps, dtype=float)
+        ca = np.ascontiguousarray(rec.get("Alpha MO coefficients", np.zeros(0)), dtype=float)
+        cb = rec.get("Beta MO coefficients")
+        cb = None if cb is None else np.ascontiguousarray(cb, dtype=float)
+        h = C.c_void_p()
+        e = _err()
+        _check(L.kumo_molecule_from_arrays(
+            len(z), z.ctypes.data_as(_I), _dp(charges), _dp(xyz), len(types), types.ctypes.data_as(_I),
+            nprim.ctypes.data_as(_I), atom.ctypes.data_as(_I), _dp(ex), _dp(co), _dp(pc) if pc is not None else None,
+            _dp(sxyz), n, _dp(pt), _dp(ps) if ps is not None else None, int(rec["Number of alpha electrons"]),
+            int(rec["Number of beta electrons"]), _dp(ca) if ca.size else None, ca.size // n,
+            _dp(cb) if cb is not None else None, 0 if cb is None else cb.size // n, C.byref(h), e, 512), e)
+        return cls(h)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().kumo_molecule_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> Dict[str, object]:
+        i = _Info()
+        lib().kumo_molecule_info_get(self._h, C.byref(i))
+        return {"natoms": i.natoms, "nbasis": i.nbasis, "nalpha": i.nalpha, "nbeta": i.nbeta,
+                "nmo_alpha": i.nmo_alpha, "nmo_beta": i.nmo_beta, "unrestricted": bool(i.unrestricted),
+                "ao_mo_eligible": bool(i.ao_mo_eligible), "check_errors": list(i.check_errors),
+                "nblocks": i.nblocks, "device_bytes": i.device_bytes}
+
+    def atoms(self) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        n = self.info()["natoms"]
+        z = np.zeros(n, dtype=np.int32)
+        q = np.zeros(n)
+        x = np.zeros(3 * n)
+        lib().kumo_molecule_atoms(self._h, z.ctypes.data_as(_I), _dp(q), _dp(x))
+        return z, q, x.reshape(n, 3)
+
+    def blocks(self) -> List[Tuple[int, int, int, int, int, float]]:
+        out = []
+        for i in range(self.info()["nblocks"]):
+            v = [C.c_int() for _ in range(5)]
+            r2 = C.c_double()
+            lib().kumo_molecule_block(self._h, i, *[C.byref(x) for x in v], C.byref(r2))
+            out.append(tuple(x.value for x in v) + (r2.value,))
+        return out
+
+    def grid_around(self, margin: float, spacing: float) -> Grid:
+        g = _Grid()
+        e = _err()
+        _check(lib().kumo_grid_around(self._h, margin, spacing, C.byref(g), e, 512), e)
+        st = np.zeros((3, 3))
+        for a in range(3):
+            for r in range(3):
+                st[r, a] = g.steps[3 * a + r]
+        return Grid(np.array(list(g.origin)), st, tuple(g.counts))
+
+    # -- kernel seams --------------------------------------------------------
+    def ao_panels(self, points: np.ndarray, order: int, precision: int = 0) -> np.ndarray:
+        """AO panels as [panel, ao, point] (BasisEvaluator::evaluate_derivatives_batch layout transposed)."""
+        pts = np.ascontiguousarray(points, dtype=float).reshape(-1, 3)
+        n = self.info()["nbasis"]
+        panels = 1 if order == 0 else (4 if order == 1 else 10)
+        out = np.zeros((panels * len(pts), n))
+        e = _err()
+        _check(lib().kumo_ao_panels(self._h, _dp(pts), len(pts), order, precision, _dp(out), e, 512), e)
+        return out.reshape(panels, len(pts), n).transpose(0, 2, 1).copy()
+
+    def screening_masks(self, grid: Grid, block_size: int, ao_order: int, threshold: float) -> np.ndarray:
+        n = self.info()["nbasis"]
+        nb = (grid.npoints + block_size - 1) // block_size
+        mask = np.zeros((nb, n), dtype=np.uint8)
+        e = _err()
+        g = grid._c()
+        _check(lib().kumo_screening_masks(self._h, C.byref(g), block_size, ao_order, threshold,
+                                          mask.ctypes.data_as(C.POINTER(C.c_ubyte)), e, 512), e)
+        return mask
+
+    def esp_pair_count(self) -> int:
+        c = C.c_longlong()
+        e = _err()
+        _check(lib().kumo_esp_pair_count(self._h, C.byref(c), e, 512), e)
+        return c.value
+
+
+class Evaluator:
+    """chem-kumo's Evaluator over the C ABI (host arrays in and out)."""
+
+    def __init__(self, molecule: Molecule, block_size: int = 128, backend: int = 0, threshold: float = 1e-12,
+                 potential_tolerance: float = 0.0, precision: int = 0):
+        self.m = molecule
+        self.opt = _options(block_size, backend, threshold, potential_tolerance, precision)
+
+    def _outs(self, props, n):
+        outs = [np.zeros((channels(p.kind), n)) for p in props]
+        ptrs = (_D * max(len(props), 1))(*[_dp(o) for o in outs])
+        return outs, ptrs
+
+    def evaluate_grid(self, grid: Grid, props: Sequence[Property]) -> Tuple[List[np.ndarray], int]:
+        outs, ptrs = self._outs(props, grid.npoints)
+        used = C.c_int()
+        e = _err()
+        g = grid._c()
+        _check(lib().kumo_evaluate_grid(self.m._h, C.byref(self.opt), C.byref(g), _props(props), len(props), ptrs,
+                                        C.byref(used), e, 512), e)
+        return outs, used.value
+
+    def evaluate_points(self, points: np.ndarray, props: Sequence[Property]) -> Tuple[List[np.ndarray], int]:
+        pts = np.ascontiguousarray(points, dtype=float).reshape(-1, 3)
+        outs, ptrs = self._outs(props, len(pts))
+        used = C.c_int()
+        e = _err()
+        _check(lib().kumo_evaluate_points(self.m._h, C.byref(self.opt), _dp(pts), len(pts), _props(props),
+                                          len(props), ptrs, C.byref(used), e, 512), e)
+        return outs, used.value
+
+    def evaluate_grid_device(self, grid: Grid, props: Sequence[Property], outputs: Sequence[int],
+                             stream: int = 0) -> int:
+        """outputs: device pointers (e.g. torch tensor data_ptr()), one per property."""
+        ptrs = (_D * max(len(props), 1))(*[C.cast(C.c_void_p(int(o)), _D) for o in outputs])
+        used = C.c_int()
+        e = _err()
+        g = grid._c()
+        _check(lib().kumo_evaluate_grid_device(self.m._h, C.byref(self.opt), C.byref(g), _props(props), len(props),
+                                               ptrs, C.c_void_p(stream), C.byref(used), e, 512), e)
+        return used.value
+
+    def evaluate_points_device(self, points_ptr: int, npoints: int, props: Sequence[Property],
+                               outputs: Sequence[int], stream: int = 0) -> int:
+        ptrs = (_D * max(len(props), 1))(*[C.cast(C.c_void_p(int(o)), _D) for o in outputs])
+        used = C.c_int()
+        e = _err()
+        _check(lib().kumo_evaluate_points_device(self.m._h, C.byref(self.opt), C.cast(C.c_void_p(points_ptr), _D),
+                                                 npoints, _props(props), len(props), ptrs, C.c_void_p(stream),
+                                                 C.byref(used), e, 512), e)
+        return used.value
+
+
+def boys(t: np.ndarray, nvalues: int) -> np.ndarray:
+    t = np.ascontiguousarray(t, dtype=float).ravel()
+    out = np.zeros((len(t), nvalues))
+    e = _err()
+    _check(lib().kumo_boys(_dp(t), len(t), nvalues, _dp(out), e, 512), e)
+    return out
+
+
+def write_cube(path: str, grid: Grid, z, charges, xyz, values: np.ndarray, comment: str = "Electron density",
+               orbital_index: int = 0) -> None:
+    z = np.ascontiguousarray(z, dtype=np.int32)
+    q = np.ascontiguousarray(charges, dtype=float)
+    x = np.ascontiguousarray(xyz, dtype=float).ravel()
+    v = np.ascontiguousarray(values, dtype=float).ravel()
+    e = _err()
+    g = grid._c()
+    _check(lib().kumo_write_cube(path.encode(), comment.encode(), C.byref(g), len(z), z.ctypes.data_as(_I), _dp(q),
+                                 _dp(x), _dp(v), orbital_index, e, 512), e)
+
+
+def set_device(device: int) -> None:
+    e = _err()
+    _check(lib().kumo_set_device(int(device), e, 512), e)
+
+
+def profile_enable(on: bool = True) -> None:
+    lib().kumo_profile_enable(1 if on else 0)
+
+
+def profile_reset() -> None:
+    lib().kumo_profile_reset()
+
+
+def profile_read() -> Dict[str, Dict[str, float]]:
+    arr = (_ProfileEntry * 16)()
+    n = lib().kumo_profile_read(arr, 16)
+    if n < 0:
+        raise KumoError(3, "profile read failed")
+    return {arr[i].name.decode(): {"launches": arr[i].launches, "ms": arr[i].ms, "kept_rows": arr[i].kept_rows,
+                                   "units": arr[i].units, "flops": arr[i].flops, "bytes": arr[i].bytes}
+            for i in range(n)}

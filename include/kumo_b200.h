@@ -1,0 +1,202 @@
+/*
+ * kumo_b200.h: C ABI of the B200 grid evaluator for chem-kumo.
+ *
+ * Plain pointers and sizes only.  Every entry point returns a kumo_status
+ * and, where it takes one, writes a one-line message into `err` (errlen
+ * bytes, NUL-terminated).  Status codes map the exception types of the
+ * chem-kumo C++ API: KUMO_INVALID_ARGUMENT = std::invalid_argument,
+ * KUMO_OUT_OF_RANGE = std::out_of_range, KUMO_RUNTIME_ERROR =
+ * std::runtime_error; device failures are KUMO_CUDA_ERROR and never abort.
+ *
+ * Reference interfaces are cited as path:line inside the chem-kumo 2.1.0
+ * sources.  Layout conventions:
+ *  - points: 3 x N, point j at points[3j .. 3j+2] (bohr), like the columns of
+ *    the reference's Eigen::Matrix<double, 3, Dynamic>;
+ *  - a grid: origin[3], steps[9] with steps[3a + r] = component r of the step
+ *    vector of axis a, counts[3]; values in Field order (k fastest);
+ *  - property outputs: channels(kind) arrays of N doubles, component-major
+ *    (gradient x, y, z; Hessian xx, xy, xz, yy, yz, zz).
+ */
+#ifndef KUMO_B200_H
+#define KUMO_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KUMO_B200_ABI_VERSION 1
+
+typedef enum {
+    KUMO_OK = 0,
+    KUMO_INVALID_ARGUMENT = 1,
+    KUMO_OUT_OF_RANGE = 2,
+    KUMO_RUNTIME_ERROR = 3,
+    KUMO_CUDA_ERROR = 4,
+    KUMO_OUT_OF_MEMORY = 5
+} kumo_status;
+
+/* Backend (include/chem/kumo/evaluator.hpp:403): 0 AUTO, 1 AO_P, 2 AO_MO. */
+/* Precision: 0 FP64, 1 mixed (FP32 AO values, tensor-core contractions). */
+
+/* One requested property (include/chem/kumo/evaluator.hpp:174-187): kind is
+ * the PropertyKind value (evaluator.hpp:109-153), component the
+ * DensityComponent (spin.hpp: Total 0, Alpha 1, Beta 2, Difference 3),
+ * channel the SpinChannel (Alpha 0, Beta 1), orbital_index one-based. */
+typedef struct {
+    int kind;
+    int component;
+    int channel;
+    long long orbital_index;
+} kumo_property;
+
+/* EvaluationOptions (include/chem/kumo/evaluator.hpp:406-441) plus the
+ * arithmetic precision. */
+typedef struct {
+    long long block_size;       /* 1..128 on the device (default 128) */
+    int backend;
+    double screening_threshold; /* default 1e-12 */
+    double potential_tolerance; /* 0: exact electrostatic potential */
+    int precision;
+} kumo_options;
+
+typedef struct {
+    double origin[3];
+    double steps[9];
+    int counts[3];
+} kumo_grid;
+
+typedef struct {
+    int natoms;
+    int nbasis;
+    int nalpha, nbeta;
+    int nmo_alpha, nmo_beta;
+    int unrestricted;
+    int ao_mo_eligible;        /* ElectronicStructureInfo::ao_mo_eligible() */
+    double check_errors[4];    /* total abs, total rel, spin abs, spin rel */
+    int nblocks;               /* AO blocks after splitting SP shells */
+    long long device_bytes;    /* HBM held by the resident copy (0 before first use) */
+} kumo_molecule_info;
+
+/* Opaque molecule: the host Molecule and its device-resident copy (AO
+ * tables, density matrices, MO coefficients). */
+typedef struct kumo_molecule kumo_molecule;
+
+/* Fill *opt with the reference defaults (block 128, AUTO, 1e-12, 1e-8, FP64). */
+void kumo_default_options(kumo_options* opt);
+
+/* Select the CUDA device used by the calls of this thread (one process per
+ * GPU; no counterpart in the CPU-only reference). */
+int kumo_set_device(int device, char* err, size_t errlen);
+
+/* Molecule::from_fchk (include/chem/kumo/density.hpp:218; src/molecule.cpp:153-180). */
+int kumo_molecule_from_fchk(const char* path, kumo_molecule** out, char* err, size_t errlen);
+
+/* Molecule from in-memory FCHK records (the records read by
+ * src/basis.cpp:21-48 and src/molecule.cpp:39-180): shell types, primitive
+ * counts, shell-to-atom map (one-based), exponents, contraction and P(S=P)
+ * coefficients (p_coefs may be NULL), shell coordinates; packed lower
+ * triangles of the total and spin density matrices (spin may be NULL);
+ * MO coefficients MO by MO (AO fastest; beta NULL for restricted). */
+int kumo_molecule_from_arrays(int natoms, const int* atomic_numbers, const double* nuclear_charges,
+                              const double* coordinates, int nshell, const int* shell_types,
+                              const int* nprim, const int* shell_atom, const double* exponents,
+                              const double* coefs, const double* p_coefs, const double* shell_xyz,
+                              int nbasis, const double* packed_total, const double* packed_spin,
+                              int nalpha, int nbeta, const double* alpha_mos, int nmo_alpha,
+                              const double* beta_mos, int nmo_beta, kumo_molecule** out, char* err,
+                              size_t errlen);
+
+void kumo_molecule_destroy(kumo_molecule* m);
+
+/* Molecule::atoms, electronic_structure_info, basis_size, occupied_count,
+ * orbital_count (include/chem/kumo/density.hpp:221-256). */
+int kumo_molecule_info_get(const kumo_molecule* m, kumo_molecule_info* info);
+/* atomic numbers (natoms), nuclear charges (natoms), positions (3 natoms). */
+int kumo_molecule_atoms(const kumo_molecule* m, int* z, double* charges, double* xyz);
+/* Prepared AO block i (BasisEvaluator::PreparedBlock,
+ * include/chem/kumo/basis_evaluator.hpp:118-131): l, nprim, AO offset, AO
+ * count, pure flag and squared cutoff radius. */
+int kumo_molecule_block(const kumo_molecule* m, int i, int* l, int* nprim, int* offset, int* count,
+                        int* pure, double* cutoff_r2);
+
+/* Evaluator::evaluate(const Grid&, const Request&)
+ * (include/chem/kumo/evaluator.hpp:506; src/evaluator.cpp:804-809).
+ * outputs[i] (host) receives property i; *backend_used = 1 AO_P or 2 AO_MO. */
+int kumo_evaluate_grid(const kumo_molecule* m, const kumo_options* opt, const kumo_grid* grid,
+                       const kumo_property* props, int nprops, double* const* outputs,
+                       int* backend_used, char* err, size_t errlen);
+
+/* Evaluator::evaluate(points, request) (include/chem/kumo/evaluator.hpp:516-518;
+ * src/evaluator.cpp:821-826); points and outputs on the host. */
+int kumo_evaluate_points(const kumo_molecule* m, const kumo_options* opt, const double* points,
+                         long long npoints, const kumo_property* props, int nprops,
+                         double* const* outputs, int* backend_used, char* err, size_t errlen);
+
+/* Device-resident forms of the two calls above: outputs (and points) are
+ * device pointers, work is queued on `stream` (a cudaStream_t, NULL for the
+ * default stream) and the call returns once it is queued. */
+int kumo_evaluate_grid_device(const kumo_molecule* m, const kumo_options* opt, const kumo_grid* grid,
+                              const kumo_property* props, int nprops, double* const* outputs,
+                              void* stream, int* backend_used, char* err, size_t errlen);
+int kumo_evaluate_points_device(const kumo_molecule* m, const kumo_options* opt,
+                                const double* device_points, long long npoints,
+                                const kumo_property* props, int nprops, double* const* outputs,
+                                void* stream, int* backend_used, char* err, size_t errlen);
+
+/* BasisEvaluator::evaluate_derivatives_batch / evaluate_batch
+ * (include/chem/kumo/basis_evaluator.hpp:101-115; src/basis_evaluator.cpp:512-678)
+ * on the device: order 0 (values), 1 or 2; out (host) is nao x (panels*npts)
+ * column-major, component c of point j in column c*npts + j.  npts <= 128. */
+int kumo_ao_panels(const kumo_molecule* m, const double* points, int npts, int order, int precision,
+                   double* out, char* err, size_t errlen);
+
+/* Screening masks of significant_aos (src/ao_screening.hpp:35-50) for the
+ * blocks of `block_size` points of a grid: mask (host) is nblocks x nao bytes,
+ * 1 where the AO is kept.  ao_order selects the panels (0, 1 or 2). */
+int kumo_screening_masks(const kumo_molecule* m, const kumo_grid* grid, long long block_size,
+                         int ao_order, double threshold, unsigned char* mask, char* err,
+                         size_t errlen);
+
+/* detail::boys_function (src/boys_function.cpp:47-76) on the device:
+ * out[i * nvalues + m] = F_m(t[i]), nvalues <= 33 (host arrays). */
+int kumo_boys(const double* t, long long n, int nvalues, double* out, char* err, size_t errlen);
+
+/* Number of primitive pairs of the electrostatic potential
+ * (ElectrostaticPotential::primitive_pair_count, src/electrostatic_potential.hpp:61). */
+int kumo_esp_pair_count(const kumo_molecule* m, long long* count, char* err, size_t errlen);
+
+/* Field::write_cube / write_orbital_cube (include/chem/kumo/density.hpp:120-128;
+ * src/cube.cpp:70-111); orbital_index 0 writes a density Cube. */
+int kumo_write_cube(const char* path, const char* comment, const kumo_grid* grid, int natoms,
+                    const int* atomic_numbers, const double* charges, const double* xyz,
+                    const double* values, long long orbital_index, char* err, size_t errlen);
+
+/* Grid::around / line / plane (include/chem/kumo/density.hpp:72-91). */
+int kumo_grid_around(const kumo_molecule* m, double margin, double spacing, kumo_grid* out,
+                     char* err, size_t errlen);
+
+/* Kernel timing of the evaluation waves (no counterpart in the reference,
+ * whose benchmarks time whole calls): when enabled, every launch of the
+ * device kernels is bracketed by CUDA events on its stream and the kept AO
+ * rows of every screening block are summed on the device. */
+typedef struct {
+    char name[32];
+    int launches;
+    double ms;        /* summed event time */
+    double kept_rows; /* sum over blocks of the kept AO rows */
+    double units;     /* blocks (AO build, contractions) or point-pair interactions (ESP) */
+    double flops;     /* algorithmic FLOPs of the contractions */
+    double bytes;
+} kumo_profile_entry;
+
+void kumo_profile_enable(int on);
+void kumo_profile_reset(void);
+/* Synchronizes and returns the number of entries written (<= max_entries). */
+int kumo_profile_read(kumo_profile_entry* out, int max_entries);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

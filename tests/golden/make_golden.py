@@ -1,0 +1,136 @@
+"""Build the golden fixtures of this directory from chem-kumo's own test data.
+
+Run once in a checkout that has the chem-kumo sources (argument: their root):
+
+    python tests/golden/make_golden.py /path/to/chem-kumo
+
+It copies the three small FCHK inputs of the reference tests (O2, water
+def2-TZVP, acrolein) and stores, for each reference Cube file used below, the
+Cube header (origin, step vectors, counts, atoms) and a seeded sample of its
+grid points with their values:
+
+* Gaussian ``cubegen`` densities of O2 (total, alpha, beta, spin) and acrolein,
+  checked in chem-kumo by ``tests/cube_reference_test.cpp:146-160``
+  (max abs <= 2e-3, relative L1 <= 1e-5); Gaussian MO cubes checked by
+  ``tests/orbital_reference_test.cpp`` (<= 2e-4);
+* Multiwfn Cube files of derived fields of water and O2, checked by
+  ``tests/multiwfn_reference_test.cpp:351-420`` (2e-5 relative, field-specific
+  extras).
+
+Gaussian Cube headers round the step to six decimals; the standard 1/6 bohr
+step is restored exactly as ``tests/cube_reference_test.cpp:27-37`` does.
+"""
+from __future__ import annotations
+
+import gzip
+import os
+import shutil
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+GAUSSIAN = [
+    ("o2_density", "o2.fchk.gz", "data/o2_density.cube"),
+    ("o2_alpha", "o2.fchk.gz", "data/o2_alpha.cube"),
+    ("o2_beta", "o2.fchk.gz", "data/o2_beta.cube"),
+    ("o2_spin", "o2.fchk.gz", "data/o2_spin.cube"),
+    ("acrolein_density", "acrolein.fchk.gz", "data/acrolein_density.cube"),
+    ("o2_alpha_mo_9", "o2.fchk.gz", "data/mo_reference_cubes/o2_alpha_mo_9.cube"),
+    ("o2_beta_mo_7", "o2.fchk.gz", "data/mo_reference_cubes/o2_beta_mo_7.cube"),
+    ("acrolein_mo_15", "acrolein.fchk.gz", "data/mo_reference_cubes/acrolein_mo_15.cube"),
+]
+
+MULTIWFN = [
+    ("h2o_elf", "h2o_b3lyp_def2tzvp.fchk.gz"),
+    ("h2o_rdg", "h2o_b3lyp_def2tzvp.fchk.gz"),
+    ("h2o_sign_lambda2_rho", "h2o_b3lyp_def2tzvp.fchk.gz"),
+    ("h2o_esp", "h2o_b3lyp_def2tzvp.fchk.gz"),
+    ("h2o_lol", "h2o_b3lyp_def2tzvp.fchk.gz"),
+    ("h2o_iri", "h2o_b3lyp_def2tzvp.fchk.gz"),
+    ("h2o_dori", "h2o_b3lyp_def2tzvp.fchk.gz"),
+    ("h2o_kinetic_k", "h2o_b3lyp_def2tzvp.fchk.gz"),
+    ("h2o_kinetic_g", "h2o_b3lyp_def2tzvp.fchk.gz"),
+    ("h2o_potential_energy", "h2o_b3lyp_def2tzvp.fchk.gz"),
+    ("h2o_energy_density", "h2o_b3lyp_def2tzvp.fchk.gz"),
+    ("h2o_shannon", "h2o_b3lyp_def2tzvp.fchk.gz"),
+    ("h2o_fisher", "h2o_b3lyp_def2tzvp.fchk.gz"),
+    ("h2o_elf_ts", "h2o_b3lyp_def2tzvp.fchk.gz"),
+    ("h2o_lol_ts", "h2o_b3lyp_def2tzvp.fchk.gz"),
+    ("o2_elf", "o2.fchk.gz"),
+    ("o2_esp", "o2.fchk.gz"),
+    ("o2_lol", "o2.fchk.gz"),
+    ("o2_spin_polarization", "o2.fchk.gz"),
+]
+
+FCHK_SOURCES = {
+    "o2.fchk.gz": "data/o2.fchk.gz",
+    "acrolein.fchk.gz": "data/acrolein.fchk.gz",
+    "h2o_b3lyp_def2tzvp.fchk.gz": "data/hybrids/h2o_b3lyp_def2tzvp.fchk.gz",
+}
+
+
+def read_cube(path: str):
+    opener = gzip.open if path.endswith(".gz") else open
+    with opener(path, "rt") as f:
+        lines = f.read().split("\n")
+    head = lines[2].split()
+    natoms = int(head[0])
+    origin = np.array([float(x) for x in head[1:4]])
+    counts = []
+    steps = np.zeros((3, 3))  # column a = step vector of axis a
+    for a in range(3):
+        parts = lines[3 + a].split()
+        counts.append(int(parts[0]))
+        steps[:, a] = [float(x) for x in parts[1:4]]
+    atoms = []
+    for i in range(abs(natoms)):
+        parts = lines[6 + i].split()
+        atoms.append([float(x) for x in parts[:5]])
+    start = 6 + abs(natoms)
+    if natoms < 0:
+        start += 1  # orbital cube: "NMO index" line
+    values = np.array([float(t.replace("D", "E")) for line in lines[start:] for t in line.split()])
+    assert values.size == counts[0] * counts[1] * counts[2], path
+    return origin, steps, np.array(counts), np.array(atoms), values
+
+
+def recover_standard_step(steps: np.ndarray) -> np.ndarray:
+    steps = steps.copy()
+    h = 1.0 / 6.0
+    for a in range(3):
+        if abs(steps[a, a] - h) < 0.5e-6 + 1e-12:
+            steps[a, a] = h
+    return steps
+
+
+def sample(values: np.ndarray, rng: np.random.Generator, n_random: int, n_top: int) -> np.ndarray:
+    idx = rng.choice(values.size, size=min(n_random, values.size), replace=False)
+    top = np.argsort(-np.abs(values))[:n_top]
+    return np.unique(np.concatenate([idx, top]))
+
+
+def main(root: str) -> None:
+    tests = os.path.join(root, "tests")
+    for name, rel in FCHK_SOURCES.items():
+        shutil.copyfile(os.path.join(tests, rel), os.path.join(HERE, name))
+    rng = np.random.default_rng(2024)
+    for key, fchk, rel in GAUSSIAN:
+        origin, steps, counts, atoms, values = read_cube(os.path.join(tests, rel))
+        steps = recover_standard_step(steps)
+        idx = sample(values, rng, 6000, 300)
+        np.savez_compressed(os.path.join(HERE, f"gaussian_{key}.npz"), fchk=fchk, origin=origin,
+                            steps=steps, counts=counts, atoms=atoms, index=idx.astype(np.int64),
+                            values=values[idx], total_abs=np.abs(values).sum(), npoints=values.size)
+    for key, fchk in MULTIWFN:
+        origin, steps, counts, atoms, values = read_cube(os.path.join(tests, "data", "multiwfn", key + ".cube.gz"))
+        idx = sample(values, rng, 4000, 100)
+        np.savez_compressed(os.path.join(HERE, f"multiwfn_{key}.npz"), fchk=fchk, origin=origin,
+                            steps=steps, counts=counts, atoms=atoms, index=idx.astype(np.int64),
+                            values=values[idx], npoints=values.size)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,277 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle and with
+chem-kumo's golden data.  Tolerances: FP64 fields within 1e-12 of the oracle
+in the scaled metric max|gpu - ref| / max(1, max|ref|)
+(tests/density_screening_test.cpp:137-150 of chem-kumo); screening masks and
+point order bit-exact; mixed precision within 1e-7 of FP64 in the same
+metric."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden_points, scaled_error
+
+import kumo_b200 as K
+from kumo_b200 import synth
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+P = K.PropertyKind
+D = K.DensityComponent
+
+
+@pytest.fixture(scope="module")
+def water28(tmp_path_factory):
+    path = str(tmp_path_factory.mktemp("w") / "water_28.fchk")
+    synth.write_fchk(synth.water(0), path)
+    return path
+
+
+def _pair(path):
+    return K.Molecule.from_fchk(path), O.OracleMolecule.from_fchk(path)
+
+
+def _box_points(xyz, n, seed, margin=2.5):
+    rng = np.random.default_rng(seed)
+    lo, hi = xyz.min(0) - margin, xyz.max(0) + margin
+    pts = rng.uniform(lo, hi, (n, 3))
+    pts[: len(xyz)] = xyz  # include the nuclei themselves
+    return pts
+
+
+@pytest.mark.parametrize("name", ["o2.fchk.gz", "h2o_b3lyp_def2tzvp.fchk.gz", "acrolein.fchk.gz"])
+def test_ao_panels_fp64(name):
+    m, o = _pair(os.path.join(GOLDEN, name))
+    pts = _box_points(o.atom_xyz.reshape(-1, 3), 128, 1)
+    for order in (0, 1, 2):
+        g = m.ao_panels(pts, order)
+        r = o.ao_values(pts)[None] if order == 0 else o.ao_derivatives(pts, order)
+        scale = np.maximum(np.abs(r), 1e-300)
+        rel = np.abs(g - r) / scale
+        # Same operation order as the oracle: differences only where CUDA's
+        # exp and the host libm differ in the last bit.
+        assert np.mean(g == r) > 0.95
+        assert np.max(rel[np.abs(r) > 1e-280]) < 1e-13
+        assert np.array_equal(g == 0.0, r == 0.0)  # cutoff zeros identical
+
+
+@pytest.mark.parametrize("order,thr", [(0, 1e-12), (1, 1e-12), (2, 1e-12), (2, 1e-3), (2, 0.0)])
+def test_screening_masks_bit_exact(order, thr):
+    path = os.path.join(GOLDEN, "acrolein.fchk.gz")
+    m, o = _pair(path)
+    grid = m.grid_around(2.0, 0.45)
+    gm = m.screening_masks(grid, 128, order, thr)
+    pts = grid.points()
+    for b in range(gm.shape[0]):
+        blk = pts[b * 128:(b + 1) * 128]
+        if order == 0:
+            panels = o.ao_values(blk)[None]
+        else:
+            panels = o.ao_derivatives(blk, order)
+        mx = np.abs(panels).max(axis=(0, 2))
+        ref = np.ones(o.n, bool) if thr == 0.0 else mx > thr
+        assert np.array_equal(gm[b].astype(bool), ref), f"block {b}"
+
+
+FIELDS = [(P.Density, D.Total), (P.Gradient, D.Total), (P.Laplacian, D.Total), (P.Tau, D.Total), (P.Elf, D.Total)]
+
+
+def _compare(outs, refs, tol, props):
+    for p, a, r in zip(props, outs, refs):
+        err = scaled_error(a, r)
+        assert err <= tol, f"{p}: {err}"
+
+
+def test_water28_fields_full_grid(water28):
+    """Config 0 workload: rho, grad rho, lap rho (and tau, ELF) on the 64^3 grid."""
+    m, o = _pair(water28)
+    origin, steps, counts = synth.workload_grid("water_28", o.atom_xyz.reshape(-1, 3))
+    grid = K.Grid(origin, steps, counts)
+    props = [K.density(k, c) for k, c in FIELDS]
+    outs, used = K.Evaluator(m).evaluate_grid(grid, props)
+    refs, rused = o.evaluate([(int(p.kind), int(p.component), 0, 0) for p in props], grid=(origin, steps, counts))
+    assert used == rused == 2
+    _compare(outs, refs, 1e-12, props)
+
+
+ALL_DENSITY = [(P.Density, D.Total), (P.Density, D.Alpha), (P.Density, D.Beta), (P.Density, D.Difference),
+               (P.Gradient, D.Total), (P.Gradient, D.Alpha), (P.Hessian, D.Total), (P.Hessian, D.Beta),
+               (P.Laplacian, D.Total), (P.Laplacian, D.Difference), (P.Tau, D.Total), (P.Tau, D.Beta),
+               (P.Elf, D.Total), (P.Elf, D.Alpha), (P.ReducedGradient, D.Total), (P.SignLambda2Density, D.Total),
+               (P.Lol, D.Total), (P.Lol, D.Beta), (P.InteractionRegionIndicator, D.Total),
+               (P.DensityOverlapRegionsIndicator, D.Total), (P.HamiltonianKineticEnergy, D.Total),
+               (P.PotentialEnergyDensity, D.Total), (P.EnergyDensity, D.Total), (P.SpinPolarization, D.Difference),
+               (P.ShannonEntropyDensity, D.Total), (P.FisherInformationDensity, D.Total), (P.TauComponents, D.Alpha),
+               (P.HamiltonianKineticEnergyComponents, D.Total), (P.PotentialKineticRatio, D.Total),
+               (P.EnergyDensityPerElectron, D.Total), (P.KineticEnergyPerElectron, D.Total),
+               (P.ElfTsirelsonStash, D.Total), (P.LolTsirelsonStash, D.Beta)]
+
+
+@pytest.mark.parametrize("backend", [K.Backend.AO_MO, K.Backend.AO_P])
+@pytest.mark.parametrize("name", ["o2.fchk.gz", "h2o_b3lyp_def2tzvp.fchk.gz"])
+def test_all_density_properties(name, backend):
+    m, o = _pair(os.path.join(GOLDEN, name))
+    grid = m.grid_around(2.0, 0.5)
+    props = [K.density(k, c) for k, c in ALL_DENSITY]
+    tuples = [(int(p.kind), int(p.component), 0, 0) for p in props]
+    outs, used = K.Evaluator(m, backend=backend).evaluate_grid(grid, props)
+    refs, rused = o.evaluate(tuples, grid=(grid.origin, grid.steps, grid.counts), backend=int(backend))
+    assert used == rused == int(backend)
+    for p, a, r in zip(props, outs, refs):
+        if p.kind == P.SignLambda2Density:
+            # The sign of lambda2 is rounding-dependent only where lambda2 ~ 0.
+            close = np.isclose(a, r, rtol=1e-10, atol=1e-12)
+            assert np.mean(close) > 0.999 and np.array_equal(np.abs(a) > 0, np.abs(r) > 0)
+            assert scaled_error(np.abs(a), np.abs(r)) <= 1e-12
+            continue
+        tol = 1e-12
+        if p.kind in (P.Elf, P.Lol, P.ElfTsirelsonStash, P.LolTsirelsonStash, P.ReducedGradient,
+                      P.InteractionRegionIndicator, P.DensityOverlapRegionsIndicator, P.SpinPolarization,
+                      P.PotentialKineticRatio, P.EnergyDensityPerElectron, P.KineticEnergyPerElectron):
+            # Ratios of small densities amplify the 1e-16 rounding of the
+            # contraction order in the low-density tails; compare where the
+            # density is not negligible.
+            rho = refs[0][0]
+            mask = rho > 1e-6
+            a, r = a[:, mask], r[:, mask]
+            tol = 1e-9
+        assert scaled_error(a, r) <= tol, f"{p}: {scaled_error(a, r)}"
+
+
+@pytest.mark.parametrize("block", [1, 7, 32, 37, 128])
+def test_block_sizes(block):
+    m, o = _pair(os.path.join(GOLDEN, "acrolein.fchk.gz"))
+    grid = m.grid_around(1.5, 0.6)
+    props = [K.density(P.Density), K.density(P.Gradient), K.density(P.Laplacian)]
+    tuples = [(int(p.kind), int(p.component), 0, 0) for p in props]
+    outs, _ = K.Evaluator(m, block_size=block).evaluate_grid(grid, props)
+    refs, _ = o.evaluate(tuples, grid=(grid.origin, grid.steps, grid.counts), block_size=block)
+    _compare(outs, refs, 1e-12, props)
+
+
+def test_points_path_and_grid_agree():
+    m, o = _pair(os.path.join(GOLDEN, "o2.fchk.gz"))
+    grid = m.grid_around(1.0, 0.7)
+    pts = grid.points()
+    props = [K.density(P.Density), K.density(P.Gradient), K.density(P.Elf)]
+    a, _ = K.Evaluator(m).evaluate_grid(grid, props)
+    b, _ = K.Evaluator(m).evaluate_points(pts, props)
+    refs, _ = o.evaluate([(int(p.kind), 0, 0, 0) for p in props], points=pts)
+    _compare(b, refs, 1e-12, props)
+    _compare(a, [x for x in b], 1e-12, props)
+
+
+def test_grid_path_densities_ao_p():
+    """AO-P densities on a grid take the values-only path (src/density.cpp:366-444)."""
+    m, o = _pair(os.path.join(GOLDEN, "o2.fchk.gz"))
+    grid = m.grid_around(2.0, 0.4)
+    props = [K.density(P.Density, c) for c in (D.Total, D.Alpha, D.Beta, D.Difference)]
+    outs, used = K.Evaluator(m, backend=K.Backend.AO_P).evaluate_grid(grid, props)
+    refs, _ = o.evaluate([(0, int(c), 0, 0) for c in (0, 1, 2, 3)], grid=(grid.origin, grid.steps, grid.counts),
+                         backend=1)
+    assert used == 1
+    _compare(outs, refs, 1e-12, props)
+
+
+def test_orbitals():
+    m, o = _pair(os.path.join(GOLDEN, "o2.fchk.gz"))
+    grid = m.grid_around(1.5, 0.5)
+    props = [K.orbital(9), K.orbital(7, K.SpinChannel.Beta), K.orbital(3, K.SpinChannel.Alpha, P.OrbitalGradient),
+             K.orbital(3, K.SpinChannel.Beta, P.OrbitalHessian)]
+    outs, _ = K.Evaluator(m).evaluate_grid(grid, props)
+    pts = grid.points()
+    refs = []
+    for p in props:
+        ch = p.channel
+        n = o.n
+        c = (o.c_beta if (ch == 1 and o.c_beta is not None) else o.c_alpha)[(p.orbital_index - 1) * n:p.orbital_index * n]
+        if p.kind == P.Orbital:
+            refs.append((c @ o.ao_values(pts))[None])
+        else:
+            panels = o.ao_derivatives(pts, 2)
+            sel = [1, 2, 3] if p.kind == P.OrbitalGradient else [4, 5, 6, 7, 8, 9]
+            refs.append(np.stack([c @ panels[s] for s in sel]))
+    _compare(outs, refs, 1e-12, props)
+    # At arbitrary points every orbital property takes the orbital pass.
+    outs2, _ = K.Evaluator(m).evaluate_points(pts, props)
+    _compare(outs2, refs, 1e-12, props)
+
+
+def test_golden_gaussian_cubes_on_gpu():
+    for key, comp in [("o2_density", 0), ("o2_spin", 3), ("acrolein_density", 0)]:
+        g = np.load(os.path.join(GOLDEN, f"gaussian_{key}.npz"))
+        m = K.Molecule.from_fchk(os.path.join(GOLDEN, str(g["fchk"])))
+        outs, _ = K.Evaluator(m, backend=K.Backend.AO_P).evaluate_points(golden_points(g), [K.density(P.Density, comp)])
+        v, ref = outs[0][0], g["values"]
+        assert np.max(np.abs(v - ref)) <= 2e-3
+        assert np.abs(v - ref).sum() / np.abs(ref).sum() <= 1e-5
+
+
+def test_golden_multiwfn_on_gpu():
+    for key, kind, comp, rel, abs_ in [("h2o_elf", 6, 0, 2e-5, 0.0), ("h2o_rdg", 7, 0, 2e-5, 0.0),
+                                       ("h2o_sign_lambda2_rho", 8, 0, 2e-5, 0.0), ("o2_elf", 6, 0, 2e-5, 0.0),
+                                       ("o2_lol", 10, 0, 2e-5, 0.0)]:
+        g = np.load(os.path.join(GOLDEN, f"multiwfn_{key}.npz"))
+        m = K.Molecule.from_fchk(os.path.join(GOLDEN, str(g["fchk"])))
+        outs, _ = K.Evaluator(m).evaluate_points(golden_points(g), [K.Property(kind, comp)])
+        ratio = np.abs(outs[0][0] - g["values"]) / (rel * np.abs(g["values"]) + abs_ + 1e-300)
+        assert ratio.max() <= 1.0, key
+
+
+def test_esp_exact_vs_oracle_and_multiwfn():
+    for name in ["h2o_esp", "o2_esp"]:
+        g = np.load(os.path.join(GOLDEN, f"multiwfn_{name}.npz"))
+        path = os.path.join(GOLDEN, str(g["fchk"]))
+        m, o = _pair(path)
+        pts = golden_points(g)[:1500]
+        outs, _ = K.Evaluator(m, potential_tolerance=0.0).evaluate_points(pts, [K.density(P.ElectrostaticPotential)])
+        ref = O.OracleESP(o).evaluate(pts)
+        assert scaled_error(outs[0][0], ref) <= 1e-12
+        assert m.esp_pair_count() == O.OracleESP(o).pair_count
+        d = np.min(np.linalg.norm(pts[:, None, :] - o.atom_xyz.reshape(-1, 3)[None], axis=2), axis=1)
+        keep = d >= 1e-3
+        ratio = np.abs(outs[0][0] - g["values"][:1500])[keep] / (2e-5 * np.abs(g["values"][:1500][keep]) + 1e-7)
+        assert ratio.max() <= 1.0
+
+
+def test_boys_device_matches_oracle():
+    t = np.concatenate([np.linspace(0.0, 45.0, 2001), [1e-9, 39.999999, 40.0, 200.0, 1e4]])
+    got = K.boys(t, 13)
+    ref = np.stack([O.boys(x, 13) for x in t])
+    assert np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300)) <= 1e-14
+
+
+def test_mixed_precision_water(water28):
+    m = K.Molecule.from_fchk(water28)
+    origin, steps, counts = synth.workload_grid("water_28", m.atoms()[2])
+    grid = K.Grid(origin, steps, counts)
+    props = [K.density(k, c) for k, c in FIELDS]
+    f64, _ = K.Evaluator(m).evaluate_grid(grid, props)
+    mix, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_grid(grid, props)
+    for p, a, r in zip(props, mix, f64):
+        assert scaled_error(a, r) <= 1e-6, (p, scaled_error(a, r))
+
+
+def test_device_api_matches_host():
+    import torch
+    m = K.Molecule.from_fchk(os.path.join(GOLDEN, "h2o_b3lyp_def2tzvp.fchk.gz"))
+    grid = m.grid_around(2.0, 0.3)
+    props = [K.density(P.Density), K.density(P.Gradient), K.density(P.Elf)]
+    host, _ = K.Evaluator(m).evaluate_grid(grid, props)
+    outs = [torch.zeros(K.channels(p.kind) * grid.npoints, dtype=torch.float64, device="cuda") for p in props]
+    stream = torch.cuda.current_stream().cuda_stream
+    K.Evaluator(m).evaluate_grid_device(grid, props, [o.data_ptr() for o in outs], stream)
+    torch.cuda.synchronize()
+    for h, d in zip(host, outs):
+        assert np.array_equal(h.ravel(), d.cpu().numpy())
+
+
+def test_repeatable():
+    m = K.Molecule.from_fchk(os.path.join(GOLDEN, "acrolein.fchk.gz"))
+    grid = m.grid_around(2.0, 0.4)
+    props = [K.density(P.Density), K.density(P.Laplacian), K.density(P.Elf)]
+    a, _ = K.Evaluator(m).evaluate_grid(grid, props)
+    b, _ = K.Evaluator(m).evaluate_grid(grid, props)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)

@@ -1,0 +1,115 @@
+"""Pins the CPU oracle against chem-kumo's own golden data (no GPU).
+
+The oracle is the checker of the CUDA path, so it is itself checked first:
+against Gaussian cubegen densities and MO cubes (tolerances of
+tests/cube_reference_test.cpp:146-160 and tests/orbital_reference_test.cpp),
+Multiwfn derived-field and ESP cubes (tests/multiwfn_reference_test.cpp:1-20,
+351-420) and the Boys-function known answers (tests/boys_function_test.cpp:63-131).
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+from scipy import integrate, special
+
+from conftest import GOLDEN, golden_points
+
+import oracle as O
+
+
+def _mol(name):
+    return O.OracleMolecule.from_fchk(os.path.join(GOLDEN, name))
+
+
+@pytest.mark.parametrize("key,component", [("o2_density", 0), ("o2_alpha", 1), ("o2_beta", 2), ("o2_spin", 3),
+                                           ("acrolein_density", 0)])
+def test_gaussian_density_cubes(key, component):
+    g = np.load(os.path.join(GOLDEN, f"gaussian_{key}.npz"))
+    m = _mol(str(g["fchk"]))
+    outs, used = m.evaluate([(0, component, 0, 0)], points=golden_points(g), backend=1)
+    v, ref = outs[0][0], g["values"]
+    assert used == 1
+    assert np.max(np.abs(v - ref)) <= 2e-3
+    assert np.abs(v - ref).sum() / np.abs(ref).sum() <= 1e-5
+
+
+@pytest.mark.parametrize("key,channel,index", [("o2_alpha_mo_9", 0, 9), ("o2_beta_mo_7", 1, 7),
+                                               ("acrolein_mo_15", 0, 15)])
+def test_gaussian_orbital_cubes(key, channel, index):
+    g = np.load(os.path.join(GOLDEN, f"gaussian_{key}.npz"))
+    m = _mol(str(g["fchk"]))
+    outs, _ = m.evaluate([(5, 0, channel, index)], points=golden_points(g))
+    assert np.max(np.abs(outs[0][0] - g["values"])) <= 2e-4
+
+
+# kind, component, relative tolerance, absolute tolerance, nucleus exclusion
+MULTIWFN = [
+    ("h2o_elf", 6, 0, 2e-5, 0.0, 0.0),
+    ("h2o_rdg", 7, 0, 2e-5, 0.0, 0.0),
+    ("h2o_sign_lambda2_rho", 8, 0, 2e-5, 0.0, 0.0),
+    ("o2_elf", 6, 0, 2e-5, 0.0, 0.0),
+    ("h2o_lol", 10, 0, 2e-5, 0.0, 0.0),
+    ("o2_lol", 10, 0, 2e-5, 0.0, 0.0),
+    ("h2o_iri", 11, 0, 5e-5, 0.0, 0.0),
+    ("h2o_dori", 12, 0, 2e-5, 1e-5, 0.0),
+    ("o2_spin_polarization", 16, 3, 2e-5, 1e-6, 0.0),
+    ("h2o_fisher", 18, 0, 1e-4, 0.0, 0.0),
+    ("h2o_elf_ts", 35, 0, 2e-5, 0.0, 0.0),
+    ("h2o_esp", 9, 0, 2e-5, 1e-7, 1e-3),
+    ("o2_esp", 9, 0, 2e-5, 1e-7, 1e-3),
+]
+
+
+@pytest.mark.parametrize("key,kind,component,rel,abs_,excl", MULTIWFN)
+def test_multiwfn_cubes(key, kind, component, rel, abs_, excl):
+    g = np.load(os.path.join(GOLDEN, f"multiwfn_{key}.npz"))
+    m = _mol(str(g["fchk"]))
+    pts = golden_points(g)
+    outs, _ = m.evaluate([(kind, component, 0, 0)], points=pts)
+    v, ref = outs[0][0], g["values"]
+    keep = np.ones(len(pts), bool)
+    if excl:
+        d = np.min(np.linalg.norm(pts[:, None, :] - m.atom_xyz.reshape(-1, 3)[None], axis=2), axis=1)
+        keep = d >= excl
+    ratio = np.abs(v - ref)[keep] / (rel * np.abs(ref[keep]) + abs_ + 1e-300)
+    assert ratio.max() <= 1.0
+
+
+def test_energy_densities_multiwfn():
+    # K, V, H on the scale |tau| + |lap rho| / 4 (tests/multiwfn_reference_test.cpp:140-150).
+    for key, kind in [("h2o_kinetic_k", 13), ("h2o_potential_energy", 14), ("h2o_energy_density", 15)]:
+        g = np.load(os.path.join(GOLDEN, f"multiwfn_{key}.npz"))
+        m = _mol(str(g["fchk"]))
+        outs, _ = m.evaluate([(kind, 0, 0, 0), (4, 0, 0, 0), (3, 0, 0, 0)], points=golden_points(g))
+        scale = np.abs(outs[1][0]) + 0.25 * np.abs(outs[2][0])
+        assert np.max(np.abs(outs[0][0] - g["values"]) / (5e-5 * scale + 1e-300)) <= 1.0
+
+
+def test_boys_known_answers():
+    # F_m(0) = 1/(2m+1); F_0(T) = sqrt(pi/T) erf(sqrt T) / 2; recurrence.
+    f0 = O.boys(0.0, 33)
+    assert np.max(np.abs(f0 - 1.0 / (2 * np.arange(33) + 1))) <= 1e-14
+    for t in [1e-6, 0.013, 0.4, 2.5, 17.3, 39.99, 40.0, 55.0, 300.0]:
+        v = O.boys(t, 13)
+        exact0 = 0.5 * math.sqrt(math.pi / t) * math.erf(math.sqrt(t))
+        assert abs(v[0] - exact0) <= 1e-14 * max(1.0, exact0)
+        for m in range(12):
+            # 2T F_{m+1} = (2m+1) F_m - exp(-T)
+            assert abs(2 * t * v[m + 1] - ((2 * m + 1) * v[m] - math.exp(-t))) <= 1e-13 * max(1.0, v[m])
+    for t in [0.3, 7.7, 33.3]:
+        v = O.boys(t, 9)
+        for m in range(9):
+            # F_m(T) = gamma(m + 1/2) P(m + 1/2, T) / (2 T^(m + 1/2)), and by quadrature.
+            a = m + 0.5
+            ref = special.gamma(a) * special.gammainc(a, t) / (2.0 * t ** a)
+            quad, _ = integrate.quad(lambda x: x ** (2 * m) * math.exp(-t * x * x), 0.0, 1.0, epsabs=0, epsrel=1e-13)
+            assert abs(v[m] - ref) <= 1e-13 * ref
+            assert abs(v[m] - quad) <= 1e-12 * ref
+
+
+def test_boys_invalid_input():
+    with pytest.raises(ValueError):
+        O.boys(-1.0, 3)
+    with pytest.raises(ValueError):
+        O.boys(1.0, 40)
