@@ -166,6 +166,10 @@ def main() -> None:
     ap.add_argument("--ref-blocks", type=int, default=96)
     ap.add_argument("--cpu-blocks", type=int, default=96)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--grid-n", type=int, default=0, help="points per axis (default: the workload's 128)")
+    ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
+                    help="time one form only (small profiling cases)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -194,6 +198,10 @@ def main() -> None:
     m = K.Molecule.from_fchk(fchk)
     _, _, xyz = m.atoms()
     origin, steps, counts = synth.workload_grid(WORKLOAD, xyz)
+    if args.grid_n:
+        spacing = steps[0, 0]
+        origin = xyz.mean(axis=0) - 0.5 * spacing * (args.grid_n - 1)
+        counts = (args.grid_n,) * 3
     grid = K.Grid(origin, steps, counts)
     n = grid.npoints
     props = _props(K)
@@ -231,6 +239,14 @@ def main() -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    if args.only:
+        # Small profiling case: warm-up and timed steps of one form only.
+        for _ in range(args.warmup):
+            step(args.only)
+        t = timed(args.only, args.steps)
+        if rank == 0:
+            print(json.dumps({"only": args.only, "points": n, "ms_per_step": float(np.mean(t))}))
+        return
     for _ in range(args.warmup):
         step("mixed")
         step("fp64")
@@ -272,13 +288,13 @@ def main() -> None:
     e2e_eval = K.Evaluator(m, precision=K.Precision.Mixed)
     e2e_eval.evaluate_grid(grid, props)
     e2e_times = []
-    for _ in range(max(2, args.steps // 2)):
+    for _ in range(0 if args.no_e2e else max(2, args.steps // 2)):
         if world > 1:
             dist.barrier()
         t0 = time.perf_counter()
         e2e_eval.evaluate_grid(grid, props)
         e2e_times.append(time.perf_counter() - t0)
-    e2e_s = max_over_ranks(float(np.median(e2e_times)))
+    e2e_s = max_over_ranks(float(np.median(e2e_times)) if e2e_times else float("nan"))
 
     if rank == 0:
         peaks, peak_kind = _peaks()
