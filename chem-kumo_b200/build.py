@@ -38,6 +38,7 @@ CUDA_UNITS = {
     "csrc/host/evaluator.cu": [],
     "csrc/host/capi.cu": [],
     "csrc/host/profile.cu": [],
+    "csrc/host/noalloc.cu": [],
 }
 CXX_UNITS = [
     "csrc/host/fchk.cpp",

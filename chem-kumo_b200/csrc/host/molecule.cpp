@@ -246,6 +246,13 @@ detail::DeviceMolecule& Molecule::device() const {
     return *device_;
 }
 
+const detail::DeviceMolecule* Molecule::device_if_resident() const {
+    std::lock_guard<std::mutex> lock(*device_mutex_);
+    int dev = 0;
+    detail::check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    return (device_ && device_->device == dev) ? device_.get() : nullptr;
+}
+
 std::size_t Molecule::device_bytes() const {
     std::lock_guard<std::mutex> lock(*device_mutex_);
     return device_ ? device_->bytes : 0;

@@ -123,6 +123,9 @@ public:
     detail::DeviceMolecule& device() const;
     /// Bytes of device memory held by the resident copy (0 before first use).
     std::size_t device_bytes() const;
+    /// The device copy on the current CUDA device if it already exists, else
+    /// null; never allocates (internal).
+    const detail::DeviceMolecule* device_if_resident() const;
 
 private:
     Molecule() = default;

@@ -154,6 +154,7 @@ EXPORTS = [
     "kumo_evaluate_points", "kumo_evaluate_grid_device", "kumo_evaluate_points_device", "kumo_ao_panels",
     "kumo_screening_masks", "kumo_boys", "kumo_esp_pair_count", "kumo_write_cube", "kumo_grid_around",
     "kumo_profile_enable", "kumo_profile_reset", "kumo_profile_read", "kumo_set_device",
+    "kumo_evaluate_points_noalloc",
 ]
 
 
@@ -197,6 +198,8 @@ def lib():
         L.kumo_grid_around.argtypes = [C.c_void_p, C.c_double, C.c_double, C.POINTER(_Grid), *eb]
         L.kumo_profile_enable.argtypes = [C.c_int]
         L.kumo_set_device.argtypes = [C.c_int, *eb]
+        L.kumo_evaluate_points_noalloc.argtypes = [C.c_void_p, C.POINTER(_Options), _D, C.c_longlong,
+                                                   C.POINTER(_Property), C.c_int, C.POINTER(_D), C.c_void_p, *eb]
         L.kumo_profile_read.argtypes = [C.POINTER(_ProfileEntry), C.c_int]
         _lib = L
     return _lib
@@ -426,6 +429,22 @@ class Evaluator:
                                                  npoints, _props(props), len(props), ptrs, C.c_void_p(stream),
                                                  C.byref(used), e, 512), e)
         return used.value
+
+
+def evaluate_points_noalloc(molecule: Molecule, points_ptr: int, npoints: int, props: Sequence[Property],
+                            outputs: Sequence[int], stream: int = 0, block_size: int = 128,
+                            threshold: float = 1e-12) -> None:
+    """kumo_evaluate_points_noalloc: density properties at device points with no
+    device allocation (FP64, AO-MO), for callers that cannot let the library
+    call cudaMalloc.  The molecule must already have its device copy (any
+    earlier evaluation of it on this device creates it); overlapping calls race
+    on the library's fixed scratch array."""
+    ptrs = (_D * max(len(props), 1))(*[C.cast(C.c_void_p(int(o)), _D) for o in outputs])
+    opt = _options(block_size, 0, threshold, 0.0, 0)
+    e = _err()
+    _check(lib().kumo_evaluate_points_noalloc(molecule._h, C.byref(opt), C.cast(C.c_void_p(points_ptr), _D),
+                                              npoints, _props(props), len(props), ptrs, C.c_void_p(stream), e,
+                                              512), e)
 
 
 def boys(t: np.ndarray, nvalues: int) -> np.ndarray:

@@ -145,6 +145,26 @@ int kumo_evaluate_points_device(const kumo_molecule* m, const kumo_options* opt,
                                 const kumo_property* props, int nprops, double* const* outputs,
                                 void* stream, int* backend_used, char* err, size_t errlen);
 
+/* No counterpart in the reference.  Density properties at device points,
+ * FP64 AO-MO path, without allocating any device memory: for hosts that
+ * cannot let a library call cudaMalloc (a serving process that budgets every
+ * byte of HBM itself, an application whose memory manager owns the device,
+ * or code that must not risk cudaMalloc blocking until the device is idle).
+ * The AO scratch is a fixed 64 MiB array that the library reserves in every
+ * GPU that loads it, until exit.  The molecule's device copy must already
+ * exist (any earlier evaluation of it on this device makes it); points and
+ * outputs are device memory supplied by the caller, the work is queued on
+ * `stream`.  The first call on each device looks up the array's address;
+ * make it before any stream capture.  All calls share the array, so calls
+ * whose work overlaps on the GPU race: serialize them.  A molecule whose
+ * scratch for one 128-point block exceeds the array is rejected with
+ * KUMO_INVALID_ARGUMENT.  opt: block_size 1..128, backend AUTO or AO_MO,
+ * precision FP64 (NULL for the defaults). */
+int kumo_evaluate_points_noalloc(const kumo_molecule* m, const kumo_options* opt,
+                                 const double* device_points, long long npoints,
+                                 const kumo_property* props, int nprops, double* const* outputs,
+                                 void* stream, char* err, size_t errlen);
+
 /* BasisEvaluator::evaluate_derivatives_batch / evaluate_batch
  * (include/chem/kumo/basis_evaluator.hpp:101-115; src/basis_evaluator.cpp:512-678)
  * on the device: order 0 (values), 1 or 2; out (host) is nao x (panels*npts)
