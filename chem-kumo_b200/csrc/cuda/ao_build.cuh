@@ -13,15 +13,18 @@
 // kept if max |value| over every panel of the reference's AO order and every
 // point of the block exceeds the threshold (threshold 0 keeps every row).
 //
-// Thread j of the CTA owns point j of the block; the CTA walks the AO blocks
-// in order, stages each block's exponents and weights in shared memory,
-// computes its panels into a shared staging tile, reduces the per-AO maxima
-// over the block, and copies the kept rows out with coalesced stores.
+// Thread j of the CTA owns point j of the block.  The CTA first bounds its
+// points with a box and lists, in AO order, the AO blocks whose cutoff sphere
+// reaches the box (the others give exact zeros everywhere and, with a
+// positive threshold, no kept row); it then walks that list with each
+// block's exponents and weights staged in shared memory (double-buffered),
+// computes the panels into a shared staging tile, reduces the per-AO maxima
+// over the block and copies the kept rows out with coalesced stores.
 #pragma once
 
-#include "kumo_device.cuh"
-
 #include <utility>
+
+#include "kumo_device.cuh"
 
 namespace kumo_dev {
 
@@ -49,15 +52,23 @@ __host__ __device__ constexpr int cart_power(int l, int k, int axis) {
     return 0;
 }
 
+// exp(-a r^2) for a radial factor: FP64 as the reference; in FP32 the
+// argument is reduced in FP64 (-a r^2 log2 e = n + f, |f| <= 1/2) so that the
+// factor keeps FP32 relative accuracy for large a r^2.
 template <typename T>
-struct MathOf;
+struct RadialExp;
 template <>
-struct MathOf<double> {
-    __device__ static double ex(double x) { return exp(x); }
+struct RadialExp<double> {
+    __device__ static double of(double a, double r2) { return exp(-a * r2); }
 };
 template <>
-struct MathOf<float> {
-    __device__ static float ex(float x) { return expf(x); }
+struct RadialExp<float> {
+    __device__ static float of(double a, double r2) {
+        const double t = -a * r2 * 1.4426950408889634;  // log2(e)
+        const double n = rint(t);
+        if (n < -149.0) return 0.0f;
+        return ldexpf(exp2f(static_cast<float>(t - n)), static_cast<int>(n));
+    }
 };
 
 // 1D factors of src/basis_evaluator.cpp:594-603 for power m:
@@ -83,11 +94,17 @@ __device__ __forceinline__ void static_for(Fn&& fn) {
     static_for_impl(std::make_integer_sequence<int, N>{}, fn);
 }
 
-// Stage layout: stage[(m * P + c) * 128 + j].
-template <typename T, int L, bool PURE, int ORDER, int P>
+template <int MAXL>
+struct MaxOut {
+    static constexpr int v = (MAXL + 1) * (MAXL + 2) / 2;
+};
+
+// Panels of one shell for the thread's point into stage[(m * P + c) * 128 + j],
+// with maxabs[m] the largest |value| over the panels of the AO order.
+template <typename T, int L, bool PURE, int ORDER, int P, int NMAX>
 __device__ __forceinline__ void shell_panels(const T (&pure)[3][135], const T* s_w, const T* s_exps,
                                              const T* s_rad, int nprim, T rx, T ry, T rz, bool inside,
-                                             T* stage, T (&maxabs)[15]) {
+                                             T* stage, T (&maxabs)[NMAX]) {
     constexpr int NC = Cart<L>::NC;
     constexpr int NOUT = PURE ? 2 * L + 1 : NC;
     constexpr int TL = L >= 2 ? L - 2 : 0;
@@ -100,8 +117,6 @@ __device__ __forceinline__ void shell_panels(const T (&pure)[3][135], const T* s
         yp[n] = yp[n - 1] * ry;
         zp[n] = zp[n - 1] * rz;
     }
-#pragma unroll
-    for (int m = 0; m < NOUT; ++m) maxabs[m] = (T)0;
 
     if constexpr (ORDER == 0) {
         // evaluate_into_impl: cart[k] = ((x^px y^py) z^pz) * sum_p W_kp e^(-a_p r^2)
@@ -189,61 +204,76 @@ __device__ __forceinline__ void shell_panels(const T (&pure)[3][135], const T* s
             }
         }
         if constexpr (ORDER == 2) {
-            // Group 1: second-derivative panels xx, xy, xz, yy, yz, zz.
-            T acc[NOUT][6];
+            // Second-derivative panels in two halves (xx, xy, xz), (yy, yz, zz)
+            // to bound the live accumulators; each panel's sum over primitives
+            // is independent, so the halves give the same values as one pass.
+            static_for<2>([&](auto hc) {
+                constexpr int H = decltype(hc)::value;
+                T acc[NOUT][3];
 #pragma unroll
-            for (int m = 0; m < NOUT; ++m)
+                for (int m = 0; m < NOUT; ++m)
 #pragma unroll
-                for (int c = 0; c < 6; ++c) acc[m][c] = (T)0;
-            static_for<NC>([&](auto kc) {
-                constexpr int k = decltype(kc)::value;
-                constexpr int px = cart_power(L, k, 0), py = cart_power(L, k, 1), pz = cart_power(L, k, 2);
-                T s[6] = {0, 0, 0, 0, 0, 0};
-                for (int p = 0; p < nprim; ++p) {
-                    const T a = s_exps[p];
-                    const T weight = s_w[k * nprim + p] * s_rad[p * kBlockPoints + j];
-                    const T fx0 = xp[px], fy0 = yp[py], fz0 = zp[pz];
-                    const T fx1 = factor1<T, px>(xp, a, rx);
-                    const T fy1 = factor1<T, py>(yp, a, ry);
-                    const T fz1 = factor1<T, pz>(zp, a, rz);
-                    const T fx2 = factor2<T, px>(xp, a, rx);
-                    const T fy2 = factor2<T, py>(yp, a, ry);
-                    const T fz2 = factor2<T, pz>(zp, a, rz);
-                    s[0] = s[0] + weight * fx2 * fy0 * fz0;
-                    s[1] = s[1] + weight * fx1 * fy1 * fz0;
-                    s[2] = s[2] + weight * fx1 * fy0 * fz1;
-                    s[3] = s[3] + weight * fx0 * fy2 * fz0;
-                    s[4] = s[4] + weight * fx0 * fy1 * fz1;
-                    s[5] = s[5] + weight * fx0 * fy0 * fz2;
-                }
-                if constexpr (PURE) {
-#pragma unroll
-                    for (int m = 0; m < NOUT; ++m) {
-                        const T t = pure[TL][m * NC + k];
-                        if (t != (T)0) {
-#pragma unroll
-                            for (int c = 0; c < 6; ++c) acc[m][c] = acc[m][c] + t * s[c];
+                    for (int c = 0; c < 3; ++c) acc[m][c] = (T)0;
+                static_for<NC>([&](auto kc) {
+                    constexpr int k = decltype(kc)::value;
+                    constexpr int px = cart_power(L, k, 0), py = cart_power(L, k, 1), pz = cart_power(L, k, 2);
+                    T s[3] = {0, 0, 0};
+                    for (int p = 0; p < nprim; ++p) {
+                        const T a = s_exps[p];
+                        const T weight = s_w[k * nprim + p] * s_rad[p * kBlockPoints + j];
+                        const T fx0 = xp[px], fy0 = yp[py], fz0 = zp[pz];
+                        const T fy1 = factor1<T, py>(yp, a, ry);
+                        const T fz1 = factor1<T, pz>(zp, a, rz);
+                        if constexpr (H == 0) {
+                            const T fx1 = factor1<T, px>(xp, a, rx);
+                            const T fx2 = factor2<T, px>(xp, a, rx);
+                            s[0] = s[0] + weight * fx2 * fy0 * fz0;
+                            s[1] = s[1] + weight * fx1 * fy1 * fz0;
+                            s[2] = s[2] + weight * fx1 * fy0 * fz1;
+                        } else {
+                            const T fy2 = factor2<T, py>(yp, a, ry);
+                            const T fz2 = factor2<T, pz>(zp, a, rz);
+                            s[0] = s[0] + weight * fx0 * fy2 * fz0;
+                            s[1] = s[1] + weight * fx0 * fy1 * fz1;
+                            s[2] = s[2] + weight * fx0 * fy0 * fz2;
                         }
                     }
-                } else {
+                    if constexpr (PURE) {
 #pragma unroll
-                    for (int c = 0; c < 6; ++c) acc[k][c] = s[c];
+                        for (int m = 0; m < NOUT; ++m) {
+                            const T t = pure[TL][m * NC + k];
+                            if (t != (T)0) {
+#pragma unroll
+                                for (int c = 0; c < 3; ++c) acc[m][c] = acc[m][c] + t * s[c];
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) acc[k][c] = s[c];
+                    }
+                });
+#pragma unroll
+                for (int m = 0; m < NOUT; ++m) {
+                    T mx = maxabs[m];
+                    T h[3];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        h[c] = inside ? acc[m][c] : (T)0;
+                        const T av = h[c] < 0 ? -h[c] : h[c];
+                        mx = av > mx ? av : mx;
+                        if constexpr (P == kPanelsFull) stage[(m * P + 4 + 3 * H + c) * kBlockPoints + j] = h[c];
+                    }
+                    if constexpr (P == kPanelsLaplacian) {
+                        // Laplacian panel (xx + yy) + zz.
+                        T* lap = &stage[(m * P + 4) * kBlockPoints + j];
+                        if constexpr (H == 0)
+                            *lap = h[0];
+                        else
+                            *lap = (*lap + h[0]) + h[2];
+                    }
+                    maxabs[m] = mx;
                 }
             });
-#pragma unroll
-            for (int m = 0; m < NOUT; ++m) {
-                T mx = maxabs[m];
-                T h[6];
-#pragma unroll
-                for (int c = 0; c < 6; ++c) {
-                    h[c] = inside ? acc[m][c] : (T)0;
-                    const T av = h[c] < 0 ? -h[c] : h[c];
-                    mx = av > mx ? av : mx;
-                    if constexpr (P == kPanelsFull) stage[(m * P + 4 + c) * kBlockPoints + j] = h[c];
-                }
-                if constexpr (P == kPanelsLaplacian) stage[(m * P + 4) * kBlockPoints + j] = (h[0] + h[3]) + h[5];
-                maxabs[m] = mx;
-            }
         }
     }
 }
@@ -258,22 +288,37 @@ __device__ __forceinline__ T warp_max(T v) {
     return v;
 }
 
+__device__ __forceinline__ double warp_min_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_max_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
 // One CTA per screening block.  Dynamic shared memory: the staging tile
-// (max_count * P * 128 values of T) followed by the radial factors
-// (kMaxPrim * 128 values).
-template <typename T, int ORDER, int P>
-__global__ void __launch_bounds__(kBlockPoints) ao_build_kernel(const __grid_constant__ AoBuildParams<T> prm) {
+// (max_count * P * 128 values of T), the radial factors (kMaxPrim * 128
+// values of T) and the list of AO blocks within reach (nblocks ints).
+template <typename T, int ORDER, int P, int MAXL>
+__global__ void __launch_bounds__(kBlockPoints, sizeof(T) == 8 ? 3 : 5) ao_build_kernel(const __grid_constant__ AoBuildParams<T> prm) {
+    constexpr int NW = kBlockPoints / 32;
+    constexpr int NMAX = MaxOut<MAXL>::v;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* stage = reinterpret_cast<T*>(smem_raw);
     T* s_rad = stage + (size_t)prm.basis.max_count * P * kBlockPoints;
-    __shared__ T s_exps[kMaxPrim];
-    __shared__ T s_w[15 * kMaxPrim];
-    __shared__ T s_red[kBlockPoints / 32][16];
-    __shared__ int s_keep[16];
+    int* s_list = reinterpret_cast<int*>(s_rad + (size_t)kMaxPrim * kBlockPoints);
+    __shared__ T s_exps[2][kMaxPrim];
+    __shared__ T s_w[2][15 * kMaxPrim];
+    __shared__ T s_red[2][NW][16];
+    __shared__ double s_box[NW][6];
+    __shared__ int s_count[NW];
 
     const int blk = blockIdx.x;
     if (blk >= prm.nblocks) return;
-    const int j = threadIdx.x;
+    const int j = threadIdx.x, warp = j >> 5, lane = j & 31;
     const long long start = prm.first_point + (long long)blk * prm.block_size;
     long long b = prm.src.count - start;
     if (b > prm.block_size) b = prm.block_size;
@@ -287,9 +332,73 @@ __global__ void __launch_bounds__(kBlockPoints) ao_build_kernel(const __grid_con
     int* kept = out.kept + (size_t)blk * out.row_stride;
     const bool keep_all = prm.threshold == 0.0;
     const T thr = (T)prm.threshold;
-    int nk = 0;
 
-    for (int s = 0; s < B.nblocks; ++s) {
+    // Bounding box of the block's points.
+    {
+        const double big = 1.0e300;
+        double lo[3] = {valid ? px : big, valid ? py : big, valid ? pz : big};
+        double hi[3] = {valid ? px : -big, valid ? py : -big, valid ? pz : -big};
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = warp_min_d(lo[a]);
+            hi[a] = warp_max_d(hi[a]);
+        }
+        if (lane == 0)
+            for (int a = 0; a < 3; ++a) {
+                s_box[warp][a] = lo[a];
+                s_box[warp][3 + a] = hi[a];
+            }
+    }
+    __syncthreads();
+    double lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = s_box[0][a];
+        hi[a] = s_box[0][3 + a];
+        for (int w = 1; w < NW; ++w) {
+            lo[a] = fmin(lo[a], s_box[w][a]);
+            hi[a] = fmax(hi[a], s_box[w][3 + a]);
+        }
+    }
+    // AO blocks within reach of the box, in AO order.  A block is left out
+    // only if the box is farther than its cutoff radius by a relative margin
+    // that covers the rounding of both distances, so every point it leaves
+    // out is also outside the cutoff in the reference's arithmetic.
+    int nlist = 0;
+    for (int c0 = 0; c0 < B.nblocks; c0 += kBlockPoints) {
+        const int s = c0 + j;
+        bool reach = false;
+        if (s < B.nblocks) {
+            if (keep_all) {
+                reach = true;
+            } else {
+                const double4 o = B.origin_r2[s];
+                const double ox[3] = {o.x, o.y, o.z};
+                double d2 = 0.0;
+                for (int a = 0; a < 3; ++a) {
+                    const double d = fmax(0.0, fmax(lo[a] - ox[a], ox[a] - hi[a]));
+                    d2 += d * d;
+                }
+                reach = !(d2 > o.w * (1.0 + 1e-10) + 1e-300);
+            }
+        }
+        const unsigned ballot = __ballot_sync(0xffffffffu, reach);
+        if (lane == 0) s_count[warp] = __popc(ballot);
+        __syncthreads();
+        int before = nlist;
+        for (int w = 0; w < warp; ++w) before += s_count[w];
+        if (reach) s_list[before + __popc(ballot & ((1u << lane) - 1u))] = s;
+        int total = 0;
+        for (int w = 0; w < NW; ++w) total += s_count[w];
+        __syncthreads();
+        nlist += total;
+    }
+
+    const T* gexp = sizeof(T) == 8 ? (const T*)B.exps : (const T*)B.exps_f;
+    const T* gw = sizeof(T) == 8 ? (const T*)B.weights : (const T*)B.weights_f;
+    const double* gexp64 = B.exps;
+    int nk = 0;
+    for (int it = 0; it < nlist; ++it) {
+        const int buf = it & 1;
+        const int s = s_list[it];
         const double4 o = B.origin_r2[s];
         const int4 inf = B.info[s];
         const int l = inf.x & 0xff;
@@ -302,25 +411,22 @@ __global__ void __launch_bounds__(kBlockPoints) ao_build_kernel(const __grid_con
         const double dx = px - o.x, dy = py - o.y, dz = pz - o.z;
         const double r2d = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
         const bool inside = valid && (r2d <= o.w);
-        const int any_inside = __syncthreads_or(inside);
-        if (!any_inside && !keep_all) continue;
-        // Stage this block's exponents and weights.
-        const T* gexp = sizeof(T) == 8 ? (const T*)B.exps : (const T*)B.exps_f;
-        const T* gw = sizeof(T) == 8 ? (const T*)B.weights : (const T*)B.weights_f;
-        if (j < nprim) s_exps[j] = gexp[inf.y + j];
-        for (int q = j; q < ncart * nprim; q += kBlockPoints) s_w[q] = gw[inf.z + q];
+        // Stage this block's exponents and weights (double-buffered, so one
+        // barrier per block suffices).
+        if (j < nprim) s_exps[buf][j] = gexp[inf.y + j];
+        for (int q = j; q < ncart * nprim; q += kBlockPoints) s_w[buf][q] = gw[inf.z + q];
         __syncthreads();
-        const T r2 = sizeof(T) == 8 ? (T)r2d : (T)((T)dx * (T)dx + (T)dy * (T)dy + (T)dz * (T)dz);
         if (inside)
-            for (int p = 0; p < nprim; ++p) s_rad[p * kBlockPoints + j] = MathOf<T>::ex(-s_exps[p] * r2);
-        T maxabs[15];
+            for (int p = 0; p < nprim; ++p) s_rad[p * kBlockPoints + j] = RadialExp<T>::of(gexp64[inf.y + p], r2d);
+        T maxabs[NMAX];
         const T rx = (T)dx, ry = (T)dy, rz = (T)dz;
         // Each thread only reads its own radial factors, so no barrier is needed here.
         switch (l | (pure ? 16 : 0)) {
-#define KUMO_SHELL(LL, PP)                                                                        \
-    case (LL) | ((PP) ? 16 : 0):                                                                 \
-        shell_panels<T, LL, PP, ORDER, P>(prm.pure, s_w, s_exps, s_rad, nprim, rx, ry, rz, inside, stage, \
-                                          maxabs);                                                        \
+#define KUMO_SHELL(LL, PP)                                                                                \
+    case (LL) | ((PP) ? 16 : 0):                                                                          \
+        if constexpr (LL <= MAXL)                                                                         \
+            shell_panels<T, (LL <= MAXL ? LL : 0), PP, ORDER, P, NMAX>(prm.pure, s_w[buf], s_exps[buf], s_rad, \
+                                                                      nprim, rx, ry, rz, inside, stage, maxabs); \
         break;
             KUMO_SHELL(0, false) KUMO_SHELL(1, false) KUMO_SHELL(2, false) KUMO_SHELL(3, false)
             KUMO_SHELL(4, false) KUMO_SHELL(2, true) KUMO_SHELL(3, true) KUMO_SHELL(4, true)
@@ -328,31 +434,25 @@ __global__ void __launch_bounds__(kBlockPoints) ao_build_kernel(const __grid_con
             default: break;
         }
         // Block-wide maximum per AO of the shell.
-        const int warp = j >> 5, lane = j & 31;
 #pragma unroll
-        for (int m = 0; m < 15; ++m) {
+        for (int m = 0; m < NMAX; ++m) {
             if (m < count) {
                 const T w = warp_max(maxabs[m]);
-                if (lane == 0) s_red[warp][m] = w;
+                if (lane == 0) s_red[buf][warp][m] = w;
             }
         }
         __syncthreads();
-        if (j < count) {
-            T mx = s_red[0][j];
-#pragma unroll
-            for (int w = 1; w < kBlockPoints / 32; ++w) mx = s_red[w][j] > mx ? s_red[w][j] : mx;
-            s_keep[j] = keep_all || mx > thr;
-        }
-        __syncthreads();
         for (int m = 0; m < count; ++m) {
-            if (!s_keep[m]) continue;
+            T mx = s_red[buf][0][m];
+#pragma unroll
+            for (int w = 1; w < NW; ++w) mx = s_red[buf][w][m] > mx ? s_red[buf][w][m] : mx;
+            if (!(keep_all || mx > thr)) continue;
 #pragma unroll
             for (int c = 0; c < P; ++c)
                 panels[((size_t)c * out.row_stride + nk) * kBlockPoints + j] = stage[(m * P + c) * kBlockPoints + j];
-            if (j == 0) kept[nk] = (inf.w) + m;
+            if (j == 0) kept[nk] = inf.w + m;
             ++nk;
         }
-        __syncthreads();
     }
     if (j == 0) out.nkept[blk] = nk;
 }

@@ -12,6 +12,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -90,6 +91,25 @@ private:
     cudaStream_t stream_ = nullptr;
 };
 
+// The wave scratch comes from the device's default stream-ordered pool.  With
+// the pool's default release threshold (0) every synchronization hands the
+// memory back to the driver and the next evaluation maps it again, which
+// blocks the host for tens to hundreds of milliseconds per call; keep it
+// cached instead (once per device).
+void keep_pool_memory() {
+    static std::once_flag flags[64];
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= 64) return;
+    std::call_once(flags[dev], [dev] {
+        cudaMemPool_t pool;
+        check_cuda(cudaDeviceGetDefaultMemPool(&pool, dev), "cudaDeviceGetDefaultMemPool");
+        unsigned long long keep = ~0ull;
+        check_cuda(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep),
+                   "cudaMemPoolSetAttribute");
+    });
+}
+
 std::size_t scratch_budget() {
     if (const char* e = std::getenv("KUMO_SCRATCH_MB")) {
         const long long mb = std::atoll(e);
@@ -149,6 +169,7 @@ public:
     void execute(const std::vector<std::pair<Property, double*>>& outs) {
         outs_ = outs;
         if (n_ == 0) return;
+        keep_pool_memory();
         dev_ = &mol_.device();
         src_ = kumo_dev::PointSource{};
         src_.count = static_cast<long long>(n_);
