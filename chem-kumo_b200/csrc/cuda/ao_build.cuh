@@ -450,7 +450,10 @@ __global__ void __launch_bounds__(kBlockPoints, sizeof(T) == 8 ? 3 : 5) ao_build
 #pragma unroll
             for (int c = 0; c < P; ++c)
                 panels[((size_t)c * out.row_stride + nk) * kBlockPoints + j] = stage[(m * P + c) * kBlockPoints + j];
-            if (j == 0) kept[nk] = inf.w + m;
+            if (j == 0) {
+                kept[nk] = inf.w + m;
+                if (out.rowmax) out.rowmax[(size_t)blk * out.row_stride + nk] = static_cast<float>(mx);
+            }
             ++nk;
         }
     }

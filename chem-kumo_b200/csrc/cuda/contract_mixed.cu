@@ -1,16 +1,174 @@
-// Mixed-precision AO-MO contraction (CUDA-core form): one CTA per 32 points
-// of a block, 8 warps; FP32 products accumulated in FP32 within each K tile of
-// 16 AOs and folded into FP64 accumulators after every tile, so the FP32
-// rounding error grows with the tile length, not with the number of AOs.
+// Mixed-precision AO-MO contraction on the tcgen05 tensor cores.
+//
+// One CTA (8 warps) per 128-point screening block computes, for every AO
+// panel c and occupied MO i, X_c[point][i] = sum_k phi_c[k][point] C[k][i]
+// over the block's kept AO rows k, as an M=128 (points) x N (MOs) x K (AOs)
+// product per panel with the accumulators in tensor memory (column c*N + i,
+// lane = point).  Each FP32 AO value a and each coefficient b is written as
+// three BF16 pieces (a = a0 + a1 + a2 exactly, each piece the BF16 rounding
+// of what the previous ones leave); the six products a_i b_j with i + j <= 2
+// give the product to about 2^-24 relative, the same as one FP32 product.
+//
+// Pipeline per K step of 16 AO rows: all threads load the FP32 panel rows,
+// split them into the three pieces and store them in shared memory in the
+// MN-major no-swizzle core-matrix layout (8 points x 8 AO rows of 16 bytes);
+// the coefficient pieces (split once at upload) are gathered by cp.async;
+// one thread issues the 6 x npanel MMAs and commits them to the stage's
+// mbarrier.  Stages are reused once that mbarrier reports the MMAs done, so
+// the loads and splits of step t+1 overlap the MMAs of step t.  After the
+// last step the 8 warps read the accumulators (tcgen05.ld, 32 lanes per warp,
+// warps w and w+4 sharing lanes and splitting the MOs), fold them into the
+// per-point FP64 sums of src/density.cpp:275-325 and the fields are stored.
+//
+// Every wait on an mbarrier is bounded; a wait that runs out sets *status,
+// stores NaN for the block's points, and the CTA waits (bounded again) for
+// its MMAs before it frees tensor memory and returns.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <stdexcept>
+#include <string>
+
 #include "mixed.cuh"
 
 namespace kumo_dev {
 namespace {
 
-__device__ __forceinline__ void cp_async16f(void* smem, const void* gmem, bool valid) {
-    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    const int n = valid ? 16 : 0;
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+constexpr int kThreads = 256;
+constexpr unsigned kATile = 4096;            // 128 points x 16 rows x 2 B
+constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s per wait
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits until the phase with the given parity has completed; false if that
+// did not happen within kWaitNs.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_ns() - t0 > kWaitNs) return false;
+    return true;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(unsigned* slot, unsigned ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(unsigned taddr, unsigned ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(unsigned long long* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// D[tmem] (+)= A[smem] * B[smem], BF16 inputs, FP32 accumulators.
+__device__ __forceinline__ void tc_mma(unsigned d_tmem, unsigned long long adesc, unsigned long long bdesc,
+                                       unsigned idesc, unsigned accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u)
+        : "memory");
+}
+
+// Shared-memory matrix descriptor, no swizzle: start address, leading byte
+// offset (between core matrices along K), stride byte offset (between core
+// matrices along M or N), descriptor version 1.
+__device__ __forceinline__ unsigned long long smem_desc(unsigned saddr, unsigned lbo, unsigned sbo) {
+    return static_cast<unsigned long long>((saddr >> 4) & 0x3FFFu) |
+           (static_cast<unsigned long long>((lbo >> 4) & 0x3FFFu) << 16) |
+           (static_cast<unsigned long long>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// MN-major, M = 128, N = n.
+__device__ __forceinline__ unsigned instr_desc(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | (static_cast<unsigned>(n >> 3) << 17) |
+           (static_cast<unsigned>(128 >> 4) << 24);
+}
+
+// MG (8 or 4) consecutive FP32 columns of the warp's 32 lanes.
+template <int MG>
+__device__ __forceinline__ void tmem_ld(unsigned taddr, unsigned (&r)[MG]) {
+    if constexpr (MG == 8) {
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                     : "r"(taddr));
+    } else {
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                     : "r"(taddr));
+    }
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// Orders later uses of r after the preceding wait::ld.
+template <int MG>
+__device__ __forceinline__ void reg_fence(unsigned (&r)[MG]) {
+    if constexpr (MG == 8)
+        asm volatile("" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]));
+    else
+        asm volatile("" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]));
+}
+
+__device__ __forceinline__ void cp_async16(unsigned saddr, const void* gmem, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(saddr), "l"(gmem), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+
+__device__ __forceinline__ unsigned bf2_bits(__nv_bfloat162 h) { return *reinterpret_cast<unsigned*>(&h); }
+
+// Three BF16 pieces of 8 FP32 values (x = p0 + p1 + p2 exactly).
+__device__ __forceinline__ void split8(const float4& lo, const float4& hi, uint4& p0, uint4& p1, uint4& p2) {
+    const float x[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+    unsigned a[4], b[4], c[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float u = x[2 * i], v = x[2 * i + 1];
+        const __nv_bfloat162 h0 = __floats2bfloat162_rn(u, v);
+        const float2 f0 = __bfloat1622float2(h0);
+        const float ru = __fsub_rn(u, f0.x), rv = __fsub_rn(v, f0.y);
+        const __nv_bfloat162 h1 = __floats2bfloat162_rn(ru, rv);
+        const float2 f1 = __bfloat1622float2(h1);
+        const __nv_bfloat162 h2 = __floats2bfloat162_rn(__fsub_rn(ru, f1.x), __fsub_rn(rv, f1.y));
+        a[i] = bf2_bits(h0);
+        b[i] = bf2_bits(h1);
+        c[i] = bf2_bits(h2);
+    }
+    p0 = make_uint4(a[0], a[1], a[2], a[3]);
+    p1 = make_uint4(b[0], b[1], b[2], b[3]);
+    p2 = make_uint4(c[0], c[1], c[2], c[3]);
 }
 
 template <int P>
@@ -18,25 +176,32 @@ struct NQm {
     static constexpr int v = P == 1 ? 1 : P == 4 ? 7 : P == 5 ? 8 : 19;
 };
 
-template <int P, int MPT>
-__device__ __forceinline__ void fold(const double (&acc)[P][MPT], double (&q)[NQm<P>::v]) {
+// Per-point sums over MOs of products of panel values (the order of
+// src/density.cpp:292-318): q0 = sum X0^2, q[1+a] = sum X0 Xa, q[4+a] = sum
+// Xa^2, then X0 Xlap (P = 5) or X0 H_h and the gradient products (P = 10).
+template <int P, int MG>
+__device__ __forceinline__ void fold(const double (&xs)[P][MG], double (&q)[NQm<P>::v], int nvalid) {
 #pragma unroll
-    for (int t = 0; t < MPT; ++t) {
-        q[0] += acc[0][t] * acc[0][t];
+    for (int t = 0; t < MG; ++t) {
+        if (t >= nvalid) break;
+        double x[P];
+#pragma unroll
+        for (int c = 0; c < P; ++c) x[c] = xs[c][t];
+        q[0] += x[0] * x[0];
         if constexpr (P >= 4) {
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-                q[1 + a] += acc[0][t] * acc[1 + a][t];
-                q[4 + a] += acc[1 + a][t] * acc[1 + a][t];
+                q[1 + a] += x[0] * x[1 + a];
+                q[4 + a] += x[1 + a] * x[1 + a];
             }
         }
-        if constexpr (P == 5) q[7] += acc[0][t] * acc[4][t];
+        if constexpr (P == 5) q[7] += x[0] * x[4];
         if constexpr (P == 10) {
             constexpr int pa[6] = {0, 0, 0, 1, 1, 2}, pc[6] = {0, 1, 2, 1, 2, 2};
 #pragma unroll
             for (int h = 0; h < 6; ++h) {
-                q[7 + h] += acc[0][t] * acc[4 + h][t];
-                q[13 + h] += acc[1 + pa[h]][t] * acc[1 + pc[h]][t];
+                q[7 + h] += x[0] * x[4 + h];
+                q[13 + h] += x[1 + pa[h]] * x[1 + pc[h]];
             }
         }
     }
@@ -61,149 +226,332 @@ __device__ __forceinline__ void record(const double* f, int ao_order, DevDD& d) 
     }
 }
 
-template <int P, int MPT, int KT>
-__global__ void __launch_bounds__(256, 1) contract_mixed_kernel(const __grid_constant__ ContractMixedParams prm) {
-    constexpr int MOC = 8 * MPT;
-    constexpr int Q = NQm<P>::v;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    float* phs = reinterpret_cast<float*>(smraw);            // [2][KT][P][32]
-    float* cs = phs + 2 * KT * P * 32;                        // [2][KT][MOC]
-    double* red = reinterpret_cast<double*>(cs + 2 * KT * MOC);  // [8][Q][32]
-    double* fin = red + 8 * Q * 32;                           // [2][Q][32]
+// Rows of a block put in ascending order of their block maximum (at most
+// this many rows; larger blocks keep AO order).
+constexpr int kSortCap = 8192;
+constexpr int kBuckets = 128;
 
-    const int blk = blockIdx.x >> 2;
-    const int j0 = (blockIdx.x & 3) * 32;
-    const long long start = prm.first_point + (long long)blk * prm.block_size;
-    long long b = prm.count - start;
-    if (b > prm.block_size) b = prm.block_size;
-    if (j0 >= b) return;
+template <int P, int S>
+struct Smem {
+    static constexpr int Q = NQm<P>::v;
+    static constexpr unsigned a_bytes = 3u * P * kATile;  // one stage of A pieces
+    __host__ __device__ static unsigned b_bytes(int ncols) { return 3u * 32u * static_cast<unsigned>(ncols); }
+    static size_t total(int ncols) {
+        return S * (static_cast<size_t>(a_bytes) + b_bytes(ncols)) + sizeof(double) * Q * 128 +
+               (sizeof(int) + 1) * kSortCap + sizeof(int) * kBuckets + 8 * S + 16;
+    }
+};
+
+template <int P, int S>
+__global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __grid_constant__ ContractMixedParams prm) {
+    using L = Smem<P, S>;
+    constexpr int Q = L::Q;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int N = prm.ncols;
+    const unsigned b_bytes = L::b_bytes(N);
+    unsigned char* a_st = sm;
+    unsigned char* b_st = sm + S * L::a_bytes;
+    double* red = reinterpret_cast<double*>(b_st + S * b_bytes);
+    int* perm = reinterpret_cast<int*>(red + Q * 128);
+    int* bucket_start = perm + kSortCap;
+    unsigned char* keys = reinterpret_cast<unsigned char*>(bucket_start + kBuckets);
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(keys + kSortCap);
+    unsigned* tslot = reinterpret_cast<unsigned*>(bar + S);
+
+    const int blk = blockIdx.x;
+    const long long start = prm.first_point + static_cast<long long>(blk) * prm.block_size;
+    long long bcount = prm.count - start;
+    if (bcount > prm.block_size) bcount = prm.block_size;
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     const AoScratch<float>& scr = prm.scr;
     const int nk = scr.nkept[blk];
-    const float* pbase = scr.panels + (size_t)blk * P * scr.row_stride * kBlockPoints + j0;
-    const int* kept = scr.kept + (size_t)blk * scr.row_stride;
+    const int ntiles = (nk + 15) / 16;
+    const float* pbase = scr.panels + static_cast<size_t>(blk) * P * scr.row_stride * kBlockPoints;
+    const int* kept = scr.kept + static_cast<size_t>(blk) * scr.row_stride;
 
-    for (int ci = 0; ci < prm.nchannels; ++ci) {
-        const MoChannelF ch = prm.ch[ci];
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (w == 0) tmem_alloc(tslot, static_cast<unsigned>(prm.tmem_cols));
+    // K order: rows in ascending order of their block maximum (a stable
+    // counting sort on the FP32 exponent), so that the accumulators are small
+    // while most rows are added and the largest terms come last.  The
+    // tensor-core accumulation truncates, and its error grows with the
+    // magnitude of the accumulator at each step.
+    const bool sorted = scr.rowmax != nullptr && nk <= kSortCap;
+    if (sorted) {
+        const float* rmax = scr.rowmax + static_cast<size_t>(blk) * scr.row_stride;
+        for (int k = tid; k < nk; k += kThreads) {
+            const int e = static_cast<int>((__float_as_uint(rmax[k]) >> 23) & 0xffu) - 127 + kBuckets / 2;
+            keys[k] = static_cast<unsigned char>(e < 0 ? 0 : (e >= kBuckets ? kBuckets - 1 : e));
+        }
+        __syncthreads();
+        int cnt = 0;
+        if (tid < kBuckets) {
+            for (int k = 0; k < nk; ++k) cnt += keys[k] == tid;
+            bucket_start[tid] = cnt;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            int run = 0;
+            for (int b = 0; b < kBuckets; ++b) {
+                const int c = bucket_start[b];
+                bucket_start[b] = run;
+                run += c;
+            }
+        }
+        __syncthreads();
+        if (tid < kBuckets && cnt > 0) {
+            int pos = bucket_start[tid];
+            for (int k = 0; k < nk; ++k)
+                if (keys[k] == tid) perm[pos++] = k;
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = *tslot;
+    const int G = prm.groups;
+    const unsigned gcols = static_cast<unsigned>(P * N);  // columns of one accumulator group
+
+    // This thread's A unit: AO row kh*8 + k8 of each K step, points 8g..8g+7.
+    const int k8 = tid & 7, g = (tid >> 3) & 15, kh = tid >> 7;
+    const unsigned a_off = static_cast<unsigned>(g * 128 + kh * 2048 + k8 * 16);
+    const unsigned idesc = instr_desc(N);
+    const int quarter = w & 3, half = w >> 2;
+    const int point = quarter * 32 + lane;
+
+    bool failed = false;
+    long long gtile = 0;  // K steps issued so far (all passes)
+    DevDD chan_dd[2];
+    dd_zero(chan_dd[0]);
+    dd_zero(chan_dd[1]);
+
+    for (int ci = 0; ci < prm.nchannels && !failed; ++ci) {
+        const MoChannelTC ch = prm.ch[ci];
         double q[Q];
 #pragma unroll
         for (int i = 0; i < Q; ++i) q[i] = 0.0;
-        for (int mo0 = 0; mo0 < ch.nocc; mo0 += MOC) {
-            double acc[P][MPT];
+        for (int n0 = 0; n0 < ch.nocc && !failed; n0 += N) {
+            float4 ra[P][2];
+            auto load_a = [&](int t) {
+                const int k = t * 16 + kh * 8 + k8;
+                const bool ok = k < nk;
+                const int row = ok ? (sorted ? perm[k] : k) : 0;
 #pragma unroll
-            for (int c = 0; c < P; ++c)
-#pragma unroll
-                for (int t = 0; t < MPT; ++t) acc[c][t] = 0.0;
-            const int ntiles = (nk + KT - 1) / KT;
-            auto load_tile = [&](int tile, int buf) {
-                const int k0 = tile * KT;
-                float* ph = phs + buf * KT * P * 32;
-                for (int c = tid; c < KT * P * 8; c += 256) {
-                    const int kk = c / (P * 8), rem = c % (P * 8), cc = rem / 8, jj = (rem % 8) * 4;
-                    const bool ok = k0 + kk < nk;
-                    const float* src = pbase + ((size_t)cc * scr.row_stride + (ok ? k0 + kk : 0)) * kBlockPoints + jj;
-                    cp_async16f(ph + (kk * P + cc) * 32 + jj, src, ok);
+                for (int c = 0; c < P; ++c) {
+                    if (ok) {
+                        const float4* src = reinterpret_cast<const float4*>(
+                            pbase + (static_cast<size_t>(c) * scr.row_stride + row) * kBlockPoints + g * 8);
+                        ra[c][0] = __ldcs(src);
+                        ra[c][1] = __ldcs(src + 1);
+                    } else {
+                        ra[c][0] = ra[c][1] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
                 }
-                float* cb = cs + buf * KT * MOC;
-                for (int c = tid; c < KT * MOC / 4; c += 256) {
-                    const int kk = c / (MOC / 4), col = (c % (MOC / 4)) * 4;
-                    const bool ok = (k0 + kk < nk) && (mo0 + col < ch.ldc);
-                    const float* src = ch.ct + (size_t)(ok ? kept[k0 + kk] : 0) * ch.ldc + (ok ? mo0 + col : 0);
-                    cp_async16f(cb + kk * MOC + col, src, ok);
-                }
-                asm volatile("cp.async.commit_group;\n" ::);
             };
-            if (ntiles > 0) load_tile(0, 0);
-            for (int t = 0; t < ntiles; ++t) {
-                if (t + 1 < ntiles) {
-                    load_tile(t + 1, (t + 1) & 1);
-                    asm volatile("cp.async.wait_group 1;\n" ::);
-                } else {
-                    asm volatile("cp.async.wait_group 0;\n" ::);
+            if (ntiles > 0) load_a(0);
+            for (int t = 0; t < ntiles; ++t, ++gtile) {
+                const int s = static_cast<int>(gtile % S);
+                if (gtile >= S && !mbar_wait(&bar[s], static_cast<unsigned>((gtile / S - 1) & 1))) failed = true;
+                // A pieces of this step.
+                unsigned char* ast = a_st + s * L::a_bytes;
+#pragma unroll
+                for (int c = 0; c < P; ++c) {
+                    uint4 p0, p1, p2;
+                    split8(ra[c][0], ra[c][1], p0, p1, p2);
+                    *reinterpret_cast<uint4*>(ast + (0 * P + c) * kATile + a_off) = p0;
+                    *reinterpret_cast<uint4*>(ast + (1 * P + c) * kATile + a_off) = p1;
+                    *reinterpret_cast<uint4*>(ast + (2 * P + c) * kATile + a_off) = p2;
                 }
-                __syncthreads();
-                const float* ph = phs + (t & 1) * KT * P * 32;
-                const float* cb = cs + (t & 1) * KT * MOC + w * MPT;
-                float part[P][MPT];
+                if (t + 1 < ntiles) load_a(t + 1);
+                // Coefficient pieces of this step: 3 pieces x 16 rows x N/8 chunks of 16 B.
+                const unsigned bst = smem_u32(b_st + s * b_bytes);
+                const int nchunk = 3 * 16 * (N / 8);
+                for (int v = tid; v < nchunk; v += kThreads) {
+                    const int r8 = v & 7;
+                    const int rest = v >> 3;
+                    const int ng = rest % (N / 8);
+                    const int rest2 = rest / (N / 8);
+                    const int rh = rest2 & 1, piece = rest2 >> 1;
+                    const int k = t * 16 + rh * 8 + r8;
+                    const int col = n0 + ng * 8;
+                    const bool ok = k < nk && col < ch.ldn;
+                    const int row = ok ? (sorted ? perm[k] : k) : 0;
+                    const std::uint16_t* src =
+                        ch.cs + (ok ? piece * ch.piece_stride + static_cast<long long>(kept[row]) * ch.ldn + col : 0);
+                    cp_async16(bst + static_cast<unsigned>(piece * 32 * N + ng * 128 + rh * (N * 16) + r8 * 16), src,
+                               ok);
+                }
+                asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                if (__syncthreads_or(failed)) {
+                    failed = true;
+                    break;
+                }
+                if (tid == 0) {
+                    tc_fence_after();
+                    const unsigned ab = smem_u32(ast), bb = bst;
+                    // K steps go round-robin to G accumulator groups.
+                    const unsigned dg = tmem + static_cast<unsigned>(t % G) * gcols;
+                    constexpr int pi[6] = {1, 0, 2, 0, 1, 0}, pj[6] = {1, 2, 0, 1, 0, 0};
+#pragma unroll
+                    for (int c = 0; c < P; ++c) {
+#pragma unroll
+                        for (int e = 0; e < 6; ++e) {
+                            const unsigned long long ad = smem_desc(ab + (pi[e] * P + c) * kATile, 2048u, 128u);
+                            const unsigned long long bd =
+                                smem_desc(bb + static_cast<unsigned>(pj[e] * 32 * N), static_cast<unsigned>(N * 16), 128u);
+                            tc_mma(dg + static_cast<unsigned>(c * N), ad, bd, idesc, (t >= G || e > 0) ? 1u : 0u);
+                        }
+                    }
+                    tc_commit(&bar[s]);
+                }
+            }
+            if (failed || ntiles == 0) continue;
+            // Accumulators of this pass complete once the last step's commit arrives.
+            const long long last = gtile - 1;
+            if (!mbar_wait(&bar[last % S], static_cast<unsigned>((last / S) & 1))) failed = true;
+            if (__syncthreads_or(failed)) {
+                failed = true;
+                break;
+            }
+            tc_fence_after();
+            const int nvalid = ch.nocc - n0 < N ? ch.nocc - n0 : N;
+            const int i_lo = half * (N / 2), i_hi = min(nvalid, (half + 1) * (N / 2));
+            const unsigned lane_addr = tmem + (static_cast<unsigned>(quarter * 32) << 16);
+            const int ng = ntiles < G ? ntiles : G;
+            constexpr int MG = P == 10 ? 4 : 8;
+            for (int i0 = i_lo; i0 < i_hi; i0 += MG) {
+                // tcgen05.ld is warp-collective: the trip count depends on the
+                // half only; columns past the last MO are read and ignored.
+                double x[P][MG];
 #pragma unroll
                 for (int c = 0; c < P; ++c)
 #pragma unroll
-                    for (int tt = 0; tt < MPT; ++tt) part[c][tt] = 0.f;
-#pragma unroll 4
-                for (int kk = 0; kk < KT; ++kk) {
-                    float phi[P];
-#pragma unroll
-                    for (int c = 0; c < P; ++c) phi[c] = ph[(kk * P + c) * 32 + lane];
-                    float cv[MPT];
-#pragma unroll
-                    for (int t4 = 0; t4 < MPT / 4; ++t4) {
-                        const float4 v = reinterpret_cast<const float4*>(cb + kk * MOC)[t4];
-                        cv[4 * t4] = v.x;
-                        cv[4 * t4 + 1] = v.y;
-                        cv[4 * t4 + 2] = v.z;
-                        cv[4 * t4 + 3] = v.w;
-                    }
+                    for (int u = 0; u < MG; ++u) x[c][u] = 0.0;
+                for (int gi = 0; gi < ng; ++gi) {
+                    unsigned v[P][MG];
 #pragma unroll
                     for (int c = 0; c < P; ++c)
+                        tmem_ld<MG>(lane_addr + static_cast<unsigned>(gi) * gcols + static_cast<unsigned>(c * N + i0), v[c]);
+                    tmem_wait_ld();
 #pragma unroll
-                        for (int tt = 0; tt < MPT; ++tt) part[c][tt] = fmaf(phi[c], cv[tt], part[c][tt]);
+                    for (int c = 0; c < P; ++c) {
+                        reg_fence<MG>(v[c]);
+#pragma unroll
+                        for (int u = 0; u < MG; ++u) x[c][u] += static_cast<double>(__uint_as_float(v[c][u]));
+                    }
                 }
-#pragma unroll
-                for (int c = 0; c < P; ++c)
-#pragma unroll
-                    for (int tt = 0; tt < MPT; ++tt) acc[c][tt] += (double)part[c][tt];
-                __syncthreads();
+                fold<P, MG>(x, q, i_hi - i0);
             }
-            fold<P, MPT>(acc, q);
+            tc_fence_before();
+            __syncthreads();
         }
+        if (failed) break;
+        // Sum the two halves' partial sums of this channel.
+        if (half == 1)
 #pragma unroll
-        for (int i = 0; i < Q; ++i) red[(w * Q + i) * 32 + lane] = q[i];
+            for (int i = 0; i < Q; ++i) red[i * 128 + point] = q[i];
         __syncthreads();
-        for (int i = tid; i < Q * 32; i += 256) {
-            const int qi = i / 32, l = i % 32;
-            double s = red[qi * 32 + l];
+        if (half == 0) {
 #pragma unroll
-            for (int ww = 1; ww < 8; ++ww) s += red[(ww * Q + qi) * 32 + l];
-            fin[(ci * Q + qi) * 32 + l] = s;
+            for (int i = 0; i < Q; ++i) q[i] += red[i * 128 + point];
+            record<P>(q, prm.ao_order, ch.role == 1 ? chan_dd[0] : chan_dd[1]);
         }
         __syncthreads();
     }
-    if (w != 0 || j0 + lane >= b) return;
-    double f[Q];
-    DevDD alpha, beta, comp[4];
-    dd_zero(alpha);
-    dd_zero(beta);
-    for (int ci = 0; ci < prm.nchannels; ++ci) {
-        for (int i = 0; i < Q; ++i) f[i] = fin[(ci * Q + i) * 32 + lane];
-        record<P>(f, prm.ao_order, prm.ch[ci].role == 1 ? alpha : beta);
+
+    if (failed) {
+        if (tid == 0) atomicOr(prm.status, 1u);
+        // Let the MMAs already issued finish before tensor memory is freed.
+        for (int s = 0; s < S; ++s) {
+            const long long last = gtile - 1 - ((gtile - 1 - s) % S + S) % S;
+            if (last >= 0) (void)mbar_wait(&bar[last % S], static_cast<unsigned>((last / S) & 1));
+        }
     }
-    if (prm.beta_is_alpha) beta = alpha;
-    const bool full = P == 10 && prm.ao_order == 2;
-    comp[1] = alpha;
-    comp[2] = beta;
-    comp[0] = dd_combine(alpha, beta, 1.0, 1.0, full);
-    comp[3] = dd_combine(alpha, beta, -1.0, 1.0, full);
-    store_point(prm.spec, comp, start + j0 + lane);
+    tc_fence_before();
+    __syncthreads();
+    if (w == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, static_cast<unsigned>(prm.tmem_cols));
+    }
+    if (half != 0 || point >= bcount) return;
+    DevDD comp[4];
+    if (failed) {
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        DevDD d;
+        d.value = d.lap = d.tau = nan;
+        for (int i = 0; i < 3; ++i) d.grad[i] = d.tau_axes[i] = nan;
+        for (int i = 0; i < 6; ++i) d.hess[i] = nan;
+        comp[0] = comp[1] = comp[2] = comp[3] = d;
+    } else {
+        DevDD alpha = chan_dd[0], beta = chan_dd[1];
+        if (prm.beta_is_alpha) beta = alpha;
+        const bool full = P == 10 && prm.ao_order == 2;
+        comp[1] = alpha;
+        comp[2] = beta;
+        comp[0] = dd_combine(alpha, beta, 1.0, 1.0, full);
+        comp[3] = dd_combine(alpha, beta, -1.0, 1.0, full);
+    }
+    store_point(prm.spec, comp, start + point);
 }
 
-template <int P, int MPT, int KT>
+template <int P, int S>
 void launch(const ContractMixedParams& p, cudaStream_t stream) {
-    constexpr int MOC = 8 * MPT;
-    constexpr int Q = NQm<P>::v;
-    const size_t smem = sizeof(float) * (size_t)(2 * KT * P * 32 + 2 * KT * MOC) + sizeof(double) * (size_t)(8 * Q * 32 + 2 * Q * 32);
-    cudaFuncSetAttribute(contract_mixed_kernel<P, MPT, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    contract_mixed_kernel<P, MPT, KT><<<p.nblocks * 4, 256, smem, stream>>>(p);
+    // The whole 227 KB of shared memory per CTA: one CTA per SM, so each CTA's
+    // tensor-memory allocation is granted at once, and every address a matrix
+    // descriptor can reach from a stage lies inside the CTA's allocation.
+    constexpr size_t kMaxSmem = 227u * 1024u;
+    if (Smem<P, S>::total(p.ncols) > kMaxSmem) throw std::invalid_argument("tensor-core contraction: stages exceed shared memory");
+    const size_t smem = kMaxSmem;
+    cudaFuncSetAttribute(contract_mixed_kernel<P, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    contract_mixed_kernel<P, S><<<p.nblocks, kThreads, smem, stream>>>(p);
 }
+
+__device__ unsigned g_pipeline_status;
 
 }  // namespace
 
+unsigned* pipeline_status_word() {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_pipeline_status) != cudaSuccess) throw std::runtime_error("cudaGetSymbolAddress (status)");
+    return static_cast<unsigned*>(p);
+}
+
+unsigned take_pipeline_status() {
+    unsigned v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_pipeline_status, sizeof v) != cudaSuccess)
+        throw std::runtime_error("cudaMemcpyFromSymbol (status)");
+    if (v) {
+        const unsigned zero = 0;
+        cudaMemcpyToSymbol(g_pipeline_status, &zero, sizeof zero);
+    }
+    return v;
+}
+
+void mixed_columns(int npanel, int nocc16, int& ncols, int& groups, int& tmem_cols) {
+    const int maxn = std::min(256, (512 / npanel) / 16 * 16);
+    const int n = std::max(16, nocc16);
+    const int passes = (n + maxn - 1) / maxn;
+    ncols = ((n + passes - 1) / passes + 15) / 16 * 16;
+    groups = std::max(1, std::min(4, 512 / (npanel * ncols)));
+    const int need = groups * npanel * ncols;
+    tmem_cols = 32;
+    while (tmem_cols < need) tmem_cols *= 2;
+}
+
 void launch_contract_mixed(const ContractMixedParams& p, int npanel, cudaStream_t stream) {
+    if (p.ncols < 16 || p.ncols % 16 != 0 || p.ncols > 256 || p.groups < 1 ||
+        p.groups * npanel * p.ncols > 512 || p.tmem_cols > 512)
+        throw std::invalid_argument("tensor-core contraction: unsupported MO column count");
     switch (npanel) {
-        case 1: launch<1, 16, 16>(p, stream); break;
-        case 4: launch<4, 16, 16>(p, stream); break;
-        case 5: launch<5, 16, 16>(p, stream); break;
-        case 10: launch<10, 8, 16>(p, stream); break;
-        default: break;
+        case 1: launch<1, 2>(p, stream); break;
+        case 4: launch<4, 2>(p, stream); break;
+        case 5: launch<5, 2>(p, stream); break;
+        case 10: launch<10, 1>(p, stream); break;
+        default: throw std::invalid_argument("tensor-core contraction: unsupported panel count");
     }
 }
 

@@ -90,6 +90,7 @@ struct AoScratch {
     int* nkept = nullptr;
     int row_stride = 0;   // >= nao
     int npanel = 0;
+    float* rowmax = nullptr;  // optional: block maximum |value| of each kept row
 };
 
 // Parameters of the AO build of one wave.

@@ -1,16 +1,21 @@
-// Mixed-precision contraction of the AO-MO path: FP32 AO panels and FP32 MO
-// coefficients, products accumulated in FP32 per K tile, and the per-point
-// reductions (rho, grad, tau, Laplacian/Hessian) and fields in FP64.
+// Mixed-precision contraction of the AO-MO path on the fifth-generation
+// tensor cores: FP32 AO panels and FP64 MO coefficients are each split into
+// three BF16 pieces, the six products whose pieces sum to order <= 2 are
+// accumulated by tcgen05.mma in FP32 in tensor memory, and the per-point
+// reductions (rho, grad, tau, Laplacian/Hessian) and fields are done in FP64.
 #pragma once
+
+#include <cstdint>
 
 #include "fields.cuh"
 #include "kumo_device.cuh"
 
 namespace kumo_dev {
 
-struct MoChannelF {
-    const float* ct = nullptr;  // [nao][ldc], MO contiguous
-    int ldc = 0;
+struct MoChannelTC {
+    const std::uint16_t* cs = nullptr;  // [3][nao][ldn] BF16 pieces, MO contiguous
+    long long piece_stride = 0;         // nao * ldn
+    int ldn = 0;                        // multiple of 16, >= nocc
     int nocc = 0;
     int role = 0;  // 1 alpha, 2 beta
 };
@@ -22,11 +27,24 @@ struct ContractMixedParams {
     long long count = 0;
     int nblocks = 0;
     int nchannels = 0;
-    MoChannelF ch[2];
+    MoChannelTC ch[2];
     int beta_is_alpha = 0;
     int ao_order = 2;
+    int ncols = 16;       // MO columns per pass (multiple of 16, npanel * ncols <= 512)
+    int groups = 1;       // accumulator groups (K steps round-robin), groups * npanel * ncols <= 512
+    int tmem_cols = 32;   // power of two >= groups * npanel * ncols
     FieldSpec spec;
+    unsigned* status = nullptr;  // set nonzero if a pipeline wait ran out
 };
+
+// MO columns per pass, accumulator groups and tensor-memory columns for
+// npanel panels and at most nocc16 (a multiple of 16) occupied MOs per channel.
+void mixed_columns(int npanel, int nocc16, int& ncols, int& groups, int& tmem_cols);
+
+// Device word the contraction sets when a pipeline wait runs out (per device),
+// and a synchronous read-and-clear of it.
+unsigned* pipeline_status_word();
+unsigned take_pipeline_status();
 
 void launch_contract_mixed(const ContractMixedParams& p, int npanel, cudaStream_t stream);
 

@@ -2,6 +2,7 @@
 #include "device_state.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 namespace chem::kumo::detail {
@@ -9,6 +10,38 @@ namespace chem::kumo::detail {
 void throw_cuda(cudaError_t e, const char* what) {
     throw std::runtime_error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
 }
+
+namespace {
+
+// BF16 (8-bit significand) rounding of a double, to nearest with ties to even,
+// in two steps: to FP32 with round-to-odd (so the second rounding cannot
+// double-round), then to BF16 by integer rounding of the FP32 bits.
+std::uint16_t bf16_bits(double x) {
+    float f = static_cast<float>(x);
+    if (std::isfinite(f) && static_cast<double>(f) != x) {
+        std::uint32_t u;
+        std::memcpy(&u, &f, 4);
+        // Round to odd: truncate toward zero, then set the last bit.
+        const float t = std::fabs(static_cast<double>(f)) > std::fabs(x) ? std::nextafter(f, 0.0f) : f;
+        std::memcpy(&u, &t, 4);
+        u |= 1u;
+        std::memcpy(&f, &u, 4);
+    }
+    std::uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u) return static_cast<std::uint16_t>(u >> 16);
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return static_cast<std::uint16_t>(u >> 16);
+}
+
+double bf16_value(std::uint16_t h) {
+    const std::uint32_t u = static_cast<std::uint32_t>(h) << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return static_cast<double>(f);
+}
+
+}  // namespace
 
 template <typename T>
 T* DeviceMolecule::upload(const T* host, std::size_t count) {
@@ -76,7 +109,7 @@ DeviceMolecule::DeviceMolecule(const Molecule& m) {
     if (nmo_alpha) c_alpha = upload(ca.data(), ca.size());
     if (unrestricted && nmo_beta) c_beta = upload(cb.data(), cb.size());
     if (!unrestricted) c_beta = c_alpha;
-    auto transpose_occ = [&](const Matrix& c, int nocc, int& ld, double*& dst, float*& dst_f) {
+    auto transpose_occ = [&](const Matrix& c, int nocc, int& ld, double*& dst, int& ldn, std::uint16_t*& dst_s) {
         // Rows padded to a multiple of 4 so that every 16-byte chunk of a row
         // (2 doubles, 4 floats) lies inside the row.
         ld = std::max(4, (nocc + 3) / 4 * 4);
@@ -84,14 +117,24 @@ DeviceMolecule::DeviceMolecule(const Molecule& m) {
         for (int o = 0; o < nocc && static_cast<std::size_t>(o) < c.cols(); ++o)
             for (std::size_t a = 0; a < n; ++a) t[a * static_cast<std::size_t>(ld) + static_cast<std::size_t>(o)] = c(a, static_cast<std::size_t>(o));
         dst = upload(t.data(), t.size());
-        std::vector<float> tf(t.begin(), t.end());
-        dst_f = upload(tf.data(), tf.size());
+        ldn = std::max(16, (nocc + 15) / 16 * 16);
+        std::vector<std::uint16_t> pieces(3 * n * static_cast<std::size_t>(ldn), 0);
+        for (std::size_t a = 0; a < n; ++a)
+            for (int o = 0; o < nocc && static_cast<std::size_t>(o) < c.cols(); ++o) {
+                double rest = c(a, static_cast<std::size_t>(o));
+                for (int k = 0; k < 3; ++k) {
+                    const std::uint16_t h = bf16_bits(rest);
+                    pieces[(k * n + a) * static_cast<std::size_t>(ldn) + static_cast<std::size_t>(o)] = h;
+                    rest -= bf16_value(h);
+                }
+            }
+        dst_s = upload(pieces.data(), pieces.size());
     };
     nocc_alpha = static_cast<int>(m.occupied_count(SpinChannel::Alpha));
     nocc_beta = static_cast<int>(m.occupied_count(SpinChannel::Beta));
     if (nmo_alpha) {
-        transpose_occ(ca, nocc_alpha, ldc_alpha, ct_alpha, ct_alpha_f);
-        transpose_occ(unrestricted ? cb : ca, nocc_beta, ldc_beta, ct_beta, ct_beta_f);
+        transpose_occ(ca, nocc_alpha, ldc_alpha, ct_alpha, ldn_alpha, cs_alpha);
+        transpose_occ(unrestricted ? cb : ca, nocc_beta, ldc_beta, ct_beta, ldn_beta, cs_beta);
     }
 }
 

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <cstdint>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -31,9 +32,12 @@ struct DeviceMolecule {
     int ldc_alpha = 0, nocc_alpha = 0;
     double* ct_beta = nullptr;
     int ldc_beta = 0, nocc_beta = 0;
-    // FP32 copies of the occupied MOs for the mixed form.
-    float* ct_alpha_f = nullptr;
-    float* ct_beta_f = nullptr;
+    // Occupied MOs of the mixed form as three BF16 pieces (c = c0 + c1 + c2,
+    // each the BF16 rounding of what the previous pieces leave), stored
+    // [piece][AO][MO] with rows of ldn MOs (a multiple of 16, zero padded).
+    std::uint16_t* cs_alpha = nullptr;
+    std::uint16_t* cs_beta = nullptr;
+    int ldn_alpha = 0, ldn_beta = 0;
     // All MO coefficients, one MO per column (n x nmo), for amplitudes.
     double* c_alpha = nullptr;
     int nmo_alpha = 0;

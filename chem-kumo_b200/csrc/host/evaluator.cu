@@ -306,10 +306,8 @@ private:
         const int nb = static_cast<int>(mol_.occupied_count(SpinChannel::Beta));
         beta_is_alpha = need_a && need_b && !mol_.unrestricted() && na == nb;
         int nch = 0;
-        auto ct = [&](bool beta) -> const double* {
-            if (mixed) return reinterpret_cast<const double*>(beta ? dev_->ct_beta_f : dev_->ct_alpha_f);
-            return beta ? dev_->ct_beta : dev_->ct_alpha;
-        };
+        (void)mixed;
+        auto ct = [&](bool beta) -> const double* { return beta ? dev_->ct_beta : dev_->ct_alpha; };
         if (need_a && na > 0) ch[nch++] = {ct(false), dev_->ldc_alpha, na, 1};
         if (need_b && !beta_is_alpha && nb > 0) ch[nch++] = {ct(true), dev_->ldc_beta, nb, 2};
         return nch;
@@ -362,14 +360,15 @@ private:
         const int nao = dev_->basis.nao;
         const int stride = (nao + 7) / 8 * 8;
         const std::size_t per_block = sizeof(float) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints +
-                                      sizeof(int) * ((std::size_t)stride + 1);
+                                      sizeof(int) * ((std::size_t)stride + 1) + sizeof(float) * (std::size_t)stride;
         const int W = wave_blocks(nblocks, per_block);
         DeviceAlloc panels(sizeof(float) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints * W, stream_);
         DeviceAlloc kept(sizeof(int) * (std::size_t)stride * W, stream_);
         DeviceAlloc nkept(sizeof(int) * (std::size_t)W, stream_);
         kumo_dev::AoBuildParams<float> bp = build_params<float>(opt_.screening_threshold);
         bp.block_size = static_cast<long long>(bs);
-        bp.out = {panels.as<float>(), kept.as<int>(), nkept.as<int>(), stride, npanel};
+        DeviceAlloc rowmax(sizeof(float) * (std::size_t)stride * W, stream_);
+        bp.out = {panels.as<float>(), kept.as<int>(), nkept.as<int>(), stride, npanel, rowmax.as<float>()};
         kumo_dev::ContractMixedParams cp{};
         cp.scr = bp.out;
         cp.block_size = static_cast<long long>(bs);
@@ -377,8 +376,16 @@ private:
         bool bia = false;
         kumo_dev::MoChannel ch[2];
         cp.nchannels = mo_channels(needed, ch, bia, true);
-        for (int i = 0; i < cp.nchannels; ++i)
-            cp.ch[i] = {reinterpret_cast<const float*>(ch[i].ct), ch[i].ldc, ch[i].nocc, ch[i].role};
+        int nocc16 = 16;
+        for (int i = 0; i < cp.nchannels; ++i) {
+            const bool beta = ch[i].role == 2;
+            const int ldn = beta ? dev_->ldn_beta : dev_->ldn_alpha;
+            cp.ch[i] = {beta ? dev_->cs_beta : dev_->cs_alpha, static_cast<long long>(nao) * ldn, ldn, ch[i].nocc,
+                        ch[i].role};
+            nocc16 = std::max(nocc16, (ch[i].nocc + 15) / 16 * 16);
+        }
+        kumo_dev::mixed_columns(npanel, nocc16, cp.ncols, cp.groups, cp.tmem_cols);
+        cp.status = kumo_dev::pipeline_status_word();
         cp.beta_is_alpha = bia;
         cp.ao_order = ao_order;
         cp.spec = spec;
@@ -607,6 +614,13 @@ std::vector<Property> unique_keys(const Request& request) {
     return keys;
 }
 
+// A tensor-core pipeline wait that ran out leaves NaN in its block's outputs
+// and a flag on the device; host-returning calls turn the flag into an error.
+void check_pipeline_status(Precision precision) {
+    if (precision == Precision::Mixed && kumo_dev::take_pipeline_status() != 0)
+        throw std::runtime_error("mixed-precision contraction: a tensor-core pipeline wait timed out");
+}
+
 }  // namespace
 
 Results Evaluator::evaluate(const Grid& grid, const Request& request) const {
@@ -629,6 +643,7 @@ Results Evaluator::evaluate(const Grid& grid, const Request& request) const {
     std::vector<double> host(total);
     if (total) check_cuda(cudaMemcpy(host.data(), out.as<double>(), sizeof(double) * total, cudaMemcpyDeviceToHost),
                           "cudaMemcpy (results)");
+    check_pipeline_status(options_.precision);
     off = 0;
     for (const auto& k : keys) {
         PropertyField f;
@@ -669,6 +684,7 @@ Results Evaluator::evaluate(Points points, const Request& request) const {
     std::vector<double> host(total);
     if (total) check_cuda(cudaMemcpy(host.data(), out.as<double>(), sizeof(double) * total, cudaMemcpyDeviceToHost),
                           "cudaMemcpy (results)");
+    check_pipeline_status(options_.precision);
     off = 0;
     for (const auto& k : keys) {
         PropertyField f;

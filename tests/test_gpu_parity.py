@@ -259,6 +259,51 @@ def test_mixed_precision_water(water28):
     assert scaled_error(mix[4], f64[4]) <= 1e-5
 
 
+# Panel counts of the tensor-core contraction: 1 (values), 4 (+gradient),
+# 5 (+Laplacian panel), 10 (+full Hessian); every density component.
+MIXED_CASES = {
+    "values": [P.Density],
+    "gradient": [P.Density, P.Gradient, P.Tau, P.Elf],
+    "laplacian": [P.Density, P.Gradient, P.Laplacian, P.Tau],
+    "hessian": [P.Density, P.Hessian, P.Laplacian],
+}
+
+
+@pytest.mark.parametrize("case", list(MIXED_CASES))
+@pytest.mark.parametrize("name", ["o2.fchk.gz", "acrolein.fchk.gz"])
+def test_mixed_tensor_core_panels_and_components(name, case):
+    m, o = _pair(os.path.join(GOLDEN, name))
+    pts = _box_points(o.atom_xyz.reshape(-1, 3), 3000, 5)
+    comps = [D.Total, D.Alpha, D.Beta, D.Difference] if name == "o2.fchk.gz" else [D.Total]
+    props = [K.density(k, c) for k in MIXED_CASES[case] for c in comps
+             if not (k == P.Elf and c == D.Difference)]  # ELF of the spin density is undefined
+    f64, _ = K.Evaluator(m, backend=K.Backend.AO_MO).evaluate_points(pts, props)
+    mix, used = K.Evaluator(m, backend=K.Backend.AO_MO, precision=K.Precision.Mixed).evaluate_points(pts, props)
+    assert used == int(K.Backend.AO_MO)
+    total = {p.kind: r for p, r in zip(props, f64) if p.component == D.Total}
+    for p, a, r in zip(props, mix, f64):
+        assert np.all(np.isfinite(a)), p
+        tol = 1e-5 if p.kind == P.Elf else 1e-6
+        # alpha - beta cancels: its FP32-level error follows the channels'
+        # scale, so it is measured against the total of the same kind.
+        scale = max(1.0, np.abs(total[p.kind]).max()) if p.component == D.Difference else max(1.0, np.abs(r).max())
+        err = np.abs(a - r).max() / scale
+        assert err <= tol, (p, err)
+
+
+def test_mixed_tensor_core_several_mo_passes(synth_cache):
+    # 76 occupied MOs: with the full Hessian (10 panels) a pass holds 48 MO
+    # columns of tensor memory, so the contraction takes two passes.
+    path = synth.workload_fchk("organic_740", synth_cache)
+    m = K.Molecule.from_fchk(path)
+    pts = _box_points(m.atoms()[2], 2048, 9)
+    props = [K.density(P.Density), K.density(P.Hessian), K.density(P.Gradient), K.density(P.Laplacian)]
+    f64, _ = K.Evaluator(m).evaluate_points(pts, props)
+    mix, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_points(pts, props)
+    for p, a, r in zip(props, mix, f64):
+        assert scaled_error(a, r) <= 1e-6, (p, scaled_error(a, r))
+
+
 def test_device_api_matches_host():
     import torch
     m = K.Molecule.from_fchk(os.path.join(GOLDEN, "h2o_b3lyp_def2tzvp.fchk.gz"))
