@@ -30,7 +30,7 @@ HOST_CXX = "g++"
 # Translation units and their extra flags.
 CUDA_UNITS = {
     "csrc/cuda/ao_build_f64.cu": ["-fmad=false"],
-    "csrc/cuda/ao_build_f32.cu": [],
+    "csrc/cuda/ao_mixed.cu": [],
     "csrc/cuda/contract_f64.cu": [],
     "csrc/cuda/contract_mixed.cu": [],
     "csrc/cuda/esp.cu": [],

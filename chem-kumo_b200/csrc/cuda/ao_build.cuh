@@ -24,33 +24,10 @@
 
 #include <utility>
 
+#include "ao_common.cuh"
 #include "kumo_device.cuh"
 
 namespace kumo_dev {
-
-template <int L>
-struct Cart {
-    static constexpr int NC = (L + 1) * (L + 2) / 2;
-};
-
-// Gaussian Cartesian order (src/basis_evaluator.cpp:135-152) as a constexpr table.
-__host__ __device__ constexpr int cart_power(int l, int k, int axis) {
-    constexpr int d[6][3] = {{2, 0, 0}, {0, 2, 0}, {0, 0, 2}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
-    constexpr int f[10][3] = {{3, 0, 0}, {0, 3, 0}, {0, 0, 3}, {1, 2, 0}, {2, 1, 0},
-                              {2, 0, 1}, {1, 0, 2}, {0, 1, 2}, {0, 2, 1}, {1, 1, 1}};
-    if (l == 0) return 0;
-    if (l == 1) return k == axis ? 1 : 0;
-    if (l == 2) return d[k][axis];
-    if (l == 3) return f[k][axis];
-    // l >= 4: lexicographic in (lx, ly)
-    int n = 0;
-    for (int lx = 0; lx <= l; ++lx)
-        for (int ly = 0; ly <= l - lx; ++ly) {
-            if (n == k) return axis == 0 ? lx : (axis == 1 ? ly : l - lx - ly);
-            ++n;
-        }
-    return 0;
-}
 
 // exp(-a r^2) for a radial factor: FP64 as the reference; in FP32 the
 // argument is reduced in FP64 (-a r^2 log2 e = n + f, |f| <= 1/2) so that the
@@ -84,20 +61,6 @@ __device__ __forceinline__ T factor2(const T* xp, T a, T x) {
     const T t1 = M >= 2 ? (T)(M * (M - 1)) * xp[M >= 2 ? M - 2 : 0] : (T)0;
     return t1 - (T)2 * a * (T)(2 * M + 1) * xp[M] + (T)4 * a * a * x * x * xp[M];
 }
-
-template <int... Is, typename Fn>
-__device__ __forceinline__ void static_for_impl(std::integer_sequence<int, Is...>, Fn&& fn) {
-    (fn(std::integral_constant<int, Is>{}), ...);
-}
-template <int N, typename Fn>
-__device__ __forceinline__ void static_for(Fn&& fn) {
-    static_for_impl(std::make_integer_sequence<int, N>{}, fn);
-}
-
-template <int MAXL>
-struct MaxOut {
-    static constexpr int v = (MAXL + 1) * (MAXL + 2) / 2;
-};
 
 // Panels of one shell for the thread's point into stage[(m * P + c) * 128 + j],
 // with maxabs[m] the largest |value| over the panels of the AO order.
@@ -278,27 +241,6 @@ __device__ __forceinline__ void shell_panels(const T (&pure)[3][135], const T* s
     }
 }
 
-template <typename T>
-__device__ __forceinline__ T warp_max(T v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const T w = __shfl_xor_sync(0xffffffffu, v, o);
-        v = w > v ? w : v;
-    }
-    return v;
-}
-
-__device__ __forceinline__ double warp_min_d(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-__device__ __forceinline__ double warp_max_d(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-
 // One CTA per screening block.  Dynamic shared memory: the staging tile
 // (max_count * P * 128 values of T), the radial factors (kMaxPrim * 128
 // values of T) and the list of AO blocks within reach (nblocks ints).
@@ -333,64 +275,7 @@ __global__ void __launch_bounds__(kBlockPoints, sizeof(T) == 8 ? 3 : 5) ao_build
     const bool keep_all = prm.threshold == 0.0;
     const T thr = (T)prm.threshold;
 
-    // Bounding box of the block's points.
-    {
-        const double big = 1.0e300;
-        double lo[3] = {valid ? px : big, valid ? py : big, valid ? pz : big};
-        double hi[3] = {valid ? px : -big, valid ? py : -big, valid ? pz : -big};
-        for (int a = 0; a < 3; ++a) {
-            lo[a] = warp_min_d(lo[a]);
-            hi[a] = warp_max_d(hi[a]);
-        }
-        if (lane == 0)
-            for (int a = 0; a < 3; ++a) {
-                s_box[warp][a] = lo[a];
-                s_box[warp][3 + a] = hi[a];
-            }
-    }
-    __syncthreads();
-    double lo[3], hi[3];
-    for (int a = 0; a < 3; ++a) {
-        lo[a] = s_box[0][a];
-        hi[a] = s_box[0][3 + a];
-        for (int w = 1; w < NW; ++w) {
-            lo[a] = fmin(lo[a], s_box[w][a]);
-            hi[a] = fmax(hi[a], s_box[w][3 + a]);
-        }
-    }
-    // AO blocks within reach of the box, in AO order.  A block is left out
-    // only if the box is farther than its cutoff radius by a relative margin
-    // that covers the rounding of both distances, so every point it leaves
-    // out is also outside the cutoff in the reference's arithmetic.
-    int nlist = 0;
-    for (int c0 = 0; c0 < B.nblocks; c0 += kBlockPoints) {
-        const int s = c0 + j;
-        bool reach = false;
-        if (s < B.nblocks) {
-            if (keep_all) {
-                reach = true;
-            } else {
-                const double4 o = B.origin_r2[s];
-                const double ox[3] = {o.x, o.y, o.z};
-                double d2 = 0.0;
-                for (int a = 0; a < 3; ++a) {
-                    const double d = fmax(0.0, fmax(lo[a] - ox[a], ox[a] - hi[a]));
-                    d2 += d * d;
-                }
-                reach = !(d2 > o.w * (1.0 + 1e-10) + 1e-300);
-            }
-        }
-        const unsigned ballot = __ballot_sync(0xffffffffu, reach);
-        if (lane == 0) s_count[warp] = __popc(ballot);
-        __syncthreads();
-        int before = nlist;
-        for (int w = 0; w < warp; ++w) before += s_count[w];
-        if (reach) s_list[before + __popc(ballot & ((1u << lane) - 1u))] = s;
-        int total = 0;
-        for (int w = 0; w < NW; ++w) total += s_count[w];
-        __syncthreads();
-        nlist += total;
-    }
+    const int nlist = block_shell_list(B, valid, px, py, pz, keep_all, s_list, s_box, s_count);
 
     const T* gexp = sizeof(T) == 8 ? (const T*)B.exps : (const T*)B.exps_f;
     const T* gw = sizeof(T) == 8 ? (const T*)B.weights : (const T*)B.weights_f;

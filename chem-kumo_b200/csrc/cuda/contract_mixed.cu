@@ -238,7 +238,7 @@ struct Smem {
     __host__ __device__ static unsigned b_bytes(int ncols) { return 3u * 32u * static_cast<unsigned>(ncols); }
     static size_t total(int ncols) {
         return S * (static_cast<size_t>(a_bytes) + b_bytes(ncols)) + sizeof(double) * Q * 128 +
-               (sizeof(int) + 1) * kSortCap + sizeof(int) * kBuckets + 8 * S + 16;
+               (sizeof(int) + 1) * kSortCap + sizeof(int) * (kBuckets + 4) + 8 * S + 16;
     }
 };
 
@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
     double* red = reinterpret_cast<double*>(b_st + S * b_bytes);
     int* perm = reinterpret_cast<int*>(red + Q * 128);
     int* bucket_start = perm + kSortCap;
-    unsigned char* keys = reinterpret_cast<unsigned char*>(bucket_start + kBuckets);
+    unsigned char* keys = reinterpret_cast<unsigned char*>(bucket_start + kBuckets + 4);
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(keys + kSortCap);
     unsigned* tslot = reinterpret_cast<unsigned*>(bar + S);
 
@@ -264,8 +264,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
     if (bcount > prm.block_size) bcount = prm.block_size;
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     const AoScratch<float>& scr = prm.scr;
-    const int nk = scr.nkept[blk];
-    const int ntiles = (nk + 15) / 16;
+    int nk = scr.nkept[blk];
     const float* pbase = scr.panels + static_cast<size_t>(blk) * P * scr.row_stride * kBlockPoints;
     const int* kept = scr.kept + static_cast<size_t>(blk) * scr.row_stride;
 
@@ -279,12 +278,18 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
     // while most rows are added and the largest terms come last.  The
     // tensor-core accumulation truncates, and its error grows with the
     // magnitude of the accumulator at each step.
+    // Rows whose block maximum is not above the screening threshold are left
+    // out here (src/ao_screening.hpp:35-50 on the FP32 panels; threshold 0
+    // keeps every row).
     const bool sorted = scr.rowmax != nullptr && nk <= kSortCap;
     if (sorted) {
-        const float* rmax = scr.rowmax + static_cast<size_t>(blk) * scr.row_stride;
+        const float4* rmax = reinterpret_cast<const float4*>(scr.rowmax + static_cast<size_t>(blk) * scr.row_stride * 4);
         for (int k = tid; k < nk; k += kThreads) {
-            const int e = static_cast<int>((__float_as_uint(rmax[k]) >> 23) & 0xffu) - 127 + kBuckets / 2;
-            keys[k] = static_cast<unsigned char>(e < 0 ? 0 : (e >= kBuckets ? kBuckets - 1 : e));
+            const float4 v = rmax[k];
+            const float mx = fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w));
+            const int e = static_cast<int>((__float_as_uint(mx) >> 23) & 0xffu) - 127 + kBuckets / 2;
+            const bool keep = prm.threshold == 0.0f || mx > prm.threshold;
+            keys[k] = keep ? static_cast<unsigned char>(e < 0 ? 0 : (e >= kBuckets ? kBuckets - 1 : e)) : 0xffu;
         }
         __syncthreads();
         int cnt = 0;
@@ -300,6 +305,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
                 bucket_start[b] = run;
                 run += c;
             }
+            bucket_start[kBuckets] = run;
         }
         __syncthreads();
         if (tid < kBuckets && cnt > 0) {
@@ -307,7 +313,9 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
             for (int k = 0; k < nk; ++k)
                 if (keys[k] == tid) perm[pos++] = k;
         }
+        nk = bucket_start[kBuckets];
     }
+    const int ntiles = (nk + 15) / 16;
     tc_fence_before();
     __syncthreads();
     tc_fence_after();

@@ -21,6 +21,7 @@ struct MoChannelTC {
 };
 
 struct ContractMixedParams {
+    // AO rows of the wave's blocks (ao_mixed layout, rowmax with 4 entries per row).
     AoScratch<float> scr;
     long long first_point = 0;
     long long block_size = 128;
@@ -33,6 +34,7 @@ struct ContractMixedParams {
     int ncols = 16;       // MO columns per pass (multiple of 16, npanel * ncols <= 512)
     int groups = 1;       // accumulator groups (K steps round-robin), groups * npanel * ncols <= 512
     int tmem_cols = 32;   // power of two >= groups * npanel * ncols
+    float threshold = 0.0f;      // screening threshold on the rows' block maxima
     FieldSpec spec;
     unsigned* status = nullptr;  // set nonzero if a pipeline wait ran out
 };

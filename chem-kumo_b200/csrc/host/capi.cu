@@ -116,7 +116,7 @@ struct DevBuf {
 };
 
 template <typename T>
-void run_ao_build(const detail::DeviceMolecule& d, const kumo_dev::PointSource& src, long long block_size, int nblocks,
+[[maybe_unused]] void run_ao_build(const detail::DeviceMolecule& d, const kumo_dev::PointSource& src, long long block_size, int nblocks,
                   int order, int npanel, double threshold, kumo_dev::AoScratch<T> out, long long first_point) {
     kumo_dev::AoBuildParams<T> p{};
     p.basis = d.basis;
@@ -340,12 +340,31 @@ int kumo_ao_panels(const kumo_molecule* m, const double* points, int npts, int o
                                  {panels.as<double>(), kept.as<int>(), nkept.as<int>(), nao, npanel}, 0);
             detail::check_cuda(cudaMemcpy(host.data(), panels.as<double>(), sizeof(double) * cells, cudaMemcpyDeviceToHost), "cudaMemcpy");
         } else {
-            DevBuf panels(sizeof(float) * cells);
-            run_ao_build<float>(d, src, npts, 1, order, npanel, 0.0,
-                                {panels.as<float>(), kept.as<int>(), nkept.as<int>(), nao, npanel}, 0);
+            // Mixed-form AO build: rows of the AO blocks within reach, kept[row] = AO index.
+            DevBuf panels(sizeof(float) * cells), rowmax(sizeof(float) * 4 * nao);
+            kumo_dev::AoMixedParams p{};
+            p.basis = d.basis;
+            p.prims = d.mix_prims;
+            p.src = src;
+            p.block_size = npts;
+            p.nblocks = 1;
+            std::memcpy(p.tpure, d.tpure_g, sizeof p.tpure);
+            std::memcpy(p.gcart, d.gcart, sizeof p.gcart);
+            p.out = {panels.as<float>(), kept.as<int>(), nkept.as<int>(), nao, npanel, rowmax.as<float>()};
+            kumo_dev::launch_ao_mixed(p, npanel, nullptr);
+            detail::check_cuda(cudaGetLastError(), "ao_mixed launch");
             std::vector<float> hf(cells);
+            std::vector<int> rows(static_cast<std::size_t>(nao));
+            int nrows = 0;
             detail::check_cuda(cudaMemcpy(hf.data(), panels.as<float>(), sizeof(float) * cells, cudaMemcpyDeviceToHost), "cudaMemcpy");
-            std::copy(hf.begin(), hf.end(), host.begin());
+            detail::check_cuda(cudaMemcpy(&nrows, nkept.as<int>(), sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy");
+            detail::check_cuda(cudaMemcpy(rows.data(), kept.as<int>(), sizeof(int) * nao, cudaMemcpyDeviceToHost), "cudaMemcpy");
+            std::fill(host.begin(), host.end(), 0.0);
+            for (int c = 0; c < npanel; ++c)
+                for (int r = 0; r < nrows; ++r)
+                    for (int j = 0; j < kumo_dev::kBlockPoints; ++j)
+                        host[(static_cast<std::size_t>(c) * nao + rows[r]) * kumo_dev::kBlockPoints + j] =
+                            hf[(static_cast<std::size_t>(c) * nao + r) * kumo_dev::kBlockPoints + j];
         }
         // scratch [c][ao][point] -> out column-major nao x (panels * npts)
         for (int c = 0; c < npanel; ++c)

@@ -79,6 +79,32 @@ DeviceMolecule::DeviceMolecule(const Molecule& m) {
         max_count = std::max(max_count, static_cast<int>(b.count));
     }
     std::vector<float> exps_f(exps.begin(), exps.end()), weights_f(weights.begin(), weights.end());
+    // g_k = ((2x-1)!!(2y-1)!!(2z-1)!!)^(-1/2) of each Cartesian component; the
+    // first component of every order (x^l, or z^l for l >= 4) has g = ((2l-1)!!)^(-1/2).
+    auto odd_df = [](int n) {
+        double r = 1.0;
+        for (int k = n; k > 1; k -= 2) r *= k;
+        return r;
+    };
+    std::vector<kumo_dev::MixPrim> mix(exps.size());
+    for (const auto& b : blocks) {
+        const auto& pw = b.powers;
+        const double g0 = 1.0 / std::sqrt(odd_df(2 * pw[0].x - 1) * odd_df(2 * pw[0].y - 1) * odd_df(2 * pw[0].z - 1));
+        const std::size_t np = b.exponents.size();
+        const std::size_t first = static_cast<std::size_t>(&b - blocks.data());
+        const std::size_t p0 = static_cast<std::size_t>(info[first].y);
+        for (std::size_t p = 0; p < np; ++p) {
+            const double a = b.exponents[p];
+            mix[p0 + p] = {a * 1.4426950408889634, static_cast<float>(a), static_cast<float>(b.weights[p] / g0)};
+        }
+    }
+    mix_prims = upload(mix.data(), mix.size());
+    for (int l = 0; l <= kumo_dev::kMaxL; ++l) {
+        const auto cart = gaussian_cartesian_order(l);
+        for (std::size_t k = 0; k < cart.size(); ++k)
+            gcart[l][k] = static_cast<float>(
+                1.0 / std::sqrt(odd_df(2 * cart[k].x - 1) * odd_df(2 * cart[k].y - 1) * odd_df(2 * cart[k].z - 1)));
+    }
     basis.nblocks = static_cast<int>(blocks.size());
     basis.nao = static_cast<int>(n);
     basis.max_l = max_l;
@@ -95,6 +121,11 @@ DeviceMolecule::DeviceMolecule(const Molecule& m) {
             for (std::size_t c = 0; c < t.cols(); ++c) {
                 pure_d[l - 2][r * t.cols() + c] = t(r, c);
                 pure_f[l - 2][r * t.cols() + c] = static_cast<float>(t(r, c));
+                tpure_g[l - 2][r * t.cols() + c] = static_cast<float>(t(r, c) * gcart[l][c]);
+                // The mixed AO kernel skips the entries this predicate calls zero.
+                const auto cart = gaussian_cartesian_order(l);
+                if (t(r, c) != 0.0 && !kumo_dev::solid_harmonic_nonzero(l, static_cast<int>(r), cart[c].x, cart[c].y))
+                    throw std::logic_error("Cartesian-to-pure pattern mismatch");
             }
     }
     const Matrix pt = m.density_matrix(DensityComponent::Total);

@@ -10,6 +10,7 @@
 #include <string>
 #include <vector>
 
+#include "../cuda/ao_mixed.cuh"
 #include "../cuda/kumo_device.cuh"
 
 namespace chem::kumo::detail {
@@ -25,6 +26,11 @@ struct DeviceMolecule {
     kumo_dev::DevBasis basis;
     double pure_d[3][135] = {};
     float pure_f[3][135] = {};
+    // Mixed-form AO build: per primitive a log2(e), a and the radial factor u
+    // (weights = u_p g_k), T[m][k] g_k for pure blocks, g_k for Cartesian ones.
+    kumo_dev::MixPrim* mix_prims = nullptr;
+    float tpure_g[3][135] = {};
+    float gcart[5][15] = {};
     double* p_total = nullptr;  // n x n
     double* p_spin = nullptr;
     // Occupied MOs transposed [AO][MO], rows padded to a multiple of 4.

@@ -360,14 +360,19 @@ private:
         const int nao = dev_->basis.nao;
         const int stride = (nao + 7) / 8 * 8;
         const std::size_t per_block = sizeof(float) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints +
-                                      sizeof(int) * ((std::size_t)stride + 1) + sizeof(float) * (std::size_t)stride;
+                                      sizeof(int) * ((std::size_t)stride + 1) + sizeof(float) * 4 * (std::size_t)stride;
         const int W = wave_blocks(nblocks, per_block);
         DeviceAlloc panels(sizeof(float) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints * W, stream_);
         DeviceAlloc kept(sizeof(int) * (std::size_t)stride * W, stream_);
         DeviceAlloc nkept(sizeof(int) * (std::size_t)W, stream_);
-        kumo_dev::AoBuildParams<float> bp = build_params<float>(opt_.screening_threshold);
+        DeviceAlloc rowmax(sizeof(float) * 4 * (std::size_t)stride * W, stream_);
+        kumo_dev::AoMixedParams bp{};
+        bp.basis = dev_->basis;
+        bp.prims = dev_->mix_prims;
+        bp.src = src_;
         bp.block_size = static_cast<long long>(bs);
-        DeviceAlloc rowmax(sizeof(float) * (std::size_t)stride * W, stream_);
+        std::memcpy(bp.tpure, dev_->tpure_g, sizeof bp.tpure);
+        std::memcpy(bp.gcart, dev_->gcart, sizeof bp.gcart);
         bp.out = {panels.as<float>(), kept.as<int>(), nkept.as<int>(), stride, npanel, rowmax.as<float>()};
         kumo_dev::ContractMixedParams cp{};
         cp.scr = bp.out;
@@ -386,6 +391,7 @@ private:
         }
         kumo_dev::mixed_columns(npanel, nocc16, cp.ncols, cp.groups, cp.tmem_cols);
         cp.status = kumo_dev::pipeline_status_word();
+        cp.threshold = static_cast<float>(opt_.screening_threshold);
         cp.beta_is_alpha = bia;
         cp.ao_order = ao_order;
         cp.spec = spec;
@@ -394,7 +400,7 @@ private:
             bp.first_point = static_cast<long long>(b0 * bs);
             bp.nblocks = nb;
             int tok = detail::profile_begin(detail::kProfAoBuild, stream_);
-            kumo_dev::launch_ao_build<float>(bp, ao_order, npanel, stream_);
+            kumo_dev::launch_ao_mixed(bp, npanel, stream_);
             detail::profile_end(tok, stream_);
             cp.first_point = bp.first_point;
             cp.nblocks = nb;

@@ -56,6 +56,22 @@ def test_ao_panels_fp64(name):
         assert np.array_equal(g == 0.0, r == 0.0)  # cutoff zeros identical
 
 
+@pytest.mark.parametrize("name", ["o2.fchk.gz", "h2o_b3lyp_def2tzvp.fchk.gz", "acrolein.fchk.gz"])
+def test_ao_panels_mixed_fp32(name):
+    # FP32 AO build of the mixed form (factorised radial sums): each panel row
+    # within FP32 accuracy of the oracle's FP64 values, relative to the row's
+    # largest magnitude; cutoff zeros identical.
+    m, o = _pair(os.path.join(GOLDEN, name))
+    pts = _box_points(o.atom_xyz.reshape(-1, 3), 128, 3)
+    for order in (0, 1, 2):
+        g = m.ao_panels(pts, order, precision=1)
+        r = o.ao_values(pts)[None] if order == 0 else o.ao_derivatives(pts, order)
+        scale = np.maximum(np.abs(r).max(axis=2, keepdims=True), 1e-300)
+        assert np.max(np.abs(g - r) / scale) < 2e-6, (order, np.max(np.abs(g - r) / scale))
+        assert np.all(g[r == 0.0] == 0.0)  # cutoff zeros stay exact zeros
+        assert np.all(np.abs(r[(g == 0.0) & (r != 0.0)]) < 1e-30)  # FP32 underflow only
+
+
 @pytest.mark.parametrize("order,thr", [(0, 1e-12), (1, 1e-12), (2, 1e-12), (2, 1e-3), (2, 0.0)])
 def test_screening_masks_bit_exact(order, thr):
     path = os.path.join(GOLDEN, "acrolein.fchk.gz")
