@@ -2,6 +2,7 @@
 #include "kumo_b200.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -10,6 +11,8 @@
 #include <vector>
 
 #include "../cuda/esp.cuh"
+#include "../cuda/mixed.cuh"
+#include "grid_geometry.hpp"
 #include "chem/kumo/evaluator.hpp"
 #include "device_state.hpp"
 #include "profile.hpp"
@@ -96,13 +99,46 @@ Request to_request(const kumo_property* props, int n) {
     return r;
 }
 
-void copy_results(const Results& res, const Request& req, double* const* outputs, std::size_t n) {
+// Evaluation into the caller's host arrays: device outputs from the
+// stream-ordered pool, the device evaluation, then one device-to-host copy per
+// property straight into the caller's array (no intermediate host copies;
+// with page-locked caller arrays the copies run at full link speed).
+template <typename Launch>
+Backend evaluate_to_host(const Request& req, std::size_t n, double* const* outputs, Precision precision,
+                         Launch&& launch) {
     const auto& props = req.properties();
+    std::vector<std::size_t> count(props.size());
+    std::size_t total = 0;
     for (std::size_t i = 0; i < props.size(); ++i) {
-        const auto& f = res.get(props[i]);
-        for (std::size_t c = 0; c < f.components.size(); ++c)
-            std::copy(f.components[c].begin(), f.components[c].end(), outputs[i] + c * n);
+        count[i] = property_channels(props[i].kind) * n;
+        total += count[i];
     }
+    void* dev = nullptr;
+    if (total) detail::check_cuda(cudaMallocAsync(&dev, sizeof(double) * total, nullptr), "cudaMallocAsync (outputs)");
+    struct Free {
+        void* p;
+        ~Free() {
+            if (p) cudaFreeAsync(p, nullptr);
+        }
+    } guard{dev};
+    std::vector<double*> dptr(props.size());
+    std::size_t off = 0;
+    for (std::size_t i = 0; i < props.size(); ++i) {
+        dptr[i] = static_cast<double*>(dev) + off;
+        off += count[i];
+    }
+    if (total)
+        detail::check_cuda(cudaMemsetAsync(dev, 0, sizeof(double) * total, nullptr), "cudaMemsetAsync (outputs)");
+    const Backend used = launch(dptr.data());
+    for (std::size_t i = 0; i < props.size(); ++i)
+        if (count[i])
+            detail::check_cuda(cudaMemcpyAsync(outputs[i], dptr[i], sizeof(double) * count[i], cudaMemcpyDeviceToHost,
+                                               nullptr),
+                               "cudaMemcpyAsync (results)");
+    detail::check_cuda(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize (results)");
+    if (precision == Precision::Mixed && kumo_dev::take_pipeline_status() != 0)
+        throw std::runtime_error("mixed-precision contraction: a tensor-core pipeline wait timed out");
+    return used;
 }
 
 struct DevBuf {
@@ -271,11 +307,14 @@ int kumo_evaluate_grid(const kumo_molecule* m, const kumo_options* opt, const ku
         if (!m) throw std::invalid_argument("null molecule");
         const Grid g = to_grid(grid);
         const Request req = to_request(props, nprops);
-        Evaluator ev(m->mol, to_options(opt));
-        const Results res = ev.evaluate(g, req);
-        if (backend_used) *backend_used = static_cast<int>(res.backend_used());
-        const std::size_t n = static_cast<std::size_t>(g.counts[0]) * g.counts[1] * g.counts[2];
-        copy_results(res, req, outputs, n);
+        const EvaluationOptions o = to_options(opt);
+        Evaluator ev(m->mol, o);
+        const std::size_t n = detail::validated_point_count(g);
+        ev.validate(req);
+        if (!outputs && nprops > 0) throw std::invalid_argument("null outputs");
+        const Backend b = evaluate_to_host(req, n, outputs, o.precision,
+                                           [&](double* const* d) { return ev.evaluate_device(g, req, d, nullptr); });
+        if (backend_used) *backend_used = static_cast<int>(b);
     });
 }
 
@@ -285,10 +324,27 @@ int kumo_evaluate_points(const kumo_molecule* m, const kumo_options* opt, const 
     return guarded(err, errlen, [&] {
         if (!m || npoints < 0 || (npoints > 0 && !points)) throw std::invalid_argument("invalid points");
         const Request req = to_request(props, nprops);
-        Evaluator ev(m->mol, to_options(opt));
-        const Results res = ev.evaluate(Points{points, static_cast<std::size_t>(npoints)}, req);
-        if (backend_used) *backend_used = static_cast<int>(res.backend_used());
-        copy_results(res, req, outputs, static_cast<std::size_t>(npoints));
+        const EvaluationOptions o = to_options(opt);
+        Evaluator ev(m->mol, o);
+        const std::size_t n = static_cast<std::size_t>(npoints);
+        for (std::size_t i = 0; i < 3 * n; ++i)
+            if (!std::isfinite(points[i])) throw std::invalid_argument("evaluation points must be finite");
+        ev.validate(req);
+        if (!outputs && nprops > 0) throw std::invalid_argument("null outputs");
+        void* dpts = nullptr;
+        detail::check_cuda(cudaMallocAsync(&dpts, sizeof(double) * 3 * std::max<std::size_t>(n, 1), nullptr),
+                           "cudaMallocAsync (points)");
+        struct Free {
+            void* p;
+            ~Free() { cudaFreeAsync(p, nullptr); }
+        } guard{dpts};
+        if (n)
+            detail::check_cuda(cudaMemcpyAsync(dpts, points, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, nullptr),
+                               "cudaMemcpyAsync (points)");
+        const Backend b = evaluate_to_host(req, n, outputs, o.precision, [&](double* const* d) {
+            return ev.evaluate_device(Points{static_cast<const double*>(dpts), n}, req, d, nullptr);
+        });
+        if (backend_used) *backend_used = static_cast<int>(b);
     });
 }
 

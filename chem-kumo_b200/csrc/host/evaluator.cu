@@ -706,6 +706,8 @@ Results Evaluator::evaluate(Points points, const Request& request) const {
     return res;
 }
 
+void Evaluator::validate(const Request& request) const { Run run(*this, nullptr, nullptr, 0, request, nullptr); }
+
 Backend Evaluator::evaluate_device(const Grid& grid, const Request& request, double* const* outputs, void* stream) const {
     const std::size_t n = detail::validated_point_count(grid);
     Run run(*this, &grid, nullptr, n, request, static_cast<cudaStream_t>(stream));

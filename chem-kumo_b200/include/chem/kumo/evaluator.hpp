@@ -197,6 +197,10 @@ public:
     /// written on `stream` (a cudaStream_t); returns the backend used.  The
     /// points of evaluate_device(Points) are a device array.
     Backend evaluate_device(const Grid& grid, const Request& request, double* const* outputs, void* stream) const;
+    /// The request checks evaluate() makes before any device work (backend
+    /// eligibility, orbital indices, block size, potential tolerance); throws
+    /// the same exceptions.
+    void validate(const Request& request) const;
     Backend evaluate_device(Points device_points, const Request& request, double* const* outputs,
                             void* stream) const;
 

@@ -386,13 +386,24 @@ class Evaluator:
         self.m = molecule
         self.opt = _options(block_size, backend, threshold, potential_tolerance, precision)
 
-    def _outs(self, props, n):
-        outs = [np.zeros((channels(p.kind), n)) for p in props]
+    def _outs(self, props, n, out=None):
+        if out is None:
+            outs = [np.empty((channels(p.kind), n)) for p in props]
+        else:
+            # Caller arrays (e.g. page-locked, reused across calls): C-contiguous float64 of the right size.
+            outs = list(out)
+            if len(outs) != len(props):
+                raise InvalidArgument(1, "one output array per property")
+            for o, p in zip(outs, props):
+                if (not isinstance(o, np.ndarray) or o.dtype != np.float64 or not o.flags["C_CONTIGUOUS"]
+                        or o.size != channels(p.kind) * n):
+                    raise InvalidArgument(1, "output arrays must be C-contiguous float64 of "
+                                          "channels x points elements")
         ptrs = (_D * max(len(props), 1))(*[_dp(o) for o in outs])
         return outs, ptrs
 
-    def evaluate_grid(self, grid: Grid, props: Sequence[Property]) -> Tuple[List[np.ndarray], int]:
-        outs, ptrs = self._outs(props, grid.npoints)
+    def evaluate_grid(self, grid: Grid, props: Sequence[Property], out=None) -> Tuple[List[np.ndarray], int]:
+        outs, ptrs = self._outs(props, grid.npoints, out)
         used = C.c_int()
         e = _err()
         g = grid._c()
@@ -400,9 +411,9 @@ class Evaluator:
                                         C.byref(used), e, 512), e)
         return outs, used.value
 
-    def evaluate_points(self, points: np.ndarray, props: Sequence[Property]) -> Tuple[List[np.ndarray], int]:
+    def evaluate_points(self, points: np.ndarray, props: Sequence[Property], out=None) -> Tuple[List[np.ndarray], int]:
         pts = np.ascontiguousarray(points, dtype=float).reshape(-1, 3)
-        outs, ptrs = self._outs(props, len(pts))
+        outs, ptrs = self._outs(props, len(pts), out)
         used = C.c_int()
         e = _err()
         _check(lib().kumo_evaluate_points(self.m._h, C.byref(self.opt), _dp(pts), len(pts), _props(props),
