@@ -39,6 +39,7 @@ CUDA_UNITS = {
     "csrc/host/capi.cu": [],
     "csrc/host/profile.cu": [],
     "csrc/host/noalloc.cu": [],
+    "csrc/host/server.cu": [],
 }
 CXX_UNITS = [
     "csrc/host/fchk.cpp",

@@ -14,6 +14,7 @@
 #include "../cuda/mixed.cuh"
 #include "grid_geometry.hpp"
 #include "chem/kumo/evaluator.hpp"
+#include "chem/kumo/server.hpp"
 #include "device_state.hpp"
 #include "profile.hpp"
 
@@ -547,6 +548,118 @@ int kumo_profile_read(kumo_profile_entry* out, int max_entries) {
         return -1;
     }
     return n;
+}
+
+
+struct kumo_server {
+    std::unique_ptr<Server> srv;
+};
+
+int kumo_server_create(const kumo_server_options* opt, kumo_server** out, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!out) throw std::invalid_argument("null argument");
+        ServerOptions o;
+        if (opt) {
+            o.device = opt->device;
+            if (opt->hbm_budget_bytes > 0) o.hbm_budget = static_cast<std::size_t>(opt->hbm_budget_bytes);
+            if (opt->max_active > 0) o.max_active = opt->max_active;
+            if (opt->graph_points > 0) o.graph_points = static_cast<std::size_t>(opt->graph_points);
+            if (opt->request_scratch_bytes > 0) o.request_scratch = static_cast<std::size_t>(opt->request_scratch_bytes);
+        }
+        auto s = std::make_unique<kumo_server>();
+        s->srv = std::make_unique<Server>(o);
+        *out = s.release();
+    });
+}
+
+int kumo_server_destroy(kumo_server* server) {
+    if (!server) return KUMO_OK;
+    try {
+        server->srv->drain();
+    } catch (...) {
+    }
+    delete server;
+    return KUMO_OK;
+}
+
+namespace {
+int server_submit(kumo_server* server, const kumo_molecule* m, const kumo_options* opt, const kumo_grid* grid,
+                  const double* points, long long npoints, const kumo_property* props, int nprops,
+                  double* const* outputs, unsigned long long* ticket, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!server || !m || !ticket || (nprops > 0 && !outputs)) throw std::invalid_argument("null argument");
+        ServeRequest r;
+        r.molecule = &m->mol;
+        r.options = to_options(opt);
+        r.request = to_request(props, nprops);
+        if (grid) {
+            r.grid = to_grid(grid);
+        } else {
+            if (npoints < 0 || (npoints > 0 && !points)) throw std::invalid_argument("invalid points");
+            r.points.assign(points, points + 3 * npoints);
+        }
+        r.outputs.assign(outputs, outputs + nprops);
+        *ticket = server->srv->submit(std::move(r));
+    });
+}
+}  // namespace
+
+int kumo_server_submit_grid(kumo_server* server, const kumo_molecule* m, const kumo_options* opt,
+                            const kumo_grid* grid, const kumo_property* props, int nprops,
+                            double* const* outputs, unsigned long long* ticket, char* err, size_t errlen) {
+    if (!grid) return guarded(err, errlen, [] { throw std::invalid_argument("null grid"); });
+    return server_submit(server, m, opt, grid, nullptr, 0, props, nprops, outputs, ticket, err, errlen);
+}
+
+int kumo_server_submit_points(kumo_server* server, const kumo_molecule* m, const kumo_options* opt,
+                              const double* points, long long npoints, const kumo_property* props, int nprops,
+                              double* const* outputs, unsigned long long* ticket, char* err, size_t errlen) {
+    return server_submit(server, m, opt, nullptr, points, npoints, props, nprops, outputs, ticket, err, errlen);
+}
+
+int kumo_server_wait(kumo_server* server, unsigned long long ticket, double timeout_s, int* done, char* err,
+                     size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!server) throw std::invalid_argument("null server");
+        const bool d = server->srv->wait(ticket, timeout_s);
+        if (done) *done = d ? 1 : 0;
+    });
+}
+
+int kumo_server_drain(kumo_server* server, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!server) throw std::invalid_argument("null server");
+        server->srv->drain();
+    });
+}
+
+int kumo_server_stats_get(kumo_server* server, kumo_server_stats* out, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!server || !out) throw std::invalid_argument("null argument");
+        const ServeStats s = server->srv->stats();
+        out->submitted = static_cast<long long>(s.submitted);
+        out->completed = static_cast<long long>(s.completed);
+        out->failed = static_cast<long long>(s.failed);
+        out->points = static_cast<long long>(s.points);
+        out->p50_ms = s.p50_ms;
+        out->p99_ms = s.p99_ms;
+        out->mean_ms = s.mean_ms;
+        out->max_ms = s.max_ms;
+        out->busy_s = s.busy_s;
+        out->points_per_s = s.points_per_s;
+        out->graph_captures = static_cast<long long>(s.graph_captures);
+        out->graph_replays = static_cast<long long>(s.graph_replays);
+        out->direct_runs = static_cast<long long>(s.direct_runs);
+        out->peak_bytes = static_cast<double>(s.peak_bytes);
+        out->budget_bytes = static_cast<double>(s.budget_bytes);
+    });
+}
+
+int kumo_server_reset_stats(kumo_server* server, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!server) throw std::invalid_argument("null server");
+        server->srv->reset_stats();
+    });
 }
 
 }  // extern "C"

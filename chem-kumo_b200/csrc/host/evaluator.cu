@@ -120,6 +120,15 @@ std::size_t scratch_budget() {
 
 }  // namespace
 
+namespace detail {
+// Once-per-device set-up that must not run inside a CUDA stream capture: the
+// pool's release threshold and the tensor-core status word's address.
+void prepare_device_for_capture() {
+    keep_pool_memory();
+    (void)kumo_dev::pipeline_status_word();
+}
+}  // namespace detail
+
 Evaluator::Evaluator(const Molecule& molecule, EvaluationOptions options) : molecule_(&molecule), options_(std::move(options)) {
     if (options_.block_size == 0 || options_.block_size > max_block_size)
         throw std::invalid_argument("evaluation block_size must be in [1, " + std::to_string(max_block_size) + "]");
@@ -225,8 +234,9 @@ private:
     }
 
     // Blocks per wave for a scratch of `per_block` bytes per block.
-    static int wave_blocks(std::size_t total_blocks, std::size_t per_block) {
-        std::size_t w = scratch_budget() / std::max<std::size_t>(per_block, 1);
+    int wave_blocks(std::size_t total_blocks, std::size_t per_block) const {
+        const std::size_t budget = opt_.scratch_bytes ? opt_.scratch_bytes : scratch_budget();
+        std::size_t w = budget / std::max<std::size_t>(per_block, 1);
         w = std::max<std::size_t>(1, std::min(w, total_blocks));
         w = std::min<std::size_t>(w, kumo_dev::kMaxBlocksPerWave);
         return static_cast<int>(w);

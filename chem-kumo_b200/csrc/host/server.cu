@@ -1,0 +1,600 @@
+// Serving loop (see chem/kumo/server.hpp).
+//
+// Threads: the caller's (submit / wait), one scheduler thread that owns every
+// CUDA call of the server (admission, launches, completion polling), and one
+// completion thread that copies results from page-locked staging into the
+// caller's arrays, so that large copies never hold up admission.
+//
+// Admission: FIFO; the head request starts when a slot (stream) is free and
+// the footprint sum of the active requests plus the resident molecule copies
+// stays within the HBM budget.  Footprint of a request: its outputs, its
+// points and its AO scratch (ServerOptions::request_scratch, which also sets
+// its wave size), plus the molecule's device copy when it is not resident yet
+// (molecule copies then stay resident).
+//
+// Graph path (requests of at most graph_points points): the points are padded
+// to a power-of-two bucket (>= 128) by repeating the last point, which leaves
+// the last block's bounding box and screening unchanged; one CUDA graph per
+// (molecule, options, properties, bucket) holds the whole device evaluation
+// between fixed device buffers, with page-locked staging on both sides; a
+// replay is one H2D copy, one graph launch and one D2H copy.  Concurrent
+// requests of the same key use separate graph instances.
+#include "chem/kumo/server.hpp"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <sstream>
+#include <stdexcept>
+#include <unordered_map>
+
+#include "device_state.hpp"
+#include "grid_geometry.hpp"
+
+namespace chem::kumo {
+
+namespace detail {
+void prepare_device_for_capture();
+}
+
+namespace {
+
+using clock_type = std::chrono::steady_clock;
+using detail::check_cuda;
+
+std::size_t round_bucket(std::size_t n) {
+    std::size_t b = 128;
+    while (b < n) b <<= 1;
+    return b;
+}
+
+// Device bytes a molecule's resident copy will take (DeviceMolecule).
+std::size_t molecule_bytes_estimate(const Molecule& m) {
+    const std::size_t n = m.basis_size();
+    const std::size_t nmo = m.orbital_count(SpinChannel::Alpha) + (m.unrestricted() ? m.orbital_count(SpinChannel::Beta) : 0);
+    const std::size_t occ = m.occupied_count(SpinChannel::Alpha) + m.occupied_count(SpinChannel::Beta) + 32;
+    return 2 * n * n * 8 + n * nmo * 8 + n * occ * (8 + 6) + (std::size_t(4) << 20);
+}
+
+// Grid points in the device's arithmetic (point_at: origin + ((s_a i + s_b j) + s_c k)).
+void grid_to_points(const Grid& g, std::vector<double>& pts) {
+    const std::size_t n = detail::validated_point_count(g);
+    pts.resize(3 * n);
+    std::size_t q = 0;
+    for (std::size_t i = 0; i < g.counts[0]; ++i)
+        for (std::size_t j = 0; j < g.counts[1]; ++j)
+            for (std::size_t k = 0; k < g.counts[2]; ++k, ++q)
+                for (int a = 0; a < 3; ++a) {
+                    const double di = static_cast<double>(i), dj = static_cast<double>(j), dk = static_cast<double>(k);
+                    const double t = (g.steps.m[0 + a] * di + g.steps.m[3 + a] * dj) + g.steps.m[6 + a] * dk;
+                    pts[3 * q + a] = g.origin[a] + t;
+                }
+}
+
+struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    double* d_points = nullptr;
+    double* d_out = nullptr;
+    double* h_points = nullptr;  // page-locked
+    double* h_out = nullptr;     // page-locked
+    std::size_t bucket = 0;
+    std::size_t channels = 0;
+    std::atomic<bool> busy{false};  // set by the scheduler, cleared by the completion thread
+    ~GraphEntry() {
+        if (exec) cudaGraphExecDestroy(exec);
+        cudaFree(d_points);
+        cudaFree(d_out);
+        cudaFreeHost(h_points);
+        cudaFreeHost(h_out);
+    }
+};
+
+struct Ticket {
+    bool done = false;
+    std::string error;
+    double latency_ms = 0;
+};
+
+}  // namespace
+
+struct Server::Impl {
+    ServerOptions opt;
+    std::size_t budget = 0;
+
+    mutable std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    bool stop = false;
+
+    struct Pending {
+        std::uint64_t ticket;
+        ServeRequest req;
+        clock_type::time_point t_submit;
+        std::size_t n = 0;
+        std::size_t channels = 0;
+        std::size_t footprint = 0;
+        bool graph = false;
+    };
+    struct Active {
+        Pending p;
+        cudaStream_t stream = nullptr;
+        cudaEvent_t event = nullptr;
+        GraphEntry* entry = nullptr;      // graph path
+        double* stage = nullptr;          // direct path: page-locked results
+        std::size_t stage_bytes = 0;
+        double* pstage = nullptr;         // direct path: page-locked points
+        std::size_t pstage_bytes = 0;
+        std::size_t row = 0;              // row length of the staged results (bucket or n)
+    };
+    std::deque<Pending> queue;
+    std::deque<Active> finished;  // handed to the completion thread
+    std::vector<std::pair<std::size_t, double*>> returned_stage;  // staging back from the completion thread
+    bool stop_completer = false;
+    std::unordered_map<std::uint64_t, Ticket> tickets;
+    std::uint64_t next_ticket = 1;
+
+    // Scheduler-owned state.
+    std::vector<Active> active;
+    std::vector<cudaStream_t> free_streams;
+    std::vector<cudaEvent_t> free_events;
+    std::map<std::string, std::vector<std::unique_ptr<GraphEntry>>> graphs;
+    std::multimap<std::size_t, double*> free_stage;  // page-locked staging by size
+    std::vector<const Molecule*> resident;
+    std::size_t resident_bytes = 0, active_bytes = 0;
+
+    // Statistics (guarded by mu).
+    std::vector<double> latencies;
+    ServeStats st;
+    std::optional<clock_type::time_point> t_first, t_last;
+
+    std::thread scheduler, completer;
+
+    void run_scheduler();
+    void run_completer();
+    void launch(Pending&& p);
+    GraphEntry* graph_for(const Pending& p, cudaStream_t stream);
+    double* get_stage(std::size_t bytes);
+    std::string key_of(const Pending& p) const;
+    void fail(std::uint64_t ticket, const std::string& what, clock_type::time_point t0);
+};
+
+std::string Server::Impl::key_of(const Pending& p) const {
+    std::ostringstream k;
+    const auto& o = p.req.options;
+    k << static_cast<const void*>(p.req.molecule) << '|' << static_cast<int>(o.precision) << '|'
+      << static_cast<int>(o.backend) << '|' << o.screening_threshold << '|' << o.block_size << '|'
+      << o.potential_tolerance << '|' << round_bucket(p.n);
+    for (const auto& q : p.req.request.properties())
+        k << '|' << static_cast<int>(q.kind) << ',' << static_cast<int>(q.component) << ','
+          << static_cast<int>(q.channel) << ',' << q.orbital_index;
+    return k.str();
+}
+
+double* Server::Impl::get_stage(std::size_t bytes) {
+    auto it = free_stage.lower_bound(bytes);
+    if (it != free_stage.end() && it->first <= 2 * bytes) {
+        double* p = it->second;
+        free_stage.erase(it);
+        return p;
+    }
+    void* p = nullptr;
+    check_cuda(cudaHostAlloc(&p, std::max<std::size_t>(bytes, 64), cudaHostAllocDefault), "cudaHostAlloc (staging)");
+    return static_cast<double*>(p);
+}
+
+GraphEntry* Server::Impl::graph_for(const Pending& p, cudaStream_t stream) {
+    auto& list = graphs[key_of(p)];
+    for (auto& e : list)
+        if (!e->busy) {
+            e->busy = true;
+            std::lock_guard<std::mutex> lock(mu);
+            ++st.graph_replays;
+            return e.get();
+        }
+    auto e = std::make_unique<GraphEntry>();
+    e->bucket = round_bucket(p.n);
+    e->channels = p.channels;
+    check_cuda(cudaMalloc(&e->d_points, sizeof(double) * 3 * e->bucket), "cudaMalloc (serving points)");
+    check_cuda(cudaMalloc(&e->d_out, sizeof(double) * std::max<std::size_t>(e->channels * e->bucket, 1)),
+               "cudaMalloc (serving outputs)");
+    check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&e->h_points), sizeof(double) * 3 * e->bucket, cudaHostAllocDefault),
+               "cudaHostAlloc (serving points)");
+    check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&e->h_out),
+                             sizeof(double) * std::max<std::size_t>(e->channels * e->bucket, 1), cudaHostAllocDefault),
+               "cudaHostAlloc (serving outputs)");
+    std::vector<double*> outs;
+    std::size_t off = 0;
+    for (const auto& q : p.req.request.properties()) {
+        outs.push_back(e->d_out + off * e->bucket);
+        off += property_channels(q.kind);
+    }
+    EvaluationOptions o = p.req.options;
+    o.scratch_bytes = opt.request_scratch;
+    o.progress = {};
+    const Evaluator ev(*p.req.molecule, o);
+    cudaGraph_t graph = nullptr;
+    check_cuda(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
+    try {
+        ev.evaluate_device(Points{e->d_points, e->bucket}, p.req.request, outs.data(), stream);
+    } catch (...) {
+        cudaStreamEndCapture(stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+    }
+    check_cuda(cudaStreamEndCapture(stream, &graph), "cudaStreamEndCapture");
+    const cudaError_t ie = cudaGraphInstantiate(&e->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    check_cuda(ie, "cudaGraphInstantiate");
+    e->busy = true;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        ++st.graph_captures;
+    }
+    list.push_back(std::move(e));
+    return list.back().get();
+}
+
+void Server::Impl::fail(std::uint64_t ticket, const std::string& what, clock_type::time_point t0) {
+    std::lock_guard<std::mutex> lock(mu);
+    auto& t = tickets[ticket];
+    t.done = true;
+    t.error = what;
+    t.latency_ms = std::chrono::duration<double, std::milli>(clock_type::now() - t0).count();
+    ++st.failed;
+    cv_done.notify_all();
+}
+
+void Server::Impl::launch(Pending&& p) {
+    Active a;
+    if (free_streams.empty()) {
+        cudaStream_t s;
+        check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+        free_streams.push_back(s);
+    }
+    if (free_events.empty()) {
+        cudaEvent_t e;
+        check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+        free_events.push_back(e);
+    }
+    a.stream = free_streams.back();
+    free_streams.pop_back();
+    a.event = free_events.back();
+    free_events.pop_back();
+    const Molecule& mol = *p.req.molecule;
+    const auto& props = p.req.request.properties();
+    try {
+        if (!mol.device_if_resident()) {
+            (void)mol.device();
+            resident.push_back(&mol);
+            resident_bytes += mol.device_bytes();
+        }
+        if (p.graph) {
+            if (p.req.grid) grid_to_points(*p.req.grid, p.req.points);
+            GraphEntry* e = graph_for(p, a.stream);
+            const std::size_t n = p.n, b = e->bucket;
+            std::memcpy(e->h_points, p.req.points.data(), sizeof(double) * 3 * n);
+            for (std::size_t q = n; q < b; ++q) std::memcpy(e->h_points + 3 * q, e->h_points + 3 * (n - 1), 3 * sizeof(double));
+            check_cuda(cudaMemcpyAsync(e->d_points, e->h_points, sizeof(double) * 3 * b, cudaMemcpyHostToDevice, a.stream),
+                       "cudaMemcpyAsync (serving points)");
+            check_cuda(cudaGraphLaunch(e->exec, a.stream), "cudaGraphLaunch");
+            check_cuda(cudaMemcpyAsync(e->h_out, e->d_out, sizeof(double) * e->channels * b, cudaMemcpyDeviceToHost,
+                                       a.stream),
+                       "cudaMemcpyAsync (serving results)");
+            a.entry = e;
+            a.row = b;
+        } else {
+            EvaluationOptions o = p.req.options;
+            o.scratch_bytes = opt.request_scratch;
+            o.progress = {};
+            const Evaluator ev(mol, o);
+            const std::size_t n = p.n;
+            a.stage_bytes = sizeof(double) * std::max<std::size_t>(p.channels * n, 1);
+            a.stage = get_stage(a.stage_bytes);
+            double* d_out = nullptr;
+            check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&d_out), a.stage_bytes, a.stream), "cudaMallocAsync (outputs)");
+            std::vector<double*> outs;
+            std::size_t off = 0;
+            for (const auto& q : props) {
+                outs.push_back(d_out + off * n);
+                off += property_channels(q.kind);
+            }
+            double* d_pts = nullptr;
+            if (p.req.grid) {
+                ev.evaluate_device(*p.req.grid, p.req.request, outs.data(), a.stream);
+            } else {
+                check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&d_pts), sizeof(double) * 3 * n, a.stream),
+                           "cudaMallocAsync (points)");
+                // Points go up from page-locked staging, held until the request completes.
+                a.pstage_bytes = sizeof(double) * 3 * n;
+                a.pstage = get_stage(a.pstage_bytes);
+                std::memcpy(a.pstage, p.req.points.data(), a.pstage_bytes);
+                check_cuda(cudaMemcpyAsync(d_pts, a.pstage, a.pstage_bytes, cudaMemcpyHostToDevice, a.stream),
+                           "cudaMemcpyAsync (points)");
+                ev.evaluate_device(Points{d_pts, n}, p.req.request, outs.data(), a.stream);
+            }
+            check_cuda(cudaMemcpyAsync(a.stage, d_out, a.stage_bytes, cudaMemcpyDeviceToHost, a.stream),
+                       "cudaMemcpyAsync (results)");
+            cudaFreeAsync(d_out, a.stream);
+            if (d_pts) cudaFreeAsync(d_pts, a.stream);
+            a.row = n;
+            std::lock_guard<std::mutex> lock(mu);
+            ++st.direct_runs;
+        }
+        check_cuda(cudaEventRecord(a.event, a.stream), "cudaEventRecord");
+    } catch (const std::exception& ex) {
+        // Work already queued on the stream may still read the staging: let it finish.
+        cudaStreamSynchronize(a.stream);
+        cudaGetLastError();
+        if (a.entry) a.entry->busy = false;
+        if (a.stage) free_stage.emplace(a.stage_bytes, a.stage);
+        if (a.pstage) free_stage.emplace(a.pstage_bytes, a.pstage);
+        free_streams.push_back(a.stream);
+        free_events.push_back(a.event);
+        active_bytes -= p.footprint;
+        fail(p.ticket, ex.what(), p.t_submit);
+        return;
+    }
+    a.p = std::move(p);
+    active.push_back(std::move(a));
+}
+
+void Server::Impl::run_scheduler() {
+    check_cuda(cudaSetDevice(opt.device), "cudaSetDevice");
+    detail::prepare_device_for_capture();
+    for (;;) {
+        bool progressed = false;
+        // Completed device work goes to the completion thread.
+        for (std::size_t i = 0; i < active.size();) {
+            const cudaError_t q = cudaEventQuery(active[i].event);
+            if (q == cudaErrorNotReady) {
+                ++i;
+                continue;
+            }
+            Active a = std::move(active[i]);
+            active.erase(active.begin() + static_cast<std::ptrdiff_t>(i));
+            active_bytes -= a.p.footprint;
+            free_streams.push_back(a.stream);
+            free_events.push_back(a.event);
+            progressed = true;
+            if (a.pstage) {
+                free_stage.emplace(a.pstage_bytes, a.pstage);
+                a.pstage = nullptr;
+            }
+            if (q != cudaSuccess) {
+                cudaGetLastError();
+                if (a.entry) a.entry->busy = false;
+                if (a.stage) free_stage.emplace(a.stage_bytes, a.stage);
+                fail(a.p.ticket, std::string("CUDA error: ") + cudaGetErrorString(q), a.p.t_submit);
+                continue;
+            }
+            std::lock_guard<std::mutex> lock(mu);
+            finished.push_back(std::move(a));
+            cv_work.notify_all();
+        }
+        {
+            std::unique_lock<std::mutex> lock(mu);
+            // Staging returned by the completion thread.
+            for (const auto& [bytes, ptr] : returned_stage) free_stage.emplace(bytes, ptr);
+            returned_stage.clear();
+            // Admission, in arrival order.
+            while (!queue.empty() && static_cast<int>(active.size()) < opt.max_active) {
+                Pending& head = queue.front();
+                const bool resident_now = head.req.molecule->device_if_resident() != nullptr;
+                const std::size_t need = head.footprint + (resident_now ? 0 : molecule_bytes_estimate(*head.req.molecule));
+                if (!active.empty() && resident_bytes + active_bytes + need > budget) break;
+                Pending p = std::move(head);
+                queue.pop_front();
+                lock.unlock();
+                active_bytes += p.footprint;
+                launch(std::move(p));
+                progressed = true;
+                lock.lock();
+                st.peak_bytes = std::max(st.peak_bytes, resident_bytes + active_bytes);
+            }
+            if (stop && queue.empty() && active.empty()) break;
+            if (!progressed) {
+                if (active.empty())
+                    cv_work.wait_for(lock, std::chrono::milliseconds(50));
+                else
+                    cv_work.wait_for(lock, std::chrono::microseconds(100));
+            }
+        }
+    }
+}
+
+void Server::Impl::run_completer() {
+    check_cuda(cudaSetDevice(opt.device), "cudaSetDevice");
+    for (;;) {
+        Active a;
+        {
+            std::unique_lock<std::mutex> lock(mu);
+            cv_work.wait(lock, [&] { return stop_completer || !finished.empty(); });
+            if (finished.empty()) return;
+            a = std::move(finished.front());
+            finished.pop_front();
+        }
+        const double* src = a.entry ? a.entry->h_out : a.stage;
+        const auto& props = a.p.req.request.properties();
+        std::size_t off = 0;
+        for (std::size_t i = 0; i < props.size(); ++i) {
+            const std::size_t ch = property_channels(props[i].kind);
+            for (std::size_t c = 0; c < ch; ++c)
+                std::memcpy(a.p.req.outputs[i] + c * a.p.n, src + (off + c) * a.row, sizeof(double) * a.p.n);
+            off += ch;
+        }
+        const auto now = clock_type::now();
+        std::lock_guard<std::mutex> lock(mu);
+        if (a.entry) a.entry->busy = false;
+        if (a.stage) returned_stage.emplace_back(a.stage_bytes, a.stage);
+        auto& t = tickets[a.p.ticket];
+        t.done = true;
+        t.latency_ms = std::chrono::duration<double, std::milli>(now - a.p.t_submit).count();
+        latencies.push_back(t.latency_ms);
+        ++st.completed;
+        st.points += a.p.n;
+        t_last = now;
+        cv_done.notify_all();
+        cv_work.notify_all();
+    }
+}
+
+}  // namespace chem::kumo
+
+namespace chem::kumo {
+
+Server::Server(ServerOptions options) : impl_(std::make_unique<Impl>()) {
+    Impl& m = *impl_;
+    m.opt = options;
+    if (m.opt.max_active < 1) throw std::invalid_argument("max_active must be at least 1");
+    check_cuda(cudaSetDevice(m.opt.device), "cudaSetDevice");
+    std::size_t free_b = 0, total_b = 0;
+    check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    const std::size_t cap = static_cast<std::size_t>(0.9 * static_cast<double>(free_b));
+    m.budget = m.opt.hbm_budget ? std::min(m.opt.hbm_budget, cap) : std::min<std::size_t>(150ull * 1000 * 1000 * 1000, cap);
+    m.st.budget_bytes = m.budget;
+    m.scheduler = std::thread([&m] {
+        try {
+            m.run_scheduler();
+        } catch (const std::exception& e) {
+            std::lock_guard<std::mutex> lock(m.mu);
+            for (auto& p : m.queue) {
+                auto& t = m.tickets[p.ticket];
+                t.done = true;
+                t.error = std::string("serving loop stopped: ") + e.what();
+            }
+            m.queue.clear();
+            m.cv_done.notify_all();
+        }
+    });
+    m.completer = std::thread([&m] { m.run_completer(); });
+}
+
+Server::~Server() {
+    Impl& m = *impl_;
+    {
+        std::lock_guard<std::mutex> lock(m.mu);
+        m.stop = true;
+        m.cv_work.notify_all();
+    }
+    if (m.scheduler.joinable()) m.scheduler.join();
+    {
+        std::lock_guard<std::mutex> lock(m.mu);
+        m.stop_completer = true;
+        m.cv_work.notify_all();
+    }
+    if (m.completer.joinable()) m.completer.join();
+    cudaSetDevice(m.opt.device);
+    cudaDeviceSynchronize();
+    m.graphs.clear();
+    for (auto& [b, p] : m.free_stage) cudaFreeHost(p);
+    for (auto& [b, p] : m.returned_stage) cudaFreeHost(p);
+    for (auto s : m.free_streams) cudaStreamDestroy(s);
+    for (auto e : m.free_events) cudaEventDestroy(e);
+}
+
+std::uint64_t Server::submit(ServeRequest r) {
+    Impl& m = *impl_;
+    if (!r.molecule) throw std::invalid_argument("serving request without a molecule");
+    const Evaluator ev(*r.molecule, r.options);  // option checks
+    ev.validate(r.request);
+    Impl::Pending p;
+    if (r.grid) {
+        p.n = detail::validated_point_count(*r.grid);
+    } else {
+        if (r.points.size() % 3) throw std::invalid_argument("points must hold 3 coordinates per point");
+        p.n = r.points.size() / 3;
+        for (double x : r.points)
+            if (!std::isfinite(x)) throw std::invalid_argument("evaluation points must be finite");
+    }
+    const auto& props = r.request.properties();
+    if (r.outputs.size() != props.size()) throw std::invalid_argument("one output array per property");
+    for (double* o : r.outputs)
+        if (!o && p.n) throw std::invalid_argument("null output array");
+    for (const auto& q : props) p.channels += property_channels(q.kind);
+    bool esp = false;
+    for (const auto& q : props) esp |= q.kind == PropertyKind::ElectrostaticPotential;
+    p.graph = p.n > 0 && p.n <= m.opt.graph_points && !esp;
+    const std::size_t rows = p.graph ? round_bucket(p.n) : p.n;
+    const std::size_t nblocks = (rows + 127) / 128;
+    const std::size_t per_block = 10 * r.molecule->basis_size() * 128 * 8 + 8 * r.molecule->basis_size();
+    p.footprint = p.channels * rows * 8 + 3 * rows * 8 + std::min(m.opt.request_scratch, nblocks * per_block) +
+                  (std::size_t(8) << 20);
+    if (p.footprint > m.budget) throw std::invalid_argument("request exceeds the serving HBM budget");
+    p.req = std::move(r);
+    p.t_submit = clock_type::now();
+    std::lock_guard<std::mutex> lock(m.mu);
+    p.ticket = m.next_ticket++;
+    m.tickets[p.ticket] = {};
+    ++m.st.submitted;
+    if (!m.t_first) m.t_first = p.t_submit;
+    const std::uint64_t t = p.ticket;
+    m.queue.push_back(std::move(p));
+    m.cv_work.notify_all();
+    return t;
+}
+
+bool Server::wait(std::uint64_t ticket, double timeout_s) {
+    Impl& m = *impl_;
+    std::unique_lock<std::mutex> lock(m.mu);
+    auto it = m.tickets.find(ticket);
+    if (it == m.tickets.end()) throw std::invalid_argument("unknown serving ticket");
+    const auto deadline = clock_type::now() + std::chrono::duration_cast<clock_type::duration>(
+                                                  std::chrono::duration<double>(std::max(0.0, timeout_s)));
+    m.cv_done.wait_until(lock, deadline, [&] { return m.tickets[ticket].done; });
+    const Ticket& t = m.tickets[ticket];
+    if (!t.done) return false;
+    if (!t.error.empty()) throw std::runtime_error(t.error);
+    return true;
+}
+
+void Server::drain() {
+    Impl& m = *impl_;
+    std::unique_lock<std::mutex> lock(m.mu);
+    m.cv_done.wait(lock, [&] {
+        for (const auto& [k, t] : m.tickets)
+            if (!t.done) return false;
+        return true;
+    });
+}
+
+ServeStats Server::stats() const {
+    const Impl& m = *impl_;
+    std::lock_guard<std::mutex> lock(m.mu);
+    ServeStats s = m.st;
+    std::vector<double> l = m.latencies;
+    if (!l.empty()) {
+        std::sort(l.begin(), l.end());
+        auto pct = [&](double q) {
+            const double pos = q * static_cast<double>(l.size() - 1);
+            const std::size_t i = static_cast<std::size_t>(pos);
+            const double f = pos - static_cast<double>(i);
+            return i + 1 < l.size() ? l[i] * (1 - f) + l[i + 1] * f : l[i];
+        };
+        s.p50_ms = pct(0.5);
+        s.p99_ms = pct(0.99);
+        double sum = 0;
+        for (double x : l) sum += x;
+        s.mean_ms = sum / static_cast<double>(l.size());
+        s.max_ms = l.back();
+    }
+    if (m.t_first && m.t_last) {
+        s.busy_s = std::chrono::duration<double>(*m.t_last - *m.t_first).count();
+        if (s.busy_s > 0) s.points_per_s = static_cast<double>(s.points) / s.busy_s;
+    }
+    return s;
+}
+
+void Server::reset_stats() {
+    Impl& m = *impl_;
+    std::lock_guard<std::mutex> lock(m.mu);
+    m.latencies.clear();
+    const std::size_t budget = m.st.budget_bytes;
+    m.st = ServeStats{};
+    m.st.budget_bytes = budget;
+    m.t_first.reset();
+    m.t_last.reset();
+}
+
+}  // namespace chem::kumo

@@ -160,6 +160,10 @@ struct EvaluationOptions {
     double fukui_delta = 0.1;
     ProgressCallback progress = {};
     Precision precision = Precision::FP64;
+    /// Device scratch (AO panels) of one evaluation, which sets how many
+    /// point blocks run per wave; 0 = 4 GiB (or KUMO_SCRATCH_MB).  The
+    /// serving loop sets it per request for its HBM admission.
+    std::size_t scratch_bytes = 0;
 };
 
 struct PropertyField {

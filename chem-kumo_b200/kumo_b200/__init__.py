@@ -154,8 +154,23 @@ EXPORTS = [
     "kumo_evaluate_points", "kumo_evaluate_grid_device", "kumo_evaluate_points_device", "kumo_ao_panels",
     "kumo_screening_masks", "kumo_boys", "kumo_esp_pair_count", "kumo_write_cube", "kumo_grid_around",
     "kumo_profile_enable", "kumo_profile_reset", "kumo_profile_read", "kumo_set_device",
-    "kumo_evaluate_points_noalloc",
+    "kumo_evaluate_points_noalloc", "kumo_server_create", "kumo_server_destroy", "kumo_server_submit_grid",
+    "kumo_server_submit_points", "kumo_server_wait", "kumo_server_drain", "kumo_server_stats_get",
+    "kumo_server_reset_stats",
 ]
+
+
+class _ServerOptions(C.Structure):
+    _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_double), ("max_active", C.c_int),
+                ("graph_points", C.c_longlong), ("request_scratch_bytes", C.c_double)]
+
+
+class _ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("failed", C.c_longlong),
+                ("points", C.c_longlong), ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
+                ("max_ms", C.c_double), ("busy_s", C.c_double), ("points_per_s", C.c_double),
+                ("graph_captures", C.c_longlong), ("graph_replays", C.c_longlong), ("direct_runs", C.c_longlong),
+                ("peak_bytes", C.c_double), ("budget_bytes", C.c_double)]
 
 
 class _ProfileEntry(C.Structure):
@@ -201,6 +216,18 @@ def lib():
         L.kumo_evaluate_points_noalloc.argtypes = [C.c_void_p, C.POINTER(_Options), _D, C.c_longlong,
                                                    C.POINTER(_Property), C.c_int, C.POINTER(_D), C.c_void_p, *eb]
         L.kumo_profile_read.argtypes = [C.POINTER(_ProfileEntry), C.c_int]
+        L.kumo_server_create.argtypes = [C.POINTER(_ServerOptions), C.POINTER(C.c_void_p), *eb]
+        L.kumo_server_destroy.argtypes = [C.c_void_p]
+        L.kumo_server_submit_grid.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(_Options), C.POINTER(_Grid),
+                                              C.POINTER(_Property), C.c_int, C.POINTER(_D),
+                                              C.POINTER(C.c_ulonglong), *eb]
+        L.kumo_server_submit_points.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(_Options), _D, C.c_longlong,
+                                                C.POINTER(_Property), C.c_int, C.POINTER(_D),
+                                                C.POINTER(C.c_ulonglong), *eb]
+        L.kumo_server_wait.argtypes = [C.c_void_p, C.c_ulonglong, C.c_double, _I, *eb]
+        L.kumo_server_drain.argtypes = [C.c_void_p, *eb]
+        L.kumo_server_stats_get.argtypes = [C.c_void_p, C.POINTER(_ServerStats), *eb]
+        L.kumo_server_reset_stats.argtypes = [C.c_void_p, *eb]
         _lib = L
     return _lib
 
@@ -499,3 +526,80 @@ def profile_read() -> Dict[str, Dict[str, float]]:
     return {arr[i].name.decode(): {"launches": arr[i].launches, "ms": arr[i].ms, "kept_rows": arr[i].kept_rows,
                                    "units": arr[i].units, "flops": arr[i].flops, "bytes": arr[i].bytes}
             for i in range(n)}
+
+
+class Server:
+    """Serving loop (kumo_server_*): requests of any molecules and sizes are
+    admitted in arrival order under an HBM budget and run concurrently on the
+    GPU; small ones replay captured CUDA graphs.  submit_* returns a ticket and
+    the output arrays the results will be written to; the molecule and the
+    arrays must stay alive until wait() reports the ticket done."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: float = 0.0, max_active: int = 0,
+                 graph_points: int = 0, request_scratch_bytes: float = 0.0):
+        o = _ServerOptions(int(device), float(hbm_budget_bytes), int(max_active), int(graph_points),
+                           float(request_scratch_bytes))
+        h = C.c_void_p()
+        e = _err()
+        _check(lib().kumo_server_create(C.byref(o), C.byref(h), e, 512), e)
+        self._h = h
+        self._keep: Dict[int, tuple] = {}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().kumo_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        self.close()
+
+    def _submit(self, molecule: "Molecule", props, n, evaluator_opts, grid=None, points=None, out=None):
+        outs = [np.empty((channels(p.kind), n)) for p in props] if out is None else list(out)
+        for o, p in zip(outs, props):
+            if o.dtype != np.float64 or not o.flags["C_CONTIGUOUS"] or o.size != channels(p.kind) * n:
+                raise InvalidArgument(1, "output arrays must be C-contiguous float64 of channels x points elements")
+        ptrs = (_D * max(len(props), 1))(*[_dp(o) for o in outs])
+        t = C.c_ulonglong()
+        e = _err()
+        opt = _options(**evaluator_opts)
+        if grid is not None:
+            g = grid._c()
+            _check(lib().kumo_server_submit_grid(self._h, molecule._h, C.byref(opt), C.byref(g), _props(props),
+                                                 len(props), ptrs, C.byref(t), e, 512), e)
+        else:
+            pts = np.ascontiguousarray(points, dtype=float).reshape(-1, 3)
+            _check(lib().kumo_server_submit_points(self._h, molecule._h, C.byref(opt), _dp(pts), len(pts),
+                                                   _props(props), len(props), ptrs, C.byref(t), e, 512), e)
+        self._keep[t.value] = (molecule, outs)
+        return t.value, outs
+
+    def submit_grid(self, molecule: "Molecule", grid: Grid, props: Sequence[Property], out=None, **opts):
+        return self._submit(molecule, props, grid.npoints, opts, grid=grid, out=out)
+
+    def submit_points(self, molecule: "Molecule", points: np.ndarray, props: Sequence[Property], out=None, **opts):
+        n = np.asarray(points).size // 3
+        return self._submit(molecule, props, n, opts, points=points, out=out)
+
+    def wait(self, ticket: int, timeout: float = 60.0) -> bool:
+        done = C.c_int()
+        e = _err()
+        _check(lib().kumo_server_wait(self._h, ticket, float(timeout), C.byref(done), e, 512), e)
+        if done.value:
+            self._keep.pop(ticket, None)
+        return bool(done.value)
+
+    def drain(self) -> None:
+        e = _err()
+        _check(lib().kumo_server_drain(self._h, e, 512), e)
+        self._keep.clear()
+
+    def stats(self) -> Dict[str, float]:
+        s = _ServerStats()
+        e = _err()
+        _check(lib().kumo_server_stats_get(self._h, C.byref(s), e, 512), e)
+        return {name: getattr(s, name) for name, _ in _ServerStats._fields_}
+
+    def reset_stats(self) -> None:
+        e = _err()
+        _check(lib().kumo_server_reset_stats(self._h, e, 512), e)

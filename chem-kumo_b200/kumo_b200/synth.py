@@ -365,6 +365,11 @@ WORKLOADS = {
                         grid_n=128, spacing=0.2),
     "triplet_3700": dict(make=lambda: organic("triplet_3700", {"C": 60, "N": 20, "O": 20, "H": 100}, 2,
                                               28.0, multiplicity=3), grid_n=192, spacing=0.17),
+    # Scaled-down unrestricted triplet (same generator, seed and basis as
+    # triplet_3700; 370 AOs, 39 alpha / 37 beta electrons) for parity tests
+    # that the CPU oracle finishes in seconds.
+    "triplet_370": dict(make=lambda: organic("triplet_370", {"C": 6, "N": 2, "O": 2, "H": 10}, 2,
+                                             14.0, multiplicity=3), grid_n=96, spacing=0.17),
     # C30N3O3H24 has an odd electron count; the closed-shell molecule is its cation.
     "esp_1260": dict(make=lambda: organic("esp_1260", {"C": 30, "N": 3, "O": 3, "H": 24}, 3, 15.0,
                                           charge=1), grid_n=96, spacing=0.24),

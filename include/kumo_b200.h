@@ -216,6 +216,53 @@ void kumo_profile_reset(void);
 /* Synchronizes and returns the number of entries written (<= max_entries). */
 int kumo_profile_read(kumo_profile_entry* out, int max_entries);
 
+/* ---- Serving loop (new: chem-kumo has no serving counterpart) -----------
+ * A server queues evaluation requests of any molecules and sizes, admits them
+ * in arrival order while their device-memory footprint fits an HBM budget and
+ * one of max_active slots (CUDA streams) is free, and runs the admitted ones
+ * concurrently so that their kernels overlap on the GPU; requests of at most
+ * graph_points points replay CUDA graphs captured per (molecule, options,
+ * properties, point bucket).  Results go to the caller's host arrays (which,
+ * like the molecule, must stay valid until the request is done); latency runs
+ * from submit until the results are in those arrays.  Zero / negative option
+ * fields take the defaults: budget 150 GB capped at 90% of free memory, 8
+ * slots, 65536 graph points, 1 GiB AO scratch per request. */
+typedef struct kumo_server kumo_server;
+
+typedef struct {
+    int device;
+    double hbm_budget_bytes;
+    int max_active;
+    long long graph_points;
+    double request_scratch_bytes;
+} kumo_server_options;
+
+typedef struct {
+    long long submitted, completed, failed, points;
+    double p50_ms, p99_ms, mean_ms, max_ms;
+    double busy_s;        /* first submit to last completion */
+    double points_per_s;  /* completed points / busy_s */
+    long long graph_captures, graph_replays, direct_runs;
+    double peak_bytes, budget_bytes;
+} kumo_server_stats;
+
+int kumo_server_create(const kumo_server_options* opt, kumo_server** out, char* err, size_t errlen);
+/* Waits for every submitted request, then frees the server. */
+int kumo_server_destroy(kumo_server* server);
+int kumo_server_submit_grid(kumo_server* server, const kumo_molecule* m, const kumo_options* opt,
+                            const kumo_grid* grid, const kumo_property* props, int nprops,
+                            double* const* outputs, unsigned long long* ticket, char* err, size_t errlen);
+int kumo_server_submit_points(kumo_server* server, const kumo_molecule* m, const kumo_options* opt,
+                              const double* points, long long npoints, const kumo_property* props, int nprops,
+                              double* const* outputs, unsigned long long* ticket, char* err, size_t errlen);
+/* done = 1 once the ticket's results are in the caller's arrays (within timeout_s);
+ * a failed request returns its error status and message. */
+int kumo_server_wait(kumo_server* server, unsigned long long ticket, double timeout_s, int* done, char* err,
+                     size_t errlen);
+int kumo_server_drain(kumo_server* server, char* err, size_t errlen);
+int kumo_server_stats_get(kumo_server* server, kumo_server_stats* out, char* err, size_t errlen);
+int kumo_server_reset_stats(kumo_server* server, char* err, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

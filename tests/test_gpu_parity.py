@@ -160,6 +160,67 @@ def test_all_density_properties(name, backend):
         assert scaled_error(a, r) <= tol, f"{p}: {scaled_error(a, r)}"
 
 
+TRIPLET_FIELDS = [(P.Density, D.Alpha), (P.Density, D.Beta), (P.Density, D.Difference), (P.Density, D.Total),
+                  (P.ReducedGradient, D.Total), (P.SignLambda2Density, D.Total), (P.Hessian, D.Total)]
+
+
+def _grid_blocks(grid, nblocks):
+    """Points of nblocks evenly spaced 128-point blocks of a grid (block structure kept)."""
+    pts = grid.points()
+    nb = (len(pts) + 127) // 128
+    pick = np.unique(np.linspace(0, nb - 1, nblocks).astype(int))
+    return np.concatenate([pts[b * 128:(b + 1) * 128] for b in pick])
+
+
+@pytest.mark.parametrize("backend", [K.Backend.AO_MO, K.Backend.AO_P])
+def test_unrestricted_triplet_rdg_sign_lambda2(synth_cache, backend):
+    # The unrestricted-triplet workload's path (alpha, beta and spin densities,
+    # RDG and sign(lambda2) rho from the full AO Hessian, screening threshold
+    # 1e-10) on the scaled-down molecule of the same generator: FP64 against
+    # the oracle on blocks spread over its 96^3 grid.
+    path = synth.workload_fchk("triplet_370", synth_cache)
+    m, o = _pair(path)
+    origin, steps, counts = synth.workload_grid("triplet_370", m.atoms()[2])
+    pts = _grid_blocks(K.Grid(origin, steps, counts), 48)
+    props = [K.density(k, c) for k, c in TRIPLET_FIELDS]
+    tuples = [(int(p.kind), int(p.component), 0, 0) for p in props]
+    outs, used = K.Evaluator(m, backend=backend, threshold=1e-10).evaluate_points(pts, props)
+    refs, rused = o.evaluate(tuples, points=pts, backend=int(backend), threshold=1e-10)
+    assert used == rused == int(backend)
+    rho = refs[3][0]
+    for p, a, r in zip(props, outs, refs):
+        if p.kind == P.SignLambda2Density:
+            assert np.mean(np.isclose(a, r, rtol=1e-10, atol=1e-12)) > 0.999
+            assert scaled_error(np.abs(a), np.abs(r)) <= 1e-12
+        elif p.kind == P.ReducedGradient:
+            mask = rho > 1e-6
+            assert scaled_error(a[:, mask], r[:, mask]) <= 1e-9, p
+        else:
+            assert scaled_error(a, r) <= 1e-12, (p, scaled_error(a, r))
+
+
+def test_unrestricted_triplet_mixed(synth_cache):
+    # Mixed form on the same blocks: alpha and beta channels with 39 and 37
+    # occupied MOs, full Hessian (10 panels, two MO passes of the tensor-core
+    # contraction per channel).
+    path = synth.workload_fchk("triplet_370", synth_cache)
+    m = K.Molecule.from_fchk(path)
+    origin, steps, counts = synth.workload_grid("triplet_370", m.atoms()[2])
+    pts = _grid_blocks(K.Grid(origin, steps, counts), 48)
+    props = [K.density(k, c) for k, c in TRIPLET_FIELDS if k != P.SignLambda2Density]
+    f64, _ = K.Evaluator(m, threshold=1e-10).evaluate_points(pts, props)
+    mix, _ = K.Evaluator(m, threshold=1e-10, precision=K.Precision.Mixed).evaluate_points(pts, props)
+    total = f64[3]
+    for p, a, r in zip(props, mix, f64):
+        if p.kind == P.ReducedGradient:
+            mask = total[0] > 1e-3
+            err = np.abs(a[:, mask] - r[:, mask]).max() / max(1.0, np.abs(r[:, mask]).max())
+            assert err <= 1e-5, (p, err)
+            continue
+        scale = max(1.0, np.abs(total).max()) if p.component == D.Difference else max(1.0, np.abs(r).max())
+        assert np.abs(a - r).max() / scale <= 1e-6, p
+
+
 @pytest.mark.parametrize("block", [1, 7, 32, 37, 128])
 def test_block_sizes(block):
     m, o = _pair(os.path.join(GOLDEN, "acrolein.fchk.gz"))
