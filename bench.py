@@ -157,6 +157,166 @@ def run_reference(args, rank: int) -> None:
     print(json.dumps(line))
 
 
+def serve_bench(K, synth, precision: int, seconds: float, rate: float, pool, seed: int, graph_points: int = 65536,
+                scratch_gb: float = 2.0):
+    """Serving loop under the serving workload: Poisson arrivals at `rate`
+    requests/s for `seconds`, each request one type drawn uniformly (cube of
+    40^3..160^3 points at 0.2 bohr, 200x200 plane at 0.2 bohr, 1000-point line,
+    1..1000 scattered points) on a molecule drawn from the pool, with 1-3
+    properties drawn from {rho, grad rho, lap rho, tau, ELF, LOL, MO homo-2 ..
+    lumo+2, ESP} (ESP only on lines and point sets).  Latency runs from submit
+    until the results are in the caller's arrays; the run ends when every
+    request is done."""
+    P = K.PropertyKind
+    rng = np.random.default_rng(seed)
+    srv = K.Server(max_active=8, graph_points=graph_points, request_scratch_bytes=scratch_gb * 2**30)
+    dens = [P.Density, P.Gradient, P.Laplacian, P.Tau, P.Elf, P.Lol]
+    t0 = time.perf_counter()
+    t_next = 0.0
+    tickets, kinds = [], {"cube": 0, "plane": 0, "line": 0, "points": 0}
+    while True:
+        t_next += rng.exponential(1.0 / rate)
+        if t_next > seconds:
+            break
+        m, xyz, nalpha, nmo = pool[int(rng.integers(len(pool)))]
+        c = xyz.mean(axis=0)
+        kind = ["cube", "plane", "line", "points"][int(rng.integers(4))]
+        kinds[kind] += 1
+        props = []
+        for _ in range(int(rng.integers(1, 4))):
+            choice = int(rng.integers(len(dens) + 2))
+            if choice < len(dens):
+                props.append(K.density(dens[choice]))
+            elif choice == len(dens):
+                props.append(K.orbital(int(min(max(1, nalpha + int(rng.integers(-2, 3))), nmo))))
+            elif kind in ("line", "points"):
+                props.append(K.density(P.ElectrostaticPotential))
+        if not props:
+            props = [K.density(P.Density)]
+        now = time.perf_counter() - t0
+        if t_next > now:
+            time.sleep(t_next - now)
+        if kind == "cube":
+            e = int(rng.integers(40, 161))
+            g = K.Grid(c - 0.1 * (e - 1), np.eye(3) * 0.2, (e, e, e))
+            tickets.append(srv.submit_grid(m, g, props, precision=precision)[0])
+        elif kind == "plane":
+            g = K.Grid(c - np.array([19.9, 19.9, 0.0]), np.diag([0.2, 0.2, 1.0]), (200, 200, 1))
+            tickets.append(srv.submit_grid(m, g, props, precision=precision)[0])
+        elif kind == "line":
+            a, b = xyz.min(0) - 3.0, xyz.max(0) + 3.0
+            st = (b - a) / 999.0
+            g = K.Grid(a, np.column_stack([st, [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]]), (1000, 1, 1))
+            tickets.append(srv.submit_grid(m, g, props, precision=precision)[0])
+        else:
+            n = int(rng.integers(1, 1001))
+            pts = rng.uniform(xyz.min(0) - 2.5, xyz.max(0) + 2.5, (n, 3))
+            tickets.append(srv.submit_points(m, pts, props, precision=precision)[0])
+    submit_s = time.perf_counter() - t0
+    for t in tickets:
+        srv.wait(t, 600.0)
+    s = srv.stats()
+    srv.close()
+    return {"requests": int(s["completed"]), "failed": int(s["failed"]), "p50_ms": s["p50_ms"],
+            "p99_ms": s["p99_ms"], "mean_ms": s["mean_ms"], "pts_per_s": s["points_per_s"],
+            "points": int(s["points"]), "busy_s": s["busy_s"], "graph_captures": int(s["graph_captures"]),
+            "graph_replays": int(s["graph_replays"]), "direct_runs": int(s["direct_runs"]),
+            "peak_hbm_gb": s["peak_bytes"] / 1e9, "budget_hbm_gb": s["budget_bytes"] / 1e9,
+            "host_launch_s": s["launch_s"], "host_copy_s": s["copy_s"], "queue_ms": s["queue_ms"],
+            "submit_s": submit_s, "mix": kinds}
+
+
+def surface_points(rho: np.ndarray, origin, spacing: float, iso: float = 1e-3) -> np.ndarray:
+    """Vertices of the rho = iso surface on the grid's edges (linear
+    interpolation where rho crosses iso between neighbouring points), as a
+    marching-cubes surface has them."""
+    pts = []
+    for ax in range(3):
+        a = np.take(rho, np.arange(rho.shape[ax] - 1), axis=ax)
+        b = np.take(rho, np.arange(1, rho.shape[ax]), axis=ax)
+        cross = (a - iso) * (b - iso) < 0
+        idx = np.argwhere(cross)
+        t = (iso - a[cross]) / (b[cross] - a[cross])
+        p = idx.astype(float)
+        p[:, ax] += t
+        pts.append(p)
+    ijk = np.concatenate(pts)
+    return np.asarray(origin)[None, :] + spacing * ijk
+
+
+def esp_bench(K, synth, fchk_dir: str, oracle_pts: int = 32):
+    """Electrostatic-potential workload: C30N3O3H24 cation (60 atoms, 1260 AOs),
+    exact potential (tolerance 0) on its 96^3 cube at 0.24 bohr and on the
+    rho = 0.001 surface vertices of that cube; unit: point-pair interactions."""
+    import torch
+    fchk = synth.workload_fchk("esp_1260", fchk_dir)
+    m = K.Molecule.from_fchk(fchk)
+    _, _, xyz = m.atoms()
+    origin, steps, counts = synth.workload_grid("esp_1260", xyz)
+    grid = K.Grid(origin, steps, counts)
+    n = grid.npoints
+    esp = K.density(K.PropertyKind.ElectrostaticPotential)
+    ev = K.Evaluator(m)
+    pairs = m.esp_pair_count()
+    out = torch.empty(n, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    ev.evaluate_grid_device(K.Grid(origin, steps, (8, 8, 8)), [esp], [out.data_ptr()], stream.cuda_stream)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    ms_cube = timed(lambda: ev.evaluate_grid_device(grid, [esp], [out.data_ptr()], stream.cuda_stream))
+    rho, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_grid(grid, [K.density(K.PropertyKind.Density)])
+    surf = surface_points(rho[0].reshape(counts), origin, steps[0, 0])
+    dpts = torch.tensor(surf.ravel(), dtype=torch.float64, device="cuda")
+    sout = torch.empty(len(surf), dtype=torch.float64, device="cuda")
+    ms_surf = timed(lambda: ev.evaluate_points_device(dpts.data_ptr(), len(surf), [esp], [sout.data_ptr()],
+                                                      stream.cuda_stream))
+    # Accuracy on a sample against the CPU oracle, and the oracle's own rate.
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    o = O.OracleESP(O.OracleMolecule.from_fchk(fchk))
+    pick = np.linspace(0, len(surf) - 1, oracle_pts).astype(int)
+    t0 = time.perf_counter()
+    ref = o.evaluate(surf[pick])
+    cpu_s = time.perf_counter() - t0
+    got = sout.cpu().numpy()[pick]
+    return {"workload": "esp_1260 (C30N3O3H24+, 60 atoms, 1260 AOs) exact ESP, 96^3 cube @0.24 bohr and "
+                        "rho = 0.001 surface vertices",
+            "pairs": int(pairs),
+            "cube": {"points": n, "ms": ms_cube, "pair_points_per_s": n * pairs / (ms_cube * 1e-3),
+                     "pts_per_s": n / (ms_cube * 1e-3)},
+            "surface": {"points": len(surf), "ms": ms_surf, "pair_points_per_s": len(surf) * pairs / (ms_surf * 1e-3)},
+            "scaled_err_vs_oracle": float(np.max(np.abs(got - ref)) / max(1.0, float(np.max(np.abs(ref))))),
+            "cpu_oracle": {"pair_points_per_s": oracle_pts * pairs / cpu_s, "cores": O.lib().ko_max_threads(),
+                           "sample": f"{oracle_pts} surface points, {cpu_s:.1f} s"}}
+
+
+def serving_pool(K, synth, count: int, max_atoms: int, seed: int = 7):
+    """The serving pool's molecules, built in a process pool (spawned)."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    specs = synth.serving_pool(count, seed, 3, max_atoms)
+    with cf.ProcessPoolExecutor(max_workers=min(16, os.cpu_count() or 4), mp_context=mp.get_context("spawn")) as ex:
+        recs = list(ex.map(synth.serving_records, specs))
+    pool = []
+    for r in recs:
+        m = K.Molecule.from_records(r)
+        # Resident before serving: the device copy and the potential's primitive pairs.
+        K.Evaluator(m).evaluate_points(np.zeros((1, 3)), [K.density(K.PropertyKind.Density),
+                                                          K.density(K.PropertyKind.ElectrostaticPotential)])
+        xyz = np.asarray(r["Current cartesian coordinates"], dtype=float).reshape(-1, 3)
+        nmo = int(np.asarray(r["Alpha MO coefficients"]).size // int(r["Number of basis functions"]))
+        pool.append((m, xyz, int(r["Number of alpha electrons"]), nmo))
+    return pool, [n for _, n, _ in specs]
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -168,6 +328,15 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--grid-n", type=int, default=0, help="points per axis (default: the workload's 128)")
+    ap.add_argument("--serve-seconds", type=float, default=5.0, help="arrival window of the serving run (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="mean arrivals per second")
+    ap.add_argument("--serve-pool", type=int, default=32, help="molecules in the serving pool")
+    ap.add_argument("--serve-max-atoms", type=int, default=60, help="largest molecule of the serving pool")
+    ap.add_argument("--serve-graph-points", type=int, default=65536, help="largest request replayed from a graph")
+    ap.add_argument("--serve-scratch-gb", type=float, default=2.0, help="AO scratch per serving request")
+    ap.add_argument("--serve-only", action="store_true", help="run the serving measurement only (prints its JSON)")
+    ap.add_argument("--no-esp", action="store_true", help="skip the electrostatic-potential measurement")
+    ap.add_argument("--esp-only", action="store_true", help="run the electrostatic-potential measurement only")
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="time one form only (small profiling cases)")
     args = ap.parse_args()
@@ -239,6 +408,18 @@ def main() -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    if args.esp_only:
+        if rank == 0:
+            print(json.dumps(esp_bench(K, synth, d)))
+        return
+    if args.serve_only:
+        pool, _ = serving_pool(K, synth, args.serve_pool, args.serve_max_atoms)
+        kw = dict(graph_points=args.serve_graph_points, scratch_gb=args.serve_scratch_gb)
+        res = {f: serve_bench(K, synth, int(prec), args.serve_seconds, args.serve_rate, pool, 21, **kw)
+               for f, prec in (("mixed", K.Precision.Mixed), ("fp64", K.Precision.FP64))}
+        if rank == 0:
+            print(json.dumps({"serve_only": kw, **res}))
+        return
     if args.only:
         # Small profiling case: warm-up and timed steps of one form only.
         for _ in range(args.warmup):
@@ -298,6 +479,22 @@ def main() -> None:
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(float(np.median(e2e_times)) if e2e_times else float("nan"))
 
+    esp_line = None if args.no_esp else esp_bench(K, synth, d)
+    serve = None
+    if args.serve_seconds > 0:
+        pool, sizes = serving_pool(K, synth, args.serve_pool, args.serve_max_atoms)
+        kw = dict(graph_points=args.serve_graph_points, scratch_gb=args.serve_scratch_gb)
+        serve = {"config": {"arrivals": f"Poisson {args.serve_rate:g}/s for {args.serve_seconds:g} s (seeded)",
+                            "pool": f"{len(pool)} synthetic molecules, atoms log-uniform in [3, {args.serve_max_atoms}]",
+                            "admission": "HBM budget 150 GB (capped at 90% of free memory), 8 streams, "
+                                         f"{args.serve_scratch_gb:g} GiB AO scratch per request",
+                            "graphs": f"requests <= {args.serve_graph_points} points replay CUDA graphs "
+                                      "from the second time their shape is met"},
+                 "mixed": serve_bench(K, synth, int(K.Precision.Mixed), args.serve_seconds, args.serve_rate, pool,
+                                      21, **kw),
+                 "fp64": serve_bench(K, synth, int(K.Precision.FP64), args.serve_seconds, args.serve_rate, pool,
+                                     21, **kw)}
+
     if rank == 0:
         peaks, peak_kind = _peaks()
         # Dominant kernel of the mixed step.
@@ -353,6 +550,10 @@ def main() -> None:
             "gpu_launches": launches,
             "clocks": clk,
         }
+        if serve is not None:
+            line["serve"] = serve
+        if esp_line is not None:
+            line["esp"] = esp_line
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(fchk, grid, args.cpu_blocks)
         print(json.dumps(line))

@@ -185,6 +185,13 @@ EspDevice::EspDevice(const chem::kumo::Molecule& m, cudaStream_t stream) {
                 }
         }
     }
+    // Pairs grouped by order (stable), so that each launch of the device
+    // kernel handles one order with its recursion unrolled.
+    std::stable_sort(pairs.begin(), pairs.end(), [](const EspPair& x, const EspPair& y) { return x.order < y.order; });
+    for (int L = 0; L <= kEspMaxL + 1; ++L)
+        view_.order_first[L] = std::lower_bound(pairs.begin(), pairs.end(), L,
+                                                [](const EspPair& x, int v) { return x.order < v; }) -
+                               pairs.begin();
     // Recursion table of the Hermite triples up to kEspMaxL.
     const auto all = hermite_triples(kEspMaxL);
     auto index_of = [&](int t, int u, int v) {
@@ -212,6 +219,7 @@ EspDevice::EspDevice(const chem::kumo::Molecule& m, cudaStream_t stream) {
         void* d = nullptr;
         check_cuda(cudaMalloc(&d, std::max<std::size_t>(bytes, 16)), "cudaMalloc (potential)");
         allocs_.push_back(d);
+        bytes_ += std::max<std::size_t>(bytes, 16);
         if (bytes) check_cuda(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync (potential)");
         return d;
     };
@@ -250,10 +258,155 @@ __device__ __forceinline__ void boys_device(const double* table, double T, int n
     for (int m = top; m > 0; --m) out[m - 1] = (2.0 * T * out[m] + decay) / (2.0 * m - 1.0);
 }
 
-// One thread per point; all threads of a CTA walk the pairs in order, so pair
-// data and coefficients are uniform loads.
-__global__ void __launch_bounds__(128) esp_f64_kernel(const __grid_constant__ EspParams prm) {
-    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+// Compile-time form of the recursion table (same ordering and steps as the
+// host table uploaded in EspView::recursion).
+struct HermiteTable {
+    int axis[hermite_count(kEspMaxL)];
+    int one[hermite_count(kEspMaxL)];
+    int two[hermite_count(kEspMaxL)];
+    int factor[hermite_count(kEspMaxL)];
+};
+
+constexpr HermiteTable make_hermite_table() {
+    HermiteTable h{};
+    int tt[hermite_count(kEspMaxL)] = {}, uu[hermite_count(kEspMaxL)] = {}, vv[hermite_count(kEspMaxL)] = {};
+    int n = 0;
+    for (int sum = 0; sum <= kEspMaxL; ++sum)
+        for (int t = sum; t >= 0; --t)
+            for (int u = sum - t; u >= 0; --u) {
+                tt[n] = t;
+                uu[n] = u;
+                vv[n] = sum - t - u;
+                ++n;
+            }
+    auto index_of = [&](int t, int u, int v) {
+        for (int k = 0; k < n; ++k)
+            if (tt[k] == t && uu[k] == u && vv[k] == v) return k;
+        return -1;
+    };
+    for (int k = 0; k < n; ++k) {
+        const int t = tt[k], u = uu[k], v = vv[k];
+        h.axis[k] = -1;
+        h.one[k] = -1;
+        h.two[k] = -1;
+        h.factor[k] = 0;
+        if (t > 0) {
+            h.axis[k] = 0;
+            h.one[k] = index_of(t - 1, u, v);
+            h.two[k] = t > 1 ? index_of(t - 2, u, v) : -1;
+            h.factor[k] = t - 1;
+        } else if (u > 0) {
+            h.axis[k] = 1;
+            h.one[k] = index_of(t, u - 1, v);
+            h.two[k] = u > 1 ? index_of(t, u - 2, v) : -1;
+            h.factor[k] = u - 1;
+        } else if (v > 0) {
+            h.axis[k] = 2;
+            h.one[k] = index_of(t, u, v - 1);
+            h.two[k] = v > 1 ? index_of(t, u, v - 2) : -1;
+            h.factor[k] = v - 1;
+        }
+    }
+    return h;
+}
+
+constexpr HermiteTable kHermite = make_hermite_table();
+
+// F_0..F_TOP(T) as boys_device, with exp(-T) only where a recursion needs it.
+template <int TOP>
+__device__ __forceinline__ void boys_top(const double* table, double T, double (&out)[TOP + 1]) {
+    if (T >= 40.0) {
+        out[0] = 0.5 * sqrt(3.141592653589793 / T);
+        if constexpr (TOP > 0) {
+            const double decay = exp(-T);
+#pragma unroll
+            for (int m = 0; m < TOP; ++m) out[m + 1] = ((2.0 * m + 1.0) * out[m] - decay) / (2.0 * T);
+        }
+        return;
+    }
+    const int point = static_cast<int>(llround(T / 0.05));
+    const double delta = T - point * 0.05;
+    const double* row = table + point * kBoysOrders;
+    double sum = 0.0, factor = 1.0;
+#pragma unroll
+    for (int k = 0; k < kBoysTaylor; ++k) {
+        sum += row[TOP + k] * factor;
+        factor *= -delta / (k + 1.0);
+    }
+    out[TOP] = sum;
+    if constexpr (TOP > 0) {
+        const double decay = exp(-T);
+#pragma unroll
+        for (int m = TOP; m > 0; --m) out[m - 1] = (2.0 * T * out[m] + decay) / (2.0 * m - 1.0);
+    }
+}
+
+// One level of the Hermite recursion: R^(n) from R^(n+1) in place, entries
+// K = NT-1 down to 1 of the first `live` (each entry reads lower-index entries
+// of the level above, which a descending sweep has not overwritten yet).
+template <int K, int NT>
+__device__ __forceinline__ void hermite_level(double (&R)[NT], int live, double pcx, double pcy, double pcz) {
+    if constexpr (K >= 1) {
+        if (K < live) {
+            constexpr int ax = kHermite.axis[K];
+            constexpr int one = kHermite.one[K];
+            constexpr int two = kHermite.two[K];
+            constexpr double f = static_cast<double>(kHermite.factor[K]);
+            const double X = ax == 0 ? pcx : (ax == 1 ? pcy : pcz);
+            double v = X * R[one];
+            if constexpr (two >= 0) v += f * R[two];
+            R[K] = v;
+        }
+        hermite_level<K - 1, NT>(R, live, pcx, pcy, pcz);
+    }
+}
+
+// Pairs of order L: thread = point of a 128-point tile, blockIdx.y = chunk of
+// the order's pairs; the partial sum of the chunk goes to
+// part[(slot0 + chunk) * ld + point].
+template <int L>
+__global__ void __launch_bounds__(128) esp_order_kernel(const __grid_constant__ EspParams prm, long long first,
+                                                       long long count, long long chunk, int slot0, double* part,
+                                                       long long ld) {
+    constexpr int NT = hermite_count(L);
+    const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const bool valid = q < prm.src.count;
+    double x = 0.0, y = 0.0, z = 0.0;
+    if (valid) point_at(prm.src, q, x, y, z);
+    const EspView& e = prm.esp;
+    const long long i0 = first + static_cast<long long>(blockIdx.y) * chunk;
+    const long long i1 = min(first + count, i0 + chunk);
+    double sum = 0.0;
+    for (long long i = i0; i < i1; ++i) {
+        const EspPair pr = e.pairs[i];
+        const double pcx = pr.qx - x, pcy = pr.qy - y, pcz = pr.qz - z;
+        double F[L + 1];
+        boys_top<L>(e.boys_table, pr.p * (pcx * pcx + pcy * pcy + pcz * pcz), F);
+        double power = 1.0;
+#pragma unroll
+        for (int k = 1; k <= L; ++k) {
+            power *= -2.0 * pr.p;
+            F[k] *= power;
+        }
+        double R[NT];
+#pragma unroll
+        for (int n = L; n >= 0; --n) {
+            hermite_level<NT - 1, NT>(R, hermite_count(L - n), pcx, pcy, pcz);
+            R[0] = F[n];
+        }
+        const double* c = e.coef + pr.first;
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < NT; ++k) s += c[k] * R[k];
+        sum += s;
+    }
+    if (valid) part[static_cast<long long>(slot0 + blockIdx.y) * ld + q] = sum;
+}
+
+// out = nuclear term - the partial sums in slot order.
+__global__ void __launch_bounds__(128) esp_reduce_kernel(const __grid_constant__ EspParams prm, const double* part,
+                                                        int nslots, long long ld) {
+    const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (q >= prm.src.count) return;
     double x, y, z;
     point_at(prm.src, q, x, y, z);
@@ -266,49 +419,65 @@ __global__ void __launch_bounds__(128) esp_f64_kernel(const __grid_constant__ Es
         if (at.w == 0.0 || d < 1e-8) continue;
         nuclear += at.w / d;
     }
-    constexpr int NT = hermite_count(kEspMaxL);
-    double buf0[NT], buf1[NT];
-    double seeds[kEspMaxL + 1];
     double sum = 0.0;
-    for (long long i = 0; i < e.npairs; ++i) {
-        const EspPair pr = e.pairs[i];
-        const double pcx = pr.qx - x, pcy = pr.qy - y, pcz = pr.qz - z;
-        const int L = pr.order;
-        boys_device(e.boys_table, pr.p * (pcx * pcx + pcy * pcy + pcz * pcz), L + 1, seeds);
-        double power = 1.0;
-        for (int k = 1; k <= L; ++k) {
-            power *= -2.0 * pr.p;
-            seeds[k] *= power;
-        }
-        double* prev = buf0;
-        double* cur = buf1;
-        for (int n = L; n >= 0; --n) {
-            double* t = prev;
-            prev = cur;
-            cur = t;
-            cur[0] = seeds[n];
-            const int entries = hermite_count(L - n);
-            for (int k = 1; k < entries; ++k) {
-                const int4 r = e.recursion[k];
-                const double X = r.x == 0 ? pcx : (r.x == 1 ? pcy : pcz);
-                double value = X * prev[r.y];
-                if (r.z >= 0) value += r.w * prev[r.z];
-                cur[k] = value;
-            }
-        }
-        const double* c = e.coef + pr.first;
-        const int nk = hermite_count(L);
-        double s = 0.0;
-        for (int k = 0; k < nk; ++k) s += c[k] * cur[k];
-        sum += s;
-    }
+    for (int s = 0; s < nslots; ++s) sum += part[static_cast<long long>(s) * ld + q];
     prm.out[q - prm.out_base] = nuclear - sum;
 }
 
+template <int L>
+void launch_order(const EspParams& p, long long first, long long count, long long chunk, int chunks, int slot0,
+                  double* part, long long ld, unsigned tiles, cudaStream_t stream) {
+    esp_order_kernel<L><<<dim3(tiles, static_cast<unsigned>(chunks)), 128, 0, stream>>>(p, first, count, chunk, slot0,
+                                                                                       part, ld);
+}
+
 void launch_esp_f64(const EspParams& p, cudaStream_t stream) {
+    using chem::kumo::detail::check_cuda;
     const long long n = p.src.count;
     if (n <= 0) return;
-    esp_f64_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(p);
+    const unsigned tiles = static_cast<unsigned>((n + 127) / 128);
+    const EspView& e = p.esp;
+    // Chunks per order: about 8 CTAs per SM in total, at least 64 pairs a chunk.
+    constexpr long long kTargetCtas = 8 * 148;
+    int chunks[kEspMaxL + 1] = {};
+    long long chunk_size[kEspMaxL + 1] = {};
+    int nslots = 0;
+    for (int L = 0; L <= kEspMaxL; ++L) {
+        const long long count = e.order_first[L + 1] - e.order_first[L];
+        if (count <= 0) continue;
+        long long want = (kTargetCtas * count / std::max<long long>(e.npairs, 1) + tiles - 1) / tiles;
+        want = std::max<long long>(1, std::min<long long>(want, (count + 63) / 64));
+        chunk_size[L] = (count + want - 1) / want;
+        chunks[L] = static_cast<int>((count + chunk_size[L] - 1) / chunk_size[L]);
+        nslots += chunks[L];
+    }
+    double* part = nullptr;
+    const long long ld = n;
+    if (nslots > 0)
+        check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * static_cast<size_t>(nslots) * n,
+                                   stream),
+                   "cudaMallocAsync (potential partial sums)");
+    int slot = 0;
+    for (int L = 0; L <= kEspMaxL; ++L) {
+        if (!chunks[L]) continue;
+        const long long first = e.order_first[L], count = e.order_first[L + 1] - first;
+        const long long cs = chunk_size[L];
+        const int nc = chunks[L];
+        switch (L) {
+            case 0: launch_order<0>(p, first, count, cs, nc, slot, part, ld, tiles, stream); break;
+            case 1: launch_order<1>(p, first, count, cs, nc, slot, part, ld, tiles, stream); break;
+            case 2: launch_order<2>(p, first, count, cs, nc, slot, part, ld, tiles, stream); break;
+            case 3: launch_order<3>(p, first, count, cs, nc, slot, part, ld, tiles, stream); break;
+            case 4: launch_order<4>(p, first, count, cs, nc, slot, part, ld, tiles, stream); break;
+            case 5: launch_order<5>(p, first, count, cs, nc, slot, part, ld, tiles, stream); break;
+            case 6: launch_order<6>(p, first, count, cs, nc, slot, part, ld, tiles, stream); break;
+            case 7: launch_order<7>(p, first, count, cs, nc, slot, part, ld, tiles, stream); break;
+            default: launch_order<8>(p, first, count, cs, nc, slot, part, ld, tiles, stream); break;
+        }
+        slot += nc;
+    }
+    esp_reduce_kernel<<<tiles, 128, 0, stream>>>(p, part, nslots, ld);
+    if (part) cudaFreeAsync(part, stream);
 }
 
 __global__ void boys_kernel(const double* table, const double* t, long long n, int nvalues, double* out) {

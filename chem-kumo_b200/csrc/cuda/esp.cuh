@@ -45,6 +45,8 @@ struct EspView {
     // its recursion step, the entries one and two steps down that axis (-1 if
     // none) and the factor of the second term.
     const int4* recursion = nullptr;
+    // Pairs are grouped by order: those of order L are [order_first[L], order_first[L + 1]).
+    long long order_first[kEspMaxL + 2] = {};
 };
 
 struct EspParams {
@@ -63,10 +65,12 @@ public:
     EspDevice& operator=(const EspDevice&) = delete;
     EspView view() const { return view_; }
     long long pair_count() const { return view_.npairs; }
+    std::size_t device_bytes() const { return bytes_; }
 
 private:
     EspView view_;
     std::vector<void*> allocs_;
+    std::size_t bytes_ = 0;
 };
 
 /// Boys table F_m(T_i), m < kBoysOrders, T_i = 0.05 i (src/boys_function.cpp:23-44).
@@ -74,6 +78,9 @@ std::vector<double> boys_table_host();
 /// F_0..F_{n-1}(T) on the host from the same table (src/boys_function.cpp:47-76).
 void boys_host(const double* table, double T, int n, double* out);
 
+/// Exact potential at the points of p.src: one launch per pair order over
+/// (128-point tiles x pair chunks) writing partial sums to stream-ordered
+/// scratch, then a fixed-order reduction with the nuclear term.
 void launch_esp_f64(const EspParams& p, cudaStream_t stream);
 /// F_m(T) for an array of T on the device (test seam of the Boys kernel).
 void launch_boys_f64(const double* table, const double* t, long long n, int nvalues, double* out, cudaStream_t stream);

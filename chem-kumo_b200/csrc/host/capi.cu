@@ -564,6 +564,7 @@ int kumo_server_create(const kumo_server_options* opt, kumo_server** out, char* 
             if (opt->hbm_budget_bytes > 0) o.hbm_budget = static_cast<std::size_t>(opt->hbm_budget_bytes);
             if (opt->max_active > 0) o.max_active = opt->max_active;
             if (opt->graph_points > 0) o.graph_points = static_cast<std::size_t>(opt->graph_points);
+            if (opt->graph_points < 0) o.graph_points = 0;  // no graphs
             if (opt->request_scratch_bytes > 0) o.request_scratch = static_cast<std::size_t>(opt->request_scratch_bytes);
         }
         auto s = std::make_unique<kumo_server>();
@@ -652,6 +653,9 @@ int kumo_server_stats_get(kumo_server* server, kumo_server_stats* out, char* err
         out->direct_runs = static_cast<long long>(s.direct_runs);
         out->peak_bytes = static_cast<double>(s.peak_bytes);
         out->budget_bytes = static_cast<double>(s.budget_bytes);
+        out->launch_s = s.launch_s;
+        out->copy_s = s.copy_s;
+        out->queue_ms = s.queue_ms;
     });
 }
 

@@ -1,6 +1,8 @@
 // Upload of a molecule's AO tables, density matrices and MO coefficients.
 #include "device_state.hpp"
 
+#include "../cuda/esp.cuh"
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -169,10 +171,20 @@ DeviceMolecule::DeviceMolecule(const Molecule& m) {
     }
 }
 
+kumo_dev::EspDevice& DeviceMolecule::esp_state(const Molecule& m, cudaStream_t stream) {
+    std::lock_guard<std::mutex> lock(esp_mutex);
+    if (!esp) {
+        esp = std::make_unique<kumo_dev::EspDevice>(m, stream);
+        bytes += esp->device_bytes();
+    }
+    return *esp;
+}
+
 DeviceMolecule::~DeviceMolecule() {
     int cur = -1;
     cudaGetDevice(&cur);
     if (cur != device) cudaSetDevice(device);
+    esp.reset();
     for (void* p : allocations) cudaFree(p);
     if (cur != device && cur >= 0) cudaSetDevice(cur);
 }

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <memory>
+#include <mutex>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -12,6 +14,10 @@
 
 #include "../cuda/ao_mixed.cuh"
 #include "../cuda/kumo_device.cuh"
+
+namespace kumo_dev {
+class EspDevice;
+}
 
 namespace chem::kumo::detail {
 
@@ -52,6 +58,11 @@ struct DeviceMolecule {
     bool unrestricted = false;
     std::size_t bytes = 0;
     std::vector<void*> allocations;
+    // Primitive pairs of the electrostatic potential, built on first use and
+    // kept with the molecule (their host set-up costs far more than a launch).
+    std::unique_ptr<kumo_dev::EspDevice> esp;
+    std::mutex esp_mutex;
+    kumo_dev::EspDevice& esp_state(const Molecule& m, cudaStream_t stream);
 
     explicit DeviceMolecule(const Molecule& m);
     ~DeviceMolecule();

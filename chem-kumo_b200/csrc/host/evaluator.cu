@@ -613,13 +613,9 @@ private:
     kumo_dev::PointSource src_{};
     std::vector<std::pair<Property, double*>> outs_;
     std::size_t passes_ = 0, completed_ = 0;
-    std::unique_ptr<kumo_dev::EspDevice> esp_;
 };
 
-kumo_dev::EspDevice& Evaluator::Run::esp_state() {
-    if (!esp_) esp_ = std::make_unique<kumo_dev::EspDevice>(mol_, stream_);
-    return *esp_;
-}
+kumo_dev::EspDevice& Evaluator::Run::esp_state() { return dev_->esp_state(mol_, stream_); }
 
 namespace {
 

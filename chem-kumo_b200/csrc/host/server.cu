@@ -140,6 +140,7 @@ struct Server::Impl {
     std::vector<cudaStream_t> free_streams;
     std::vector<cudaEvent_t> free_events;
     std::map<std::string, std::vector<std::unique_ptr<GraphEntry>>> graphs;
+    std::map<std::string, int> seen;  // small-request keys met so far (a graph is captured on the second)
     std::multimap<std::size_t, double*> free_stage;  // page-locked staging by size
     std::vector<const Molecule*> resident;
     std::size_t resident_bytes = 0, active_bytes = 0;
@@ -147,6 +148,8 @@ struct Server::Impl {
     // Statistics (guarded by mu).
     std::vector<double> latencies;
     ServeStats st;
+    double queue_sum_ms = 0;
+    std::size_t admitted = 0;
     std::optional<clock_type::time_point> t_first, t_last;
 
     std::thread scheduler, completer;
@@ -172,15 +175,24 @@ std::string Server::Impl::key_of(const Pending& p) const {
     return k.str();
 }
 
+// Page-locked staging in power-of-two size classes (page-locking is slow and
+// synchronises the device, so buffers are kept and reused).
+std::size_t stage_class(std::size_t bytes) {
+    std::size_t c = 4096;
+    while (c < bytes) c <<= 1;
+    return c;
+}
+
 double* Server::Impl::get_stage(std::size_t bytes) {
-    auto it = free_stage.lower_bound(bytes);
-    if (it != free_stage.end() && it->first <= 2 * bytes) {
+    const std::size_t cls = stage_class(bytes);
+    auto it = free_stage.find(cls);
+    if (it != free_stage.end()) {
         double* p = it->second;
         free_stage.erase(it);
         return p;
     }
     void* p = nullptr;
-    check_cuda(cudaHostAlloc(&p, std::max<std::size_t>(bytes, 64), cudaHostAllocDefault), "cudaHostAlloc (staging)");
+    check_cuda(cudaHostAlloc(&p, cls, cudaHostAllocDefault), "cudaHostAlloc (staging)");
     return static_cast<double*>(p);
 }
 
@@ -271,6 +283,12 @@ void Server::Impl::launch(Pending&& p) {
             resident_bytes += mol.device_bytes();
         }
         if (p.graph) {
+            // A request shape met for the first time runs the regular path;
+            // its graph is captured when the shape comes again.
+            const std::string key = key_of(p);
+            if (seen[key]++ == 0 && graphs.find(key) == graphs.end()) p.graph = false;
+        }
+        if (p.graph) {
             if (p.req.grid) grid_to_points(*p.req.grid, p.req.points);
             GraphEntry* e = graph_for(p, a.stream);
             const std::size_t n = p.n, b = e->bucket;
@@ -328,8 +346,8 @@ void Server::Impl::launch(Pending&& p) {
         cudaStreamSynchronize(a.stream);
         cudaGetLastError();
         if (a.entry) a.entry->busy = false;
-        if (a.stage) free_stage.emplace(a.stage_bytes, a.stage);
-        if (a.pstage) free_stage.emplace(a.pstage_bytes, a.pstage);
+        if (a.stage) free_stage.emplace(stage_class(a.stage_bytes), a.stage);
+        if (a.pstage) free_stage.emplace(stage_class(a.pstage_bytes), a.pstage);
         free_streams.push_back(a.stream);
         free_events.push_back(a.event);
         active_bytes -= p.footprint;
@@ -359,13 +377,13 @@ void Server::Impl::run_scheduler() {
             free_events.push_back(a.event);
             progressed = true;
             if (a.pstage) {
-                free_stage.emplace(a.pstage_bytes, a.pstage);
+                free_stage.emplace(stage_class(a.pstage_bytes), a.pstage);
                 a.pstage = nullptr;
             }
             if (q != cudaSuccess) {
                 cudaGetLastError();
                 if (a.entry) a.entry->busy = false;
-                if (a.stage) free_stage.emplace(a.stage_bytes, a.stage);
+                if (a.stage) free_stage.emplace(stage_class(a.stage_bytes), a.stage);
                 fail(a.p.ticket, std::string("CUDA error: ") + cudaGetErrorString(q), a.p.t_submit);
                 continue;
             }
@@ -388,9 +406,15 @@ void Server::Impl::run_scheduler() {
                 queue.pop_front();
                 lock.unlock();
                 active_bytes += p.footprint;
+                const auto tl = clock_type::now();
+                const double queued = std::chrono::duration<double, std::milli>(tl - p.t_submit).count();
                 launch(std::move(p));
+                const double dt = std::chrono::duration<double>(clock_type::now() - tl).count();
                 progressed = true;
                 lock.lock();
+                st.launch_s += dt;
+                queue_sum_ms += queued;
+                ++admitted;
                 st.peak_bytes = std::max(st.peak_bytes, resident_bytes + active_bytes);
             }
             if (stop && queue.empty() && active.empty()) break;
@@ -415,6 +439,7 @@ void Server::Impl::run_completer() {
             a = std::move(finished.front());
             finished.pop_front();
         }
+        const auto tc = clock_type::now();
         const double* src = a.entry ? a.entry->h_out : a.stage;
         const auto& props = a.p.req.request.properties();
         std::size_t off = 0;
@@ -426,8 +451,9 @@ void Server::Impl::run_completer() {
         }
         const auto now = clock_type::now();
         std::lock_guard<std::mutex> lock(mu);
+        st.copy_s += std::chrono::duration<double>(now - tc).count();
         if (a.entry) a.entry->busy = false;
-        if (a.stage) returned_stage.emplace_back(a.stage_bytes, a.stage);
+        if (a.stage) returned_stage.emplace_back(stage_class(a.stage_bytes), a.stage);
         auto& t = tickets[a.p.ticket];
         t.done = true;
         t.latency_ms = std::chrono::duration<double, std::milli>(now - a.p.t_submit).count();
@@ -579,6 +605,7 @@ ServeStats Server::stats() const {
         s.mean_ms = sum / static_cast<double>(l.size());
         s.max_ms = l.back();
     }
+    if (m.admitted) s.queue_ms = m.queue_sum_ms / static_cast<double>(m.admitted);
     if (m.t_first && m.t_last) {
         s.busy_s = std::chrono::duration<double>(*m.t_last - *m.t_first).count();
         if (s.busy_s > 0) s.points_per_s = static_cast<double>(s.points) / s.busy_s;
@@ -590,6 +617,8 @@ void Server::reset_stats() {
     Impl& m = *impl_;
     std::lock_guard<std::mutex> lock(m.mu);
     m.latencies.clear();
+    m.queue_sum_ms = 0;
+    m.admitted = 0;
     const std::size_t budget = m.st.budget_bytes;
     m.st = ServeStats{};
     m.st.budget_bytes = budget;

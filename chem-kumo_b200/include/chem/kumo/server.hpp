@@ -5,9 +5,10 @@
 // budget and an active slot is free, and run concurrently, each on its own
 // CUDA stream, so that their kernels overlap on the device while later
 // requests arrive (continuous batching).  Small requests (up to
-// ServerOptions::graph_points points, grids converted to explicit points) are
-// replayed from CUDA graphs captured once per (molecule, options, properties,
-// point bucket); larger ones run the regular device path.  Results land in
+// ServerOptions::graph_points points, grids converted to explicit points) whose
+// shape (molecule, options, properties, point bucket) has been met before are
+// replayed from a CUDA graph captured at the second meeting; the others run
+// the regular device path.  Results land in
 // the caller's host arrays; latency is measured from submit to the moment the
 // results are in those arrays.
 #include <chrono>
@@ -55,6 +56,9 @@ struct ServeStats {
     std::size_t graph_captures = 0, graph_replays = 0, direct_runs = 0;
     std::size_t peak_bytes = 0;           ///< largest admitted footprint sum
     std::size_t budget_bytes = 0;
+    double launch_s = 0;                  ///< scheduler host time spent issuing requests
+    double copy_s = 0;                    ///< completion-thread time copying results
+    double queue_ms = 0;                  ///< mean time from submit to admission
 };
 
 class Server {

@@ -170,7 +170,8 @@ class _ServerStats(C.Structure):
                 ("points", C.c_longlong), ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
                 ("max_ms", C.c_double), ("busy_s", C.c_double), ("points_per_s", C.c_double),
                 ("graph_captures", C.c_longlong), ("graph_replays", C.c_longlong), ("direct_runs", C.c_longlong),
-                ("peak_bytes", C.c_double), ("budget_bytes", C.c_double)]
+                ("peak_bytes", C.c_double), ("budget_bytes", C.c_double), ("launch_s", C.c_double),
+                ("copy_s", C.c_double), ("queue_ms", C.c_double)]
 
 
 class _ProfileEntry(C.Structure):

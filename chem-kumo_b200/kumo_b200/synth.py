@@ -417,6 +417,65 @@ def _packed_lower(m: np.ndarray) -> np.ndarray:
     return m[idx]
 
 
+def fchk_records(mol: SyntheticMolecule) -> Dict[str, object]:
+    """The FCHK records write_fchk would write, as read_fchk returns them
+    (for building a molecule in memory without the file round trip)."""
+    rec: Dict[str, object] = {
+        "Number of atoms": len(mol.atomic_numbers),
+        "Number of alpha electrons": mol.nalpha,
+        "Number of beta electrons": mol.nbeta,
+        "Number of basis functions": mol.nbasis,
+        "Atomic numbers": np.asarray(mol.atomic_numbers, dtype=np.int64),
+        "Nuclear charges": np.asarray(mol.atomic_numbers, dtype=float),
+        "Current cartesian coordinates": mol.coordinates.reshape(-1),
+        "Shell types": np.array([(-s.l if (s.pure and s.l >= 2) else s.l) for s in mol.shells]),
+        "Number of primitives per shell": np.array([len(s.exponents) for s in mol.shells]),
+        "Shell to atom map": np.array([s.atom + 1 for s in mol.shells]),
+        "Primitive exponents": np.concatenate([s.exponents for s in mol.shells]),
+        "Contraction coefficients": np.concatenate([s.coefficients for s in mol.shells]),
+        "Coordinates of each shell": np.concatenate([mol.coordinates[s.atom] for s in mol.shells]),
+        "Alpha MO coefficients": mol.c_alpha.T.reshape(-1),
+        "Total SCF Density": _packed_lower(mol.p_total),
+    }
+    if mol.c_beta is not None:
+        rec["Beta MO coefficients"] = mol.c_beta.T.reshape(-1)
+    if mol.nalpha != mol.nbeta:
+        rec["Spin SCF Density"] = _packed_lower(mol.p_spin)
+    return rec
+
+
+def serving_molecule(index: int, natoms: int, seed: int) -> SyntheticMolecule:
+    """One molecule of the serving pool: natoms atoms (half heavy, C:N:O =
+    3:1:1, the rest H; 3 atoms give water's composition), the same generator
+    and basis as the workloads, a box at the organic workload's atom density,
+    closed shell (the cation when the electron count is odd)."""
+    if natoms <= 3:
+        counts = {"O": 1, "H": max(0, natoms - 1)}
+    else:
+        heavy = max(1, natoms // 2)
+        c = max(1, round(0.6 * heavy))
+        nn = (heavy - c) // 2
+        counts = {"C": c, "N": nn, "O": heavy - c - nn, "H": natoms - heavy}
+    nelec = sum(ELEMENT_Z[e] * k for e, k in counts.items())
+    box = max(6.0, 12.0 * (natoms / 40.0) ** (1.0 / 3.0))
+    return organic(f"serve_{index}_{natoms}", counts, seed, box, charge=nelec % 2)
+
+
+def serving_pool(count: int = 32, seed: int = 7, min_atoms: int = 3, max_atoms: int = 200) -> List[Tuple[int, int, int]]:
+    """(index, atoms, seed) of the serving pool: atom counts log-uniform in
+    [min_atoms, max_atoms] from a seeded generator."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(math.log(min_atoms), math.log(max_atoms + 1), count)).astype(int)
+    return [(i, int(max(min_atoms, min(max_atoms, n))), seed * 1000 + i) for i, n in enumerate(sizes)]
+
+
+def serving_records(spec: Tuple[int, int, int]) -> Dict[str, object]:
+    """FCHK records of one serving-pool molecule (index, atoms, seed); a
+    module-level function so that a process pool can build the pool."""
+    index, natoms, seed = spec
+    return fchk_records(serving_molecule(index, natoms, seed))
+
+
 def write_fchk(mol: SyntheticMolecule, path: str) -> None:
     """Write the molecule as an FCHK file (gzip-compressed if the path ends in .gz)."""
     opener = gzip.open if path.endswith(".gz") else open

@@ -224,9 +224,9 @@ int kumo_profile_read(kumo_profile_entry* out, int max_entries);
  * graph_points points replay CUDA graphs captured per (molecule, options,
  * properties, point bucket).  Results go to the caller's host arrays (which,
  * like the molecule, must stay valid until the request is done); latency runs
- * from submit until the results are in those arrays.  Zero / negative option
- * fields take the defaults: budget 150 GB capped at 90% of free memory, 8
- * slots, 65536 graph points, 1 GiB AO scratch per request. */
+ * from submit until the results are in those arrays.  Zero option fields take
+ * the defaults: budget 150 GB capped at 90% of free memory, 8 slots, 65536
+ * graph points (negative: no graphs), 1 GiB AO scratch per request. */
 typedef struct kumo_server kumo_server;
 
 typedef struct {
@@ -244,6 +244,9 @@ typedef struct {
     double points_per_s;  /* completed points / busy_s */
     long long graph_captures, graph_replays, direct_runs;
     double peak_bytes, budget_bytes;
+    double launch_s;  /* scheduler host time issuing requests */
+    double copy_s;    /* completion-thread time copying results */
+    double queue_ms;  /* mean submit-to-admission time */
 } kumo_server_stats;
 
 int kumo_server_create(const kumo_server_options* opt, kumo_server** out, char* err, size_t errlen);
