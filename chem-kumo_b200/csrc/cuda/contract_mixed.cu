@@ -291,28 +291,49 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
             const bool keep = prm.threshold == 0.0f || mx > prm.threshold;
             keys[k] = keep ? static_cast<unsigned char>(e < 0 ? 0 : (e >= kBuckets ? kBuckets - 1 : e)) : 0xffu;
         }
+        for (int b = tid; b <= kBuckets; b += kThreads) bucket_start[b] = 0;
         __syncthreads();
-        int cnt = 0;
-        if (tid < kBuckets) {
-            for (int k = 0; k < nk; ++k) cnt += keys[k] == tid;
-            bucket_start[tid] = cnt;
-        }
+        for (int k = tid; k < nk; k += kThreads)
+            if (keys[k] != 0xffu) atomicAdd(&bucket_start[keys[k]], 1);
         __syncthreads();
-        if (tid == 0) {
-            int run = 0;
-            for (int b = 0; b < kBuckets; ++b) {
-                const int c = bucket_start[b];
-                bucket_start[b] = run;
-                run += c;
+        if (w == 0) {
+            // Exclusive scan of the 128 bucket counts, 4 buckets per lane.
+            int c[4], local = 0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                c[i] = bucket_start[4 * lane + i];
+                local += c[i];
             }
-            bucket_start[kBuckets] = run;
+            int incl = local;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            int run = incl - local;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                bucket_start[4 * lane + i] = run;
+                run += c[i];
+            }
+            if (lane == 31) bucket_start[kBuckets] = incl;
+            __syncwarp();
+            // Stable scatter in row order, 32 rows at a time.
+            for (int base = 0; base < nk; base += 32) {
+                const int k = base + lane;
+                const unsigned key = k < nk ? keys[k] : 0xffu;
+                const unsigned same = __match_any_sync(0xffffffffu, key);
+                const int rank = __popc(same & ((1u << lane) - 1u));
+                const int start = key != 0xffu ? bucket_start[key] : 0;
+                __syncwarp();
+                if (key != 0xffu) {
+                    perm[start + rank] = k;
+                    if (rank == __popc(same) - 1) bucket_start[key] = start + rank + 1;
+                }
+                __syncwarp();
+            }
         }
         __syncthreads();
-        if (tid < kBuckets && cnt > 0) {
-            int pos = bucket_start[tid];
-            for (int k = 0; k < nk; ++k)
-                if (keys[k] == tid) perm[pos++] = k;
-        }
         nk = bucket_start[kBuckets];
     }
     const int ntiles = (nk + 15) / 16;
@@ -327,6 +348,14 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
     const int k8 = tid & 7, g = (tid >> 3) & 15, kh = tid >> 7;
     const unsigned a_off = static_cast<unsigned>(g * 128 + kh * 2048 + k8 * 16);
     const unsigned idesc = instr_desc(N);
+    // Descriptors of stage 0, piece 0, panel 0; the start-address field (in
+    // 16-byte units) is advanced by plain addition.
+    const unsigned long long a_desc0 = smem_desc(smem_u32(a_st), 2048u, 128u);
+    const unsigned long long b_desc0 = smem_desc(smem_u32(b_st), static_cast<unsigned>(N * 16), 128u);
+    // Gather of the coefficient chunks: chunk v = ((piece * 2 + rh) * N/8 + ng) * 8 + r8;
+    // division by N/8 (< 64) as a multiply-shift, exact for v / 8 < 2^10.
+    const unsigned nb8 = static_cast<unsigned>(N / 8);
+    const unsigned nb8_mul = (65536u + nb8 - 1u) / nb8;
     const int quarter = w & 3, half = w >> 2;
     const int point = quarter * 32 + lane;
 
@@ -359,10 +388,37 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
                     }
                 }
             };
-            if (ntiles > 0) load_a(0);
+            // Coefficient pieces of step t into stage `stage`: 3 pieces x 16 rows x
+            // N/8 chunks of 16 B, one cp.async group.
+            auto load_b = [&](int t, int stage) {
+                const unsigned bst = smem_u32(b_st + stage * b_bytes);
+                const int nchunk = 3 * 16 * (N / 8);
+                for (int v = tid; v < nchunk; v += kThreads) {
+                    const int r8 = v & 7;
+                    const unsigned rest = static_cast<unsigned>(v) >> 3;
+                    const unsigned rest2 = (rest * nb8_mul) >> 16;
+                    const int ng = static_cast<int>(rest - rest2 * nb8);
+                    const int rh = static_cast<int>(rest2 & 1u), piece = static_cast<int>(rest2 >> 1);
+                    const int k = t * 16 + rh * 8 + r8;
+                    const int col = n0 + ng * 8;
+                    const bool ok = k < nk && col < ch.ldn;
+                    const int row = ok ? (sorted ? perm[k] : k) : 0;
+                    const std::uint16_t* src =
+                        ch.cs + (ok ? piece * ch.piece_stride + static_cast<long long>(kept[row]) * ch.ldn + col : 0);
+                    cp_async16(bst + static_cast<unsigned>(piece * 32 * N + ng * 128 + rh * (N * 16) + r8 * 16), src,
+                               ok);
+                }
+                asm volatile("cp.async.commit_group;" ::: "memory");
+            };
+            // Step t+1's stage is released by the MMAs of step t+1-S, which are
+            // waited for at the end of step t; its coefficient pieces are then
+            // fetched while step t+1's AO pieces are split.
+            if (ntiles > 0) {
+                load_a(0);
+                load_b(0, static_cast<int>(gtile % S));
+            }
             for (int t = 0; t < ntiles; ++t, ++gtile) {
                 const int s = static_cast<int>(gtile % S);
-                if (gtile >= S && !mbar_wait(&bar[s], static_cast<unsigned>((gtile / S - 1) & 1))) failed = true;
                 // A pieces of this step.
                 unsigned char* ast = a_st + s * L::a_bytes;
 #pragma unroll
@@ -374,25 +430,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
                     *reinterpret_cast<uint4*>(ast + (2 * P + c) * kATile + a_off) = p2;
                 }
                 if (t + 1 < ntiles) load_a(t + 1);
-                // Coefficient pieces of this step: 3 pieces x 16 rows x N/8 chunks of 16 B.
-                const unsigned bst = smem_u32(b_st + s * b_bytes);
-                const int nchunk = 3 * 16 * (N / 8);
-                for (int v = tid; v < nchunk; v += kThreads) {
-                    const int r8 = v & 7;
-                    const int rest = v >> 3;
-                    const int ng = rest % (N / 8);
-                    const int rest2 = rest / (N / 8);
-                    const int rh = rest2 & 1, piece = rest2 >> 1;
-                    const int k = t * 16 + rh * 8 + r8;
-                    const int col = n0 + ng * 8;
-                    const bool ok = k < nk && col < ch.ldn;
-                    const int row = ok ? (sorted ? perm[k] : k) : 0;
-                    const std::uint16_t* src =
-                        ch.cs + (ok ? piece * ch.piece_stride + static_cast<long long>(kept[row]) * ch.ldn + col : 0);
-                    cp_async16(bst + static_cast<unsigned>(piece * 32 * N + ng * 128 + rh * (N * 16) + r8 * 16), src,
-                               ok);
-                }
-                asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+                asm volatile("cp.async.wait_group 0;" ::: "memory");
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 if (__syncthreads_or(failed)) {
                     failed = true;
@@ -400,7 +438,9 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
                 }
                 if (tid == 0) {
                     tc_fence_after();
-                    const unsigned ab = smem_u32(ast), bb = bst;
+                    const unsigned long long as = a_desc0 + ((static_cast<unsigned>(s) * L::a_bytes) >> 4);
+                    const unsigned long long bs = b_desc0 + ((static_cast<unsigned>(s) * b_bytes) >> 4);
+                    const unsigned bpiece = (32u * static_cast<unsigned>(N)) >> 4;
                     // K steps go round-robin to G accumulator groups.
                     const unsigned dg = tmem + static_cast<unsigned>(t % G) * gcols;
                     constexpr int pi[6] = {1, 0, 2, 0, 1, 0}, pj[6] = {1, 2, 0, 1, 0, 0};
@@ -408,13 +448,17 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
                     for (int c = 0; c < P; ++c) {
 #pragma unroll
                         for (int e = 0; e < 6; ++e) {
-                            const unsigned long long ad = smem_desc(ab + (pi[e] * P + c) * kATile, 2048u, 128u);
-                            const unsigned long long bd =
-                                smem_desc(bb + static_cast<unsigned>(pj[e] * 32 * N), static_cast<unsigned>(N * 16), 128u);
+                            const unsigned long long ad = as + static_cast<unsigned>(((pi[e] * P + c) * kATile) >> 4);
+                            const unsigned long long bd = bs + static_cast<unsigned>(pj[e]) * bpiece;
                             tc_mma(dg + static_cast<unsigned>(c * N), ad, bd, idesc, (t >= G || e > 0) ? 1u : 0u);
                         }
                     }
                     tc_commit(&bar[s]);
+                }
+                if (t + 1 < ntiles) {
+                    const long long w = gtile + 1 - S;
+                    if (w >= 0 && !mbar_wait(&bar[w % S], static_cast<unsigned>((w / S) & 1))) failed = true;
+                    load_b(t + 1, static_cast<int>((gtile + 1) % S));
                 }
             }
             if (failed || ntiles == 0) continue;
@@ -430,7 +474,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
             const int i_lo = half * (N / 2), i_hi = min(nvalid, (half + 1) * (N / 2));
             const unsigned lane_addr = tmem + (static_cast<unsigned>(quarter * 32) << 16);
             const int ng = ntiles < G ? ntiles : G;
-            constexpr int MG = P == 10 ? 4 : 8;
+            constexpr int MG = 4;
             for (int i0 = i_lo; i0 < i_hi; i0 += MG) {
                 // tcgen05.ld is warp-collective: the trip count depends on the
                 // half only; columns past the last MO are read and ignored.
@@ -472,6 +516,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
     }
 
     if (failed) {
+        asm volatile("cp.async.wait_group 0;" ::: "memory");  // no copy in flight at exit
         if (tid == 0) atomicOr(prm.status, 1u);
         // Let the MMAs already issued finish before tensor memory is freed.
         for (int s = 0; s < S; ++s) {

@@ -168,9 +168,6 @@ public:
         }
         if (opt_.block_size > static_cast<std::size_t>(kumo_dev::kBlockPoints))
             throw std::invalid_argument("the B200 evaluator supports block_size up to 128");
-        if (plan_.needs_esp() && opt_.potential_tolerance != 0.0)
-            throw std::invalid_argument(
-                "the B200 evaluator computes the electrostatic potential exactly: set potential_tolerance to 0");
     }
 
     Backend backend() const { return backend_; }
@@ -582,9 +579,9 @@ private:
         double* out = nullptr;
         for (const auto& [key, ptr] : outs_)
             if (key.kind == PropertyKind::ElectrostaticPotential) out = ptr;
-        if (opt_.potential_tolerance != 0.0)
-            throw std::invalid_argument(
-                "the B200 evaluator computes the electrostatic potential exactly: set potential_tolerance to 0");
+        // Every primitive pair is evaluated exactly, so the result meets any
+        // potential_tolerance >= 0 (src/electrostatic_potential.cpp:501-521
+        // bounds the far-field error by the tolerance; here it is rounding).
         kumo_dev::EspDevice& esp = esp_state();
         kumo_dev::EspParams ep{};
         ep.esp = esp.view();

@@ -317,6 +317,20 @@ def test_esp_exact_vs_oracle_and_multiwfn():
         assert ratio.max() <= 1.0
 
 
+@pytest.mark.parametrize("tol", [1e-8, 1e-6])
+def test_esp_with_tolerance_within_bound(tol):
+    # chem-kumo's potential_tolerance bounds the error at every point
+    # (src/electrostatic_potential.cpp:501-521); the device evaluates every
+    # pair exactly, so grids and points agree with the exact oracle to rounding.
+    m, o = _pair(os.path.join(GOLDEN, "acrolein.fchk.gz"))
+    grid = m.grid_around(2.0, 0.6)
+    esp = [K.density(P.ElectrostaticPotential)]
+    got, _ = K.Evaluator(m, potential_tolerance=tol).evaluate_grid(grid, esp)
+    ref = O.OracleESP(o).evaluate(grid.points())
+    assert np.max(np.abs(got[0][0] - ref)) <= tol
+    assert scaled_error(got[0][0], ref) <= 1e-12
+
+
 def test_boys_device_matches_oracle():
     t = np.concatenate([np.linspace(0.0, 45.0, 2001), [1e-9, 39.999999, 40.0, 200.0, 1e4]])
     got = K.boys(t, 13)
