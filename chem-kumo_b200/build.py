@@ -33,6 +33,7 @@ CUDA_UNITS = {
     "csrc/cuda/ao_mixed.cu": [],
     "csrc/cuda/contract_f64.cu": [],
     "csrc/cuda/contract_mixed.cu": [],
+    "csrc/cuda/contract_p_mixed.cu": [],
     "csrc/cuda/esp.cu": [],
     "csrc/host/device_state.cu": [],
     "csrc/host/evaluator.cu": [],

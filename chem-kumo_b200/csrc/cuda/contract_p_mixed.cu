@@ -1,0 +1,344 @@
+// Mixed-precision AO-P contraction on the tcgen05 tensor cores: the
+// reference's density_derivatives_shared (src/density.cpp:150-229) with
+// Y = P[kept, kept] Phi[kept, panels 0..3] as tensor-core products.
+//
+// One CTA (8 warps) per 128-point block.  For each density matrix needed
+// (total and/or spin) and each chunk of 128 kept columns k, the CTA computes
+// Y_c[point][k] = sum_j Phi_c[j][point] P[j][k] for the value and gradient
+// panels c = 0..3 (M = 128 points, N = 128 columns, K = the kept rows j, four
+// accumulators of 128 columns = all 512 tensor-memory columns).  Operands are
+// split into three BF16 pieces as in the AO-MO contraction (the FP32 panels
+// on the fly, P once at upload); the B tile of a K step is gathered from the
+// pieces of P through the block's kept AO indices.  The epilogue reads Y from
+// tensor memory and folds it, column by column, with the block's FP32 panel
+// values of that column into the per-point FP64 partial sums of the FP64
+// AO-P kernel (q0 = sum Y0 phi, q[1+a] = sum Y0 d_a phi, q[4+a] = sum Y_a
+// d_a phi, then the Laplacian or Hessian terms).  Rows are screened and put
+// in ascending order of their block maximum as in the AO-MO contraction.
+// Every mbarrier wait is bounded; on expiry the CTA flags *status, stores NaN
+// and frees tensor memory after a bounded wait for its MMAs.
+#include <algorithm>
+#include <stdexcept>
+
+#include "mixed.cuh"
+#include "tc_common.cuh"
+
+namespace kumo_dev {
+namespace {
+
+constexpr int kPL = 4;        // left (Y) panels
+constexpr int kCols = 128;    // columns k per chunk (N of the MMA)
+constexpr int kStages = 2;
+
+template <int P>
+struct NQp {
+    static constexpr int v = P == 4 ? 7 : P == 5 ? 8 : 19;
+};
+
+template <int P>
+__device__ __forceinline__ void record_p(const double* f, int ao_order, DevDD& d) {
+    dd_zero(d);
+    d.value = f[0];
+    if (ao_order == 0) return;
+    for (int a = 0; a < 3; ++a) {
+        d.grad[a] = 2.0 * f[1 + a];
+        d.tau_axes[a] = 0.5 * f[4 + a];
+        d.tau += d.tau_axes[a];
+    }
+    if (ao_order < 2) return;
+    if constexpr (P == 10) {
+        for (int h = 0; h < 6; ++h) d.hess[h] = 2.0 * (f[7 + h] + f[13 + h]);
+        d.lap = (d.hess[0] + d.hess[3]) + d.hess[5];
+    } else if constexpr (P == 5) {
+        d.lap = 2.0 * f[7] + 2.0 * ((f[4] + f[5]) + f[6]);
+    }
+}
+
+template <int P>
+struct SmemP {
+    static constexpr int Q = NQp<P>::v;
+    static constexpr unsigned a_bytes = 3u * kPL * kATile;
+    static constexpr unsigned b_bytes = 3u * 32u * kCols;
+    static constexpr size_t total = kStages * (static_cast<size_t>(a_bytes) + b_bytes) + sizeof(double) * Q * 128 +
+                                    sizeof(int) * 2 * kCols + (sizeof(int) + 1) * kSortCap +
+                                    sizeof(int) * (kBuckets + 4) + 8 * kStages + 16;
+};
+
+template <int P>
+__global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __grid_constant__ ContractPMixedParams prm) {
+    using L = SmemP<P>;
+    constexpr int Q = L::Q;
+    constexpr int S = kStages;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    unsigned char* a_st = sm;
+    unsigned char* b_st = sm + S * L::a_bytes;
+    double* red = reinterpret_cast<double*>(b_st + S * L::b_bytes);
+    int* colrow = reinterpret_cast<int*>(red + Q * 128);  // block row of each chunk column (-1: none)
+    int* colao = colrow + kCols;                          // its AO index
+    int* perm = colao + kCols;
+    int* bucket_start = perm + kSortCap;
+    unsigned char* keys = reinterpret_cast<unsigned char*>(bucket_start + kBuckets + 4);
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(keys + kSortCap);
+    unsigned* tslot = reinterpret_cast<unsigned*>(bar + S);
+
+    const int blk = blockIdx.x;
+    const long long start = prm.first_point + static_cast<long long>(blk) * prm.block_size;
+    long long bcount = prm.count - start;
+    if (bcount > prm.block_size) bcount = prm.block_size;
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    const AoScratch<float>& scr = prm.scr;
+    int nk = scr.nkept[blk];
+    const size_t pstride = static_cast<size_t>(scr.row_stride) * kBlockPoints;
+    const float* pbase = scr.panels + static_cast<size_t>(blk) * P * pstride;
+    const int* kept = scr.kept + static_cast<size_t>(blk) * scr.row_stride;
+    const long long n = prm.nao;
+
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (w == 0) tmem_alloc(tslot, 512u);
+    bool sorted = false;
+    nk = block_row_order(scr.rowmax ? scr.rowmax + static_cast<size_t>(blk) * scr.row_stride * 4 : nullptr, nk,
+                         prm.threshold, perm, bucket_start, keys, sorted);
+    const int ntiles = (nk + 15) / 16;
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = *tslot;
+
+    const int k8 = tid & 7, g = (tid >> 3) & 15, kh = tid >> 7;
+    const unsigned a_off = static_cast<unsigned>(g * 128 + kh * 2048 + k8 * 16);
+    const unsigned idesc = instr_desc(kCols);
+    const unsigned long long a_desc0 = smem_desc(smem_u32(a_st), 2048u, 128u);
+    const unsigned long long b_desc0 = smem_desc(smem_u32(b_st), static_cast<unsigned>(kCols * 16), 128u);
+    const int quarter = w & 3, half = w >> 2;
+    const int point = quarter * 32 + lane;
+
+    bool failed = false;
+    long long gtile = 0;
+    DevDD tot, spn;
+    dd_zero(tot);
+    dd_zero(spn);
+    const std::uint16_t* mats[2];
+    int roles[2], nmat = 0;
+    if (prm.total_needed) {
+        mats[nmat] = prm.p_total_s;
+        roles[nmat++] = 0;
+    }
+    if (prm.spin_needed) {
+        mats[nmat] = prm.p_spin_s;
+        roles[nmat++] = 3;
+    }
+    const long long piece_stride = n * n;
+
+    for (int mi = 0; mi < nmat && !failed; ++mi) {
+        const std::uint16_t* Pm = mats[mi];
+        double q[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) q[i] = 0.0;
+        for (int c0 = 0; c0 < nk && !failed; c0 += kCols) {
+            for (int c = tid; c < kCols; c += kThreads) {
+                const int r = c0 + c < nk ? (sorted ? perm[c0 + c] : c0 + c) : -1;
+                colrow[c] = r;
+                colao[c] = r >= 0 ? kept[r] : -1;
+            }
+            __syncthreads();
+            float4 ra[kPL][2];
+            auto load_a = [&](int t) {
+                const int k = t * 16 + kh * 8 + k8;
+                const bool ok = k < nk;
+                const int row = ok ? (sorted ? perm[k] : k) : 0;
+#pragma unroll
+                for (int c = 0; c < kPL; ++c) {
+                    if (ok) {
+                        const float4* src =
+                            reinterpret_cast<const float4*>(pbase + static_cast<size_t>(c) * pstride +
+                                                            static_cast<size_t>(row) * kBlockPoints + g * 8);
+                        ra[c][0] = __ldcs(src);
+                        ra[c][1] = __ldcs(src + 1);
+                    } else {
+                        ra[c][0] = ra[c][1] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+                }
+            };
+            // B tile of step t: P pieces at (kept row of K row j, kept column c),
+            // 3 pieces x 16 rows x 16 groups of 8 columns; unit v = ((piece*2 + jh)*16 + cg)*8 + j8.
+            auto load_b = [&](int t, int stage) {
+                unsigned char* bst = b_st + stage * L::b_bytes;
+                for (int v = tid; v < 3 * 16 * (kCols / 8); v += kThreads) {
+                    const int j8 = v & 7, cg = (v >> 3) & 15, jh = (v >> 7) & 1, piece = v >> 8;
+                    const int j = t * 16 + jh * 8 + j8;
+                    const int rao = j < nk ? kept[sorted ? perm[j] : j] : -1;
+                    unsigned short h[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        const int cao = colao[cg * 8 + u];
+                        h[u] = (rao >= 0 && cao >= 0) ? Pm[piece * piece_stride + static_cast<long long>(rao) * n + cao]
+                                                      : static_cast<unsigned short>(0);
+                    }
+                    const uint4 val = make_uint4(h[0] | (static_cast<unsigned>(h[1]) << 16),
+                                                 h[2] | (static_cast<unsigned>(h[3]) << 16),
+                                                 h[4] | (static_cast<unsigned>(h[5]) << 16),
+                                                 h[6] | (static_cast<unsigned>(h[7]) << 16));
+                    *reinterpret_cast<uint4*>(bst + piece * 32 * kCols + cg * 128 + jh * (kCols * 16) + j8 * 16) = val;
+                }
+            };
+            if (ntiles > 0) {
+                load_a(0);
+                load_b(0, static_cast<int>(gtile % S));
+            }
+            for (int t = 0; t < ntiles; ++t, ++gtile) {
+                const int s = static_cast<int>(gtile % S);
+                unsigned char* ast = a_st + s * L::a_bytes;
+#pragma unroll
+                for (int c = 0; c < kPL; ++c) {
+                    uint4 p0, p1, p2;
+                    split8(ra[c][0], ra[c][1], p0, p1, p2);
+                    *reinterpret_cast<uint4*>(ast + (0 * kPL + c) * kATile + a_off) = p0;
+                    *reinterpret_cast<uint4*>(ast + (1 * kPL + c) * kATile + a_off) = p1;
+                    *reinterpret_cast<uint4*>(ast + (2 * kPL + c) * kATile + a_off) = p2;
+                }
+                if (t + 1 < ntiles) load_a(t + 1);
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                if (__syncthreads_or(failed)) {
+                    failed = true;
+                    break;
+                }
+                if (tid == 0) {
+                    tc_fence_after();
+                    const unsigned long long as = a_desc0 + ((static_cast<unsigned>(s) * L::a_bytes) >> 4);
+                    const unsigned long long bs = b_desc0 + ((static_cast<unsigned>(s) * L::b_bytes) >> 4);
+                    constexpr unsigned bpiece = (32u * kCols) >> 4;
+                    constexpr int pi[6] = {1, 0, 2, 0, 1, 0}, pj[6] = {1, 2, 0, 1, 0, 0};
+#pragma unroll
+                    for (int c = 0; c < kPL; ++c) {
+#pragma unroll
+                        for (int e = 0; e < 6; ++e) {
+                            const unsigned long long ad = as + static_cast<unsigned>(((pi[e] * kPL + c) * kATile) >> 4);
+                            const unsigned long long bd = bs + static_cast<unsigned>(pj[e]) * bpiece;
+                            tc_mma(tmem + static_cast<unsigned>(c * kCols), ad, bd, idesc, (t > 0 || e > 0) ? 1u : 0u);
+                        }
+                    }
+                    tc_commit(&bar[s]);
+                }
+                if (t + 1 < ntiles) {
+                    const long long wt = gtile + 1 - S;
+                    if (wt >= 0 && !mbar_wait(&bar[wt % S], static_cast<unsigned>((wt / S) & 1))) failed = true;
+                    load_b(t + 1, static_cast<int>((gtile + 1) % S));
+                }
+            }
+            if (failed || ntiles == 0) continue;
+            const long long last = gtile - 1;
+            if (!mbar_wait(&bar[last % S], static_cast<unsigned>((last / S) & 1))) failed = true;
+            if (__syncthreads_or(failed)) {
+                failed = true;
+                break;
+            }
+            tc_fence_after();
+            // Fold: columns [half*64, half*64 + 64) of the chunk, 4 at a time.
+            const unsigned lane_addr = tmem + (static_cast<unsigned>(quarter * 32) << 16);
+            const int c_hi = min(nk - c0, (half + 1) * (kCols / 2));
+            for (int i0 = half * (kCols / 2); i0 < c_hi; i0 += 4) {
+                unsigned v[kPL][4];
+#pragma unroll
+                for (int c = 0; c < kPL; ++c) tmem_ld<4>(lane_addr + static_cast<unsigned>(c * kCols + i0), v[c]);
+                tmem_wait_ld();
+#pragma unroll
+                for (int c = 0; c < kPL; ++c) reg_fence<4>(v[c]);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (i0 + u >= c_hi) break;
+                    const int r = colrow[i0 + u];
+                    const float* row = pbase + static_cast<size_t>(r) * kBlockPoints + point;
+                    double y[kPL];
+#pragma unroll
+                    for (int c = 0; c < kPL; ++c) y[c] = static_cast<double>(__uint_as_float(v[c][u]));
+                    const double f0 = row[0];
+                    q[0] += f0 * y[0];
+                    double fa[3];
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        fa[a] = row[(1 + a) * pstride];
+                        q[1 + a] += fa[a] * y[0];
+                        q[4 + a] += fa[a] * y[1 + a];
+                    }
+                    if constexpr (P == 5) q[7] += static_cast<double>(row[4 * pstride]) * y[0];
+                    if constexpr (P == 10) {
+                        constexpr int pa[6] = {0, 0, 0, 1, 1, 2}, pc[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+                        for (int h = 0; h < 6; ++h) {
+                            q[7 + h] += static_cast<double>(row[(4 + h) * pstride]) * y[0];
+                            q[13 + h] += fa[pa[h]] * y[1 + pc[h]];
+                        }
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncthreads();
+        }
+        if (failed) break;
+        if (half == 1)
+#pragma unroll
+            for (int i = 0; i < Q; ++i) red[i * 128 + point] = q[i];
+        __syncthreads();
+        if (half == 0) {
+#pragma unroll
+            for (int i = 0; i < Q; ++i) q[i] += red[i * 128 + point];
+            record_p<P>(q, prm.ao_order, roles[mi] == 0 ? tot : spn);
+        }
+        __syncthreads();
+    }
+
+    if (failed) {
+        if (tid == 0) atomicOr(prm.status, 1u);
+        for (int s = 0; s < S; ++s) {
+            const long long last = gtile - 1 - ((gtile - 1 - s) % S + S) % S;
+            if (last >= 0) (void)mbar_wait(&bar[last % S], static_cast<unsigned>((last / S) & 1));
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (w == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, 512u);
+    }
+    if (half != 0 || point >= bcount) return;
+    DevDD comp[4];
+    if (failed) {
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        DevDD d;
+        d.value = d.lap = d.tau = nan;
+        for (int i = 0; i < 3; ++i) d.grad[i] = d.tau_axes[i] = nan;
+        for (int i = 0; i < 6; ++i) d.hess[i] = nan;
+        comp[0] = comp[1] = comp[2] = comp[3] = d;
+    } else {
+        const bool full = P == 10 && prm.ao_order == 2;
+        comp[0] = tot;
+        comp[3] = spn;
+        comp[1] = dd_combine(tot, spn, 1.0, 0.5, full);
+        comp[2] = dd_combine(tot, spn, -1.0, 0.5, full);
+    }
+    store_point(prm.spec, comp, start + point);
+}
+
+template <int P>
+void launch(const ContractPMixedParams& p, cudaStream_t stream) {
+    constexpr size_t kMaxSmem = 227u * 1024u;
+    static_assert(SmemP<P>::total <= kMaxSmem, "AO-P stages exceed shared memory");
+    cudaFuncSetAttribute(contract_p_mixed_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMaxSmem));
+    contract_p_mixed_kernel<P><<<p.nblocks, kThreads, kMaxSmem, stream>>>(p);
+}
+
+}  // namespace
+
+void launch_contract_p_mixed(const ContractPMixedParams& p, int npanel, cudaStream_t stream) {
+    switch (npanel) {
+        case 4: launch<4>(p, stream); break;
+        case 5: launch<5>(p, stream); break;
+        case 10: launch<10>(p, stream); break;
+        default: throw std::invalid_argument("tensor-core AO-P contraction: unsupported panel count");
+    }
+}
+
+}  // namespace kumo_dev

@@ -39,6 +39,27 @@ struct ContractMixedParams {
     unsigned* status = nullptr;  // set nonzero if a pipeline wait ran out
 };
 
+// AO-P form (density_derivatives_shared): Y = P[kept, kept] Phi[kept, 0..3]
+// on the tensor cores, folded with the FP32 panels (4, 5 or 10 of them).
+struct ContractPMixedParams {
+    AoScratch<float> scr;  // ao_mixed layout
+    long long first_point = 0;
+    long long block_size = 128;
+    long long count = 0;
+    int nblocks = 0;
+    int nao = 0;
+    const std::uint16_t* p_total_s = nullptr;  // [3][nao][nao] BF16 pieces of P_total
+    const std::uint16_t* p_spin_s = nullptr;   // same for P_spin
+    int total_needed = 0;
+    int spin_needed = 0;
+    int ao_order = 2;
+    float threshold = 0.0f;
+    FieldSpec spec;
+    unsigned* status = nullptr;
+};
+
+void launch_contract_p_mixed(const ContractPMixedParams& p, int npanel, cudaStream_t stream);
+
 // MO columns per pass, accumulator groups and tensor-memory columns for
 // npanel panels and at most nocc16 (a multiple of 16) occupied MOs per channel.
 void mixed_columns(int npanel, int nocc16, int& ncols, int& groups, int& tmem_cols);

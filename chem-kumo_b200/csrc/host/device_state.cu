@@ -133,6 +133,21 @@ DeviceMolecule::DeviceMolecule(const Molecule& m) {
     const Matrix pt = m.density_matrix(DensityComponent::Total);
     const Matrix ps = m.density_matrix(DensityComponent::Difference);
     p_total = upload(pt.data(), pt.size());
+    auto split_matrix = [&](const Matrix& m) {
+        std::vector<std::uint16_t> pieces(3 * n * n);
+        for (std::size_t r = 0; r < n; ++r)
+            for (std::size_t c = 0; c < n; ++c) {
+                double rest = m(r, c);
+                for (int k = 0; k < 3; ++k) {
+                    const std::uint16_t h = bf16_bits(rest);
+                    pieces[(static_cast<std::size_t>(k) * n + r) * n + c] = h;
+                    rest -= bf16_value(h);
+                }
+            }
+        return upload(pieces.data(), pieces.size());
+    };
+    p_total_s = split_matrix(pt);
+    p_spin_s = split_matrix(ps);
     p_spin = upload(ps.data(), ps.size());
     unrestricted = m.unrestricted();
     const Matrix& ca = m.mo_coefficients(SpinChannel::Alpha);

@@ -47,6 +47,10 @@ struct DeviceMolecule {
     // Occupied MOs of the mixed form as three BF16 pieces (c = c0 + c1 + c2,
     // each the BF16 rounding of what the previous pieces leave), stored
     // [piece][AO][MO] with rows of ldn MOs (a multiple of 16, zero padded).
+    // P_total and P_spin as three BF16 pieces [piece][row][col] for the mixed
+    // AO-P form.
+    std::uint16_t* p_total_s = nullptr;
+    std::uint16_t* p_spin_s = nullptr;
     std::uint16_t* cs_alpha = nullptr;
     std::uint16_t* cs_beta = nullptr;
     int ldn_alpha = 0, ldn_beta = 0;

@@ -285,8 +285,11 @@ private:
             else
                 mo_pass_f64(std::max(0, ao_order), npanel, needed, spec);
         } else {
-            p_pass_f64(std::max(1, ao_order), npanel == kumo_dev::kPanelsValue ? kumo_dev::kPanelsGradient : npanel,
-                       needed, spec);
+            const int np = npanel == kumo_dev::kPanelsValue ? kumo_dev::kPanelsGradient : npanel;
+            if (opt_.precision == Precision::Mixed)
+                p_pass_mixed(std::max(1, ao_order), np, needed, spec);
+            else
+                p_pass_f64(std::max(1, ao_order), np, needed, spec);
         }
         completed_ += n_;
     }
@@ -416,6 +419,57 @@ private:
             detail::profile_end(tok, stream_);
             count_contraction(detail::kProfContractMixed, bp.out.nkept, nb, npanel, cp.nchannels, cp.ch[0].nocc,
                               cp.nchannels > 1 ? cp.ch[1].nocc : 0, sizeof(float));
+            report(std::min(n_, (b0 + nb) * bs));
+        }
+    }
+
+    // Mixed AO-P form: FP32 AO rows (ao_mixed) and the tensor-core
+    // Y = P[kept, kept] Phi contraction (density_derivatives_shared).
+    void p_pass_mixed(int ao_order, int npanel, const std::array<bool, 4>& needed, const kumo_dev::FieldSpec& spec) {
+        const std::size_t bs = block_size();
+        const std::size_t nblocks = (n_ + bs - 1) / bs;
+        const int nao = dev_->basis.nao;
+        const int stride = (nao + 7) / 8 * 8;
+        const std::size_t per_block = sizeof(float) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints +
+                                      sizeof(int) * ((std::size_t)stride + 1) + sizeof(float) * 4 * (std::size_t)stride;
+        const int W = wave_blocks(nblocks, per_block);
+        DeviceAlloc panels(sizeof(float) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints * W, stream_);
+        DeviceAlloc kept(sizeof(int) * (std::size_t)stride * W, stream_);
+        DeviceAlloc nkept(sizeof(int) * (std::size_t)W, stream_);
+        DeviceAlloc rowmax(sizeof(float) * 4 * (std::size_t)stride * W, stream_);
+        kumo_dev::AoMixedParams bp{};
+        bp.basis = dev_->basis;
+        bp.prims = dev_->mix_prims;
+        bp.src = src_;
+        bp.block_size = static_cast<long long>(bs);
+        std::memcpy(bp.tpure, dev_->tpure_g, sizeof bp.tpure);
+        std::memcpy(bp.gcart, dev_->gcart, sizeof bp.gcart);
+        bp.out = {panels.as<float>(), kept.as<int>(), nkept.as<int>(), stride, npanel, rowmax.as<float>()};
+        kumo_dev::ContractPMixedParams cp{};
+        cp.scr = bp.out;
+        cp.block_size = static_cast<long long>(bs);
+        cp.count = static_cast<long long>(n_);
+        cp.nao = nao;
+        cp.p_total_s = dev_->p_total_s;
+        cp.p_spin_s = dev_->p_spin_s;
+        cp.total_needed = needed[0] || needed[1] || needed[2];
+        cp.spin_needed = needed[3] || needed[1] || needed[2];
+        cp.ao_order = ao_order;
+        cp.threshold = static_cast<float>(opt_.screening_threshold);
+        cp.spec = spec;
+        cp.status = kumo_dev::pipeline_status_word();
+        for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
+            const int nb = static_cast<int>(std::min<std::size_t>(W, nblocks - b0));
+            bp.first_point = static_cast<long long>(b0 * bs);
+            bp.nblocks = nb;
+            int tok = detail::profile_begin(detail::kProfAoBuild, stream_);
+            kumo_dev::launch_ao_mixed(bp, npanel, stream_);
+            detail::profile_end(tok, stream_);
+            cp.first_point = bp.first_point;
+            cp.nblocks = nb;
+            tok = detail::profile_begin(detail::kProfContractP, stream_);
+            kumo_dev::launch_contract_p_mixed(cp, npanel, stream_);
+            detail::profile_end(tok, stream_);
             report(std::min(n_, (b0 + nb) * bs));
         }
     }

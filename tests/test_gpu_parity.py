@@ -382,6 +382,42 @@ def test_mixed_tensor_core_panels_and_components(name, case):
         assert err <= tol, (p, err)
 
 
+@pytest.mark.parametrize("case", ["gradient", "laplacian", "hessian"])
+@pytest.mark.parametrize("name", ["o2.fchk.gz", "acrolein.fchk.gz"])
+def test_mixed_tensor_core_ao_p(name, case):
+    # The AO-P form (Y = P Phi on the tensor cores) against the FP64 AO-P path,
+    # every density component.
+    m, o = _pair(os.path.join(GOLDEN, name))
+    pts = _box_points(o.atom_xyz.reshape(-1, 3), 2500, 6)
+    comps = [D.Total, D.Alpha, D.Beta, D.Difference] if name == "o2.fchk.gz" else [D.Total]
+    props = [K.density(k, c) for k in MIXED_CASES[case] for c in comps if not (k == P.Elf and c == D.Difference)]
+    f64, used = K.Evaluator(m, backend=K.Backend.AO_P).evaluate_points(pts, props)
+    mix, used_m = K.Evaluator(m, backend=K.Backend.AO_P, precision=K.Precision.Mixed).evaluate_points(pts, props)
+    assert used == used_m == int(K.Backend.AO_P)
+    total = {p.kind: r for p, r in zip(props, f64) if p.component == D.Total}
+    for p, a, r in zip(props, mix, f64):
+        assert np.all(np.isfinite(a)), p
+        if p.kind == P.Elf:
+            # Y = sum_j phi_j P_jk sums many cancelling density-matrix entries,
+            # and D = tau - |grad rho|^2 / 8 rho of ELF cancels again: the
+            # mixed AO-P form holds ELF to 1e-4 (the AO-MO form to 1e-5).
+            assert np.abs(a - r).max() <= 1e-4, (p, np.abs(a - r).max())
+            continue
+        scale = max(1.0, np.abs(total[p.kind]).max()) if p.component == D.Difference else max(1.0, np.abs(r).max())
+        assert np.abs(a - r).max() / scale <= 1e-6, (p, np.abs(a - r).max() / scale)
+
+
+def test_mixed_tensor_core_ao_p_many_column_chunks(synth_cache):
+    # 740 AOs: about six 128-column chunks of Y per block.
+    m = K.Molecule.from_fchk(synth.workload_fchk("organic_740", synth_cache))
+    pts = _box_points(m.atoms()[2], 1024, 4)
+    props = [K.density(P.Density), K.density(P.Gradient), K.density(P.Laplacian), K.density(P.Tau)]
+    f64, _ = K.Evaluator(m, backend=K.Backend.AO_P).evaluate_points(pts, props)
+    mix, _ = K.Evaluator(m, backend=K.Backend.AO_P, precision=K.Precision.Mixed).evaluate_points(pts, props)
+    for p, a, r in zip(props, mix, f64):
+        assert scaled_error(a, r) <= 1e-6, (p, scaled_error(a, r))
+
+
 def test_mixed_tensor_core_several_mo_passes(synth_cache):
     # 76 occupied MOs: with the full Hessian (10 panels) a pass holds 48 MO
     # columns of tensor memory, so the contraction takes two passes.
