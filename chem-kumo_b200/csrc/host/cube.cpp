@@ -2,12 +2,15 @@
 // src/cube.cpp:70-111 (six decimals in the header, %13.5e values, six per
 // line and a break after every run along the third axis).
 #include <algorithm>
+#include <charconv>
 #include <cinttypes>
 #include <cmath>
 #include <cstdio>
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "chem/kumo/density.hpp"
 
@@ -49,20 +52,32 @@ void write_field_cube(const std::filesystem::path& path, const std::string& comm
     }
     if (is_orbital) std::fprintf(o, "%5d%5zu\n", 1, orbital);
     const std::size_t nz = static_cast<std::size_t>(grid.counts[2]);
-    // Buffered formatting of the values: 13 characters per value.
-    std::string buf;
-    buf.reserve(1 << 20);
-    char tmp[32];
-    for (std::size_t i = 0; i < values.size(); ++i) {
-        const int len = std::snprintf(tmp, sizeof tmp, "%13.5e", values[i]);
-        buf.append(tmp, static_cast<std::size_t>(len));
-        if ((i + 1) % 6 == 0 || (i + 1) % nz == 0) buf.push_back('\n');
-        if (buf.size() > (1 << 20) - 64) {
-            std::fwrite(buf.data(), 1, buf.size(), o);
-            buf.clear();
+    // The values: %13.5e (std::to_chars gives the same correctly rounded
+    // digits as printf), a break after every sixth value of the whole array
+    // and after each run along the third axis; formatted on all host threads,
+    // each taking a contiguous range of runs, then written in order.
+    const std::size_t runs = nz ? values.size() / nz : 0;
+    const std::size_t nthreads =
+        std::max<std::size_t>(1, std::min<std::size_t>(std::thread::hardware_concurrency(), runs / 64 + 1));
+    std::vector<std::string> parts(nthreads);
+    auto format = [&](std::size_t t) {
+        const std::size_t r0 = runs * t / nthreads, r1 = runs * (t + 1) / nthreads;
+        std::string& buf = parts[t];
+        buf.reserve((r1 - r0) * nz * 14 + (r1 - r0) + 16);
+        char tmp[32];
+        for (std::size_t i = r0 * nz; i < r1 * nz; ++i) {
+            const auto res = std::to_chars(tmp, tmp + sizeof tmp, values[i], std::chars_format::scientific, 5);
+            const std::size_t len = static_cast<std::size_t>(res.ptr - tmp);
+            if (len < 13) buf.append(13 - len, ' ');
+            buf.append(tmp, len);
+            if ((i + 1) % 6 == 0 || (i + 1) % nz == 0) buf.push_back('\n');
         }
-    }
-    std::fwrite(buf.data(), 1, buf.size(), o);
+    };
+    std::vector<std::thread> pool;
+    for (std::size_t t = 1; t < nthreads; ++t) pool.emplace_back(format, t);
+    format(0);
+    for (auto& th : pool) th.join();
+    for (const auto& b : parts) std::fwrite(b.data(), 1, b.size(), o);
     if (std::ferror(o)) throw std::runtime_error(is_orbital ? "orbital cube write failed" : "cube write failed");
 }
 
