@@ -164,3 +164,23 @@ def test_grid_around_matches_reference_formula():
     np.testing.assert_array_equal(g.origin, lo - 3.0)
     for k in range(3):
         assert g.counts[k] == max(2, int(np.ceil((hi[k] - lo[k] + 6.0) / 0.3) + 1))
+
+
+def test_cube_values_match_printf_formatting(tmp_path):
+    # The threaded writer formats with to_chars; its text must equal printf's
+    # %13.5e (chem-kumo's src/cube.cpp:100-110) for any double, line breaks
+    # after every sixth value and after each run along the third axis.
+    rng = np.random.default_rng(3)
+    g = K.Grid(np.zeros(3), np.eye(3) * 0.3, (7, 5, 11))
+    v = rng.standard_normal(g.npoints) * 10.0 ** rng.integers(-300, 300, g.npoints)
+    v[:4] = [0.0, -0.0, 1.0, 9.999995e-5]
+    path = str(tmp_path / "f.cube")
+    K.write_cube(path, g, np.array([1], dtype=np.int32), np.ones(1), np.zeros((1, 3)), v)
+    body = open(path).read().split("\n")[7:]
+    expect, line = [], ""
+    for i, x in enumerate(v):
+        line += "%13.5e" % x
+        if (i + 1) % 6 == 0 or (i + 1) % 11 == 0:
+            expect.append(line)
+            line = ""
+    assert body[:len(expect)] == expect
