@@ -71,6 +71,36 @@ struct ContractPParams {
     FieldSpec spec;
 };
 
+// Orbital-energy sums (src/orbital_energy_fields.hpp:14-264): with the MO
+// columns of each set scaled as the reference scales them (sqrt(n_i) for the
+// occupied, sqrt(w) for the attachment, sqrt(g_i) for the Fukui sets), per
+// point D_s = sum_(i in s) X_i^2 and E_s = sum_(i in s) e_i X_i^2, X = C_s^T phi
+// over every AO (values, shell cutoff only); then the fields of
+// store_orbital_energy_block (src/evaluator.cpp:480-516).
+constexpr int kOrbitalEnergySets = 5;  // occupied, virtual, attachment, Fukui +, Fukui -
+constexpr int kOrbitalEnergyChunk = 128;
+
+struct OrbitalEnergyParams {
+    AoScratch<double> scr;  // values, every AO kept (threshold 0), in AO order
+    long long first_point = 0;
+    long long block_size = 128;
+    long long count = 0;
+    int nblocks = 0;
+    const double* w = nullptr;           // [nao][ldw]: the sets' columns, each set padded to 128-column chunks
+    int ldw = 0;
+    int nchunks = 0;
+    const int* chunk_set = nullptr;      // set of each chunk
+    const double* col_energy = nullptr;  // e_i of each column (0 for padding)
+    int have_virtuals = 0;
+    int have_fukui = 0;
+    int nout = 0;
+    int kinds[9];     // PropertyKind of each output
+    double* outs[9];
+    long long out_base = 0;
+};
+
+void launch_orbital_energy_f64(const OrbitalEnergyParams& p, cudaStream_t stream);
+
 void launch_contract_mo_f64(const ContractMoParams& p, int npanel, cudaStream_t stream);
 void launch_contract_p_f64(const ContractPParams& p, int npanel, cudaStream_t stream);
 void launch_density_values_f64(const ContractPParams& p, cudaStream_t stream);

@@ -235,6 +235,151 @@ void launch_contract_mo_f64(const ContractMoParams& p, int npanel, cudaStream_t 
     }
 }
 
+// Orbital-energy sums: one CTA per 32 points of a block, 8 warps x 16
+// columns of each 128-column chunk, cp.async double-buffered tiles of the AO
+// values and of the column rows; per point the ten set sums are reduced
+// across the warps in a fixed order and the fields are stored.
+template <int KT>
+__global__ void __launch_bounds__(256, 1) orbital_energy_f64_kernel(const __grid_constant__ OrbitalEnergyParams prm) {
+    constexpr int MPT = 16;
+    constexpr int MOC = 8 * MPT;
+    constexpr int NS = kOrbitalEnergySets;
+    extern __shared__ __align__(16) double sm[];
+    double* phs = sm;                  // [2][KT][32]
+    double* cs = phs + 2 * KT * 32;    // [2][KT][MOC]
+    double* red = cs + 2 * KT * MOC;   // [8][2 NS][32]
+
+    const int blk = blockIdx.x >> 2;
+    const int j0 = (blockIdx.x & 3) * 32;
+    const long long start = prm.first_point + (long long)blk * prm.block_size;
+    long long b = prm.count - start;
+    if (b > prm.block_size) b = prm.block_size;
+    if (j0 >= b) return;
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    const AoScratch<double>& scr = prm.scr;
+    const int nk = scr.nkept[blk];
+    const double* pbase = scr.panels + (size_t)blk * scr.row_stride * kBlockPoints + j0;
+    const int* kept = scr.kept + (size_t)blk * scr.row_stride;
+
+    double D[NS], E[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) D[s] = E[s] = 0.0;
+    const int ntiles = (nk + KT - 1) / KT;
+    for (int chunk = 0; chunk < prm.nchunks; ++chunk) {
+        const int mo0 = chunk * MOC;
+        double acc[MPT];
+#pragma unroll
+        for (int t = 0; t < MPT; ++t) acc[t] = 0.0;
+        auto load_tile = [&](int tile, int buf) {
+            const int k0 = tile * KT;
+            double* ph = phs + buf * KT * 32;
+            for (int c = tid; c < KT * 16; c += 256) {
+                const int kk = c / 16, jj = (c % 16) * 2;
+                const bool ok = k0 + kk < nk;
+                cp_async16(ph + kk * 32 + jj, pbase + (size_t)(ok ? k0 + kk : 0) * kBlockPoints + jj, ok);
+            }
+            double* cb = cs + buf * KT * MOC;
+            for (int c = tid; c < KT * MOC / 2; c += 256) {
+                const int kk = c / (MOC / 2), col = (c % (MOC / 2)) * 2;
+                const bool ok = k0 + kk < nk;
+                const double* src = prm.w + (size_t)(ok ? kept[k0 + kk] : 0) * prm.ldw + mo0 + col;
+                cp_async16(cb + kk * MOC + col, src, ok);
+            }
+            cp_async_commit();
+        };
+        if (ntiles > 0) load_tile(0, 0);
+        for (int t = 0; t < ntiles; ++t) {
+            if (t + 1 < ntiles) {
+                load_tile(t + 1, (t + 1) & 1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+            const double* ph = phs + (t & 1) * KT * 32;
+            const double* cb = cs + (t & 1) * KT * MOC + w * MPT;
+#pragma unroll 4
+            for (int kk = 0; kk < KT; ++kk) {
+                const double phi = ph[kk * 32 + lane];
+#pragma unroll
+                for (int t2 = 0; t2 < MPT / 2; ++t2) {
+                    const double2 v = reinterpret_cast<const double2*>(cb + kk * MOC)[t2];
+                    acc[2 * t2] = fma(phi, v.x, acc[2 * t2]);
+                    acc[2 * t2 + 1] = fma(phi, v.y, acc[2 * t2 + 1]);
+                }
+            }
+            __syncthreads();
+        }
+        const int set = prm.chunk_set[chunk];
+        const double* e = prm.col_energy + mo0 + w * MPT;
+        double d = 0.0, en = 0.0;
+#pragma unroll
+        for (int t = 0; t < MPT; ++t) {
+            const double x2 = acc[t] * acc[t];
+            d += x2;
+            en += e[t] * x2;
+        }
+#pragma unroll
+        for (int s = 0; s < NS; ++s)
+            if (s == set) {
+                D[s] += d;
+                E[s] += en;
+            }
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        red[(w * 2 * NS + s) * 32 + lane] = D[s];
+        red[(w * 2 * NS + NS + s) * 32 + lane] = E[s];
+    }
+    __syncthreads();
+    if (w != 0 || j0 + lane >= b) return;
+    double tot[2 * NS];
+#pragma unroll
+    for (int i = 0; i < 2 * NS; ++i) {
+        double v = red[i * 32 + lane];
+#pragma unroll
+        for (int ww = 1; ww < 8; ++ww) v += red[(ww * 2 * NS + i) * 32 + lane];
+        tot[i] = v;
+    }
+    // store_orbital_energy_block (src/evaluator.cpp:485-516).
+    const double rho = tot[0];
+    const double alie = rho > 0.0 ? tot[NS + 0] / rho : 0.0;
+    double lea = 0.0, attachment = 0.0;
+    if (prm.have_virtuals) {
+        const double vir = tot[1];
+        lea = vir > 0.0 ? -tot[NS + 1] / vir : 0.0;
+        attachment = rho > 0.0 ? tot[NS + 2] / rho : 0.0;
+    }
+    double plus = 0.0, minus = 0.0;
+    if (prm.have_fukui) {
+        plus = tot[3];
+        minus = tot[4];
+    }
+    const long long q = start + j0 + lane - prm.out_base;
+    for (int o = 0; o < prm.nout; ++o) {
+        double v;
+        switch (prm.kinds[o]) {
+            case 19: v = alie; break;                  // AverageLocalIonizationEnergy
+            case 20: v = lea; break;                   // LocalElectronAffinity
+            case 21: v = attachment; break;            // LocalElectronAttachmentEnergy
+            case 22: v = 0.5 * (alie + lea); break;    // LocalElectronegativity
+            case 23: v = 0.5 * (alie - lea); break;    // LocalHardness
+            case 26: v = plus; break;                  // OrbitalWeightedFukuiPlus
+            case 27: v = minus; break;                 // OrbitalWeightedFukuiMinus
+            case 28: v = 0.5 * (plus + minus); break;  // OrbitalWeightedFukuiZero
+            default: v = plus - minus; break;          // OrbitalWeightedDualDescriptor
+        }
+        prm.outs[o][q] = v;
+    }
+}
+
+void launch_orbital_energy_f64(const OrbitalEnergyParams& p, cudaStream_t stream) {
+    constexpr int KT = 16;
+    const size_t smem = sizeof(double) * (size_t)(2 * KT * 32 + 2 * KT * 128 + 8 * 2 * kOrbitalEnergySets * 32);
+    cudaFuncSetAttribute(orbital_energy_f64_kernel<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    orbital_energy_f64_kernel<KT><<<p.nblocks * 4, 256, smem, stream>>>(p);
+}
+
 // MO amplitudes (and derivatives) of up to 8 selected MOs: thread per point,
 // summing over every AO in order, as selected^T * phi.
 __global__ void __launch_bounds__(128) orbitals_f64_kernel(const __grid_constant__ OrbitalParams prm) {

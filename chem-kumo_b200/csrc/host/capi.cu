@@ -73,6 +73,7 @@ EvaluationOptions to_options(const kumo_options* o) {
     e.potential_tolerance = o->potential_tolerance;
     if (o->precision != 0 && o->precision != 1) throw std::invalid_argument("unknown precision");
     e.precision = o->precision ? Precision::Mixed : Precision::FP64;
+    e.fukui_delta = o->fukui_delta;
     return e;
 }
 
@@ -180,6 +181,7 @@ void kumo_default_options(kumo_options* opt) {
     opt->screening_threshold = default_screening_threshold;
     opt->potential_tolerance = 1e-8;
     opt->precision = 0;
+    opt->fukui_delta = 0.1;
 }
 
 int kumo_set_device(int device, char* err, size_t errlen) {

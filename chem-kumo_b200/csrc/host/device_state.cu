@@ -195,6 +195,24 @@ kumo_dev::EspDevice& DeviceMolecule::esp_state(const Molecule& m, cudaStream_t s
     return *esp;
 }
 
+const DeviceMolecule::OrbitalEnergyDevice& DeviceMolecule::orbital_energy_state(const Molecule& m,
+                                                                                const OrbitalEnergyNeeds& needs,
+                                                                                const std::string& what) {
+    std::lock_guard<std::mutex> lock(esp_mutex);
+    for (const auto& e : orbital_energy)
+        if (e->needs == needs) return *e;
+    const OrbitalEnergyColumns cols = orbital_energy_columns(m, needs, what);
+    auto e = std::make_unique<OrbitalEnergyDevice>();
+    e->needs = needs;
+    e->ldw = static_cast<int>(cols.ldw);
+    e->nchunks = static_cast<int>(cols.chunk_set.size());
+    e->w = upload(cols.w.data(), cols.w.size());
+    e->energy = upload(cols.energy.data(), cols.energy.size());
+    e->chunk_set = upload(cols.chunk_set.data(), cols.chunk_set.size());
+    orbital_energy.push_back(std::move(e));
+    return *orbital_energy.back();
+}
+
 DeviceMolecule::~DeviceMolecule() {
     int cur = -1;
     cudaGetDevice(&cur);

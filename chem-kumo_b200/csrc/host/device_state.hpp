@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "orbital_energy.hpp"
 #include "../cuda/ao_mixed.cuh"
 #include "../cuda/kumo_device.cuh"
 
@@ -67,6 +68,19 @@ struct DeviceMolecule {
     std::unique_ptr<kumo_dev::EspDevice> esp;
     std::mutex esp_mutex;
     kumo_dev::EspDevice& esp_state(const Molecule& m, cudaStream_t stream);
+    // Scaled MO columns of the orbital-energy sums, one entry per set of
+    // needs met so far, built on first use and kept with the molecule.
+    struct OrbitalEnergyDevice {
+        OrbitalEnergyNeeds needs;
+        double* w = nullptr;  // [nao][ldw]
+        int ldw = 0;
+        int nchunks = 0;
+        int* chunk_set = nullptr;
+        double* energy = nullptr;
+    };
+    std::vector<std::unique_ptr<OrbitalEnergyDevice>> orbital_energy;
+    const OrbitalEnergyDevice& orbital_energy_state(const Molecule& m, const OrbitalEnergyNeeds& needs,
+                                                    const std::string& what);
 
     explicit DeviceMolecule(const Molecule& m);
     ~DeviceMolecule();

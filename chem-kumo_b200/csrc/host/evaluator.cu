@@ -156,9 +156,18 @@ public:
         : mol_(*ev.molecule_), opt_(ev.options_), grid_(grid), points_(device_points), n_(n), stream_(stream),
           plan_(detail::Plan::from(request)) {
         backend_ = detail::choose_backend(opt_.backend, mol_.electronic_structure_info().ao_mo_eligible(), plan_);
+        // The orbital-energy checks come first, naming the most restrictive
+        // group (src/evaluator.cpp:579-597).
+        if (plan_.orbital_energies) {
+            oe_needs_.virtuals = plan_.virtual_orbitals;
+            oe_needs_.fukui = plan_.orbital_weighted_fukui;
+            oe_needs_.fukui_delta = opt_.fukui_delta;
+            oe_what_ = plan_.orbital_weighted_fukui ? "the orbital-weighted Fukui function or dual descriptor"
+                       : plan_.virtual_orbitals    ? "the local electron affinity and related fields"
+                                                   : "the average local ionization energy";
+            detail::check_orbital_energy_fields(mol_, oe_needs_, oe_what_);
+        }
         for (const auto& p : request.properties()) {
-            if (detail::is_orbital_energy_kind(p.kind))
-                throw std::invalid_argument("orbital-energy fields are not evaluated by the B200 grid evaluator");
             // Orbital requests are checked before any pass (src/evaluator.cpp:623-636).
             if (detail::is_orbital_kind(p.kind)) {
                 const auto& c = mol_.mo_coefficients(p.channel);
@@ -191,7 +200,7 @@ public:
         bool point_path = false;
         for (const auto& c : plan_.c) point_path |= uses_point_path(c, backend_, grid);
         // Progress over all passes, src/evaluator.cpp:599-607.
-        passes_ = (point_path ? 1 : 0) + (plan_.needs_esp() ? 1 : 0);
+        passes_ = (point_path ? 1 : 0) + (plan_.needs_esp() ? 1 : 0) + (plan_.orbital_energies ? 1 : 0);
         bool orbital_pass = false;
         bool grid_orbitals[2] = {false, false};
         std::size_t grid_densities = 0;
@@ -209,6 +218,7 @@ public:
 
         if (point_path) point_pass();
         if (plan_.needs_esp()) potential_pass();
+        if (plan_.orbital_energies) orbital_energy_pass();
         if (orbital_pass) orbital_pass_run(false);
         for (const auto& [key, ptr] : outs_)
             if (on_grid_path(key, backend_, grid) && key.kind == PropertyKind::Density) grid_density_pass(key, ptr);
@@ -616,6 +626,51 @@ private:
         completed_ += n_;
     }
 
+    // Orbital-energy fields (src/evaluator.cpp:676-682): per block the AO
+    // values with every AO kept (evaluate_batch: shell cutoff only), then the
+    // set sums over the scaled MO columns and the fields from them.
+    void orbital_energy_pass() {
+        const auto& st = dev_->orbital_energy_state(mol_, oe_needs_, oe_what_);
+        const std::size_t bs = block_size();
+        const std::size_t nblocks = (n_ + bs - 1) / bs;
+        const int nao = dev_->basis.nao;
+        const std::size_t per_block =
+            sizeof(double) * (std::size_t)nao * kumo_dev::kBlockPoints + sizeof(int) * ((std::size_t)nao + 1);
+        const int W = wave_blocks(nblocks, per_block);
+        DeviceAlloc panels(sizeof(double) * (std::size_t)nao * kumo_dev::kBlockPoints * W, stream_);
+        DeviceAlloc kept(sizeof(int) * (std::size_t)nao * W, stream_);
+        DeviceAlloc nkept(sizeof(int) * (std::size_t)W, stream_);
+        kumo_dev::AoBuildParams<double> bp = build_params<double>(0.0);
+        bp.block_size = static_cast<long long>(bs);
+        bp.out = {panels.as<double>(), kept.as<int>(), nkept.as<int>(), nao, 1};
+        kumo_dev::OrbitalEnergyParams op{};
+        op.scr = bp.out;
+        op.block_size = static_cast<long long>(bs);
+        op.count = static_cast<long long>(n_);
+        op.w = st.w;
+        op.ldw = st.ldw;
+        op.nchunks = st.nchunks;
+        op.chunk_set = st.chunk_set;
+        op.col_energy = st.energy;
+        op.have_virtuals = oe_needs_.virtuals ? 1 : 0;
+        op.have_fukui = oe_needs_.fukui ? 1 : 0;
+        for (const auto& [key, ptr] : outs_) {
+            if (!detail::is_orbital_energy_kind(key.kind)) continue;
+            op.kinds[op.nout] = static_cast<int>(key.kind);
+            op.outs[op.nout++] = ptr;
+        }
+        for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
+            const int nb = static_cast<int>(std::min<std::size_t>(W, nblocks - b0));
+            bp.first_point = static_cast<long long>(b0 * bs);
+            bp.nblocks = nb;
+            kumo_dev::launch_ao_build<double>(bp, 0, 1, stream_);
+            op.first_point = bp.first_point;
+            op.nblocks = nb;
+            kumo_dev::launch_orbital_energy_f64(op, stream_);
+        }
+        completed_ += n_;
+    }
+
     void run_orbital_waves(kumo_dev::AoBuildParams<double>& bp, kumo_dev::OrbitalParams& op, std::size_t nblocks, int W,
                            std::size_t bs, int order, int npanel) {
         for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
@@ -664,6 +719,8 @@ private:
     kumo_dev::PointSource src_{};
     std::vector<std::pair<Property, double*>> outs_;
     std::size_t passes_ = 0, completed_ = 0;
+    detail::OrbitalEnergyNeeds oe_needs_;
+    std::string oe_what_;
 };
 
 kumo_dev::EspDevice& Evaluator::Run::esp_state() { return dev_->esp_state(mol_, stream_); }

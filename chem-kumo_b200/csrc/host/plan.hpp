@@ -49,10 +49,28 @@ inline bool is_orbital_energy_kind(PropertyKind k) {
     }
 }
 
+// Names of the orbital-energy fields in error messages
+// (src/evaluation_plan.hpp:112-130).
+inline const char* orbital_energy_name(PropertyKind kind) {
+    switch (kind) {
+        case PropertyKind::AverageLocalIonizationEnergy: return "the average local ionization energy";
+        case PropertyKind::LocalElectronAffinity: return "the local electron affinity";
+        case PropertyKind::LocalElectronAttachmentEnergy: return "the local electron attachment energy";
+        case PropertyKind::LocalElectronegativity: return "the local electronegativity";
+        case PropertyKind::LocalHardness: return "the local hardness";
+        case PropertyKind::OrbitalWeightedFukuiPlus: return "the orbital-weighted Fukui function f+";
+        case PropertyKind::OrbitalWeightedFukuiMinus: return "the orbital-weighted Fukui function f-";
+        case PropertyKind::OrbitalWeightedFukuiZero: return "the orbital-weighted Fukui function f0";
+        default: return "the orbital-weighted dual descriptor";
+    }
+}
+
 struct Plan {
     std::array<ComponentNeeds, 4> c{};
     bool orbitals = false;
     bool orbital_energies = false;
+    bool virtual_orbitals = false;        // the virtual-orbital sums are needed too
+    bool orbital_weighted_fukui = false;  // the orbital-weighted Fukui sums are needed too
     int max_order = -1;
 
     static std::size_t idx(DensityComponent d) { return static_cast<std::size_t>(d); }
@@ -154,10 +172,27 @@ struct Plan {
                     plan.c[idx(DensityComponent::Total)].value_input = true;
                     n.value_input = true;
                     break;
+                case PropertyKind::AverageLocalIonizationEnergy:
+                    total_only(p, orbital_energy_name(p.kind));
+                    plan.orbital_energies = true;
+                    break;
+                case PropertyKind::LocalElectronAffinity:
+                case PropertyKind::LocalElectronAttachmentEnergy:
+                case PropertyKind::LocalElectronegativity:
+                case PropertyKind::LocalHardness:
+                    total_only(p, orbital_energy_name(p.kind));
+                    plan.orbital_energies = true;
+                    plan.virtual_orbitals = true;
+                    break;
+                case PropertyKind::OrbitalWeightedFukuiPlus:
+                case PropertyKind::OrbitalWeightedFukuiMinus:
+                case PropertyKind::OrbitalWeightedFukuiZero:
+                case PropertyKind::OrbitalWeightedDualDescriptor:
+                    total_only(p, orbital_energy_name(p.kind));
+                    plan.orbital_energies = true;
+                    plan.orbital_weighted_fukui = true;
+                    break;
                 default:
-                    if (is_orbital_energy_kind(p.kind))
-                        throw std::invalid_argument(
-                            "orbital-energy fields are not evaluated by the B200 grid evaluator");
                     throw std::invalid_argument("unknown property kind");
             }
         }

@@ -130,7 +130,7 @@ class _Property(C.Structure):
 
 class _Options(C.Structure):
     _fields_ = [("block_size", C.c_longlong), ("backend", C.c_int), ("screening_threshold", C.c_double),
-                ("potential_tolerance", C.c_double), ("precision", C.c_int)]
+                ("potential_tolerance", C.c_double), ("precision", C.c_int), ("fukui_delta", C.c_double)]
 
 
 class _Grid(C.Structure):
@@ -276,8 +276,10 @@ class Grid:
         return self.origin[None, :] + ijk @ np.asarray(self.steps).T
 
 
-def _options(block_size=128, backend=0, threshold=1e-12, potential_tolerance=0.0, precision=0) -> _Options:
-    return _Options(int(block_size), int(backend), float(threshold), float(potential_tolerance), int(precision))
+def _options(block_size=128, backend=0, threshold=1e-12, potential_tolerance=0.0, precision=0,
+             fukui_delta=0.1) -> _Options:
+    return _Options(int(block_size), int(backend), float(threshold), float(potential_tolerance), int(precision),
+                    float(fukui_delta))
 
 
 def _props(props: Sequence[Property]):
@@ -410,9 +412,9 @@ class Evaluator:
     """chem-kumo's Evaluator over the C ABI (host arrays in and out)."""
 
     def __init__(self, molecule: Molecule, block_size: int = 128, backend: int = 0, threshold: float = 1e-12,
-                 potential_tolerance: float = 0.0, precision: int = 0):
+                 potential_tolerance: float = 0.0, precision: int = 0, fukui_delta: float = 0.1):
         self.m = molecule
-        self.opt = _options(block_size, backend, threshold, potential_tolerance, precision)
+        self.opt = _options(block_size, backend, threshold, potential_tolerance, precision, fukui_delta)
 
     def _outs(self, props, n, out=None):
         if out is None:

@@ -59,6 +59,7 @@ typedef struct {
     double screening_threshold; /* default 1e-12 */
     double potential_tolerance; /* 0: exact electrostatic potential */
     int precision;
+    double fukui_delta;         /* Gaussian width of the orbital-weighted Fukui weights (default 0.1 hartree) */
 } kumo_options;
 
 typedef struct {
@@ -83,7 +84,7 @@ typedef struct {
  * tables, density matrices, MO coefficients). */
 typedef struct kumo_molecule kumo_molecule;
 
-/* Fill *opt with the reference defaults (block 128, AUTO, 1e-12, 1e-8, FP64). */
+/* Fill *opt with the reference defaults (block 128, AUTO, 1e-12, 1e-8, FP64, Fukui delta 0.1). */
 void kumo_default_options(kumo_options* opt);
 
 /* Select the CUDA device used by the calls of this thread (one process per

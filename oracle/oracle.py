@@ -243,6 +243,76 @@ class OracleMolecule:
         return res
 
 
+# -- orbital-energy fields ------------------------------------------------------
+ORBITAL_ENERGY_KINDS = (19, 20, 21, 22, 23, 26, 27, 28, 29)
+
+
+def _fukui_weights(e: np.ndarray, mu: float, delta: float) -> np.ndarray:
+    """Normalized Gaussian weights (src/orbital_energy_fields.hpp:77-97)."""
+    x = -((mu - e) / delta) ** 2
+    g = np.exp(x - x.max())
+    return g / g.sum()
+
+
+def orbital_energy_fields(mol: OracleMolecule, pts: np.ndarray, kinds: Sequence[int],
+                          fukui_delta: float = 0.1) -> List[np.ndarray]:
+    """ALIE, LEA, LEAE, local electronegativity and hardness, and the
+    orbital-weighted Fukui functions at `pts` [N, 3]: the orbital sums of
+    src/orbital_energy_fields.hpp:145-264 over the AO values of every shell
+    (evaluate_batch), then the fields of src/evaluator.cpp:480-516."""
+    n = mol.n
+    rec = mol.rec
+    phi = mol.ao_values(pts)  # [nao, N]
+    ca = mol.c_alpha.reshape(mol.nmo_alpha, n).T
+    ea = np.asarray(rec["Alpha Orbital Energies"], dtype=float)
+    na, nb = mol.nalpha, mol.nbeta
+    occ, occ_e, vir, vir_e, att, att_e = [], [], [], [], [], []
+
+    def channel(c, e, occupied, doubly, weight):
+        for i in range(c.shape[1]):
+            if i < occupied:
+                occ.append(np.sqrt(2.0 if i < doubly else 1.0) * c[:, i])
+                occ_e.append(abs(e[i]))
+            else:
+                vir.append(c[:, i])
+                vir_e.append(e[i])
+                if e[i] < 0.0:
+                    att.append(np.sqrt(weight) * c[:, i])
+                    att_e.append(e[i])
+
+    if mol.unrestricted:
+        cb = mol.c_beta.reshape(mol.nmo_beta, n).T
+        eb = np.asarray(rec["Beta Orbital Energies"], dtype=float)
+        channel(ca, ea, na, 0, 1.0)
+        channel(cb, eb, nb, 0, 1.0)
+    else:
+        channel(ca, ea, max(na, nb), min(na, nb), 2.0)
+
+    def sums(cols, energies):
+        if not cols:
+            return np.zeros(phi.shape[1]), np.zeros(phi.shape[1])
+        x2 = (np.array(cols) @ phi) ** 2
+        return x2.sum(0), np.asarray(energies) @ x2
+
+    rho, e_occ = sums(occ, occ_e)
+    d_vir, e_vir = sums(vir, vir_e)
+    _, e_att = sums(att, att_e)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        alie = np.where(rho > 0, e_occ / rho, 0.0)
+        lea = np.where(d_vir > 0, -e_vir / d_vir, 0.0)
+        attach = np.where(rho > 0, e_att / rho, 0.0)
+    plus = minus = np.zeros(phi.shape[1])
+    if any(k >= 26 for k in kinds):
+        mu = 0.5 * (ea[na - 1] + ea[na])
+        gp = _fukui_weights(ea[na:], mu, fukui_delta)
+        gm = _fukui_weights(ea[:na], mu, fukui_delta)
+        plus = gp @ ((ca[:, na:].T @ phi) ** 2)
+        minus = gm @ ((ca[:, :na].T @ phi) ** 2)
+    table = {19: alie, 20: lea, 21: attach, 22: 0.5 * (alie + lea), 23: 0.5 * (alie - lea),
+             26: plus, 27: minus, 28: 0.5 * (plus + minus), 29: plus - minus}
+    return [table[k].copy() for k in kinds]
+
+
 def _channels(kind: int) -> int:
     return 3 if kind in (1, 24, 30, 31) else (6 if kind in (2, 25) else 1)
 

@@ -62,6 +62,22 @@ MULTIWFN = [
     ("o2_esp", "o2.fchk.gz"),
     ("o2_lol", "o2.fchk.gz"),
     ("o2_spin_polarization", "o2.fchk.gz"),
+    # Orbital-energy fields (tests/REFERENCE_CUBES.md, "Orbital-energy fields"
+    # and "Orbital-weighted Fukui functions").
+    ("acrolein_alie", "acrolein.fchk.gz"),
+    ("acrolein_lea", "acrolein.fchk.gz"),
+    ("acrolein_leae", "acrolein.fchk.gz"),
+    ("acrolein_local_electronegativity", "acrolein.fchk.gz"),
+    ("acrolein_local_hardness", "acrolein.fchk.gz"),
+    ("o2_alie", "o2.fchk.gz"),
+    ("o2_lea", "o2.fchk.gz"),
+    ("o2_leae", "o2.fchk.gz"),
+    ("acrolein_ow_fukui_plus", "acrolein.fchk.gz"),
+    ("acrolein_ow_fukui_minus", "acrolein.fchk.gz"),
+    ("acrolein_ow_fukui_zero", "acrolein.fchk.gz"),
+    ("acrolein_ow_dual_descriptor", "acrolein.fchk.gz"),
+    ("h2o_ow_fukui_plus", "h2o_b3lyp_def2tzvp.fchk.gz"),
+    ("h2o_ow_fukui_minus", "h2o_b3lyp_def2tzvp.fchk.gz"),
 ]
 
 FCHK_SOURCES = {

@@ -280,6 +280,54 @@ def test_orbitals():
     _compare(outs2, refs, 1e-12, props)
 
 
+OE_ALL = [19, 20, 21, 22, 23, 26, 27, 28, 29]
+
+
+@pytest.mark.parametrize("name,kinds", [("acrolein.fchk.gz", OE_ALL), ("h2o_b3lyp_def2tzvp.fchk.gz", OE_ALL),
+                                        ("o2.fchk.gz", [19, 20, 21, 22, 23])])
+def test_orbital_energy_fields(name, kinds):
+    # ALIE, LEA, LEAE, chi, eta and the orbital-weighted Fukui functions
+    # against the oracle's restatement, at box points (nuclei included), with
+    # ragged blocks, and on a grid.
+    m, o = _pair(os.path.join(GOLDEN, name))
+    props = [K.density(k) for k in kinds]
+    pts = _box_points(o.atom_xyz.reshape(-1, 3), 3000, 5)
+    refs = O.orbital_energy_fields(o, pts, kinds)
+    for bs in (128, 37):
+        outs, _ = K.Evaluator(m, block_size=bs).evaluate_points(pts, props)
+        _compare(outs, [r[None] for r in refs], 1e-12, props)
+    grid = m.grid_around(2.0, 0.3)
+    outs, _ = K.Evaluator(m).evaluate_grid(grid, props)
+    refs = O.orbital_energy_fields(o, grid.points(), kinds)
+    _compare(outs, [r[None] for r in refs], 1e-12, props)
+
+
+def test_orbital_energy_fields_with_density_and_delta():
+    # Mixed with point-path fields and orbitals in one request, a non-default
+    # Fukui delta, and the mixed precision (the orbital-energy pass is FP64).
+    m, o = _pair(os.path.join(GOLDEN, "acrolein.fchk.gz"))
+    pts = _box_points(o.atom_xyz.reshape(-1, 3), 1500, 9)
+    props = [K.density(P.Density), K.density(P.OrbitalWeightedFukuiPlus), K.density(P.AverageLocalIonizationEnergy),
+             K.orbital(15), K.density(P.OrbitalWeightedDualDescriptor)]
+    refs = O.orbital_energy_fields(o, pts, [26, 19, 29], fukui_delta=0.05)
+    for prec in (K.Precision.FP64, K.Precision.Mixed):
+        outs, _ = K.Evaluator(m, fukui_delta=0.05, precision=prec).evaluate_points(pts, props)
+        _compare([outs[1], outs[2], outs[4]], [r[None] for r in refs], 1e-12, [props[1], props[2], props[4]])
+        alone, _ = K.Evaluator(m).evaluate_points(pts, [K.density(P.Density)])
+        if prec == K.Precision.FP64:
+            assert np.array_equal(outs[0], alone[0])
+
+
+@pytest.mark.parametrize("key,kind,abs_", [("acrolein_alie", 19, 0.0), ("o2_lea", 20, 0.0), ("o2_leae", 21, 1e-10),
+                                           ("acrolein_local_hardness", 23, 0.0)])
+def test_orbital_energy_multiwfn_cubes_on_gpu(key, kind, abs_):
+    g = np.load(os.path.join(GOLDEN, f"multiwfn_{key}.npz"))
+    m = K.Molecule.from_fchk(os.path.join(GOLDEN, str(g["fchk"])))
+    outs, _ = K.Evaluator(m).evaluate_points(golden_points(g), [K.density(kind)])
+    v, ref = outs[0][0], g["values"]
+    assert np.max(np.abs(v - ref) / (2e-5 * np.abs(ref) + abs_ + 1e-300)) <= 1.0
+
+
 def test_golden_gaussian_cubes_on_gpu():
     for key, comp in [("o2_density", 0), ("o2_spin", 3), ("acrolein_density", 0)]:
         g = np.load(os.path.join(GOLDEN, f"gaussian_{key}.npz"))

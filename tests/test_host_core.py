@@ -96,6 +96,37 @@ def test_request_validation_errors():
     _expect(K.InvalidArgument, lambda: ev.evaluate_points(np.array([[np.nan, 0, 0]]), [K.density(P.Density)]))
 
 
+def test_orbital_energy_validation_errors():
+    # The checks of src/orbital_energy_fields.hpp:114-143 with their messages,
+    # naming the most restrictive group requested (src/evaluator.cpp:583-588).
+    P = K.PropertyKind
+    D = K.DensityComponent
+    o2 = K.Molecule.from_fchk(os.path.join(GOLDEN, "o2.fchk.gz"))
+    g = o2.grid_around(1.0, 0.5)
+    msg = _expect(K.InvalidArgument,
+                  lambda: K.Evaluator(o2).evaluate_grid(g, [K.density(P.AverageLocalIonizationEnergy),
+                                                            K.density(P.OrbitalWeightedFukuiPlus)]))
+    assert msg.startswith("the orbital-weighted Fukui function or dual descriptor is defined only for a restricted "
+                          "closed-shell calculation"), msg
+    msg = _expect(K.InvalidArgument, lambda: K.Evaluator(o2).evaluate_grid(g, [K.density(P.Elf),
+                                                                               K.density(P.LocalHardness, D.Alpha)]))
+    assert "only for the total density" in msg
+    msg = _expect(K.InvalidArgument, lambda: K.Evaluator(o2, fukui_delta=0.0).evaluate_grid(
+        g, [K.density(P.OrbitalWeightedFukuiMinus)]))
+    assert "fukui_delta" in msg
+    rec = dict(synth.read_fchk(os.path.join(GOLDEN, "acrolein.fchk.gz")))
+    # Molecule.from_records carries no orbital energies.
+    m = K.Molecule.from_records(rec)
+    msg = _expect(K.InvalidArgument, lambda: K.Evaluator(m).evaluate_grid(
+        m.grid_around(1.0, 0.5), [K.density(P.LocalElectronAffinity)]))
+    assert msg == "the local electron affinity and related fields needs the FCHK orbital energies", msg
+    rec["Total SCF Density"] = np.asarray(rec["Total SCF Density"]) * 1.01
+    m = K.Molecule.from_records(rec)
+    msg = _expect(K.InvalidArgument, lambda: K.Evaluator(m).evaluate_grid(
+        m.grid_around(1.0, 0.5), [K.density(P.AverageLocalIonizationEnergy)]))
+    assert msg.startswith("the average local ionization energy needs occupied MOs that reproduce"), msg
+
+
 def test_ao_mo_requires_eligible(tmp_path):
     # A density matrix that the MOs do not reproduce makes AO-MO ineligible.
     rec = synth.read_fchk(os.path.join(GOLDEN, "o2.fchk.gz"))
