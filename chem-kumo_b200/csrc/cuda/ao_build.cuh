@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(kBlockPoints, sizeof(T) == 8 ? 3 : 5) ao_build
     const bool keep_all = prm.threshold == 0.0;
     const T thr = (T)prm.threshold;
 
-    const int nlist = block_shell_list(B, valid, px, py, pz, keep_all, s_list, s_box, s_count);
+    const int nlist = block_shell_list(B, valid, px, py, pz, keep_all && !prm.keep_reaching, s_list, s_box, s_count);
 
     const T* gexp = sizeof(T) == 8 ? (const T*)B.exps : (const T*)B.exps_f;
     const T* gw = sizeof(T) == 8 ? (const T*)B.weights : (const T*)B.weights_f;

@@ -34,7 +34,7 @@ struct ContractMoParams {
 };
 
 struct OrbitalParams {
-    AoScratch<double> scr;  // every AO kept (threshold 0), in AO order
+    AoScratch<double> scr;  // threshold 0: every AO of the shells reaching the block, in AO order
     long long first_point = 0;
     long long block_size = 128;
     long long count = 0;
@@ -81,7 +81,7 @@ constexpr int kOrbitalEnergySets = 5;  // occupied, virtual, attachment, Fukui +
 constexpr int kOrbitalEnergyChunk = 128;
 
 struct OrbitalEnergyParams {
-    AoScratch<double> scr;  // values, every AO kept (threshold 0), in AO order
+    AoScratch<double> scr;  // values, threshold 0 (every AO of the shells reaching the block), AO order
     long long first_point = 0;
     long long block_size = 128;
     long long count = 0;

@@ -391,14 +391,17 @@ __global__ void __launch_bounds__(128) orbitals_f64_kernel(const __grid_constant
     if (j >= b) return;
     const AoScratch<double>& scr = prm.scr;
     const double* base = scr.panels + (size_t)blk * prm.npanel * scr.row_stride * kBlockPoints + j;
+    const int* kept = scr.kept + (size_t)blk * scr.row_stride;
+    const int nk = scr.nkept[blk];
     const long long q = start + j;
     for (int s = 0; s < prm.nsel; ++s) {
         const double* c = prm.coef[s];
         for (int ch = 0; ch < prm.nchan[s]; ++ch) {
             const int panel = prm.first_channel[s] + ch;
             const double* ph = base + (size_t)panel * scr.row_stride * kBlockPoints;
+            // Kept rows in AO order: the AOs left out are cutoff zeros here.
             double acc = 0.0;
-            for (int k = 0; k < prm.nao; ++k) acc += c[k] * ph[(size_t)k * kBlockPoints];
+            for (int k = 0; k < nk; ++k) acc += c[kept[k]] * ph[(size_t)k * kBlockPoints];
             prm.out[s][ch * prm.stride + (q - prm.out_base)] = acc;
         }
     }

@@ -90,14 +90,19 @@ __device__ __forceinline__ void record(const double* f, int ao_order, DevDD& d) 
     }
 }
 
+// Shared memory of one CTA: S stages of AO pieces, SB = S + 1 stages of
+// coefficient pieces (fetched two K steps ahead), the cross-warp sums, the
+// row order and the AO index of each K row in that order.
 template <int P, int S>
 struct Smem {
     static constexpr int Q = NQm<P>::v;
+    static constexpr int SB = S + 1;
     static constexpr unsigned a_bytes = 3u * P * kATile;  // one stage of A pieces
     __host__ __device__ static unsigned b_bytes(int ncols) { return 3u * 32u * static_cast<unsigned>(ncols); }
     static size_t total(int ncols) {
-        return S * (static_cast<size_t>(a_bytes) + b_bytes(ncols)) + sizeof(double) * Q * 128 +
-               (sizeof(int) + 1) * kSortCap + sizeof(int) * (kBuckets + 4) + 8 * S + 16;
+        return S * static_cast<size_t>(a_bytes) + SB * static_cast<size_t>(b_bytes(ncols)) +
+               sizeof(double) * Q * 128 + (sizeof(int) + 1 + sizeof(std::uint16_t)) * kSortCap +
+               sizeof(int) * (kBuckets + 4) + 8 * S + 16;
     }
 };
 
@@ -105,15 +110,17 @@ template <int P, int S>
 __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __grid_constant__ ContractMixedParams prm) {
     using L = Smem<P, S>;
     constexpr int Q = L::Q;
+    constexpr int SB = L::SB;
     extern __shared__ __align__(1024) unsigned char sm[];
     const int N = prm.ncols;
     const unsigned b_bytes = L::b_bytes(N);
     unsigned char* a_st = sm;
     unsigned char* b_st = sm + S * L::a_bytes;
-    double* red = reinterpret_cast<double*>(b_st + S * b_bytes);
+    double* red = reinterpret_cast<double*>(b_st + SB * b_bytes);
     int* perm = reinterpret_cast<int*>(red + Q * 128);
     int* bucket_start = perm + kSortCap;
-    unsigned char* keys = reinterpret_cast<unsigned char*>(bucket_start + kBuckets + 4);
+    std::uint16_t* aoidx = reinterpret_cast<std::uint16_t*>(bucket_start + kBuckets + 4);
+    unsigned char* keys = reinterpret_cast<unsigned char*>(aoidx + kSortCap);
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(keys + kSortCap);
     unsigned* tslot = reinterpret_cast<unsigned*>(bar + S);
 
@@ -138,6 +145,12 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
     bool sorted = false;
     nk = block_row_order(scr.rowmax ? scr.rowmax + static_cast<size_t>(blk) * scr.row_stride * 4 : nullptr, nk,
                          prm.threshold, perm, bucket_start, keys, sorted);
+    // AO index of each K row, in K order, so that the coefficient gathers
+    // need no dependent global load (blocks of up to kSortCap rows and
+    // bases below 65536 functions; others read the kept list).
+    const bool have_idx = nk <= kSortCap && scr.row_stride <= 65535;
+    if (have_idx)
+        for (int k = tid; k < nk; k += kThreads) aoidx[k] = static_cast<std::uint16_t>(kept[sorted ? perm[k] : k]);
     const int ntiles = (nk + 15) / 16;
     tc_fence_before();
     __syncthreads();
@@ -204,23 +217,26 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
                     const int k = t * 16 + rh * 8 + r8;
                     const int col = n0 + ng * 8;
                     const bool ok = k < nk && col < ch.ldn;
-                    const int row = ok ? (sorted ? perm[k] : k) : 0;
+                    const int ao = ok ? (have_idx ? static_cast<int>(aoidx[k]) : kept[sorted ? perm[k] : k]) : 0;
                     const std::uint16_t* src =
-                        ch.cs + (ok ? piece * ch.piece_stride + static_cast<long long>(kept[row]) * ch.ldn + col : 0);
+                        ch.cs + (ok ? piece * ch.piece_stride + static_cast<long long>(ao) * ch.ldn + col : 0);
                     cp_async16(bst + static_cast<unsigned>(piece * 32 * N + ng * 128 + rh * (N * 16) + r8 * 16), src,
                                ok);
                 }
                 asm volatile("cp.async.commit_group;" ::: "memory");
             };
-            // Step t+1's stage is released by the MMAs of step t+1-S, which are
-            // waited for at the end of step t; its coefficient pieces are then
-            // fetched while step t+1's AO pieces are split.
+            // Step t+1's AO stage is released by the MMAs of step t+1-S, which
+            // are waited for at the end of step t.  Coefficient pieces run two
+            // steps ahead in SB = S + 1 stages: step t+2's stage was last read
+            // by the MMAs of step t+2-SB = t+1-S, complete by then too.
             if (ntiles > 0) {
                 load_a(0);
-                load_b(0, static_cast<int>(gtile % S));
+                load_b(0, static_cast<int>(gtile % SB));
+                if (ntiles > 1) load_b(1, static_cast<int>((gtile + 1) % SB));
             }
             for (int t = 0; t < ntiles; ++t, ++gtile) {
                 const int s = static_cast<int>(gtile % S);
+                const int sb = static_cast<int>(gtile % SB);
                 // A pieces of this step.
                 unsigned char* ast = a_st + s * L::a_bytes;
 #pragma unroll
@@ -232,7 +248,12 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
                     *reinterpret_cast<uint4*>(ast + (2 * P + c) * kATile + a_off) = p2;
                 }
                 if (t + 1 < ntiles) load_a(t + 1);
-                asm volatile("cp.async.wait_group 0;" ::: "memory");
+                // This step's coefficient group is complete; step t+1's may
+                // still be in flight.
+                if (t + 1 < ntiles)
+                    asm volatile("cp.async.wait_group 1;" ::: "memory");
+                else
+                    asm volatile("cp.async.wait_group 0;" ::: "memory");
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 if (__syncthreads_or(failed)) {
                     failed = true;
@@ -241,7 +262,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
                 if (tid == 0) {
                     tc_fence_after();
                     const unsigned long long as = a_desc0 + ((static_cast<unsigned>(s) * L::a_bytes) >> 4);
-                    const unsigned long long bs = b_desc0 + ((static_cast<unsigned>(s) * b_bytes) >> 4);
+                    const unsigned long long bs = b_desc0 + ((static_cast<unsigned>(sb) * b_bytes) >> 4);
                     const unsigned bpiece = (32u * static_cast<unsigned>(N)) >> 4;
                     // K steps go round-robin to G accumulator groups.
                     const unsigned dg = tmem + static_cast<unsigned>(t % G) * gcols;
@@ -260,7 +281,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
                 if (t + 1 < ntiles) {
                     const long long w = gtile + 1 - S;
                     if (w >= 0 && !mbar_wait(&bar[w % S], static_cast<unsigned>((w / S) & 1))) failed = true;
-                    load_b(t + 1, static_cast<int>((gtile + 1) % S));
+                    if (t + 2 < ntiles) load_b(t + 2, static_cast<int>((gtile + 2) % SB));
                 }
             }
             if (failed || ntiles == 0) continue;

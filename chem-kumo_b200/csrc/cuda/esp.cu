@@ -437,7 +437,8 @@ void launch_esp_f64(const EspParams& p, cudaStream_t stream) {
     if (n <= 0) return;
     const unsigned tiles = static_cast<unsigned>((n + 127) / 128);
     const EspView& e = p.esp;
-    // Chunks per order: about 8 CTAs per SM in total, at least 64 pairs a chunk.
+    // Chunks per order: each order's launch (they run one after another)
+    // gets about 8 CTAs per SM, with at least 64 pairs a chunk.
     constexpr long long kTargetCtas = 8 * 148;
     int chunks[kEspMaxL + 1] = {};
     long long chunk_size[kEspMaxL + 1] = {};
@@ -445,7 +446,7 @@ void launch_esp_f64(const EspParams& p, cudaStream_t stream) {
     for (int L = 0; L <= kEspMaxL; ++L) {
         const long long count = e.order_first[L + 1] - e.order_first[L];
         if (count <= 0) continue;
-        long long want = (kTargetCtas * count / std::max<long long>(e.npairs, 1) + tiles - 1) / tiles;
+        long long want = (kTargetCtas + tiles - 1) / tiles;
         want = std::max<long long>(1, std::min<long long>(want, (count + 63) / 64));
         chunk_size[L] = (count + want - 1) / want;
         chunks[L] = static_cast<int>((count + chunk_size[L] - 1) / chunk_size[L]);

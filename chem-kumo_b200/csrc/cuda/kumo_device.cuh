@@ -102,6 +102,10 @@ struct AoBuildParams {
     long long block_size = 128;    // points per screening block (<= 128)
     int nblocks = 0;               // blocks in this wave
     double threshold = 1e-12;      // screening threshold (0 keeps every AO)
+    // With threshold 0: keep every AO of the shells whose cutoff sphere reaches
+    // the block's bounding box (the other AOs are cutoff zeros at every point
+    // of the block), instead of every AO of the basis.
+    int keep_reaching = 0;
     AoScratch<T> out;
     T pure[3][135];                // Cartesian-to-pure matrices, l = 2..4, row-major
 };

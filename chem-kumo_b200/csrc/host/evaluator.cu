@@ -597,6 +597,7 @@ private:
             DeviceAlloc kept(sizeof(int) * (std::size_t)nao * W, stream_);
             DeviceAlloc nkept(sizeof(int) * (std::size_t)W, stream_);
             kumo_dev::AoBuildParams<double> bp = build_params<double>(0.0);
+            bp.keep_reaching = 1;
             bp.block_size = static_cast<long long>(bs);
             bp.out = {panels.as<double>(), kept.as<int>(), nkept.as<int>(), nao, npanel};
             kumo_dev::OrbitalParams op{};
@@ -641,6 +642,7 @@ private:
         DeviceAlloc kept(sizeof(int) * (std::size_t)nao * W, stream_);
         DeviceAlloc nkept(sizeof(int) * (std::size_t)W, stream_);
         kumo_dev::AoBuildParams<double> bp = build_params<double>(0.0);
+        bp.keep_reaching = 1;
         bp.block_size = static_cast<long long>(bs);
         bp.out = {panels.as<double>(), kept.as<int>(), nkept.as<int>(), nao, 1};
         kumo_dev::OrbitalEnergyParams op{};

@@ -5,9 +5,11 @@
 #include "device_state.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <limits>
 #include <stdexcept>
+#include <thread>
 
 namespace chem::kumo {
 namespace {
@@ -68,7 +70,11 @@ std::vector<Atom> read_atoms(const FormattedCheckpoint& f) {
 }
 
 // Frobenius norms of P_total - (Pa + Pb) and P_spin - (Pa - Pb) with
-// Pa = Ca,occ Ca,occ^T and Pb likewise, and of the four matrices.
+// Pa = Ca,occ Ca,occ^T and Pb likewise, and of the four matrices.  Rows are
+// taken in tiles of 32 (each tile of Pa and Pb stays in cache while the
+// occupied columns stream past once) spread over the host threads; the
+// per-tile sums are added in tile order, so the result does not depend on
+// the thread count.
 struct CheckNorms {
     double total_err = 0, spin_err = 0, total = 0, rtotal = 0, spin = 0, rspin = 0;
 };
@@ -76,31 +82,59 @@ struct CheckNorms {
 CheckNorms check_norms(const Matrix& total, const Matrix& spin, const Matrix& ca, std::size_t na,
                        const Matrix& cb, std::size_t nb) {
     const std::size_t n = total.rows();
-    std::vector<double> pa(n * n, 0.0), pb(n * n, 0.0);
-    auto outer = [n](const Matrix& c, std::size_t nocc, std::vector<double>& p) {
-        for (std::size_t o = 0; o < nocc; ++o) {
-            const double* col = c.col(o);
-            for (std::size_t i = 0; i < n; ++i) {
-                const double ci = col[i];
-                double* row = p.data() + i * n;
-                for (std::size_t j = 0; j < n; ++j) row[j] += ci * col[j];
+    constexpr std::size_t tile = 32;
+    const std::size_t ntiles = (n + tile - 1) / tile;
+    std::vector<CheckNorms> part(ntiles);
+    auto run_tile = [&](std::size_t t, std::vector<double>& pa, std::vector<double>& pb) {
+        const std::size_t i0 = t * tile, rows = std::min(tile, n - i0);
+        std::fill(pa.begin(), pa.begin() + rows * n, 0.0);
+        std::fill(pb.begin(), pb.begin() + rows * n, 0.0);
+        auto outer = [&](const Matrix& c, std::size_t nocc, std::vector<double>& p) {
+            for (std::size_t o = 0; o < nocc; ++o) {
+                const double* col = c.col(o);
+                for (std::size_t r = 0; r < rows; ++r) {
+                    const double ci = col[i0 + r];
+                    double* row = p.data() + r * n;
+                    for (std::size_t j = 0; j < n; ++j) row[j] += ci * col[j];
+                }
             }
-        }
+        };
+        outer(ca, na, pa);
+        outer(cb, nb, pb);
+        CheckNorms r;
+        for (std::size_t q = 0; q < rows; ++q)
+            for (std::size_t j = 0; j < n; ++j) {
+                const double rt = pa[q * n + j] + pb[q * n + j], rs = pa[q * n + j] - pb[q * n + j];
+                const double tv = total(i0 + q, j), sv = spin(i0 + q, j);
+                r.total_err += (tv - rt) * (tv - rt);
+                r.spin_err += (sv - rs) * (sv - rs);
+                r.total += tv * tv;
+                r.rtotal += rt * rt;
+                r.spin += sv * sv;
+                r.rspin += rs * rs;
+            }
+        part[t] = r;
     };
-    outer(ca, na, pa);
-    outer(cb, nb, pb);
+    const std::size_t nthreads =
+        std::max<std::size_t>(1, std::min<std::size_t>(std::thread::hardware_concurrency(), ntiles));
+    std::atomic<std::size_t> next{0};
+    auto worker = [&] {
+        std::vector<double> pa(tile * n), pb(tile * n);
+        for (std::size_t t; (t = next.fetch_add(1)) < ntiles;) run_tile(t, pa, pb);
+    };
+    std::vector<std::thread> pool;
+    for (std::size_t k = 1; k < nthreads; ++k) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
     CheckNorms r;
-    for (std::size_t i = 0; i < n; ++i)
-        for (std::size_t j = 0; j < n; ++j) {
-            const double rt = pa[i * n + j] + pb[i * n + j], rs = pa[i * n + j] - pb[i * n + j];
-            const double t = total(i, j), s = spin(i, j);
-            r.total_err += (t - rt) * (t - rt);
-            r.spin_err += (s - rs) * (s - rs);
-            r.total += t * t;
-            r.rtotal += rt * rt;
-            r.spin += s * s;
-            r.rspin += rs * rs;
-        }
+    for (const auto& p : part) {
+        r.total_err += p.total_err;
+        r.spin_err += p.spin_err;
+        r.total += p.total;
+        r.rtotal += p.rtotal;
+        r.spin += p.spin;
+        r.rspin += p.rspin;
+    }
     return r;
 }
 

@@ -228,61 +228,73 @@ def _os_1d(la: int, lb: int, p: np.ndarray, xpa: np.ndarray, xpb: np.ndarray) ->
     return s
 
 
-def overlap_matrix(shells: List[ShellSpec], coords: np.ndarray, chunk: int = 2048) -> np.ndarray:
+def overlap_matrix(shells: List[ShellSpec], coords: np.ndarray, chunk: int = 4096) -> np.ndarray:
+    """AO overlap matrix (Obara-Saika), vectorised over block pairs of the same
+    angular momenta: exponents, weights and transforms are gathered per angular
+    momentum once, and each chunk of pairs is written back with one scatter."""
     blocks, n = _blocks(shells, coords)
     S = np.zeros((n, n))
     maxp = max(len(b[2]) for b in blocks)
-    # Group block pairs (a <= b) by (la, lb).
-    groups: Dict[Tuple[int, int], List[Tuple[int, int]]] = {}
-    for ia in range(len(blocks)):
-        for ib in range(ia, len(blocks)):
-            groups.setdefault((blocks[ia][1], blocks[ib][1]), []).append((ia, ib))
-    for (la, lb), pairs in groups.items():
-        ca = cartesian_order(la)
-        cb = cartesian_order(lb)
-        for c0 in range(0, len(pairs), chunk):
-            sub = pairs[c0:c0 + chunk]
-            m = len(sub)
-            A = np.array([blocks[i][0] for i, _ in sub])
-            B = np.array([blocks[j][0] for _, j in sub])
-            ea = np.ones((m, maxp))
-            eb = np.ones((m, maxp))
-            wa = np.zeros((m, len(ca), maxp))
-            wb = np.zeros((m, len(cb), maxp))
-            for q, (i, j) in enumerate(sub):
-                na = len(blocks[i][2])
-                nb = len(blocks[j][2])
-                ea[q, :na] = blocks[i][2]
-                eb[q, :nb] = blocks[j][2]
-                wa[q, :, :na] = blocks[i][3]
-                wb[q, :, :nb] = blocks[j][3]
-            alpha = ea[:, :, None]
-            beta = eb[:, None, :]
-            p = alpha + beta
-            mu = alpha * beta / p
-            s00 = np.ones_like(p) * (math.pi / p) ** 1.5
-            tabs = []
-            for ax in range(3):
-                ax_a = A[:, ax][:, None, None]
-                ax_b = B[:, ax][:, None, None]
-                P = (alpha * ax_a + beta * ax_b) / p
-                s00 = s00 * np.exp(-mu * (ax_a - ax_b) ** 2)
-                tabs.append(_os_1d(la, lb, p, P - ax_a, P - ax_b))
-            # prim[q, pa, pb, ka, kb]
-            prim = np.empty((m, maxp, maxp, len(ca), len(cb)))
-            for ka, (ax, ay, az) in enumerate(ca):
-                for kb, (bx, by, bz) in enumerate(cb):
-                    prim[..., ka, kb] = (s00 * tabs[0][..., ax, bx] * tabs[1][..., ay, by]
-                                         * tabs[2][..., az, bz])
-            cart = np.einsum("qkp,qlr,qprkl->qkl", wa, wb, prim, optimize=True)
-            for q, (i, j) in enumerate(sub):
-                ta = blocks[i][4]
-                tb = blocks[j][4]
-                blk = ta @ cart[q] @ tb.T
-                oi = blocks[i][5]
-                oj = blocks[j][5]
-                S[oi:oi + blk.shape[0], oj:oj + blk.shape[1]] = blk
-                S[oj:oj + blk.shape[1], oi:oi + blk.shape[0]] = blk.T
+    by_l: Dict[int, Dict[str, np.ndarray]] = {}
+    for l in sorted({b[1] for b in blocks}):
+        idx = [i for i, b in enumerate(blocks) if b[1] == l]
+        ncart = len(cartesian_order(l))
+        exps = np.ones((len(idx), maxp))
+        wts = np.zeros((len(idx), ncart, maxp))
+        for r, i in enumerate(idx):
+            k = len(blocks[i][2])
+            exps[r, :k] = blocks[i][2]
+            wts[r, :, :k] = blocks[i][3]
+        t = blocks[idx[0]][4]
+        if any(blocks[i][4].shape != t.shape or not np.array_equal(blocks[i][4], t) for i in idx):
+            raise ValueError("blocks of one angular momentum must share their transform")
+        by_l[l] = {"idx": np.array(idx), "exps": exps, "w": wts, "t": t,
+                   "origin": np.array([blocks[i][0] for i in idx]),
+                   "off": np.array([blocks[i][5] for i in idx])}
+    ls = sorted(by_l)
+    for ai, la in enumerate(ls):
+        for lb in ls[ai:]:
+            A_, B_ = by_l[la], by_l[lb]
+            # Every unordered block pair once: all (a, b) across two angular
+            # momenta, a <= b in the block order within one.
+            ga, gb = np.meshgrid(np.arange(len(A_["idx"])), np.arange(len(B_["idx"])), indexing="ij")
+            keep = A_["idx"][ga] <= B_["idx"][gb] if la == lb else np.ones(ga.shape, bool)
+            # Pairs whose most diffuse primitives still overlap by less than
+            # exp(-100) are left at zero (far below the rounding of S).
+            amin = A_["exps"].min(1)[ga]
+            bmin = B_["exps"].min(1)[gb]
+            r2 = ((A_["origin"][ga] - B_["origin"][gb]) ** 2).sum(-1)
+            keep &= amin * bmin / (amin + bmin) * r2 <= 100.0
+            qa, qb = ga[keep], gb[keep]
+            ca, cb = cartesian_order(la), cartesian_order(lb)
+            ta, tb = A_["t"], B_["t"]
+            for c0 in range(0, len(qa), chunk):
+                ia, ib = qa[c0:c0 + chunk], qb[c0:c0 + chunk]
+                A = A_["origin"][ia]
+                B = B_["origin"][ib]
+                alpha = A_["exps"][ia][:, :, None]
+                beta = B_["exps"][ib][:, None, :]
+                p = alpha + beta
+                mu = alpha * beta / p
+                s00 = np.ones_like(p) * (math.pi / p) ** 1.5
+                tabs = []
+                for ax in range(3):
+                    ax_a = A[:, ax][:, None, None]
+                    ax_b = B[:, ax][:, None, None]
+                    P = (alpha * ax_a + beta * ax_b) / p
+                    s00 = s00 * np.exp(-mu * (ax_a - ax_b) ** 2)
+                    tabs.append(_os_1d(la, lb, p, P - ax_a, P - ax_b))
+                prim = np.empty(p.shape + (len(ca), len(cb)))
+                for ka, (ax, ay, az) in enumerate(ca):
+                    for kb, (bx, by, bz) in enumerate(cb):
+                        prim[..., ka, kb] = (s00 * tabs[0][..., ax, bx] * tabs[1][..., ay, by]
+                                             * tabs[2][..., az, bz])
+                cart = np.einsum("qkp,qlr,qprkl->qkl", A_["w"][ia], B_["w"][ib], prim, optimize=True)
+                blk = np.einsum("ak,qkl,bl->qab", ta, cart, tb, optimize=True)
+                rows = A_["off"][ia][:, None, None] + np.arange(blk.shape[1])[None, :, None]
+                cols = B_["off"][ib][:, None, None] + np.arange(blk.shape[2])[None, None, :]
+                S[rows, cols] = blk
+                S[cols, rows] = blk
     return S
 
 
@@ -315,7 +327,6 @@ def build_molecule(name: str, elements: Sequence[str], coords: np.ndarray,
         for l, e, c in basis_by_element[el]:
             shells.append(ShellSpec(ia, l, True, e.copy(), c.copy()))
     S = overlap_matrix(shells, coords)
-    eig = np.linalg.eigvalsh(S)
     orb_rng = np.random.default_rng(seed + 1000)
     ca = _orthonormal_orbitals(orb_rng, S)
     unrestricted = nalpha != nbeta
@@ -328,9 +339,7 @@ def build_molecule(name: str, elements: Sequence[str], coords: np.ndarray,
     z = np.array([ELEMENT_Z[e] for e in elements], dtype=np.int64)
     mult = nalpha - nbeta + 1
     return SyntheticMolecule(name, z, np.asarray(coords, dtype=float), shells, nalpha, nbeta,
-                             charge, mult, ca, cb, ea, eb, pa + pb, pa - pb,
-                             meta={"overlap_min_eigenvalue": float(eig[0]),
-                                   "overlap_max_eigenvalue": float(eig[-1])})
+                             charge, mult, ca, cb, ea, eb, pa + pb, pa - pb)
 
 
 def water(seed: int = 0) -> SyntheticMolecule:
