@@ -41,6 +41,8 @@ CUDA_UNITS = {
     "csrc/host/profile.cu": [],
     "csrc/host/noalloc.cu": [],
     "csrc/host/server.cu": [],
+    "csrc/cuda/isosurface.cu": [],
+    "csrc/host/surface.cu": [],
 }
 CXX_UNITS = [
     "csrc/host/fchk.cpp",

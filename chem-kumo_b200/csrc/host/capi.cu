@@ -15,11 +15,19 @@
 #include "grid_geometry.hpp"
 #include "chem/kumo/evaluator.hpp"
 #include "chem/kumo/server.hpp"
+#include "chem/kumo/surface.hpp"
 #include "device_state.hpp"
 #include "profile.hpp"
 
 struct kumo_molecule {
     chem::kumo::Molecule mol;
+};
+
+struct kumo_surface {
+    chem::kumo::TriangleMesh mesh;
+    std::vector<chem::kumo::IVec3> cells;
+    std::vector<std::vector<double>> values;
+    std::vector<chem::kumo::SurfaceStatistics> stats;
 };
 
 namespace {
@@ -75,6 +83,52 @@ EvaluationOptions to_options(const kumo_options* o) {
     e.precision = o->precision ? Precision::Mixed : Precision::FP64;
     e.fukui_delta = o->fukui_delta;
     return e;
+}
+
+void fill_stats(const SurfaceStatistics& s, kumo_surface_stats* o, long long* minima, long long cap_min,
+                long long* maxima, long long cap_max) {
+    if (o) {
+        o->area = s.area;
+        o->positive_area = s.positive_area;
+        o->negative_area = s.negative_area;
+        o->nonpolar_area = s.nonpolar_area;
+        o->minimum = s.minimum;
+        o->maximum = s.maximum;
+        o->minimum_vertex = static_cast<long long>(s.minimum_vertex);
+        o->maximum_vertex = static_cast<long long>(s.maximum_vertex);
+        o->average = s.average;
+        o->positive_average = s.positive_average;
+        o->negative_average = s.negative_average;
+        o->positive_variance = s.positive_variance;
+        o->negative_variance = s.negative_variance;
+        o->total_variance = s.total_variance;
+        o->balance = s.balance;
+        o->charge_separation = s.charge_separation;
+        o->polarity_index = s.polarity_index;
+        o->n_local_minima = static_cast<long long>(s.local_minima.size());
+        o->n_local_maxima = static_cast<long long>(s.local_maxima.size());
+    }
+    for (long long i = 0; minima && i < cap_min && i < static_cast<long long>(s.local_minima.size()); ++i)
+        minima[i] = static_cast<long long>(s.local_minima[static_cast<std::size_t>(i)]);
+    for (long long i = 0; maxima && i < cap_max && i < static_cast<long long>(s.local_maxima.size()); ++i)
+        maxima[i] = static_cast<long long>(s.local_maxima[static_cast<std::size_t>(i)]);
+}
+
+TriangleMesh to_mesh(const double* vertices, long long nv, const long long* triangles, long long nt) {
+    if (nv < 0 || nt < 0 || (nv > 0 && !vertices) || (nt > 0 && !triangles))
+        throw std::invalid_argument("invalid mesh arrays");
+    TriangleMesh mesh;
+    mesh.vertices.resize(static_cast<std::size_t>(nv));
+    for (long long v = 0; v < nv; ++v)
+        for (int r = 0; r < 3; ++r) mesh.vertices[static_cast<std::size_t>(v)][static_cast<std::size_t>(r)] = vertices[3 * v + r];
+    mesh.triangles.resize(static_cast<std::size_t>(nt));
+    for (long long t = 0; t < nt; ++t)
+        for (int r = 0; r < 3; ++r) {
+            if (triangles[3 * t + r] < 0) throw std::invalid_argument("surface triangle refers to a missing vertex");
+            mesh.triangles[static_cast<std::size_t>(t)][static_cast<std::size_t>(r)] =
+                static_cast<std::size_t>(triangles[3 * t + r]);
+        }
+    return mesh;
 }
 
 Grid to_grid(const kumo_grid* g) {
@@ -665,6 +719,161 @@ int kumo_server_reset_stats(kumo_server* server, char* err, size_t errlen) {
     return guarded(err, errlen, [&] {
         if (!server) throw std::invalid_argument("null server");
         server->srv->reset_stats();
+    });
+}
+
+int kumo_density_isosurface(const kumo_molecule* m, double isovalue, double spacing, kumo_surface** out,
+                            char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!m || !out) throw std::invalid_argument("null molecule or output");
+        auto s = std::make_unique<kumo_surface>();
+        s->mesh = density_isosurface(m->mol, isovalue, spacing);
+        *out = s.release();
+    });
+}
+
+int kumo_potential_surface(const kumo_molecule* m, double isovalue, double spacing, double tolerance,
+                           kumo_surface** out, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!m || !out) throw std::invalid_argument("null molecule or output");
+        SurfaceOptions o;
+        o.isovalue = isovalue;
+        o.spacing = spacing;
+        o.potential_tolerance = tolerance;
+        PotentialSurface p = electrostatic_potential_surface(m->mol, o);
+        auto s = std::make_unique<kumo_surface>();
+        s->mesh = std::move(p.mesh);
+        s->values.push_back(std::move(p.potential));
+        s->stats.push_back(std::move(p.statistics));
+        *out = s.release();
+    });
+}
+
+int kumo_ionization_energy_surface(const kumo_molecule* m, double isovalue, double spacing, kumo_surface** out,
+                                   char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!m || !out) throw std::invalid_argument("null molecule or output");
+        IonizationEnergySurface p = local_ionization_energy_surface(m->mol, isovalue, spacing);
+        auto s = std::make_unique<kumo_surface>();
+        s->mesh = std::move(p.mesh);
+        s->values.push_back(std::move(p.ionization_energy));
+        s->stats.push_back(std::move(p.statistics));
+        *out = s.release();
+    });
+}
+
+int kumo_map_on_density_isosurface(const kumo_molecule* m, const kumo_options* opt, const kumo_property* props,
+                                   int nprops, double isovalue, double spacing, kumo_surface** out,
+                                   int* backend_used, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!m || !out) throw std::invalid_argument("null molecule or output");
+        const Request req = to_request(props, nprops);
+        MappedSurface p = map_on_density_isosurface(m->mol, req.properties(), isovalue, spacing, to_options(opt));
+        auto s = std::make_unique<kumo_surface>();
+        s->mesh = std::move(p.mesh);
+        s->values = std::move(p.values);
+        s->stats = std::move(p.statistics);
+        if (backend_used) *backend_used = static_cast<int>(p.backend_used);
+        *out = s.release();
+    });
+}
+
+int kumo_average_local_ionization_energy(const kumo_molecule* m, const double* points, long long npoints,
+                                         double* out, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!m) throw std::invalid_argument("null molecule");
+        if (npoints < 0 || (npoints > 0 && (!points || !out))) throw std::invalid_argument("invalid points");
+        const auto v = average_local_ionization_energy(m->mol, Points{points, static_cast<std::size_t>(npoints)});
+        std::copy(v.begin(), v.end(), out);
+    });
+}
+
+int kumo_extract_isosurface(const kumo_grid* grid, const double* samples, double isovalue, kumo_scalar_fn fn,
+                            void* user, kumo_surface** out, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!out || !fn) throw std::invalid_argument("null function or output");
+        const Grid g = to_grid(grid);
+        detail::validated_point_count(g);
+        const detail::ScalarFunction f = [&](const std::vector<Vec3>& pts, std::vector<double>& values,
+                                             std::vector<Vec3>& gradients) {
+            std::vector<double> grad(3 * pts.size(), 0.0);
+            fn(pts.empty() ? nullptr : pts[0].data(), static_cast<long long>(pts.size()), values.data(), grad.data(),
+               user);
+            for (std::size_t p = 0; p < pts.size(); ++p)
+                for (int r = 0; r < 3; ++r) gradients[p][static_cast<std::size_t>(r)] = grad[3 * p + r];
+        };
+        detail::Isosurface iso = detail::extract_isosurface(g, samples, false, isovalue, f);
+        auto s = std::make_unique<kumo_surface>();
+        s->mesh = std::move(iso.mesh);
+        s->cells = std::move(iso.vertex_cells);
+        *out = s.release();
+    });
+}
+
+void kumo_surface_info(const kumo_surface* s, long long* nvertices, long long* ntriangles, int* nfields) {
+    if (nvertices) *nvertices = s ? static_cast<long long>(s->mesh.vertices.size()) : 0;
+    if (ntriangles) *ntriangles = s ? static_cast<long long>(s->mesh.triangles.size()) : 0;
+    if (nfields) *nfields = s ? static_cast<int>(s->values.size()) : 0;
+}
+
+void kumo_surface_mesh(const kumo_surface* s, double* vertices, long long* triangles, int* cells) {
+    if (!s) return;
+    for (std::size_t v = 0; v < s->mesh.vertices.size(); ++v)
+        for (int r = 0; r < 3; ++r) {
+            if (vertices) vertices[3 * v + static_cast<std::size_t>(r)] = s->mesh.vertices[v][static_cast<std::size_t>(r)];
+            if (cells && v < s->cells.size())
+                cells[3 * v + static_cast<std::size_t>(r)] = s->cells[v][static_cast<std::size_t>(r)];
+        }
+    if (triangles)
+        for (std::size_t t = 0; t < s->mesh.triangles.size(); ++t)
+            for (int r = 0; r < 3; ++r)
+                triangles[3 * t + static_cast<std::size_t>(r)] =
+                    static_cast<long long>(s->mesh.triangles[t][static_cast<std::size_t>(r)]);
+}
+
+int kumo_surface_field(const kumo_surface* s, int index, double* values, kumo_surface_stats* stats,
+                       long long* minima, long long cap_min, long long* maxima, long long cap_max, char* err,
+                       size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!s || index < 0 || index >= static_cast<int>(s->values.size()))
+            throw std::out_of_range("surface field index out of range");
+        const auto& v = s->values[static_cast<std::size_t>(index)];
+        if (values) std::copy(v.begin(), v.end(), values);
+        fill_stats(s->stats[static_cast<std::size_t>(index)], stats, minima, cap_min, maxima, cap_max);
+    });
+}
+
+void kumo_surface_destroy(kumo_surface* s) { delete s; }
+
+int kumo_surface_statistics(const double* vertices, long long nvertices, const long long* triangles,
+                            long long ntriangles, const double* values, double polar_threshold,
+                            kumo_surface_stats* out, long long* minima, long long cap_min, long long* maxima,
+                            long long cap_max, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        const TriangleMesh mesh = to_mesh(vertices, nvertices, triangles, ntriangles);
+        if (nvertices > 0 && !values) throw std::invalid_argument("surface values do not match the mesh vertices");
+        const SurfaceStatistics st = surface_statistics(
+            mesh, std::span<const double>(values, static_cast<std::size_t>(nvertices)), polar_threshold);
+        fill_stats(st, out, minima, cap_min, maxima, cap_max);
+    });
+}
+
+int kumo_write_ply(const char* path, const double* vertices, long long nvertices, const long long* triangles,
+                   long long ntriangles, const char* const* names, const double* const* values, int nfields,
+                   const char* const* comments, int ncomments, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!path) throw std::invalid_argument("null PLY path");
+        const TriangleMesh mesh = to_mesh(vertices, nvertices, triangles, ntriangles);
+        if (nfields < 0 || ncomments < 0 || (nfields > 0 && (!names || !values)) || (ncomments > 0 && !comments))
+            throw std::invalid_argument("invalid PLY fields or comments");
+        std::vector<std::pair<std::string, std::vector<double>>> fields;
+        for (int f = 0; f < nfields; ++f) {
+            if (!names[f] || (nvertices > 0 && !values[f])) throw std::invalid_argument("invalid PLY field");
+            fields.emplace_back(names[f], std::vector<double>(values[f], values[f] + nvertices));
+        }
+        std::vector<std::string> cs;
+        for (int c = 0; c < ncomments; ++c) cs.emplace_back(comments[c] ? comments[c] : "");
+        write_ply(path, mesh, fields, cs);
     });
 }
 

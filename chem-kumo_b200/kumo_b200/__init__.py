@@ -11,7 +11,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 import os
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
@@ -156,8 +156,25 @@ EXPORTS = [
     "kumo_profile_enable", "kumo_profile_reset", "kumo_profile_read", "kumo_set_device",
     "kumo_evaluate_points_noalloc", "kumo_server_create", "kumo_server_destroy", "kumo_server_submit_grid",
     "kumo_server_submit_points", "kumo_server_wait", "kumo_server_drain", "kumo_server_stats_get",
-    "kumo_server_reset_stats",
+    "kumo_server_reset_stats", "kumo_density_isosurface", "kumo_potential_surface", "kumo_ionization_energy_surface",
+    "kumo_map_on_density_isosurface", "kumo_average_local_ionization_energy", "kumo_extract_isosurface",
+    "kumo_surface_info", "kumo_surface_mesh", "kumo_surface_field", "kumo_surface_destroy",
+    "kumo_surface_statistics", "kumo_write_ply",
 ]
+
+
+class _SurfaceStats(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("area", "positive_area", "negative_area", "nonpolar_area", "minimum",
+                                          "maximum")] + \
+               [("minimum_vertex", C.c_longlong), ("maximum_vertex", C.c_longlong)] + \
+               [(n, C.c_double) for n in ("average", "positive_average", "negative_average", "positive_variance",
+                                          "negative_variance", "total_variance", "balance", "charge_separation",
+                                          "polarity_index")] + \
+               [("n_local_minima", C.c_longlong), ("n_local_maxima", C.c_longlong)]
+
+
+_SCALAR_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.c_longlong, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                         C.c_void_p)
 
 
 class _ServerOptions(C.Structure):
@@ -229,6 +246,24 @@ def lib():
         L.kumo_server_drain.argtypes = [C.c_void_p, *eb]
         L.kumo_server_stats_get.argtypes = [C.c_void_p, C.POINTER(_ServerStats), *eb]
         L.kumo_server_reset_stats.argtypes = [C.c_void_p, *eb]
+        vp = C.POINTER(C.c_void_p)
+        _LL = C.POINTER(C.c_longlong)
+        L.kumo_density_isosurface.argtypes = [C.c_void_p, C.c_double, C.c_double, vp, *eb]
+        L.kumo_potential_surface.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, vp, *eb]
+        L.kumo_ionization_energy_surface.argtypes = [C.c_void_p, C.c_double, C.c_double, vp, *eb]
+        L.kumo_map_on_density_isosurface.argtypes = [C.c_void_p, C.POINTER(_Options), C.POINTER(_Property), C.c_int,
+                                                     C.c_double, C.c_double, vp, _I, *eb]
+        L.kumo_average_local_ionization_energy.argtypes = [C.c_void_p, _D, C.c_longlong, _D, *eb]
+        L.kumo_extract_isosurface.argtypes = [C.POINTER(_Grid), _D, C.c_double, _SCALAR_FN, C.c_void_p, vp, *eb]
+        L.kumo_surface_info.argtypes = [C.c_void_p, _LL, _LL, _I]
+        L.kumo_surface_mesh.argtypes = [C.c_void_p, _D, _LL, _I]
+        L.kumo_surface_field.argtypes = [C.c_void_p, C.c_int, _D, C.POINTER(_SurfaceStats), _LL, C.c_longlong, _LL,
+                                         C.c_longlong, *eb]
+        L.kumo_surface_destroy.argtypes = [C.c_void_p]
+        L.kumo_surface_statistics.argtypes = [_D, C.c_longlong, _LL, C.c_longlong, _D, C.c_double,
+                                              C.POINTER(_SurfaceStats), _LL, C.c_longlong, _LL, C.c_longlong, *eb]
+        L.kumo_write_ply.argtypes = [C.c_char_p, _D, C.c_longlong, _LL, C.c_longlong, C.POINTER(C.c_char_p),
+                                     C.POINTER(_D), C.c_int, C.POINTER(C.c_char_p), C.c_int, *eb]
         _lib = L
     return _lib
 
@@ -606,3 +641,154 @@ class Server:
     def reset_stats(self) -> None:
         e = _err()
         _check(lib().kumo_server_reset_stats(self._h, e, 512), e)
+
+
+# ---------------------------------------------------------------------------
+# Molecular surfaces (include/chem/kumo/surface.hpp)
+# ---------------------------------------------------------------------------
+
+HARTREE_IN_KCAL_PER_MOL = 627.5094740631
+HARTREE_IN_ELECTRONVOLT = 27.211386245988
+
+
+def _stats_dict(st: "_SurfaceStats", minima, maxima) -> Dict[str, object]:
+    d = {name: getattr(st, name) for name, _ in _SurfaceStats._fields_}
+    d["local_minima"] = [int(v) for v in minima]
+    d["local_maxima"] = [int(v) for v in maxima]
+    return d
+
+
+@dataclass
+class Surface:
+    """A closed triangle mesh (bohr) with per-vertex fields and their statistics."""
+    vertices: np.ndarray                 # (nv, 3)
+    triangles: np.ndarray                # (nt, 3) int64, counter-clockwise seen from outside
+    cells: Optional[np.ndarray] = None   # (nv, 3): grid indices of each vertex's edge's lower end
+    values: List[np.ndarray] = field(default_factory=list)
+    statistics: List[Dict[str, object]] = field(default_factory=list)
+
+    def area(self) -> float:
+        a, b, c = (self.vertices[self.triangles[:, i]] for i in range(3))
+        return float(0.5 * np.linalg.norm(np.cross(b - a, c - a), axis=1).sum()) if len(self.triangles) else 0.0
+
+
+def _take_surface(h, with_cells: bool = False) -> Surface:
+    L = lib()
+    try:
+        nv, nt, nf = C.c_longlong(), C.c_longlong(), C.c_int()
+        L.kumo_surface_info(h, C.byref(nv), C.byref(nt), C.byref(nf))
+        v = np.zeros((nv.value, 3))
+        t = np.zeros((nt.value, 3), dtype=np.int64)
+        cells = np.zeros((nv.value, 3), dtype=np.int32) if with_cells else None
+        L.kumo_surface_mesh(h, _dp(v), t.ctypes.data_as(C.POINTER(C.c_longlong)),
+                            cells.ctypes.data_as(_I) if cells is not None else None)
+        surf = Surface(v, t, cells)
+        for i in range(nf.value):
+            vals = np.zeros(nv.value)
+            st = _SurfaceStats()
+            e = _err()
+            _check(L.kumo_surface_field(h, i, _dp(vals), C.byref(st), None, 0, None, 0, e, 512), e)
+            mins = np.zeros(max(1, st.n_local_minima), dtype=np.int64)
+            maxs = np.zeros(max(1, st.n_local_maxima), dtype=np.int64)
+            _check(L.kumo_surface_field(h, i, None, None, mins.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                        st.n_local_minima, maxs.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                        st.n_local_maxima, e, 512), e)
+            surf.values.append(vals)
+            surf.statistics.append(_stats_dict(st, mins[:st.n_local_minima], maxs[:st.n_local_maxima]))
+        return surf
+    finally:
+        L.kumo_surface_destroy(h)
+
+
+def density_isosurface(m: Molecule, isovalue: float = 1e-3, spacing: float = 0.25) -> Surface:
+    h, e = C.c_void_p(), _err()
+    _check(lib().kumo_density_isosurface(m._h, float(isovalue), float(spacing), C.byref(h), e, 512), e)
+    return _take_surface(h)
+
+
+def electrostatic_potential_surface(m: Molecule, isovalue: float = 1e-3, spacing: float = 0.25,
+                                    potential_tolerance: float = 1e-8) -> Surface:
+    h, e = C.c_void_p(), _err()
+    _check(lib().kumo_potential_surface(m._h, float(isovalue), float(spacing), float(potential_tolerance),
+                                        C.byref(h), e, 512), e)
+    return _take_surface(h)
+
+
+def local_ionization_energy_surface(m: Molecule, isovalue: float = 1e-3, spacing: float = 0.25) -> Surface:
+    h, e = C.c_void_p(), _err()
+    _check(lib().kumo_ionization_energy_surface(m._h, float(isovalue), float(spacing), C.byref(h), e, 512), e)
+    return _take_surface(h)
+
+
+def map_on_density_isosurface(m: Molecule, props: Sequence[Property], isovalue: float = 1e-3,
+                              spacing: float = 0.25, **options) -> Tuple[Surface, int]:
+    h, e = C.c_void_p(), _err()
+    kp = (_Property * max(1, len(props)))(*[_Property(p.kind, p.component, p.channel, p.orbital_index)
+                                            for p in props])
+    used = C.c_int(0)
+    opt = _options(**options)
+    _check(lib().kumo_map_on_density_isosurface(m._h, C.byref(opt), kp, len(props), float(isovalue), float(spacing),
+                                                C.byref(h), C.byref(used), e, 512), e)
+    return _take_surface(h), used.value
+
+
+def average_local_ionization_energy(m: Molecule, points: np.ndarray) -> np.ndarray:
+    pts = np.ascontiguousarray(points, dtype=float).reshape(-1, 3)
+    out = np.zeros(len(pts))
+    e = _err()
+    _check(lib().kumo_average_local_ionization_energy(m._h, _dp(pts), len(pts), _dp(out), e, 512), e)
+    return out
+
+
+def extract_isosurface(grid: Grid, samples: np.ndarray, isovalue: float, function) -> Surface:
+    """Isosurface f = isovalue of samples (Field order) on a grid; function(points (n, 3)) -> (values (n,),
+    gradients (n, 3)) places the vertices."""
+    samples = np.ascontiguousarray(samples, dtype=float).ravel()
+
+    def cb(pts, n, values, grads, user):
+        p = np.ctypeslib.as_array(pts, shape=(n, 3)).copy() if n else np.zeros((0, 3))
+        v, g = function(p)
+        if n:
+            np.ctypeslib.as_array(values, shape=(n,))[:] = v
+            np.ctypeslib.as_array(grads, shape=(n, 3))[:] = g
+
+    fn = _SCALAR_FN(cb)
+    h, e = C.c_void_p(), _err()
+    gc = grid._c()
+    _check(lib().kumo_extract_isosurface(C.byref(gc), _dp(samples), float(isovalue), fn, None, C.byref(h), e, 512), e)
+    return _take_surface(h, with_cells=True)
+
+
+def surface_statistics(vertices: np.ndarray, triangles: np.ndarray, values: np.ndarray,
+                       polar_threshold: float = 10.0 / HARTREE_IN_KCAL_PER_MOL) -> Dict[str, object]:
+    v = np.ascontiguousarray(vertices, dtype=float).reshape(-1, 3)
+    t = np.ascontiguousarray(triangles, dtype=np.int64).reshape(-1, 3)
+    x = np.ascontiguousarray(values, dtype=float).ravel()
+    if len(x) != len(v):
+        raise InvalidArgument(1, "surface values do not match the mesh vertices")
+    st, e = _SurfaceStats(), _err()
+    LL = C.POINTER(C.c_longlong)
+    _check(lib().kumo_surface_statistics(_dp(v), len(v), t.ctypes.data_as(LL), len(t), _dp(x), float(polar_threshold),
+                                         C.byref(st), None, 0, None, 0, e, 512), e)
+    mins = np.zeros(max(1, st.n_local_minima), dtype=np.int64)
+    maxs = np.zeros(max(1, st.n_local_maxima), dtype=np.int64)
+    _check(lib().kumo_surface_statistics(_dp(v), len(v), t.ctypes.data_as(LL), len(t), _dp(x), float(polar_threshold),
+                                         None, mins.ctypes.data_as(LL), st.n_local_minima, maxs.ctypes.data_as(LL),
+                                         st.n_local_maxima, e, 512), e)
+    return _stats_dict(st, mins[:st.n_local_minima], maxs[:st.n_local_maxima])
+
+
+def write_ply(path: str, vertices: np.ndarray, triangles: np.ndarray,
+              fields: Sequence[Tuple[str, np.ndarray]] = (), comments: Sequence[str] = ()) -> None:
+    v = np.ascontiguousarray(vertices, dtype=float).reshape(-1, 3)
+    t = np.ascontiguousarray(triangles, dtype=np.int64).reshape(-1, 3)
+    arrays = [np.ascontiguousarray(a, dtype=float).ravel() for _, a in fields]
+    for (name, _), a in zip(fields, arrays):
+        if len(a) != len(v):
+            raise InvalidArgument(1, f"PLY property '{name}' needs one value per vertex")
+    names = (C.c_char_p * max(1, len(fields)))(*[n.encode() for n, _ in fields])
+    vals = (_D * max(1, len(fields)))(*[_dp(a) for a in arrays])
+    cs = (C.c_char_p * max(1, len(comments)))(*[c.encode() for c in comments])
+    e = _err()
+    _check(lib().kumo_write_ply(str(path).encode(), _dp(v), len(v), t.ctypes.data_as(C.POINTER(C.c_longlong)), len(t),
+                                names, vals, len(fields), cs, len(comments), e, 512), e)

@@ -267,6 +267,71 @@ int kumo_server_drain(kumo_server* server, char* err, size_t errlen);
 int kumo_server_stats_get(kumo_server* server, kumo_server_stats* out, char* err, size_t errlen);
 int kumo_server_reset_stats(kumo_server* server, char* err, size_t errlen);
 
+/* ---- Molecular surfaces (include/chem/kumo/surface.hpp) ------------------
+ * A kumo_surface holds a closed triangle mesh (vertices in bohr; triangles
+ * counter-clockwise seen from outside) and, per mapped field, one value per
+ * vertex with its surface statistics. */
+typedef struct kumo_surface kumo_surface;
+
+/* SurfaceStatistics (include/chem/kumo/surface.hpp:37-77); the local minima
+ * and maxima (vertex indices, sorted) are copied separately. */
+typedef struct {
+    double area, positive_area, negative_area, nonpolar_area;
+    double minimum, maximum;
+    long long minimum_vertex, maximum_vertex;
+    double average, positive_average, negative_average;
+    double positive_variance, negative_variance, total_variance;
+    double balance, charge_separation, polarity_index;
+    long long n_local_minima, n_local_maxima;
+} kumo_surface_stats;
+
+/* density_isosurface (include/chem/kumo/surface.hpp:101-116; src/surface.cpp:329-535). */
+int kumo_density_isosurface(const kumo_molecule* m, double isovalue, double spacing, kumo_surface** out,
+                            char* err, size_t errlen);
+/* electrostatic_potential_surface (surface.hpp:118-133; src/surface.cpp:586-631): field 0
+ * is the potential (exact; any tolerance >= 0 is met). */
+int kumo_potential_surface(const kumo_molecule* m, double isovalue, double spacing, double tolerance,
+                           kumo_surface** out, char* err, size_t errlen);
+/* local_ionization_energy_surface (surface.hpp:157-165; src/surface.cpp:568-584): field 0. */
+int kumo_ionization_energy_surface(const kumo_molecule* m, double isovalue, double spacing, kumo_surface** out,
+                                   char* err, size_t errlen);
+/* map_on_density_isosurface (surface.hpp:167-192; src/surface.cpp:633-670): one field per
+ * distinct property, in request order; *backend_used as kumo_evaluate_*. */
+int kumo_map_on_density_isosurface(const kumo_molecule* m, const kumo_options* opt, const kumo_property* props,
+                                   int nprops, double isovalue, double spacing, kumo_surface** out,
+                                   int* backend_used, char* err, size_t errlen);
+/* average_local_ionization_energy at points (surface.hpp:135-155; src/surface.cpp:537-566). */
+int kumo_average_local_ionization_energy(const kumo_molecule* m, const double* points, long long npoints,
+                                         double* out, char* err, size_t errlen);
+
+/* f and its gradient at n points (3 x n, bohr): values[n], gradients[3n]. */
+typedef void (*kumo_scalar_fn)(const double* points, long long n, double* values, double* gradients, void* user);
+/* detail::extract_isosurface (src/isosurface.hpp; src/surface.cpp:296-320): the
+ * isosurface f = isovalue of host samples on a grid, vertices placed with fn. */
+int kumo_extract_isosurface(const kumo_grid* grid, const double* samples, double isovalue, kumo_scalar_fn fn,
+                            void* user, kumo_surface** out, char* err, size_t errlen);
+
+void kumo_surface_info(const kumo_surface* s, long long* nvertices, long long* ntriangles, int* nfields);
+/* vertices: 3 x nvertices; triangles: 3 x ntriangles; cells (may be NULL): the
+ * grid indices of the lower end of each vertex's edge, 3 x nvertices. */
+void kumo_surface_mesh(const kumo_surface* s, double* vertices, long long* triangles, int* cells);
+/* Field `index`: values (nvertices) and statistics; minima / maxima receive up
+ * to cap_min / cap_max vertex indices (either may be NULL). */
+int kumo_surface_field(const kumo_surface* s, int index, double* values, kumo_surface_stats* stats,
+                       long long* minima, long long cap_min, long long* maxima, long long cap_max, char* err,
+                       size_t errlen);
+void kumo_surface_destroy(kumo_surface* s);
+
+/* surface_statistics (surface.hpp:79-86; src/surface.cpp:417-531) of vertex values on a mesh. */
+int kumo_surface_statistics(const double* vertices, long long nvertices, const long long* triangles,
+                            long long ntriangles, const double* values, double polar_threshold,
+                            kumo_surface_stats* out, long long* minima, long long cap_min, long long* maxima,
+                            long long cap_max, char* err, size_t errlen);
+/* write_ply (surface.hpp:194-208; src/surface.cpp:672-720). */
+int kumo_write_ply(const char* path, const double* vertices, long long nvertices, const long long* triangles,
+                   long long ntriangles, const char* const* names, const double* const* values, int nfields,
+                   const char* const* comments, int ncomments, char* err, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif
