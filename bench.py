@@ -226,28 +226,10 @@ def serve_bench(K, synth, precision: int, seconds: float, rate: float, pool, see
             "submit_s": submit_s, "mix": kinds}
 
 
-def surface_points(rho: np.ndarray, origin, spacing: float, iso: float = 1e-3) -> np.ndarray:
-    """Vertices of the rho = iso surface on the grid's edges (linear
-    interpolation where rho crosses iso between neighbouring points), as a
-    marching-cubes surface has them."""
-    pts = []
-    for ax in range(3):
-        a = np.take(rho, np.arange(rho.shape[ax] - 1), axis=ax)
-        b = np.take(rho, np.arange(1, rho.shape[ax]), axis=ax)
-        cross = (a - iso) * (b - iso) < 0
-        idx = np.argwhere(cross)
-        t = (iso - a[cross]) / (b[cross] - a[cross])
-        p = idx.astype(float)
-        p[:, ax] += t
-        pts.append(p)
-    ijk = np.concatenate(pts)
-    return np.asarray(origin)[None, :] + spacing * ijk
-
-
 def esp_bench(K, synth, fchk_dir: str, oracle_pts: int = 32):
     """Electrostatic-potential workload: C30N3O3H24 cation (60 atoms, 1260 AOs),
     exact potential (tolerance 0) on its 96^3 cube at 0.24 bohr and on the
-    rho = 0.001 surface vertices of that cube; unit: point-pair interactions."""
+    rho = 0.001 isosurface vertices; unit: point-pair interactions."""
     import torch
     fchk = synth.workload_fchk("esp_1260", fchk_dir)
     m = K.Molecule.from_fchk(fchk)
@@ -272,8 +254,12 @@ def esp_bench(K, synth, fchk_dir: str, oracle_pts: int = 32):
         return e0.elapsed_time(e1)
 
     ms_cube = timed(lambda: ev.evaluate_grid_device(grid, [esp], [out.data_ptr()], stream.cuda_stream))
-    rho, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_grid(grid, [K.density(K.PropertyKind.Density)])
-    surf = surface_points(rho[0].reshape(counts), origin, steps[0, 0])
+    # The rho = 0.001 isosurface at the reference's default spacing (0.25 bohr):
+    # device marching tetrahedra, vertices placed on the exact isosurface.
+    t0 = time.perf_counter()
+    mesh = K.density_isosurface(m, 1e-3, 0.25)
+    surface_build_s = time.perf_counter() - t0
+    surf = mesh.vertices
     dpts = torch.tensor(surf.ravel(), dtype=torch.float64, device="cuda")
     sout = torch.empty(len(surf), dtype=torch.float64, device="cuda")
     ms_surf = timed(lambda: ev.evaluate_points_device(dpts.data_ptr(), len(surf), [esp], [sout.data_ptr()],
@@ -288,11 +274,13 @@ def esp_bench(K, synth, fchk_dir: str, oracle_pts: int = 32):
     cpu_s = time.perf_counter() - t0
     got = sout.cpu().numpy()[pick]
     return {"workload": "esp_1260 (C30N3O3H24+, 60 atoms, 1260 AOs) exact ESP, 96^3 cube @0.24 bohr and "
-                        "rho = 0.001 surface vertices",
+                        "the vertices of its rho = 0.001 isosurface (0.25 bohr construction grid)",
             "pairs": int(pairs),
             "cube": {"points": n, "ms": ms_cube, "pair_points_per_s": n * pairs / (ms_cube * 1e-3),
                      "pts_per_s": n / (ms_cube * 1e-3)},
-            "surface": {"points": len(surf), "ms": ms_surf, "pair_points_per_s": len(surf) * pairs / (ms_surf * 1e-3)},
+            "surface": {"points": len(surf), "triangles": int(len(mesh.triangles)),
+                        "build_s": surface_build_s, "ms": ms_surf,
+                        "pair_points_per_s": len(surf) * pairs / (ms_surf * 1e-3)},
             "scaled_err_vs_oracle": float(np.max(np.abs(got - ref)) / max(1.0, float(np.max(np.abs(ref))))),
             "cpu_oracle": {"pair_points_per_s": oracle_pts * pairs / cpu_s, "cores": O.lib().ko_max_threads(),
                            "sample": f"{oracle_pts} surface points, {cpu_s:.1f} s"}}

@@ -671,6 +671,14 @@ class Surface:
         a, b, c = (self.vertices[self.triangles[:, i]] for i in range(3))
         return float(0.5 * np.linalg.norm(np.cross(b - a, c - a), axis=1).sum()) if len(self.triangles) else 0.0
 
+    def volume(self) -> float:
+        """Enclosed volume from the divergence theorem about the vertex centroid."""
+        if not len(self.vertices):
+            return 0.0
+        c = self.vertices.mean(axis=0)
+        a, b, d = (self.vertices[self.triangles[:, i]] - c for i in range(3))
+        return float(np.einsum("ij,ij->i", a, np.cross(b, d)).sum() / 6.0)
+
 
 def _take_surface(h, with_cells: bool = False) -> Surface:
     L = lib()

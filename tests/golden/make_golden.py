@@ -127,6 +127,95 @@ def sample(values: np.ndarray, rng: np.random.Generator, n_random: int, n_top: i
     return np.unique(np.concatenate([idx, top]))
 
 
+# Multiwfn's quantitative surface analyses (tests/multiwfn_surface_reference_test.cpp,
+# run as listed in meson.build:746-785): fchk, mode, whether local extrema are compared.
+SURFACES = [
+    ("h2o_esp", "h2o_b3lyp_def2tzvp.fchk.gz", "esp", True),
+    ("o2_esp", "o2.fchk.gz", "esp", False),
+    ("acrolein_esp", "acrolein.fchk.gz", "esp", True),
+    ("h2o_alie", "h2o_b3lyp_def2tzvp.fchk.gz", "alie", True),
+    ("o2_alie", "o2.fchk.gz", "alie", False),
+    ("acrolein_alie", "acrolein.fchk.gz", "alie", True),
+    ("acrolein_leae", "acrolein.fchk.gz", "leae", True),
+    ("o2_leae", "o2.fchk.gz", "leae", False),
+    ("acrolein_lea", "acrolein.fchk.gz", "lea", True),
+]
+BOHR_IN_ANGSTROM = 0.529177210903
+
+
+def _numbers(text: str):
+    out = []
+    for tok in text.replace("(", " ").replace(")", " ").replace("*", " ").split():
+        try:
+            out.append(float(tok))
+        except ValueError:
+            pass
+    return out
+
+
+def _after(lines, label, index):
+    for line in lines:
+        at = line.find(label)
+        if at >= 0:
+            return _numbers(line[at + len(label):])[index]
+    raise KeyError(label)
+
+
+def _extrema(lines, kind):
+    label = f"The number of surface {kind}:"
+    for i, line in enumerate(lines):
+        if label in line:
+            count = int(_after(lines, label, 0))
+            rows = []
+            for row in lines[i + 2:i + 2 + count]:
+                v = _numbers(row)  # #, a.u., eV, kcal/mol, x, y, z (Angstrom)
+                rows.append([v[1], v[4] / BOHR_IN_ANGSTROM, v[5] / BOHR_IN_ANGSTROM, v[6] / BOHR_IN_ANGSTROM])
+            return rows
+    return []
+
+
+def surface_summaries(tests: str) -> None:
+    """The numbers the reference test compares, per summary file, in atomic
+    units where Multiwfn prints them, otherwise as printed (kcal/mol, eV)."""
+    import json
+    out = {}
+    for key, fchk, mode, extrema in SURFACES:
+        with open(os.path.join(tests, "data", "multiwfn", key + "_surface.txt")) as f:
+            lines = f.read().splitlines()
+        v = {"volume": _after(lines, "Volume:", 0), "area": _after(lines, "Overall surface area:", 0)}
+        if mode == "esp":
+            v.update(positive_area=_after(lines, "Positive surface area:", 0),
+                     negative_area=_after(lines, "Negative surface area:", 0),
+                     nonpolar_percent=_after(lines, "Nonpolar surface area (|ESP| <= 10 kcal/mol):", 1),
+                     minimum_kcal=_after(lines, "Minimal value:", 0), maximum_kcal=_after(lines, "Minimal value:", 1),
+                     average=_after(lines, "Overall average value:", 0),
+                     positive_average=_after(lines, "Positive average value:", 0),
+                     negative_average=_after(lines, "Negative average value:", 0),
+                     charge_separation_kcal=_after(lines, "Internal charge separation (Pi):", 1),
+                     polarity_index_kcal=_after(lines, "Molecular polarity index (MPI):", 1),
+                     total_variance_kcal2=_after(lines, "Overall variance (sigma^2_tot):", 1),
+                     positive_variance_kcal2=_after(lines, "Positive variance:", 1),
+                     negative_variance_kcal2=_after(lines, "Negative variance:", 1),
+                     balance=_after(lines, "Balance of charges (nu):", 0))
+        elif mode == "alie":
+            v.update(minimum=_after(lines, "Global surface minimum:", 0),
+                     maximum=_after(lines, "Global surface maximum:", 0),
+                     average=_after(lines, "Average value:", 0), variance=_after(lines, "Variance:", 0))
+        else:
+            v.update(negative_area=_after(lines, "Negative surface area:", 0),
+                     minimum_ev=_after(lines, "Minimal value:", 0), maximum_ev=_after(lines, "Minimal value:", 1),
+                     average_kcal=_after(lines, "Overall average value:", 2),
+                     variance_kcal2=_after(lines, "Overall variance:", 2))
+        entry = {"fchk": fchk, "mode": mode, "extrema": extrema, "values": v}
+        if extrema:
+            entry["minima"] = _extrema(lines, "minima")
+            if mode == "esp":
+                entry["maxima"] = _extrema(lines, "maxima")
+        out[key] = entry
+    with open(os.path.join(HERE, "multiwfn_surfaces.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+
+
 def main(root: str) -> None:
     tests = os.path.join(root, "tests")
     for name, rel in FCHK_SOURCES.items():
@@ -145,6 +234,7 @@ def main(root: str) -> None:
         np.savez_compressed(os.path.join(HERE, f"multiwfn_{key}.npz"), fchk=fchk, origin=origin,
                             steps=steps, counts=counts, atoms=atoms, index=idx.astype(np.int64),
                             values=values[idx], npoints=values.size)
+    surface_summaries(tests)
     print("golden fixtures written to", HERE)
 
 
