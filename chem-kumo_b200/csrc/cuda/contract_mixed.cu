@@ -29,6 +29,7 @@
 #include <stdexcept>
 #include <string>
 
+#include "ao_mixed_shell.cuh"
 #include "mixed.cuh"
 #include "tc_common.cuh"
 
@@ -374,6 +375,444 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
     store_point(prm.spec, comp, start + point);
 }
 
+// ---------------------------------------------------------------------------
+// Fused form: AO rows built in the kernel, K step by K step.
+//
+// Prologue: the block's bounding box, the AO blocks (shells) whose cutoff
+// sphere reaches it in index order, a bound of each one's radial part over
+// the box (sum |u_p| exp(-a_p d^2), d the distance from its centre to the
+// box), the shells ranked by that bound (ascending, ties by index: the large
+// terms are added last, as the row order of the unfused kernel does) and
+// packed greedily into K steps of at most 16 rows.  Step t: the two halves of
+// the CTA compute alternate shells of the step, thread = point, into an FP32
+// staging tile [panel][16 rows][128 points] (padding rows zeroed), which is
+// then split into BF16 pieces exactly as the unfused kernel splits the rows it
+// loads; the MMAs of step t run while step t+1 is built.
+template <int P, int S>
+struct FusedSmem {
+    static constexpr int Q = NQm<P>::v;
+    static constexpr int SB = S + 1;
+    static constexpr unsigned a_bytes = 3u * P * kATile;
+    static constexpr unsigned stg_bytes = 16u * P * 128u * 4u;
+    static constexpr unsigned prologue_bytes = 2u * 4u * kFusedMaxShells;
+    static constexpr unsigned red_bytes = 8u * Q * 128u;
+    static constexpr unsigned scratch_bytes =
+        (stg_bytes > prologue_bytes ? (stg_bytes > red_bytes ? stg_bytes : red_bytes)
+                                    : (prologue_bytes > red_bytes ? prologue_bytes : red_bytes));
+    __host__ __device__ static unsigned b_bytes(int ncols) { return 3u * 32u * static_cast<unsigned>(ncols); }
+    static size_t total(int ncols) {
+        return S * static_cast<size_t>(a_bytes) + SB * static_cast<size_t>(b_bytes(ncols)) + scratch_bytes +
+               sizeof(int) * (2 * kFusedMaxShells + 2) + sizeof(double) * 8 * 6 + sizeof(int) * 8 + 8 * S + 16;
+    }
+};
+
+template <int P, int S, int MAXL>
+__global__ void __launch_bounds__(kThreads, 1) contract_fused_kernel(const __grid_constant__ ContractFusedParams prm) {
+    using L = FusedSmem<P, S>;
+    constexpr int Q = L::Q;
+    constexpr int SB = L::SB;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int N = prm.ncols;
+    const unsigned b_bytes = L::b_bytes(N);
+    unsigned char* a_st = sm;
+    unsigned char* b_st = sm + S * L::a_bytes;
+    unsigned char* scratch = b_st + SB * b_bytes;
+    float* stg = reinterpret_cast<float*>(scratch);
+    double* red = reinterpret_cast<double*>(scratch);
+    int* s_list = reinterpret_cast<int*>(scratch);                        // prologue only
+    float* s_key = reinterpret_cast<float*>(s_list + kFusedMaxShells);    // prologue only
+    int* s_sorted = reinterpret_cast<int*>(scratch + L::scratch_bytes);
+    int* step_first = s_sorted + kFusedMaxShells;
+    double* s_box = reinterpret_cast<double*>(step_first + kFusedMaxShells + 2);
+    int* s_wcount = reinterpret_cast<int*>(s_box + 8 * 6);
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(s_wcount + 8);
+    unsigned* tslot = reinterpret_cast<unsigned*>(bar + S);
+
+    const AoMixedParams& ap = prm.ao;
+    const DevBasis& B = ap.basis;
+    const int blk = blockIdx.x;
+    const long long start = ap.first_point + static_cast<long long>(blk) * ap.block_size;
+    long long bcount = prm.count - start;
+    if (bcount > ap.block_size) bcount = ap.block_size;
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    const int pj = tid & 127;          // this thread's point in the production
+    const int phalf = tid >> 7;        // which alternate shells it builds
+    const bool pvalid = pj < bcount;
+    double px = 0.0, py = 0.0, pz = 0.0;
+    if (pvalid) point_at(ap.src, start + pj, px, py, pz);
+
+    if (tid == 0) {
+        for (int q = 0; q < S; ++q) mbar_init(&bar[q], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (w == 0) tmem_alloc(tslot, static_cast<unsigned>(prm.tmem_cols));
+
+    // Bounding box of the block's points (the first 128 threads hold them).
+    {
+        const double big = 1.0e300;
+        const bool mine = pvalid && tid < 128;
+        const double pc[3] = {px, py, pz};
+        for (int a = 0; a < 3; ++a) {
+            const double lo = warp_min_d(mine ? pc[a] : big);
+            const double hi = warp_max_d(mine ? pc[a] : -big);
+            if (lane == 0) {
+                s_box[w * 6 + a] = lo;
+                s_box[w * 6 + 3 + a] = hi;
+            }
+        }
+    }
+    __syncthreads();
+    double lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = s_box[a];
+        hi[a] = s_box[3 + a];
+        for (int q = 1; q < 8; ++q) {
+            lo[a] = fmin(lo[a], s_box[q * 6 + a]);
+            hi[a] = fmax(hi[a], s_box[q * 6 + 3 + a]);
+        }
+    }
+    // Shells within reach, in index order, with their bounds.
+    int nlist = 0;
+    for (int c0 = 0; c0 < B.nblocks; c0 += kThreads) {
+        const int sh = c0 + tid;
+        bool reach = false;
+        double d2 = 0.0;
+        if (sh < B.nblocks) {
+            const double4 o = B.origin_r2[sh];
+            const double ox[3] = {o.x, o.y, o.z};
+            for (int a = 0; a < 3; ++a) {
+                const double d = fmax(0.0, fmax(lo[a] - ox[a], ox[a] - hi[a]));
+                d2 += d * d;
+            }
+            reach = !(d2 > o.w * (1.0 + 1e-10) + 1e-300);
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, reach);
+        if (lane == 0) s_wcount[w] = __popc(bal);
+        __syncthreads();
+        int before = nlist, total = nlist;
+        for (int q = 0; q < 8; ++q) {
+            if (q < w) before += s_wcount[q];
+            total += s_wcount[q];
+        }
+        if (reach) {
+            const int pos = before + __popc(bal & ((1u << lane) - 1u));
+            const int4 inf = B.info[sh];
+            const int nprim = inf.x >> 16;
+            float bound = 0.0f;
+            for (int q = 0; q < nprim; ++q) {
+                const MixPrim pr = ap.prims[inf.y + q];
+                bound += fabsf(pr.u) * exp_neg(pr.al2, d2);
+            }
+            s_list[pos] = sh;
+            s_key[pos] = bound;
+        }
+        nlist = total;
+        __syncthreads();
+    }
+    // Rank by (bound, index) and pack into K steps.
+    for (int i = tid; i < nlist; i += kThreads) {
+        const float ki = s_key[i];
+        int rank = 0;
+        for (int q = 0; q < nlist; ++q) {
+            const float kq = s_key[q];
+            rank += (kq < ki) || (kq == ki && q < i);
+        }
+        s_sorted[rank] = s_list[i];
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int nsteps = 0, rows = 0, total_rows = 0;
+        step_first[0] = 0;
+        for (int i = 0; i < nlist; ++i) {
+            const int4 inf = B.info[s_sorted[i]];
+            const int l = inf.x & 0xff;
+            const int cnt = ((inf.x >> 8) & 1) ? 2 * l + 1 : (l + 1) * (l + 2) / 2;
+            if (rows + cnt > 16) {
+                step_first[++nsteps] = i;
+                rows = 0;
+            }
+            rows += cnt;
+            total_rows += cnt;
+        }
+        if (nlist > 0) step_first[++nsteps] = nlist;
+        s_wcount[0] = nsteps;
+        if (prm.nrows) prm.nrows[blk] = total_rows;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = *tslot;
+    const int ntiles = s_wcount[0];
+    const int G = prm.groups;
+    const unsigned gcols = static_cast<unsigned>(P * N);
+
+    const int k8 = tid & 7, g = (tid >> 3) & 15, kh = tid >> 7;
+    const unsigned a_off = static_cast<unsigned>(g * 128 + kh * 2048 + k8 * 16);
+    const unsigned idesc = instr_desc(N);
+    const unsigned long long a_desc0 = smem_desc(smem_u32(a_st), 2048u, 128u);
+    const unsigned long long b_desc0 = smem_desc(smem_u32(b_st), static_cast<unsigned>(N * 16), 128u);
+    const unsigned nb8 = static_cast<unsigned>(N / 8);
+    const unsigned nb8_mul = (65536u + nb8 - 1u) / nb8;
+    const int quarter = w & 3, half = w >> 2;
+    const int point = quarter * 32 + lane;
+
+    // AO index of row k of step t (-1 for a padding row).
+    auto row_ao = [&](int t, int k) -> int {
+        int row = 0;
+        for (int f = step_first[t]; f < step_first[t + 1]; ++f) {
+            const int4 inf = B.info[s_sorted[f]];
+            const int l = inf.x & 0xff;
+            const int cnt = ((inf.x >> 8) & 1) ? 2 * l + 1 : (l + 1) * (l + 2) / 2;
+            if (k < row + cnt) return inf.w + (k - row);
+            row += cnt;
+        }
+        return -1;
+    };
+    // FP32 rows of step t into the staging tile.
+    auto produce = [&](int t) {
+        const size_t pstride = 16 * kBlockPoints;
+        int row = 0;
+        for (int f = step_first[t]; f < step_first[t + 1]; ++f) {
+            const int sh = s_sorted[f];
+            const int4 inf = B.info[sh];
+            const int l = inf.x & 0xff;
+            const bool pure = (inf.x >> 8) & 1;
+            const int cnt = pure ? 2 * l + 1 : (l + 1) * (l + 2) / 2;
+            if (((f - step_first[t]) & 1) == phalf) {
+                const double4 o = B.origin_r2[sh];
+                const double dx = px - o.x, dy = py - o.y, dz = pz - o.z;
+                const double r2d = dx * dx + dy * dy + dz * dz;
+                const bool inside = pvalid && r2d <= o.w;
+                float* dst = stg + row * kBlockPoints + pj;
+                if (__any_sync(0xffffffffu, inside)) {
+                    float R0 = 0.0f, R1 = 0.0f, R2 = 0.0f;
+                    if (inside) {
+                        const int nprim = inf.x >> 16;
+                        for (int q = 0; q < nprim; ++q) {
+                            const MixPrim pr = ap.prims[inf.y + q];
+                            const float ue = pr.u * exp_neg(pr.al2, r2d);
+                            R0 += ue;
+                            R1 += ue * pr.alpha;
+                            R2 += ue * pr.alpha * pr.alpha;
+                        }
+                    }
+                    const float x = static_cast<float>(dx), y = static_cast<float>(dy), z = static_cast<float>(dz);
+                    const float r2 = static_cast<float>(r2d);
+                    switch (l | (pure ? 16 : 0)) {
+#define KUMO_FUSED(LL, PP)                                                                                          \
+    case (LL) | ((PP) ? 16 : 0):                                                                                    \
+        if constexpr (LL <= MAXL)                                                                                   \
+            mixed_shell<(LL <= MAXL ? LL : 0), PP, P, false>(ap, x, y, z, r2, R0, -2.0f * R1, 4.0f * R2, dst,      \
+                                                              pstride, nullptr, lane);                             \
+        break;
+                        KUMO_FUSED(0, false) KUMO_FUSED(1, false) KUMO_FUSED(2, false) KUMO_FUSED(3, false)
+                        KUMO_FUSED(4, false) KUMO_FUSED(2, true) KUMO_FUSED(3, true) KUMO_FUSED(4, true)
+#undef KUMO_FUSED
+                        default: break;
+                    }
+                } else {
+                    for (int m = 0; m < cnt; ++m)
+#pragma unroll
+                        for (int c = 0; c < P; ++c) dst[c * pstride + m * kBlockPoints] = 0.0f;
+                }
+            }
+            row += cnt;
+        }
+        // Padding rows.
+        for (int i = tid; i < (16 - row) * P * kBlockPoints; i += kThreads) {
+            const int c = i / ((16 - row) * kBlockPoints);
+            const int r = row + (i / kBlockPoints) % (16 - row);
+            stg[(c * 16 + r) * kBlockPoints + (i % kBlockPoints)] = 0.0f;
+        }
+    };
+
+    bool failed = false;
+    long long gtile = 0;
+    DevDD chan_dd[2];
+    dd_zero(chan_dd[0]);
+    dd_zero(chan_dd[1]);
+
+    for (int ci = 0; ci < prm.nchannels && !failed; ++ci) {
+        const MoChannelTC ch = prm.ch[ci];
+        double q[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) q[i] = 0.0;
+        for (int n0 = 0; n0 < ch.nocc && !failed; n0 += N) {
+            auto load_b = [&](int t, int stage) {
+                const unsigned bst = smem_u32(b_st + stage * b_bytes);
+                const int nchunk = 3 * 16 * (N / 8);
+                for (int v = tid; v < nchunk; v += kThreads) {
+                    const int r8 = v & 7;
+                    const unsigned rest = static_cast<unsigned>(v) >> 3;
+                    const unsigned rest2 = (rest * nb8_mul) >> 16;
+                    const int ng = static_cast<int>(rest - rest2 * nb8);
+                    const int rh = static_cast<int>(rest2 & 1u), piece = static_cast<int>(rest2 >> 1);
+                    const int col = n0 + ng * 8;
+                    const int ao = col < ch.ldn ? row_ao(t, rh * 8 + r8) : -1;
+                    const bool ok = ao >= 0;
+                    const std::uint16_t* src =
+                        ch.cs + (ok ? piece * ch.piece_stride + static_cast<long long>(ao) * ch.ldn + col : 0);
+                    cp_async16(bst + static_cast<unsigned>(piece * 32 * N + ng * 128 + rh * (N * 16) + r8 * 16), src,
+                               ok);
+                }
+                asm volatile("cp.async.commit_group;" ::: "memory");
+            };
+            if (ntiles > 0) {
+                load_b(0, static_cast<int>(gtile % SB));
+                if (ntiles > 1) load_b(1, static_cast<int>((gtile + 1) % SB));
+            }
+            for (int t = 0; t < ntiles; ++t, ++gtile) {
+                const int s = static_cast<int>(gtile % S);
+                const int sb = static_cast<int>(gtile % SB);
+                produce(t);
+                __syncthreads();
+                unsigned char* ast = a_st + s * L::a_bytes;
+#pragma unroll
+                for (int c = 0; c < P; ++c) {
+                    const float4* src = reinterpret_cast<const float4*>(stg + (c * 16 + kh * 8 + k8) * kBlockPoints + g * 8);
+                    uint4 p0, p1, p2;
+                    split8(src[0], src[1], p0, p1, p2);
+                    *reinterpret_cast<uint4*>(ast + (0 * P + c) * kATile + a_off) = p0;
+                    *reinterpret_cast<uint4*>(ast + (1 * P + c) * kATile + a_off) = p1;
+                    *reinterpret_cast<uint4*>(ast + (2 * P + c) * kATile + a_off) = p2;
+                }
+                if (t + 1 < ntiles)
+                    asm volatile("cp.async.wait_group 1;" ::: "memory");
+                else
+                    asm volatile("cp.async.wait_group 0;" ::: "memory");
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                if (__syncthreads_or(failed)) {
+                    failed = true;
+                    break;
+                }
+                if (tid == 0) {
+                    tc_fence_after();
+                    const unsigned long long as = a_desc0 + ((static_cast<unsigned>(s) * L::a_bytes) >> 4);
+                    const unsigned long long bs = b_desc0 + ((static_cast<unsigned>(sb) * b_bytes) >> 4);
+                    const unsigned bpiece = (32u * static_cast<unsigned>(N)) >> 4;
+                    const unsigned dg = tmem + static_cast<unsigned>(t % G) * gcols;
+                    constexpr int pi[6] = {1, 0, 2, 0, 1, 0}, pjx[6] = {1, 2, 0, 1, 0, 0};
+#pragma unroll
+                    for (int c = 0; c < P; ++c) {
+#pragma unroll
+                        for (int e = 0; e < 6; ++e) {
+                            const unsigned long long ad = as + static_cast<unsigned>(((pi[e] * P + c) * kATile) >> 4);
+                            const unsigned long long bd = bs + static_cast<unsigned>(pjx[e]) * bpiece;
+                            tc_mma(dg + static_cast<unsigned>(c * N), ad, bd, idesc, (t >= G || e > 0) ? 1u : 0u);
+                        }
+                    }
+                    tc_commit(&bar[s]);
+                }
+                if (t + 1 < ntiles) {
+                    const long long wv = gtile + 1 - S;
+                    if (wv >= 0 && !mbar_wait(&bar[wv % S], static_cast<unsigned>((wv / S) & 1))) failed = true;
+                    if (t + 2 < ntiles) load_b(t + 2, static_cast<int>((gtile + 2) % SB));
+                }
+            }
+            if (failed || ntiles == 0) continue;
+            const long long last = gtile - 1;
+            if (!mbar_wait(&bar[last % S], static_cast<unsigned>((last / S) & 1))) failed = true;
+            if (__syncthreads_or(failed)) {
+                failed = true;
+                break;
+            }
+            tc_fence_after();
+            const int nvalid = ch.nocc - n0 < N ? ch.nocc - n0 : N;
+            const int i_lo = half * (N / 2), i_hi = min(nvalid, (half + 1) * (N / 2));
+            const unsigned lane_addr = tmem + (static_cast<unsigned>(quarter * 32) << 16);
+            const int ng = ntiles < G ? ntiles : G;
+            constexpr int MG = 4;
+            for (int i0 = i_lo; i0 < i_hi; i0 += MG) {
+                double x[P][MG];
+#pragma unroll
+                for (int c = 0; c < P; ++c)
+#pragma unroll
+                    for (int u = 0; u < MG; ++u) x[c][u] = 0.0;
+                for (int gi = 0; gi < ng; ++gi) {
+                    unsigned v[P][MG];
+#pragma unroll
+                    for (int c = 0; c < P; ++c)
+                        tmem_ld<MG>(lane_addr + static_cast<unsigned>(gi) * gcols + static_cast<unsigned>(c * N + i0), v[c]);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int c = 0; c < P; ++c) {
+                        reg_fence<MG>(v[c]);
+#pragma unroll
+                        for (int u = 0; u < MG; ++u) x[c][u] += static_cast<double>(__uint_as_float(v[c][u]));
+                    }
+                }
+                fold<P, MG>(x, q, i_hi - i0);
+            }
+            tc_fence_before();
+            __syncthreads();
+        }
+        if (failed) break;
+        if (half == 1)
+#pragma unroll
+            for (int i = 0; i < Q; ++i) red[i * 128 + point] = q[i];
+        __syncthreads();
+        if (half == 0) {
+#pragma unroll
+            for (int i = 0; i < Q; ++i) q[i] += red[i * 128 + point];
+            record<P>(q, prm.ao_order, ch.role == 1 ? chan_dd[0] : chan_dd[1]);
+        }
+        __syncthreads();
+    }
+
+    if (failed) {
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        if (tid == 0) atomicOr(prm.status, 1u);
+        for (int q = 0; q < S; ++q) {
+            const long long last = gtile - 1 - ((gtile - 1 - q) % S + S) % S;
+            if (last >= 0) (void)mbar_wait(&bar[last % S], static_cast<unsigned>((last / S) & 1));
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (w == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, static_cast<unsigned>(prm.tmem_cols));
+    }
+    if (half != 0 || point >= bcount) return;
+    DevDD comp[4];
+    if (failed) {
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        DevDD d;
+        d.value = d.lap = d.tau = nan;
+        for (int i = 0; i < 3; ++i) d.grad[i] = d.tau_axes[i] = nan;
+        for (int i = 0; i < 6; ++i) d.hess[i] = nan;
+        comp[0] = comp[1] = comp[2] = comp[3] = d;
+    } else {
+        DevDD alpha = chan_dd[0], beta = chan_dd[1];
+        if (prm.beta_is_alpha) beta = alpha;
+        comp[1] = alpha;
+        comp[2] = beta;
+        comp[0] = dd_combine(alpha, beta, 1.0, 1.0, false);
+        comp[3] = dd_combine(alpha, beta, -1.0, 1.0, false);
+    }
+    store_point(prm.spec, comp, start + point);
+}
+
+template <int P, int S, int MAXL>
+void launch_fused(const ContractFusedParams& p, cudaStream_t stream) {
+    constexpr size_t kMaxSmem = 227u * 1024u;
+    if (FusedSmem<P, S>::total(p.ncols) > kMaxSmem)
+        throw std::invalid_argument("fused tensor-core contraction: stages exceed shared memory");
+    cudaFuncSetAttribute(contract_fused_kernel<P, S, MAXL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(kMaxSmem));
+    contract_fused_kernel<P, S, MAXL><<<p.ao.nblocks, kThreads, kMaxSmem, stream>>>(p);
+}
+
+template <int P>
+void fused_maxl(const ContractFusedParams& p, cudaStream_t stream) {
+    if (p.ao.basis.max_l <= 2)
+        launch_fused<P, 2, 2>(p, stream);
+    else if (p.ao.basis.max_l == 3)
+        launch_fused<P, 2, 3>(p, stream);
+    else
+        launch_fused<P, 2, 4>(p, stream);
+}
+
 template <int P, int S>
 void launch(const ContractMixedParams& p, cudaStream_t stream) {
     // The whole 227 KB of shared memory per CTA: one CTA per SM, so each CTA's
@@ -416,6 +855,24 @@ void mixed_columns(int npanel, int nocc16, int& ncols, int& groups, int& tmem_co
     const int need = groups * npanel * ncols;
     tmem_cols = 32;
     while (tmem_cols < need) tmem_cols *= 2;
+}
+
+bool contract_fused_supported(int npanel, int nshells) {
+    return (npanel == 1 || npanel == 4 || npanel == 5) && nshells <= kFusedMaxShells;
+}
+
+void launch_contract_fused(const ContractFusedParams& p, int npanel, cudaStream_t stream) {
+    if (p.ao.nblocks <= 0) return;
+    if (p.ncols < 16 || p.ncols % 16 != 0 || p.ncols > 256 || p.groups < 1 ||
+        p.groups * npanel * p.ncols > 512 || p.tmem_cols > 512)
+        throw std::invalid_argument("tensor-core contraction: unsupported MO column count");
+    if (!contract_fused_supported(npanel, p.ao.basis.nblocks))
+        throw std::invalid_argument("fused tensor-core contraction: unsupported panel or shell count");
+    switch (npanel) {
+        case 1: fused_maxl<1>(p, stream); break;
+        case 4: fused_maxl<4>(p, stream); break;
+        default: fused_maxl<5>(p, stream); break;
+    }
 }
 
 void launch_contract_mixed(const ContractMixedParams& p, int npanel, cudaStream_t stream) {

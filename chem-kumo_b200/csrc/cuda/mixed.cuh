@@ -7,6 +7,7 @@
 
 #include <cstdint>
 
+#include "ao_mixed.cuh"
 #include "fields.cuh"
 #include "kumo_device.cuh"
 
@@ -70,5 +71,30 @@ unsigned* pipeline_status_word();
 unsigned take_pipeline_status();
 
 void launch_contract_mixed(const ContractMixedParams& p, int npanel, cudaStream_t stream);
+
+// Fused form of the mixed AO-MO path: the FP32 AO rows of each K step are
+// computed in the contraction kernel itself (no panels in global memory).
+// Rows are those of the AO blocks whose cutoff sphere reaches the point
+// block, in ascending order of a bound of their radial part over the block;
+// the K steps hold whole AO blocks (zero rows pad a step).
+constexpr int kFusedMaxShells = 2048;
+
+struct ContractFusedParams {
+    AoMixedParams ao;  // basis, primitives, points, first_point, block_size, nblocks, tpure, gcart
+    long long count = 0;
+    int nchannels = 0;
+    MoChannelTC ch[2];
+    int beta_is_alpha = 0;
+    int ao_order = 2;
+    int ncols = 16;
+    int groups = 1;
+    int tmem_cols = 32;
+    FieldSpec spec;
+    unsigned* status = nullptr;
+    int* nrows = nullptr;  // optional: AO rows contracted per block (for the profiler)
+};
+
+bool contract_fused_supported(int npanel, int nshells);
+void launch_contract_fused(const ContractFusedParams& p, int npanel, cudaStream_t stream);
 
 }  // namespace kumo_dev

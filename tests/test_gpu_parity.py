@@ -530,3 +530,23 @@ def test_repeatable():
     b, _ = K.Evaluator(m).evaluate_grid(grid, props)
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
+
+
+def test_fused_mixed_form_matches_two_kernel_form():
+    # The opt-in fused mixed AO-MO kernel (AO rows built inside the
+    # tensor-core kernel, KUMO_MIXED_FUSED=1) against the two-kernel form and
+    # the oracle, at the mixed tolerance.
+    m, o = _pair(os.path.join(GOLDEN, "acrolein.fchk.gz"))
+    pts = _box_points(o.atom_xyz.reshape(-1, 3), 4000, 21)
+    props = [K.density(P.Density), K.density(P.Gradient), K.density(P.Laplacian), K.density(P.Tau)]
+    base, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_points(pts, props)
+    os.environ["KUMO_MIXED_FUSED"] = "1"
+    try:
+        fused, used = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_points(pts, props)
+    finally:
+        del os.environ["KUMO_MIXED_FUSED"]
+    ref, _ = K.Evaluator(m).evaluate_points(pts, props)
+    assert used == int(K.Backend.AO_MO)
+    for p, a, b, r in zip(props, fused, base, ref):
+        assert scaled_error(a, r) <= 1e-6, p
+        assert scaled_error(a, b) <= 1e-6, p
