@@ -1,5 +1,6 @@
 // FP64 AO build.  Compiled with -fmad=false: every product and sum of the AO
 // arithmetic is rounded as written, in the reference's order.
+#include "func_attr.cuh"
 #include "ao_build.cuh"
 
 namespace kumo_dev {
@@ -8,7 +9,7 @@ template <int ORDER, int P, int MAXL>
 static void launch(const AoBuildParams<double>& p, cudaStream_t stream) {
     const size_t smem = sizeof(double) * ((size_t)p.basis.max_count * P * kBlockPoints + (size_t)kMaxPrim * kBlockPoints) +
                         sizeof(int) * (size_t)p.basis.nblocks;
-    cudaFuncSetAttribute(ao_build_kernel<double, ORDER, P, MAXL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    ensure_dynamic_smem(reinterpret_cast<const void*>(ao_build_kernel<double, ORDER, P, MAXL>), (int)smem);
     ao_build_kernel<double, ORDER, P, MAXL><<<p.nblocks, kBlockPoints, smem, stream>>>(p);
 }
 

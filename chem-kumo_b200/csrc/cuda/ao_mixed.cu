@@ -5,6 +5,7 @@
 // without arithmetic; otherwise each thread forms the three radial sums of
 // its point and the polynomial terms of the block's components, and stores
 // the P panels of each AO row with coalesced 128-point rows.
+#include "func_attr.cuh"
 #include "ao_common.cuh"
 #include "ao_mixed.cuh"
 #include "ao_mixed_shell.cuh"
@@ -93,7 +94,7 @@ template <int P, int MAXL>
 void launch(const AoMixedParams& p, cudaStream_t stream) {
     const size_t smem = sizeof(int) * static_cast<size_t>(p.basis.nblocks > 0 ? p.basis.nblocks : 1);
     if (smem > 48 * 1024)
-        cudaFuncSetAttribute(ao_mixed_kernel<P, MAXL>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        ensure_dynamic_smem(reinterpret_cast<const void*>(ao_mixed_kernel<P, MAXL>), static_cast<int>(smem));
     ao_mixed_kernel<P, MAXL><<<p.nblocks, kBlockPoints, smem, stream>>>(p);
 }
 

@@ -10,6 +10,7 @@
 // them into per-point partial sums (rho, grad, tau axes, Hessian terms); the
 // partials of the 8 warps are summed in a fixed order, so results do not
 // depend on scheduling.
+#include "func_attr.cuh"
 #include <cstdio>
 
 #include "contract.cuh"
@@ -218,8 +219,7 @@ static void launch_mo(const ContractMoParams& p, cudaStream_t stream) {
     const size_t smem = sizeof(double) * (size_t)(2 * KT * P * 32 + 2 * KT * MOC + 2 * Q * 32);
     static bool configured = false;
     if (!configured) {
-        cudaFuncSetAttribute(contract_mo_f64_kernel<P, MPT, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
+        ensure_dynamic_smem(reinterpret_cast<const void*>(contract_mo_f64_kernel<P, MPT, KT>), (int)smem);
         configured = true;
     }
     contract_mo_f64_kernel<P, MPT, KT><<<p.nblocks * 4, 256, smem, stream>>>(p);
@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(256, 1) orbital_energy_f64_kernel(const __grid
 void launch_orbital_energy_f64(const OrbitalEnergyParams& p, cudaStream_t stream) {
     constexpr int KT = 16;
     const size_t smem = sizeof(double) * (size_t)(2 * KT * 32 + 2 * KT * 128 + 8 * 2 * kOrbitalEnergySets * 32);
-    cudaFuncSetAttribute(orbital_energy_f64_kernel<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    ensure_dynamic_smem(reinterpret_cast<const void*>(orbital_energy_f64_kernel<KT>), (int)smem);
     orbital_energy_f64_kernel<KT><<<p.nblocks * 4, 256, smem, stream>>>(p);
 }
 
@@ -608,8 +608,7 @@ static void launch_p(const ContractPParams& p, cudaStream_t stream) {
     constexpr int Q = NQ<P>::v;
     const size_t smem = sizeof(double) * (size_t)(2 * KT * NY * 32 + 2 * KT * RC + 2 * Q * 32) + sizeof(int) * RC;
     static_assert(8 * Q * 32 <= 2 * KT * NY * 32 || VALUES, "reduction buffer must fit the tile buffers");
-    cudaFuncSetAttribute(contract_p_f64_kernel<P, VALUES, RPT, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
+    ensure_dynamic_smem(reinterpret_cast<const void*>(contract_p_f64_kernel<P, VALUES, RPT, KT>), (int)smem);
     contract_p_f64_kernel<P, VALUES, RPT, KT><<<p.nblocks * 4, 256, smem, stream>>>(p);
 }
 

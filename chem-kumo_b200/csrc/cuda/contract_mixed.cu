@@ -23,6 +23,7 @@
 // Every wait on an mbarrier is bounded; a wait that runs out sets *status,
 // stores NaN for the block's points, and the CTA waits (bounded again) for
 // its MMAs before it frees tensor memory and returns.
+#include "func_attr.cuh"
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -798,8 +799,7 @@ void launch_fused(const ContractFusedParams& p, cudaStream_t stream) {
     constexpr size_t kMaxSmem = 227u * 1024u;
     if (FusedSmem<P, S>::total(p.ncols) > kMaxSmem)
         throw std::invalid_argument("fused tensor-core contraction: stages exceed shared memory");
-    cudaFuncSetAttribute(contract_fused_kernel<P, S, MAXL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(kMaxSmem));
+    ensure_dynamic_smem(reinterpret_cast<const void*>(contract_fused_kernel<P, S, MAXL>), static_cast<int>(kMaxSmem));
     contract_fused_kernel<P, S, MAXL><<<p.ao.nblocks, kThreads, kMaxSmem, stream>>>(p);
 }
 
@@ -821,7 +821,7 @@ void launch(const ContractMixedParams& p, cudaStream_t stream) {
     constexpr size_t kMaxSmem = 227u * 1024u;
     if (Smem<P, S>::total(p.ncols) > kMaxSmem) throw std::invalid_argument("tensor-core contraction: stages exceed shared memory");
     const size_t smem = kMaxSmem;
-    cudaFuncSetAttribute(contract_mixed_kernel<P, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    ensure_dynamic_smem(reinterpret_cast<const void*>(contract_mixed_kernel<P, S>), static_cast<int>(smem));
     contract_mixed_kernel<P, S><<<p.nblocks, kThreads, smem, stream>>>(p);
 }
 

@@ -17,6 +17,7 @@
 // in ascending order of their block maximum as in the AO-MO contraction.
 // Every mbarrier wait is bounded; on expiry the CTA flags *status, stores NaN
 // and frees tensor memory after a bounded wait for its MMAs.
+#include "func_attr.cuh"
 #include <algorithm>
 #include <stdexcept>
 
@@ -326,7 +327,7 @@ template <int P>
 void launch(const ContractPMixedParams& p, cudaStream_t stream) {
     constexpr size_t kMaxSmem = 227u * 1024u;
     static_assert(SmemP<P>::total <= kMaxSmem, "AO-P stages exceed shared memory");
-    cudaFuncSetAttribute(contract_p_mixed_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMaxSmem));
+    ensure_dynamic_smem(reinterpret_cast<const void*>(contract_p_mixed_kernel<P>), static_cast<int>(kMaxSmem));
     contract_p_mixed_kernel<P><<<p.nblocks, kThreads, kMaxSmem, stream>>>(p);
 }
 

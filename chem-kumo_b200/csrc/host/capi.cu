@@ -622,6 +622,8 @@ int kumo_server_create(const kumo_server_options* opt, kumo_server** out, char* 
             if (opt->graph_points > 0) o.graph_points = static_cast<std::size_t>(opt->graph_points);
             if (opt->graph_points < 0) o.graph_points = 0;  // no graphs
             if (opt->request_scratch_bytes > 0) o.request_scratch = static_cast<std::size_t>(opt->request_scratch_bytes);
+            if (opt->staging_bytes > 0) o.staging_bytes = static_cast<std::size_t>(opt->staging_bytes);
+            if (opt->staging_bytes < 0) o.staging_bytes = 0;
         }
         auto s = std::make_unique<kumo_server>();
         s->srv = std::make_unique<Server>(o);

@@ -80,6 +80,7 @@ struct GraphEntry {
     double* d_out = nullptr;
     double* h_points = nullptr;  // page-locked
     double* h_out = nullptr;     // page-locked
+    bool own_host = true;        // false when both come from the server's staging arena
     std::size_t bucket = 0;
     std::size_t channels = 0;
     std::atomic<bool> busy{false};  // set by the scheduler, cleared by the completion thread
@@ -87,8 +88,10 @@ struct GraphEntry {
         if (exec) cudaGraphExecDestroy(exec);
         cudaFree(d_points);
         cudaFree(d_out);
-        cudaFreeHost(h_points);
-        cudaFreeHost(h_out);
+        if (own_host) {
+            cudaFreeHost(h_points);
+            cudaFreeHost(h_out);
+        }
     }
 };
 
@@ -142,6 +145,27 @@ struct Server::Impl {
     std::map<std::string, std::vector<std::unique_ptr<GraphEntry>>> graphs;
     std::map<std::string, int> seen;  // small-request keys met so far (a graph is captured on the second)
     std::multimap<std::size_t, double*> free_stage;  // page-locked staging by size
+    // Page-locked arena, allocated once at start: staging buffers are carved
+    // from it (page-locking on demand synchronises the device and stalls the
+    // scheduler while the GPU is busy); beyond it, cudaHostAlloc.
+    char* arena = nullptr;
+    std::size_t arena_size = 0, arena_used = 0;
+    double* pinned(std::size_t cls, bool& from_arena) {
+        if (arena && arena_used + cls <= arena_size) {
+            double* p = reinterpret_cast<double*>(arena + arena_used);
+            arena_used += cls;
+            from_arena = true;
+            return p;
+        }
+        void* p = nullptr;
+        check_cuda(cudaHostAlloc(&p, cls, cudaHostAllocDefault), "cudaHostAlloc (staging)");
+        from_arena = false;
+        return static_cast<double*>(p);
+    }
+    bool in_arena(const void* p) const {
+        const char* c = static_cast<const char*>(p);
+        return arena && c >= arena && c < arena + arena_size;
+    }
     std::vector<const Molecule*> resident;
     std::size_t resident_bytes = 0, active_bytes = 0;
 
@@ -191,9 +215,8 @@ double* Server::Impl::get_stage(std::size_t bytes) {
         free_stage.erase(it);
         return p;
     }
-    void* p = nullptr;
-    check_cuda(cudaHostAlloc(&p, cls, cudaHostAllocDefault), "cudaHostAlloc (staging)");
-    return static_cast<double*>(p);
+    bool from_arena = false;
+    return pinned(cls, from_arena);
 }
 
 GraphEntry* Server::Impl::graph_for(const Pending& p, cudaStream_t stream) {
@@ -208,14 +231,26 @@ GraphEntry* Server::Impl::graph_for(const Pending& p, cudaStream_t stream) {
     auto e = std::make_unique<GraphEntry>();
     e->bucket = round_bucket(p.n);
     e->channels = p.channels;
-    check_cuda(cudaMalloc(&e->d_points, sizeof(double) * 3 * e->bucket), "cudaMalloc (serving points)");
-    check_cuda(cudaMalloc(&e->d_out, sizeof(double) * std::max<std::size_t>(e->channels * e->bucket, 1)),
-               "cudaMalloc (serving outputs)");
-    check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&e->h_points), sizeof(double) * 3 * e->bucket, cudaHostAllocDefault),
-               "cudaHostAlloc (serving points)");
-    check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&e->h_out),
-                             sizeof(double) * std::max<std::size_t>(e->channels * e->bucket, 1), cudaHostAllocDefault),
-               "cudaHostAlloc (serving outputs)");
+    check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&e->d_points), sizeof(double) * 3 * e->bucket, stream),
+               "cudaMallocAsync (serving points)");
+    check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&e->d_out),
+                               sizeof(double) * std::max<std::size_t>(e->channels * e->bucket, 1), stream),
+               "cudaMallocAsync (serving outputs)");
+    {
+        const std::size_t pb = stage_class(sizeof(double) * 3 * e->bucket);
+        const std::size_t ob = stage_class(sizeof(double) * std::max<std::size_t>(e->channels * e->bucket, 1));
+        if (arena && arena_used + pb + ob <= arena_size) {
+            bool unused = false;
+            e->h_points = pinned(pb, unused);
+            e->h_out = pinned(ob, unused);
+            e->own_host = false;
+        } else {
+            check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&e->h_points), pb, cudaHostAllocDefault),
+                       "cudaHostAlloc (serving points)");
+            check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&e->h_out), ob, cudaHostAllocDefault),
+                       "cudaHostAlloc (serving outputs)");
+        }
+    }
     std::vector<double*> outs;
     std::size_t off = 0;
     for (const auto& q : p.req.request.properties()) {
@@ -480,6 +515,11 @@ Server::Server(ServerOptions options) : impl_(std::make_unique<Impl>()) {
     const std::size_t cap = static_cast<std::size_t>(0.9 * static_cast<double>(free_b));
     m.budget = m.opt.hbm_budget ? std::min(m.opt.hbm_budget, cap) : std::min<std::size_t>(150ull * 1000 * 1000 * 1000, cap);
     m.st.budget_bytes = m.budget;
+    if (m.opt.staging_bytes) {
+        check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&m.arena), m.opt.staging_bytes, cudaHostAllocDefault),
+                   "cudaHostAlloc (staging arena)");
+        m.arena_size = m.opt.staging_bytes;
+    }
     m.scheduler = std::thread([&m] {
         try {
             m.run_scheduler();
@@ -514,8 +554,11 @@ Server::~Server() {
     cudaSetDevice(m.opt.device);
     cudaDeviceSynchronize();
     m.graphs.clear();
-    for (auto& [b, p] : m.free_stage) cudaFreeHost(p);
-    for (auto& [b, p] : m.returned_stage) cudaFreeHost(p);
+    for (auto& [b, p] : m.free_stage)
+        if (!m.in_arena(p)) cudaFreeHost(p);
+    for (auto& [b, p] : m.returned_stage)
+        if (!m.in_arena(p)) cudaFreeHost(p);
+    if (m.arena) cudaFreeHost(m.arena);
     for (auto s : m.free_streams) cudaStreamDestroy(s);
     for (auto e : m.free_events) cudaEventDestroy(e);
 }

@@ -36,6 +36,9 @@ struct ServerOptions {
     int max_active = 8;                      ///< requests in flight (one stream each)
     std::size_t graph_points = 65536;        ///< largest request replayed from a CUDA graph
     std::size_t request_scratch = 1ull << 30;  ///< AO scratch per request (sets its wave size)
+    /// Page-locked host arena for staging results and points, allocated once
+    /// at start (0: none, every staging buffer page-locked on demand).
+    std::size_t staging_bytes = 2ull << 30;
 };
 
 struct ServeRequest {

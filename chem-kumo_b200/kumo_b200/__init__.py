@@ -179,7 +179,7 @@ _SCALAR_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.c_longlong, C.POINTER(C.
 
 class _ServerOptions(C.Structure):
     _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_double), ("max_active", C.c_int),
-                ("graph_points", C.c_longlong), ("request_scratch_bytes", C.c_double)]
+                ("graph_points", C.c_longlong), ("request_scratch_bytes", C.c_double), ("staging_bytes", C.c_double)]
 
 
 class _ServerStats(C.Structure):
@@ -574,9 +574,9 @@ class Server:
     arrays must stay alive until wait() reports the ticket done."""
 
     def __init__(self, device: int = 0, hbm_budget_bytes: float = 0.0, max_active: int = 0,
-                 graph_points: int = 0, request_scratch_bytes: float = 0.0):
+                 graph_points: int = 0, request_scratch_bytes: float = 0.0, staging_bytes: float = 0.0):
         o = _ServerOptions(int(device), float(hbm_budget_bytes), int(max_active), int(graph_points),
-                           float(request_scratch_bytes))
+                           float(request_scratch_bytes), float(staging_bytes))
         h = C.c_void_p()
         e = _err()
         _check(lib().kumo_server_create(C.byref(o), C.byref(h), e, 512), e)

@@ -236,6 +236,7 @@ typedef struct {
     int max_active;
     long long graph_points;
     double request_scratch_bytes;
+    double staging_bytes; /* page-locked staging arena (0: 2 GiB; negative: none) */
 } kumo_server_options;
 
 typedef struct {

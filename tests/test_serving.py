@@ -103,7 +103,8 @@ def test_serving_admission_under_small_budget():
     # for memory instead of failing, every one completes, and the admitted
     # footprint never exceeds the budget.
     m = K.Molecule.from_fchk(os.path.join(GOLDEN, "acrolein.fchk.gz"))
-    srv = K.Server(hbm_budget_bytes=1.5e9, max_active=8, request_scratch_bytes=256 * 2**20)
+    # A 1 MiB staging arena: most staging falls back to page-locking on demand.
+    srv = K.Server(hbm_budget_bytes=1.5e9, max_active=8, request_scratch_bytes=256 * 2**20, staging_bytes=2**20)
     grid = m.grid_around(3.0, 0.15)
     tickets = [srv.submit_grid(m, grid, FIELDS, precision=int(K.Precision.Mixed)) for _ in range(3)]
     tickets += [srv.submit_points(m, np.random.default_rng(i).uniform(-3, 3, (500, 3)), FIELDS) for i in range(5)]
