@@ -412,12 +412,10 @@ def main() -> None:
         torch.cuda.synchronize()
         return [a.elapsed_time(b) for a, b in times]
 
+    from kumo_b200 import shard
+
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return shard.max_over_ranks(x, dist, world, device="cuda")
 
     if args.esp_only:
         if rank == 0:
