@@ -550,3 +550,20 @@ def test_fused_mixed_form_matches_two_kernel_form():
     for p, a, b, r in zip(props, fused, base, ref):
         assert scaled_error(a, r) <= 1e-6, p
         assert scaled_error(a, b) <= 1e-6, p
+
+
+def test_sharded_grid_equals_whole_grid():
+    # Two block ranges evaluated as points (as two ranks would) give the
+    # one-call grid result bit for bit.
+    from kumo_b200 import shard
+    m = K.Molecule.from_fchk(os.path.join(GOLDEN, "acrolein.fchk.gz"))
+    grid = m.grid_around(2.0, 0.3)
+    props = [K.density(P.Density), K.density(P.Gradient), K.density(P.Elf)]
+    whole, _ = K.Evaluator(m).evaluate_grid(grid, props)
+    parts = []
+    for r in range(3):
+        first, count = shard.block_range(grid.npoints, r, 3)
+        pts = shard.grid_points(grid.origin, grid.steps, grid.counts, first, count)
+        parts.append(K.Evaluator(m).evaluate_points(pts, props)[0])
+    for i in range(len(props)):
+        assert np.array_equal(np.concatenate([p[i] for p in parts], axis=1), whole[i])
