@@ -188,6 +188,20 @@ EspDevice::EspDevice(const chem::kumo::Molecule& m, cudaStream_t stream) {
     // Pairs grouped by order (stable), so that each launch of the device
     // kernel handles one order with its recursion unrolled.
     std::stable_sort(pairs.begin(), pairs.end(), [](const EspPair& x, const EspPair& y) { return x.order < y.order; });
+    // Coefficients in pair order, so that a run of pairs has one contiguous
+    // run of coefficients (the kernel stages them in batches).
+    {
+        std::vector<double> ordered;
+        ordered.reserve(coef.size());
+        for (auto& pr : pairs) {
+            const int nt = hermite_count(pr.order);
+            const std::size_t f = static_cast<std::size_t>(pr.first);
+            pr.first = static_cast<int>(ordered.size());
+            ordered.insert(ordered.end(), coef.begin() + static_cast<std::ptrdiff_t>(f),
+                           coef.begin() + static_cast<std::ptrdiff_t>(f + nt));
+        }
+        coef.swap(ordered);
+    }
     for (int L = 0; L <= kEspMaxL + 1; ++L)
         view_.order_first[L] = std::lower_bound(pairs.begin(), pairs.end(), L,
                                                 [](const EspPair& x, int v) { return x.order < v; }) -
@@ -363,12 +377,18 @@ __device__ __forceinline__ void hermite_level(double (&R)[NT], int live, double 
 
 // Pairs of order L: thread = point of a 128-point tile, blockIdx.y = chunk of
 // the order's pairs; the partial sum of the chunk goes to
-// part[(slot0 + chunk) * ld + point].
+// part[(slot0 + chunk) * ld + point].  The chunk's pairs and their
+// coefficients (contiguous, in pair order) are staged in shared memory in
+// batches by the whole CTA with coalesced loads, so the per-pair loop reads
+// them with broadcast shared loads instead of dependent global ones.
 template <int L>
 __global__ void __launch_bounds__(128) esp_order_kernel(const __grid_constant__ EspParams prm, long long first,
                                                        long long count, long long chunk, int slot0, double* part,
                                                        long long ld) {
     constexpr int NT = hermite_count(L);
+    constexpr int BATCH = (2048 / NT) < 128 ? (2048 / NT) : 128;
+    __shared__ double s_p[BATCH], s_q[BATCH][3];
+    __shared__ double s_c[BATCH * NT];
     const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     const bool valid = q < prm.src.count;
     double x = 0.0, y = 0.0, z = 0.0;
@@ -377,28 +397,42 @@ __global__ void __launch_bounds__(128) esp_order_kernel(const __grid_constant__ 
     const long long i0 = first + static_cast<long long>(blockIdx.y) * chunk;
     const long long i1 = min(first + count, i0 + chunk);
     double sum = 0.0;
-    for (long long i = i0; i < i1; ++i) {
-        const EspPair pr = e.pairs[i];
-        const double pcx = pr.qx - x, pcy = pr.qy - y, pcz = pr.qz - z;
-        double F[L + 1];
-        boys_top<L>(e.boys_table, pr.p * (pcx * pcx + pcy * pcy + pcz * pcz), F);
-        double power = 1.0;
-#pragma unroll
-        for (int k = 1; k <= L; ++k) {
-            power *= -2.0 * pr.p;
-            F[k] *= power;
+    for (long long b0 = i0; b0 < i1; b0 += BATCH) {
+        const int nb = static_cast<int>(min(static_cast<long long>(BATCH), i1 - b0));
+        __syncthreads();  // the previous batch is no longer read
+        for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+            const EspPair pr = e.pairs[b0 + t];
+            s_p[t] = pr.p;
+            s_q[t][0] = pr.qx;
+            s_q[t][1] = pr.qy;
+            s_q[t][2] = pr.qz;
         }
-        double R[NT];
+        const double* cbase = e.coef + e.pairs[b0].first;
+        for (int t = threadIdx.x; t < nb * NT; t += blockDim.x) s_c[t] = cbase[t];
+        __syncthreads();
+        for (int ib = 0; ib < nb; ++ib) {
+            const double pcx = s_q[ib][0] - x, pcy = s_q[ib][1] - y, pcz = s_q[ib][2] - z;
+            const double pp = s_p[ib];
+            double F[L + 1];
+            boys_top<L>(e.boys_table, pp * (pcx * pcx + pcy * pcy + pcz * pcz), F);
+            double power = 1.0;
 #pragma unroll
-        for (int n = L; n >= 0; --n) {
-            hermite_level<NT - 1, NT>(R, hermite_count(L - n), pcx, pcy, pcz);
-            R[0] = F[n];
+            for (int k = 1; k <= L; ++k) {
+                power *= -2.0 * pp;
+                F[k] *= power;
+            }
+            double R[NT];
+#pragma unroll
+            for (int n = L; n >= 0; --n) {
+                hermite_level<NT - 1, NT>(R, hermite_count(L - n), pcx, pcy, pcz);
+                R[0] = F[n];
+            }
+            const double* c = s_c + ib * NT;
+            double s = 0.0;
+#pragma unroll
+            for (int k = 0; k < NT; ++k) s += c[k] * R[k];
+            sum += s;
         }
-        const double* c = e.coef + pr.first;
-        double s = 0.0;
-#pragma unroll
-        for (int k = 0; k < NT; ++k) s += c[k] * R[k];
-        sum += s;
     }
     if (valid) part[static_cast<long long>(slot0 + blockIdx.y) * ld + q] = sum;
 }
