@@ -37,6 +37,12 @@
 namespace kumo_dev {
 namespace {
 
+// Threads that issue a step's MMAs (the first lane of each of the first
+// kIssuers warps, panels dealt round-robin), and the arrivals on a stage's
+// barrier.
+template <int P>
+constexpr int kIssuers = P < 8 ? P : 8;
+
 template <int P>
 struct NQm {
     static constexpr int v = P == 1 ? 1 : P == 4 ? 7 : P == 5 ? 8 : 19;
@@ -137,7 +143,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
     const int* kept = scr.kept + static_cast<size_t>(blk) * scr.row_stride;
 
     if (tid == 0) {
-        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+        for (int s = 0; s < S; ++s) mbar_init(&bar[s], kIssuers<P>);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (w == 0) tmem_alloc(tslot, static_cast<unsigned>(prm.tmem_cols));
@@ -261,7 +267,11 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
                     failed = true;
                     break;
                 }
-                if (tid == 0) {
+                if (lane == 0 && w < kIssuers<P>) {
+                    // The panels' MMAs are issued by the first lanes of
+                    // kIssuers<P> warps in parallel (disjoint accumulator
+                    // columns, one commit each on the stage's barrier):
+                    // tcgen05.mma issue waits while the tensor pipe is full.
                     tc_fence_after();
                     const unsigned long long as = a_desc0 + ((static_cast<unsigned>(s) * L::a_bytes) >> 4);
                     const unsigned long long bs = b_desc0 + ((static_cast<unsigned>(sb) * b_bytes) >> 4);
@@ -269,8 +279,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
                     // K steps go round-robin to G accumulator groups.
                     const unsigned dg = tmem + static_cast<unsigned>(t % G) * gcols;
                     constexpr int pi[6] = {1, 0, 2, 0, 1, 0}, pj[6] = {1, 2, 0, 1, 0, 0};
-#pragma unroll
-                    for (int c = 0; c < P; ++c) {
+                    for (int c = w; c < P; c += kIssuers<P>) {
 #pragma unroll
                         for (int e = 0; e < 6; ++e) {
                             const unsigned long long ad = as + static_cast<unsigned>(((pi[e] * P + c) * kATile) >> 4);
@@ -281,8 +290,8 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
                     tc_commit(&bar[s]);
                 }
                 if (t + 1 < ntiles) {
-                    const long long w = gtile + 1 - S;
-                    if (w >= 0 && !mbar_wait(&bar[w % S], static_cast<unsigned>((w / S) & 1))) failed = true;
+                    const long long wv = gtile + 1 - S;
+                    if (wv >= 0 && !mbar_wait(&bar[wv % S], static_cast<unsigned>((wv / S) & 1))) failed = true;
                     if (t + 2 < ntiles) load_b(t + 2, static_cast<int>((gtile + 2) % SB));
                 }
             }
@@ -443,7 +452,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_fused_kernel(const __gri
     if (pvalid) point_at(ap.src, start + pj, px, py, pz);
 
     if (tid == 0) {
-        for (int q = 0; q < S; ++q) mbar_init(&bar[q], 1);
+        for (int q = 0; q < S; ++q) mbar_init(&bar[q], kIssuers<P>);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (w == 0) tmem_alloc(tslot, static_cast<unsigned>(prm.tmem_cols));
@@ -686,15 +695,14 @@ __global__ void __launch_bounds__(kThreads, 1) contract_fused_kernel(const __gri
                     failed = true;
                     break;
                 }
-                if (tid == 0) {
+                if (lane == 0 && w < kIssuers<P>) {
                     tc_fence_after();
                     const unsigned long long as = a_desc0 + ((static_cast<unsigned>(s) * L::a_bytes) >> 4);
                     const unsigned long long bs = b_desc0 + ((static_cast<unsigned>(sb) * b_bytes) >> 4);
                     const unsigned bpiece = (32u * static_cast<unsigned>(N)) >> 4;
                     const unsigned dg = tmem + static_cast<unsigned>(t % G) * gcols;
                     constexpr int pi[6] = {1, 0, 2, 0, 1, 0}, pjx[6] = {1, 2, 0, 1, 0, 0};
-#pragma unroll
-                    for (int c = 0; c < P; ++c) {
+                    for (int c = w; c < P; c += kIssuers<P>) {
 #pragma unroll
                         for (int e = 0; e < 6; ++e) {
                             const unsigned long long ad = as + static_cast<unsigned>(((pi[e] * P + c) * kATile) >> 4);
