@@ -110,12 +110,24 @@ struct Smem {
     static size_t total(int ncols) {
         return S * static_cast<size_t>(a_bytes) + SB * static_cast<size_t>(b_bytes(ncols)) +
                sizeof(double) * Q * 128 + (sizeof(int) + 1 + sizeof(std::uint16_t)) * kSortCap +
-               sizeof(int) * (kBuckets + 4) + 8 * S + 16;
+               sizeof(int) * (kBuckets + 4) + 16 * S + 16;
     }
 };
 
+// With two or more AO stages the CTA has a ninth warp that only issues the
+// MMAs: the eight producer warps split the AO rows and fetch coefficients and
+// arrive (without waiting) on the stage's "full" mbarrier; the MMA warp waits
+// on it, issues the step's MMAs and commits them to the stage's "empty"
+// mbarrier, which the producers wait on before they reuse the stage.  The MMA
+// issue, which waits while the tensor pipe is full, is off the producers'
+// path, and every wait is bounded.
+template <int S>
+constexpr bool kMmaWarp = S >= 2;
+template <int S>
+constexpr int kCtaThreads = kMmaWarp<S> ? kThreads + 32 : kThreads;
+
 template <int P, int S>
-__global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __grid_constant__ ContractMixedParams prm) {
+__global__ void __launch_bounds__(kCtaThreads<S>, 1) contract_mixed_kernel(const __grid_constant__ ContractMixedParams prm) {
     using L = Smem<P, S>;
     constexpr int Q = L::Q;
     constexpr int SB = L::SB;
@@ -129,8 +141,9 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
     int* bucket_start = perm + kSortCap;
     std::uint16_t* aoidx = reinterpret_cast<std::uint16_t*>(bucket_start + kBuckets + 4);
     unsigned char* keys = reinterpret_cast<unsigned char*>(aoidx + kSortCap);
-    unsigned long long* bar = reinterpret_cast<unsigned long long*>(keys + kSortCap);
-    unsigned* tslot = reinterpret_cast<unsigned*>(bar + S);
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(keys + kSortCap);  // empty: MMAs done
+    unsigned long long* full = bar + S;                                                // full: stage written
+    unsigned* tslot = reinterpret_cast<unsigned*>(full + S);
 
     const int blk = blockIdx.x;
     const long long start = prm.first_point + static_cast<long long>(blk) * prm.block_size;
@@ -142,8 +155,13 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
     const float* pbase = scr.panels + static_cast<size_t>(blk) * P * scr.row_stride * kBlockPoints;
     const int* kept = scr.kept + static_cast<size_t>(blk) * scr.row_stride;
 
+    constexpr bool kSpec = kMmaWarp<S>;
+    const bool producer = !kSpec || tid < kThreads;
     if (tid == 0) {
-        for (int s = 0; s < S; ++s) mbar_init(&bar[s], kIssuers<P>);
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&bar[s], kSpec ? 1 : kIssuers<P>);
+            mbar_init(&full[s], kThreads);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (w == 0) tmem_alloc(tslot, static_cast<unsigned>(prm.tmem_cols));
@@ -158,7 +176,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
     // bases below 65536 functions; others read the kept list).
     const bool have_idx = nk <= kSortCap && scr.row_stride <= 65535;
     if (have_idx)
-        for (int k = tid; k < nk; k += kThreads) aoidx[k] = static_cast<std::uint16_t>(kept[sorted ? perm[k] : k]);
+        for (int k = tid; producer && k < nk; k += kThreads) aoidx[k] = static_cast<std::uint16_t>(kept[sorted ? perm[k] : k]);
     const int ntiles = (nk + 15) / 16;
     tc_fence_before();
     __syncthreads();
@@ -237,15 +255,70 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
             // are waited for at the end of step t.  Coefficient pieces run two
             // steps ahead in SB = S + 1 stages: step t+2's stage was last read
             // by the MMAs of step t+2-SB = t+1-S, complete by then too.
-            if (ntiles > 0) {
+            if (ntiles > 0 && producer) {
                 load_a(0);
                 load_b(0, static_cast<int>(gtile % SB));
                 if (ntiles > 1) load_b(1, static_cast<int>((gtile + 1) % SB));
             }
+            const unsigned bpiece = (32u * static_cast<unsigned>(N)) >> 4;
+            constexpr int pi[6] = {1, 0, 2, 0, 1, 0}, pj[6] = {1, 2, 0, 1, 0, 0};
+            // The six MMAs of panel c of K step t (stage s, coefficient stage sb).
+            auto issue_panel = [&](int t, int s, int sb, int c) {
+                const unsigned long long as = a_desc0 + ((static_cast<unsigned>(s) * L::a_bytes) >> 4);
+                const unsigned long long bs = b_desc0 + ((static_cast<unsigned>(sb) * b_bytes) >> 4);
+                // K steps go round-robin to G accumulator groups.
+                const unsigned dg = tmem + static_cast<unsigned>(t % G) * gcols;
+#pragma unroll
+                for (int e = 0; e < 6; ++e) {
+                    const unsigned long long ad = as + static_cast<unsigned>(((pi[e] * P + c) * kATile) >> 4);
+                    const unsigned long long bd = bs + static_cast<unsigned>(pj[e]) * bpiece;
+                    tc_mma(dg + static_cast<unsigned>(c * N), ad, bd, idesc, (t >= G || e > 0) ? 1u : 0u);
+                }
+            };
             for (int t = 0; t < ntiles; ++t, ++gtile) {
                 const int s = static_cast<int>(gtile % S);
                 const int sb = static_cast<int>(gtile % SB);
-                // A pieces of this step.
+                if constexpr (kSpec) {
+                    if (!producer) {
+                        // Stage s holds step t once all producers arrived on
+                        // full[s] for its (gtile / S)-th use.
+                        if (lane == 0) {
+                            if (!mbar_wait(&full[s], static_cast<unsigned>((gtile / S) & 1))) failed = true;
+                            tc_fence_after();
+#pragma unroll
+                            for (int c = 0; c < P; ++c) issue_panel(t, s, sb, c);
+                            tc_commit(&bar[s]);
+                        }
+                        __syncwarp();
+                        continue;
+                    }
+                    unsigned char* ast = a_st + s * L::a_bytes;
+#pragma unroll
+                    for (int c = 0; c < P; ++c) {
+                        uint4 p0, p1, p2;
+                        split8(ra[c][0], ra[c][1], p0, p1, p2);
+                        *reinterpret_cast<uint4*>(ast + (0 * P + c) * kATile + a_off) = p0;
+                        *reinterpret_cast<uint4*>(ast + (1 * P + c) * kATile + a_off) = p1;
+                        *reinterpret_cast<uint4*>(ast + (2 * P + c) * kATile + a_off) = p2;
+                    }
+                    if (t + 1 < ntiles) load_a(t + 1);
+                    if (t + 1 < ntiles)
+                        asm volatile("cp.async.wait_group 1;" ::: "memory");
+                    else
+                        asm volatile("cp.async.wait_group 0;" ::: "memory");
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    mbar_arrive(&full[s]);
+                    if (t + 1 < ntiles) {
+                        // Step t+1's AO stage and step t+2's coefficient stage
+                        // were last read by the MMAs of step t+1-S.
+                        const long long wv = gtile + 1 - S;
+                        if (wv >= 0 && !mbar_wait(&bar[wv % S], static_cast<unsigned>((wv / S) & 1))) failed = true;
+                        if (t + 2 < ntiles) load_b(t + 2, static_cast<int>((gtile + 2) % SB));
+                    }
+                    continue;
+                }
+                // One AO stage: all warps split, then the first lanes of
+                // kIssuers<P> warps issue the panels' MMAs.
                 unsigned char* ast = a_st + s * L::a_bytes;
 #pragma unroll
                 for (int c = 0; c < P; ++c) {
@@ -256,8 +329,6 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
                     *reinterpret_cast<uint4*>(ast + (2 * P + c) * kATile + a_off) = p2;
                 }
                 if (t + 1 < ntiles) load_a(t + 1);
-                // This step's coefficient group is complete; step t+1's may
-                // still be in flight.
                 if (t + 1 < ntiles)
                     asm volatile("cp.async.wait_group 1;" ::: "memory");
                 else
@@ -268,25 +339,8 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
                     break;
                 }
                 if (lane == 0 && w < kIssuers<P>) {
-                    // The panels' MMAs are issued by the first lanes of
-                    // kIssuers<P> warps in parallel (disjoint accumulator
-                    // columns, one commit each on the stage's barrier):
-                    // tcgen05.mma issue waits while the tensor pipe is full.
                     tc_fence_after();
-                    const unsigned long long as = a_desc0 + ((static_cast<unsigned>(s) * L::a_bytes) >> 4);
-                    const unsigned long long bs = b_desc0 + ((static_cast<unsigned>(sb) * b_bytes) >> 4);
-                    const unsigned bpiece = (32u * static_cast<unsigned>(N)) >> 4;
-                    // K steps go round-robin to G accumulator groups.
-                    const unsigned dg = tmem + static_cast<unsigned>(t % G) * gcols;
-                    constexpr int pi[6] = {1, 0, 2, 0, 1, 0}, pj[6] = {1, 2, 0, 1, 0, 0};
-                    for (int c = w; c < P; c += kIssuers<P>) {
-#pragma unroll
-                        for (int e = 0; e < 6; ++e) {
-                            const unsigned long long ad = as + static_cast<unsigned>(((pi[e] * P + c) * kATile) >> 4);
-                            const unsigned long long bd = bs + static_cast<unsigned>(pj[e]) * bpiece;
-                            tc_mma(dg + static_cast<unsigned>(c * N), ad, bd, idesc, (t >= G || e > 0) ? 1u : 0u);
-                        }
-                    }
+                    for (int c = w; c < P; c += kIssuers<P>) issue_panel(t, s, sb, c);
                     tc_commit(&bar[s]);
                 }
                 if (t + 1 < ntiles) {
@@ -295,7 +349,16 @@ __global__ void __launch_bounds__(kThreads, 1) contract_mixed_kernel(const __gri
                     if (t + 2 < ntiles) load_b(t + 2, static_cast<int>((gtile + 2) % SB));
                 }
             }
-            if (failed || ntiles == 0) continue;
+            if (ntiles == 0) continue;
+            if constexpr (kSpec) {
+                // Producers' timeouts become every thread's before the pass ends.
+                if (__syncthreads_or(failed)) {
+                    failed = true;
+                    break;
+                }
+            } else if (failed) {
+                continue;
+            }
             // Accumulators of this pass complete once the last step's commit arrives.
             const long long last = gtile - 1;
             if (!mbar_wait(&bar[last % S], static_cast<unsigned>((last / S) & 1))) failed = true;
@@ -830,7 +893,7 @@ void launch(const ContractMixedParams& p, cudaStream_t stream) {
     if (Smem<P, S>::total(p.ncols) > kMaxSmem) throw std::invalid_argument("tensor-core contraction: stages exceed shared memory");
     const size_t smem = kMaxSmem;
     ensure_dynamic_smem(reinterpret_cast<const void*>(contract_mixed_kernel<P, S>), static_cast<int>(smem));
-    contract_mixed_kernel<P, S><<<p.nblocks, kThreads, smem, stream>>>(p);
+    contract_mixed_kernel<P, S><<<p.nblocks, kCtaThreads<S>, smem, stream>>>(p);
 }
 
 __device__ unsigned g_pipeline_status;

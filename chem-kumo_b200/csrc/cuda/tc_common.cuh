@@ -40,6 +40,10 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
 
 // Waits until the phase with the given parity has completed; false if that
 // did not happen within kWaitNs.
+// One arrival (release semantics) on an mbarrier, without waiting.
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
@@ -170,16 +174,17 @@ __device__ __forceinline__ int block_row_order(const float* rowmax4, int nk, flo
     sorted = rowmax4 != nullptr && nk <= kSortCap;
     if (sorted) {
         const float4* rmax = reinterpret_cast<const float4*>(rowmax4);
-        for (int k = tid; k < nk; k += kThreads) {
+        // Threads beyond kThreads (a CTA's MMA warp) only meet the barriers.
+        for (int k = tid; tid < kThreads && k < nk; k += kThreads) {
             const float4 v = rmax[k];
             const float mx = fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w));
             const int e = static_cast<int>((__float_as_uint(mx) >> 23) & 0xffu) - 127 + kBuckets / 2;
             const bool keep = threshold == 0.0f || mx > threshold;
             keys[k] = keep ? static_cast<unsigned char>(e < 0 ? 0 : (e >= kBuckets ? kBuckets - 1 : e)) : 0xffu;
         }
-        for (int b = tid; b <= kBuckets; b += kThreads) bucket_start[b] = 0;
+        for (int b = tid; tid < kThreads && b <= kBuckets; b += kThreads) bucket_start[b] = 0;
         __syncthreads();
-        for (int k = tid; k < nk; k += kThreads)
+        for (int k = tid; tid < kThreads && k < nk; k += kThreads)
             if (keys[k] != 0xffu) atomicAdd(&bucket_start[keys[k]], 1);
         __syncthreads();
         if (w == 0) {
