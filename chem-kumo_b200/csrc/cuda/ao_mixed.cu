@@ -14,7 +14,7 @@ namespace kumo_dev {
 namespace {
 
 template <int P, int MAXL>
-__global__ void __launch_bounds__(kBlockPoints, 4) ao_mixed_kernel(const __grid_constant__ AoMixedParams prm) {
+__global__ void __launch_bounds__(kBlockPoints, (P == 10 || MAXL >= 4) ? 6 : 8) ao_mixed_kernel(const __grid_constant__ AoMixedParams prm) {
     constexpr int NW = kBlockPoints / 32;
     extern __shared__ int s_list[];
     __shared__ double s_box[NW][6];
