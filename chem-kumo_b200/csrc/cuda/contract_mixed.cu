@@ -24,9 +24,13 @@
 // stores NaN for the block's points, and the CTA waits (bounded again) for
 // its MMAs before it frees tensor memory and returns.
 #include "func_attr.cuh"
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstdint>
+#include <cstdlib>
 #include <stdexcept>
 #include <string>
 
@@ -444,6 +448,358 @@ __global__ void __launch_bounds__(kCtaThreads<S>, 1) contract_mixed_kernel(const
         comp[2] = beta;
         comp[0] = dd_combine(alpha, beta, 1.0, 1.0, full);
         comp[3] = dd_combine(alpha, beta, -1.0, 1.0, full);
+    }
+    store_point(prm.spec, comp, start + point);
+}
+
+// ---------------------------------------------------------------------------
+// Bulk-copy form (P = 1, 4, 5; two AO stages): a tenth warp fetches the FP32
+// rows of each K step into shared memory with the tensor-memory-access unit
+// (one tiled copy per kept row of a 4-D map [block][panel][row][point] with a
+// box of one row's P panels; completion counted in bytes on the stage's
+// "loaded" mbarrier) F - 1 steps ahead of the split.  The eight producer warps read
+// the rows from shared memory, arrive on the stage's "read" mbarrier, split
+// them into the BF16 pieces and fetch the coefficient pieces as above; the
+// MMA warp is the same.  No FP32 row occupies registers while it is in
+// flight, so the bytes in flight per SM are set by F.  The eight threads of
+// a quarter-warp take eight different rows, point groups of four different
+// residues mod 4 and both halves of the 32-byte group in turn, so their
+// shared-memory reads and stores each fall in eight different bank groups.
+constexpr int kBulkThreads = kThreads + 64;  // producers, MMA warp, loader warp
+constexpr unsigned kBulkRowBytes = kBlockPoints * 4u;  // one panel row
+
+template <int P>
+struct BulkSmem {
+    static constexpr int Q = NQm<P>::v;
+    static constexpr unsigned a_bytes = 3u * P * kATile;
+    static constexpr unsigned f_slot = P * kBulkRowBytes;  // one K row's P panel rows (a copy's box)
+    static constexpr unsigned f_bytes = 16u * f_slot;
+    static_assert(sizeof(double) * Q * 128 <= 2u * a_bytes, "cross-warp sums must fit in the AO stages");
+    __host__ __device__ static unsigned b_bytes(int ncols) { return 3u * 32u * static_cast<unsigned>(ncols); }
+    __host__ __device__ static unsigned cap16(int rows) { return (static_cast<unsigned>(rows) + 15u) & ~15u; }
+    static size_t total(int ncols, int F, int SB, int rows) {
+        return 2 * static_cast<size_t>(a_bytes) + F * static_cast<size_t>(f_bytes) +
+               SB * static_cast<size_t>(b_bytes(ncols)) + 4u * cap16(rows) + 8u * (4 + 2 * F) + 16;
+    }
+    // Row indices held as 16-bit values; the sort keys share the AO stages.
+    static bool rows_fit(int rows) {
+        return rows <= 65535 && sizeof(int) * (kBuckets + 4) + cap16(rows) <= 2u * a_bytes;
+    }
+};
+
+template <int P, int F, int SB>
+__global__ void __launch_bounds__(kBulkThreads, 1)
+    contract_bulk_kernel(const __grid_constant__ ContractMixedParams prm, const __grid_constant__ CUtensorMap rows) {
+    using L = BulkSmem<P>;
+    constexpr int Q = L::Q;
+    constexpr int S = 2;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int N = prm.ncols;
+    const unsigned b_bytes = L::b_bytes(N);
+    const AoScratch<float>& scr = prm.scr;
+    const unsigned cap = L::cap16(scr.row_stride);
+    unsigned char* a_st = sm;
+    unsigned char* f_st = sm + 2 * L::a_bytes;
+    unsigned char* b_st = f_st + F * L::f_bytes;
+    // The AO stages double as the sort scratch (prologue) and the cross-warp
+    // sums (between passes, when no MMA reads them).
+    double* red = reinterpret_cast<double*>(sm);
+    int* bucket_start = reinterpret_cast<int*>(sm);
+    unsigned char* keys = sm + sizeof(int) * (kBuckets + 4);
+    std::uint16_t* perm = reinterpret_cast<std::uint16_t*>(b_st + SB * b_bytes);
+    std::uint16_t* aoidx = perm + cap;
+    unsigned long long* a_empty = reinterpret_cast<unsigned long long*>(aoidx + cap);  // MMAs of the stage done
+    unsigned long long* a_full = a_empty + S;                                          // stage's pieces written
+    unsigned long long* f_full = a_full + S;                                           // stage's rows landed
+    unsigned long long* f_empty = f_full + F;                                          // stage's rows read
+    unsigned* tslot = reinterpret_cast<unsigned*>(f_empty + F);
+
+    const int blk = blockIdx.x;
+    const long long start = prm.first_point + static_cast<long long>(blk) * prm.block_size;
+    long long bcount = prm.count - start;
+    if (bcount > prm.block_size) bcount = prm.block_size;
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    int nk = scr.nkept[blk];
+    const int* kept = scr.kept + static_cast<size_t>(blk) * scr.row_stride;
+    const bool producer = tid < kThreads;
+    const bool mma_warp = w == kThreads / 32;
+    const bool loader = w == kThreads / 32 + 1;
+
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&a_empty[s], 1);
+            mbar_init(&a_full[s], kThreads);
+        }
+        for (int u = 0; u < F; ++u) {
+            mbar_init(&f_full[u], 1);
+            mbar_init(&f_empty[u], kThreads);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (w == 0) tmem_alloc(tslot, static_cast<unsigned>(prm.tmem_cols));
+    bool sorted = false;
+    nk = block_row_order(scr.rowmax ? scr.rowmax + static_cast<size_t>(blk) * scr.row_stride * 4 : nullptr, nk,
+                         prm.threshold, perm, bucket_start, keys, sorted, static_cast<int>(cap));
+    for (int k = tid; producer && k < nk; k += kThreads) aoidx[k] = static_cast<std::uint16_t>(kept[sorted ? perm[k] : k]);
+    const int ntiles = (nk + 15) / 16;
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = *tslot;
+    const int G = prm.groups;
+    const unsigned gcols = static_cast<unsigned>(P * N);
+
+    // This thread's A unit: AO row kh*8 + k8 of each K step, points 8g..8g+7,
+    // read half hf first.
+    const int k8 = tid & 7, jq = (tid >> 3) & 15, kh = (tid >> 7) & 1;
+    const int g = 4 * (jq >> 2) + ((k8 + jq) & 3);
+    const int hf = (k8 >> 2) & 1;
+    const unsigned a_off = static_cast<unsigned>(g * 128 + kh * 2048 + k8 * 16);
+    const unsigned f_off = static_cast<unsigned>((kh * 8 + k8) * L::f_slot + g * 32 + hf * 16);
+    const unsigned idesc = instr_desc(N);
+    const unsigned long long a_desc0 = smem_desc(smem_u32(a_st), 2048u, 128u);
+    const unsigned long long b_desc0 = smem_desc(smem_u32(b_st), static_cast<unsigned>(N * 16), 128u);
+    const unsigned nb8 = static_cast<unsigned>(N / 8);
+    const unsigned nb8_mul = (65536u + nb8 - 1u) / nb8;
+    const int quarter = w & 3, half = w >> 2;
+    const int point = quarter * 32 + lane;
+
+    bool failed = false;
+    long long gtile = 0;  // K steps of this thread's role so far (all passes)
+    DevDD chan_dd[2];
+    dd_zero(chan_dd[0]);
+    dd_zero(chan_dd[1]);
+
+    for (int ci = 0; ci < prm.nchannels && !failed; ++ci) {
+        const MoChannelTC ch = prm.ch[ci];
+        double q[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) q[i] = 0.0;
+        for (int n0 = 0; n0 < ch.nocc && !failed; n0 += N) {
+            auto load_b = [&](int t, int stage) {
+                const unsigned bst = smem_u32(b_st + stage * b_bytes);
+                const int nchunk = 3 * 16 * (N / 8);
+                for (int v = tid; v < nchunk; v += kThreads) {
+                    const int r8 = v & 7;
+                    const unsigned rest = static_cast<unsigned>(v) >> 3;
+                    const unsigned rest2 = (rest * nb8_mul) >> 16;
+                    const int ng = static_cast<int>(rest - rest2 * nb8);
+                    const int rh = static_cast<int>(rest2 & 1u), piece = static_cast<int>(rest2 >> 1);
+                    const int k = t * 16 + rh * 8 + r8;
+                    const int col = n0 + ng * 8;
+                    const bool ok = k < nk && col < ch.ldn;
+                    const int ao = ok ? static_cast<int>(aoidx[k]) : 0;
+                    const std::uint16_t* src =
+                        ch.cs + (ok ? piece * ch.piece_stride + static_cast<long long>(ao) * ch.ldn + col : 0);
+                    cp_async16(bst + static_cast<unsigned>(piece * 32 * N + ng * 128 + rh * (N * 16) + r8 * 16), src,
+                               ok);
+                }
+                asm volatile("cp.async.commit_group;" ::: "memory");
+            };
+            const unsigned bpiece = (32u * static_cast<unsigned>(N)) >> 4;
+            constexpr int pi[6] = {1, 0, 2, 0, 1, 0}, pj[6] = {1, 2, 0, 1, 0, 0};
+            auto issue_panel = [&](int t, int s, int sb, int c) {
+                const unsigned long long as = a_desc0 + ((static_cast<unsigned>(s) * L::a_bytes) >> 4);
+                const unsigned long long bs = b_desc0 + ((static_cast<unsigned>(sb) * b_bytes) >> 4);
+                const unsigned dg = tmem + static_cast<unsigned>(t % G) * gcols;
+#pragma unroll
+                for (int e = 0; e < 6; ++e) {
+                    const unsigned long long ad = as + static_cast<unsigned>(((pi[e] * P + c) * kATile) >> 4);
+                    const unsigned long long bd = bs + static_cast<unsigned>(pj[e]) * bpiece;
+                    tc_mma(dg + static_cast<unsigned>(c * N), ad, bd, idesc, (t >= G || e > 0) ? 1u : 0u);
+                }
+            };
+            if (mma_warp) {
+                for (int t = 0; t < ntiles; ++t, ++gtile) {
+                    const int s = static_cast<int>(gtile % S);
+                    const int sb = static_cast<int>(gtile % SB);
+                    bool ok = true;
+                    if (lane == 0) {
+                        ok = mbar_wait(&a_full[s], static_cast<unsigned>((gtile / S) & 1));
+                        if (ok) {
+                            tc_fence_after();
+#pragma unroll
+                            for (int c = 0; c < P; ++c) issue_panel(t, s, sb, c);
+                            tc_commit(&a_empty[s]);
+                        }
+                    }
+                    if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) {
+                        failed = true;  // gtile = commits issued
+                        break;
+                    }
+                }
+            } else if (loader) {
+                for (int t = 0; t < ntiles; ++t, ++gtile) {
+                    const int u = static_cast<int>(gtile % F);
+                    const int nv = nk - t * 16 < 16 ? nk - t * 16 : 16;
+                    bool ok = true;
+                    if (lane == 0) {
+                        // The stage's previous rows (step gtile - F) have been read.
+                        const long long prev = gtile - F;
+                        if (prev >= 0) ok = mbar_wait(&f_empty[u], static_cast<unsigned>((prev / F) & 1));
+                        if (ok) mbar_arrive_expect_tx(&f_full[u], static_cast<unsigned>(nv * P) * (kBlockPoints * 4u));
+                    }
+                    if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) {
+                        failed = true;  // gtile = stages issued
+                        break;
+                    }
+                    if (lane < nv) {
+                        const int k = t * 16 + lane;
+                        const int row = sorted ? static_cast<int>(perm[k]) : k;
+                        tma_load_4d(smem_u32(f_st + u * L::f_bytes + lane * L::f_slot), &rows, 0, row, 0, blk, &f_full[u]);
+                    }
+                }
+            } else {
+                if (ntiles > 0) {
+                    load_b(0, static_cast<int>(gtile % SB));
+                    if (SB > 2 && ntiles > 1) load_b(1, static_cast<int>((gtile + 1) % SB));
+                }
+                for (int t = 0; t < ntiles; ++t, ++gtile) {
+                    const int s = static_cast<int>(gtile % S);
+                    const int u = static_cast<int>(gtile % F);
+                    // Stage s was released (MMAs of step gtile - S) at the end of
+                    // the previous step; wait for this step's rows.
+                    if (!mbar_wait(&f_full[u], static_cast<unsigned>((gtile / F) & 1))) {
+                        failed = true;
+                        break;
+                    }
+                    const int k = t * 16 + kh * 8 + k8;
+                    float4 ra[P][2];
+                    if (k < nk) {
+                        const unsigned char* fs = f_st + u * L::f_bytes;
+#pragma unroll
+                        for (int c = 0; c < P; ++c) {
+                            const float4 x0 = *reinterpret_cast<const float4*>(fs + c * kBulkRowBytes + f_off);
+                            const float4 x1 = *reinterpret_cast<const float4*>(fs + c * kBulkRowBytes + (f_off ^ 16u));
+                            ra[c][0] = hf ? x1 : x0;
+                            ra[c][1] = hf ? x0 : x1;
+                        }
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < P; ++c) ra[c][0] = ra[c][1] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+                    mbar_arrive(&f_empty[u]);
+                    unsigned char* ast = a_st + s * L::a_bytes;
+#pragma unroll
+                    for (int c = 0; c < P; ++c) {
+                        uint4 p0, p1, p2;
+                        split8(ra[c][0], ra[c][1], p0, p1, p2);
+                        *reinterpret_cast<uint4*>(ast + (0 * P + c) * kATile + a_off) = p0;
+                        *reinterpret_cast<uint4*>(ast + (1 * P + c) * kATile + a_off) = p1;
+                        *reinterpret_cast<uint4*>(ast + (2 * P + c) * kATile + a_off) = p2;
+                    }
+                    // Coefficient pieces of this step: the groups committed after
+                    // it (at most SB - 2) may stay in flight.
+                    if (SB > 2 && t + 1 < ntiles)
+                        asm volatile("cp.async.wait_group 1;" ::: "memory");
+                    else
+                        asm volatile("cp.async.wait_group 0;" ::: "memory");
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    mbar_arrive(&a_full[s]);
+                    if (t + 1 < ntiles) {
+                        // Step t+1's AO stage and step t+SB-1's coefficient stage
+                        // were last read by the MMAs of step gtile - 1.
+                        const long long wv = gtile + 1 - S;
+                        if (wv >= 0 && !mbar_wait(&a_empty[wv % S], static_cast<unsigned>((wv / S) & 1))) {
+                            failed = true;
+                            break;
+                        }
+                        if (t + SB - 1 < ntiles) load_b(t + SB - 1, static_cast<int>((gtile + SB - 1) % SB));
+                    }
+                }
+            }
+            if (ntiles == 0) continue;
+            // A role's timeout becomes every thread's before the pass ends.
+            if (__syncthreads_or(failed)) {
+                failed = true;
+                break;
+            }
+            const long long last = gtile - 1;
+            if (!mbar_wait(&a_empty[last % S], static_cast<unsigned>((last / S) & 1))) failed = true;
+            if (__syncthreads_or(failed)) {
+                failed = true;
+                break;
+            }
+            tc_fence_after();
+            const int nvalid = ch.nocc - n0 < N ? ch.nocc - n0 : N;
+            // Warps 8 and 9 (half 2) read no accumulators.
+            const int i_lo = half * (N / 2), i_hi = min(nvalid, (half + 1) * (N / 2));
+            const unsigned lane_addr = tmem + (static_cast<unsigned>(quarter * 32) << 16);
+            const int ng = ntiles < G ? ntiles : G;
+            constexpr int MG = 4;
+            for (int i0 = i_lo; i0 < i_hi; i0 += MG) {
+                double x[P][MG];
+#pragma unroll
+                for (int c = 0; c < P; ++c)
+#pragma unroll
+                    for (int u = 0; u < MG; ++u) x[c][u] = 0.0;
+                for (int gi = 0; gi < ng; ++gi) {
+                    unsigned v[P][MG];
+#pragma unroll
+                    for (int c = 0; c < P; ++c)
+                        tmem_ld<MG>(lane_addr + static_cast<unsigned>(gi) * gcols + static_cast<unsigned>(c * N + i0), v[c]);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int c = 0; c < P; ++c) {
+                        reg_fence<MG>(v[c]);
+#pragma unroll
+                        for (int u = 0; u < MG; ++u) x[c][u] += static_cast<double>(__uint_as_float(v[c][u]));
+                    }
+                }
+                fold<P, MG>(x, q, i_hi - i0);
+            }
+            tc_fence_before();
+            __syncthreads();
+        }
+        if (failed) break;
+        if (half == 1)
+#pragma unroll
+            for (int i = 0; i < Q; ++i) red[i * 128 + point] = q[i];
+        __syncthreads();
+        if (half == 0) {
+#pragma unroll
+            for (int i = 0; i < Q; ++i) q[i] += red[i * 128 + point];
+            record<P>(q, prm.ao_order, ch.role == 1 ? chan_dd[0] : chan_dd[1]);
+        }
+        __syncthreads();
+    }
+
+    if (failed) {
+        if (producer) asm volatile("cp.async.wait_group 0;" ::: "memory");  // no copy in flight at exit
+        if (tid == 0) atomicOr(prm.status, 1u);
+        // The MMA warp waits for the MMAs it issued and the loader for the rows
+        // it requested (bounded), before tensor memory is freed and the CTA exits.
+        if ((mma_warp || loader) && lane == 0) {
+            const int n = mma_warp ? S : F;
+            unsigned long long* b = mma_warp ? a_empty : f_full;
+            for (int s = 0; s < n; ++s) {
+                const long long lastu = gtile - 1 - ((gtile - 1 - s) % n + n) % n;
+                if (lastu >= 0) (void)mbar_wait(&b[lastu % n], static_cast<unsigned>((lastu / n) & 1));
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (w == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, static_cast<unsigned>(prm.tmem_cols));
+    }
+    if (half != 0 || point >= bcount) return;
+    DevDD comp[4];
+    if (failed) {
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        DevDD d;
+        d.value = d.lap = d.tau = nan;
+        for (int i = 0; i < 3; ++i) d.grad[i] = d.tau_axes[i] = nan;
+        for (int i = 0; i < 6; ++i) d.hess[i] = nan;
+        comp[0] = comp[1] = comp[2] = comp[3] = d;
+    } else {
+        DevDD alpha = chan_dd[0], beta = chan_dd[1];
+        if (prm.beta_is_alpha) beta = alpha;
+        comp[1] = alpha;
+        comp[2] = beta;
+        comp[0] = dd_combine(alpha, beta, 1.0, 1.0, false);
+        comp[3] = dd_combine(alpha, beta, -1.0, 1.0, false);
     }
     store_point(prm.spec, comp, start + point);
 }
@@ -884,6 +1240,61 @@ void fused_maxl(const ContractFusedParams& p, cudaStream_t stream) {
         launch_fused<P, 2, 4>(p, stream);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (null if
+// the driver does not provide it).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }();
+    return fn;
+}
+
+// 4-D map of the FP32 panels of a wave, [block][panel][row][point], with a
+// box of one row's npanel panel rows.
+bool panel_row_map(const ContractMixedParams& p, int npanel, CUtensorMap& map) {
+    const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (encode == nullptr || reinterpret_cast<std::uintptr_t>(p.scr.panels) % 16 != 0) return false;
+    const cuuint64_t row = kBlockPoints * sizeof(float);
+    const cuuint64_t dims[4] = {static_cast<cuuint64_t>(kBlockPoints), static_cast<cuuint64_t>(p.scr.row_stride),
+                                static_cast<cuuint64_t>(npanel), static_cast<cuuint64_t>(p.nblocks)};
+    const cuuint64_t strides[3] = {row, row * p.scr.row_stride, row * p.scr.row_stride * npanel};
+    const cuuint32_t box[4] = {static_cast<cuuint32_t>(kBlockPoints), 1u, static_cast<cuuint32_t>(npanel), 1u};
+    const cuuint32_t estride[4] = {1u, 1u, 1u, 1u};
+    return encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(p.scr.panels), dims, strides, box,
+                  estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int P, int F, int SB>
+bool launch_bulk(const ContractMixedParams& p, cudaStream_t stream) {
+    constexpr size_t kMaxSmem = 227u * 1024u;
+    if (!BulkSmem<P>::rows_fit(p.scr.row_stride) || BulkSmem<P>::total(p.ncols, F, SB, p.scr.row_stride) > kMaxSmem)
+        return false;
+    CUtensorMap map;
+    if (!panel_row_map(p, P, map)) return false;
+    ensure_dynamic_smem(reinterpret_cast<const void*>(contract_bulk_kernel<P, F, SB>), static_cast<int>(kMaxSmem));
+    contract_bulk_kernel<P, F, SB><<<p.nblocks, kBulkThreads, kMaxSmem, stream>>>(p, map);
+    return true;
+}
+
+// The bulk-copy form where its stages fit (KUMO_MIXED_BULK=0 selects the
+// register-staged form, for comparison).
+template <int P>
+bool try_bulk(const ContractMixedParams& p, cudaStream_t stream) {
+    const char* e = std::getenv("KUMO_MIXED_BULK");
+    if (e != nullptr && e[0] == '0') return false;
+    if constexpr (P == 1) {
+        return launch_bulk<1, 4, 3>(p, stream) || launch_bulk<1, 2, 2>(p, stream);
+    } else {
+        return launch_bulk<P, 2, 3>(p, stream) || launch_bulk<P, 2, 2>(p, stream);
+    }
+}
+
 template <int P, int S>
 void launch(const ContractMixedParams& p, cudaStream_t stream) {
     // The whole 227 KB of shared memory per CTA: one CTA per SM, so each CTA's
@@ -951,9 +1362,9 @@ void launch_contract_mixed(const ContractMixedParams& p, int npanel, cudaStream_
         p.groups * npanel * p.ncols > 512 || p.tmem_cols > 512)
         throw std::invalid_argument("tensor-core contraction: unsupported MO column count");
     switch (npanel) {
-        case 1: launch<1, 2>(p, stream); break;
-        case 4: launch<4, 2>(p, stream); break;
-        case 5: launch<5, 2>(p, stream); break;
+        case 1: if (!try_bulk<1>(p, stream)) launch<1, 2>(p, stream); break;
+        case 4: if (!try_bulk<4>(p, stream)) launch<4, 2>(p, stream); break;
+        case 5: if (!try_bulk<5>(p, stream)) launch<5, 2>(p, stream); break;
         case 10: launch<10, 1>(p, stream); break;
         default: throw std::invalid_argument("tensor-core contraction: unsupported panel count");
     }

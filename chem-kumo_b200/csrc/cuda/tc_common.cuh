@@ -120,6 +120,23 @@ __device__ __forceinline__ void reg_fence(unsigned (&r)[MG]) {
         asm volatile("" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]));
 }
 
+// One arrival that also expects `bytes` of asynchronous copies on the phase.
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// Tiled tensor copy global -> shared of the box at (x, y, z, w) of a 4-D
+// tensor map (a __grid_constant__ parameter); x * element size must be a
+// multiple of 16 bytes and the shared address 128-byte aligned.
+__device__ __forceinline__ void tma_load_4d(unsigned saddr, const void* map, int x, int y, int z, int w,
+                                            unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(saddr),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(bar))
+        : "memory");
+}
+
 __device__ __forceinline__ void cp_async16(unsigned saddr, const void* gmem, bool valid) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(saddr), "l"(gmem), "r"(valid ? 16 : 0)
                  : "memory");
@@ -158,10 +175,12 @@ constexpr int kBuckets = 128;
 // rowmax4 holds the four per-warp maxima of each row (null: keep all rows in
 // AO order).  On return perm[0..nk) lists the kept rows (block maximum above
 // the threshold; threshold 0 keeps every row) and `sorted` says whether perm
-// is in use; keys and bucket_start are shared scratch of kSortCap bytes and
-// kBuckets + 4 ints.
-__device__ __forceinline__ int block_row_order(const float* rowmax4, int nk, float threshold, int* perm,
-                                               int* bucket_start, unsigned char* keys, bool& sorted) {
+// is in use (blocks of at most `cap` rows); keys and bucket_start are shared
+// scratch of cap bytes and kBuckets + 4 ints.
+template <typename PermT>
+__device__ __forceinline__ int block_row_order(const float* rowmax4, int nk, float threshold, PermT* perm,
+                                               int* bucket_start, unsigned char* keys, bool& sorted,
+                                               int cap = kSortCap) {
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     // K order: rows in ascending order of their block maximum (a stable
     // counting sort on the FP32 exponent), so that the accumulators are small
@@ -171,7 +190,7 @@ __device__ __forceinline__ int block_row_order(const float* rowmax4, int nk, flo
     // Rows whose block maximum is not above the screening threshold are left
     // out here (src/ao_screening.hpp:35-50 on the FP32 panels; threshold 0
     // keeps every row).
-    sorted = rowmax4 != nullptr && nk <= kSortCap;
+    sorted = rowmax4 != nullptr && nk <= cap;
     if (sorted) {
         const float4* rmax = reinterpret_cast<const float4*>(rowmax4);
         // Threads beyond kThreads (a CTA's MMA warp) only meet the barriers.
@@ -218,7 +237,7 @@ __device__ __forceinline__ int block_row_order(const float* rowmax4, int nk, flo
                 const int start = key != 0xffu ? bucket_start[key] : 0;
                 __syncwarp();
                 if (key != 0xffu) {
-                    perm[start + rank] = k;
+                    perm[start + rank] = static_cast<PermT>(k);
                     if (rank == __popc(same) - 1) bucket_start[key] = start + rank + 1;
                 }
                 __syncwarp();

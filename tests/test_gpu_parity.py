@@ -552,6 +552,29 @@ def test_fused_mixed_form_matches_two_kernel_form():
         assert scaled_error(a, b) <= 1e-6, p
 
 
+@pytest.mark.parametrize("case", ["values", "gradient", "laplacian"])
+@pytest.mark.parametrize("name", ["o2.fchk.gz", "acrolein.fchk.gz"])
+def test_bulk_copy_contraction_equals_register_staged(name, case):
+    # The bulk-copy tensor-core contraction (rows fetched by cp.async.bulk
+    # into shared memory) and the register-staged one (KUMO_MIXED_BULK=0)
+    # split the same FP32 rows and issue the same MMAs in the same order: the
+    # results agree bit for bit, and both hold the mixed tolerance.
+    m, o = _pair(os.path.join(GOLDEN, name))
+    pts = _box_points(o.atom_xyz.reshape(-1, 3), 5000, 33)
+    comps = [D.Total, D.Alpha, D.Beta] if name == "o2.fchk.gz" else [D.Total]
+    props = [K.density(k, c) for k in MIXED_CASES[case] for c in comps]
+    bulk, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_points(pts, props)
+    os.environ["KUMO_MIXED_BULK"] = "0"
+    try:
+        staged, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_points(pts, props)
+    finally:
+        del os.environ["KUMO_MIXED_BULK"]
+    ref, _ = K.Evaluator(m).evaluate_points(pts, props)
+    for p, a, b, r in zip(props, bulk, staged, ref):
+        assert np.array_equal(a, b), p
+        assert scaled_error(a, r) <= (1e-5 if p.kind == P.Elf else 1e-6), p
+
+
 def test_sharded_grid_equals_whole_grid():
     # Two block ranges evaluated as points (as two ranks would) give the
     # one-call grid result bit for bit.
