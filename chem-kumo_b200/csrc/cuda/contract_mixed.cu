@@ -265,7 +265,6 @@ __global__ void __launch_bounds__(kCtaThreads<S>, 1) contract_mixed_kernel(const
                 if (ntiles > 1) load_b(1, static_cast<int>((gtile + 1) % SB));
             }
             const unsigned bpiece = (32u * static_cast<unsigned>(N)) >> 4;
-            constexpr int pi[6] = {1, 0, 2, 0, 1, 0}, pj[6] = {1, 2, 0, 1, 0, 0};
             // The six MMAs of panel c of K step t (stage s, coefficient stage sb).
             auto issue_panel = [&](int t, int s, int sb, int c) {
                 const unsigned long long as = a_desc0 + ((static_cast<unsigned>(s) * L::a_bytes) >> 4);
@@ -274,8 +273,8 @@ __global__ void __launch_bounds__(kCtaThreads<S>, 1) contract_mixed_kernel(const
                 const unsigned dg = tmem + static_cast<unsigned>(t % G) * gcols;
 #pragma unroll
                 for (int e = 0; e < 6; ++e) {
-                    const unsigned long long ad = as + static_cast<unsigned>(((pi[e] * P + c) * kATile) >> 4);
-                    const unsigned long long bd = bs + static_cast<unsigned>(pj[e]) * bpiece;
+                    const unsigned long long ad = as + static_cast<unsigned>(((piece_a(e) * P + c) * kATile) >> 4);
+                    const unsigned long long bd = bs + static_cast<unsigned>(piece_b(e)) * bpiece;
                     tc_mma(dg + static_cast<unsigned>(c * N), ad, bd, idesc, (t >= G || e > 0) ? 1u : 0u);
                 }
             };
@@ -597,15 +596,14 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                 asm volatile("cp.async.commit_group;" ::: "memory");
             };
             const unsigned bpiece = (32u * static_cast<unsigned>(N)) >> 4;
-            constexpr int pi[6] = {1, 0, 2, 0, 1, 0}, pj[6] = {1, 2, 0, 1, 0, 0};
             auto issue_panel = [&](int t, int s, int sb, int c) {
                 const unsigned long long as = a_desc0 + ((static_cast<unsigned>(s) * L::a_bytes) >> 4);
                 const unsigned long long bs = b_desc0 + ((static_cast<unsigned>(sb) * b_bytes) >> 4);
                 const unsigned dg = tmem + static_cast<unsigned>(t % G) * gcols;
 #pragma unroll
                 for (int e = 0; e < 6; ++e) {
-                    const unsigned long long ad = as + static_cast<unsigned>(((pi[e] * P + c) * kATile) >> 4);
-                    const unsigned long long bd = bs + static_cast<unsigned>(pj[e]) * bpiece;
+                    const unsigned long long ad = as + static_cast<unsigned>(((piece_a(e) * P + c) * kATile) >> 4);
+                    const unsigned long long bd = bs + static_cast<unsigned>(piece_b(e)) * bpiece;
                     tc_mma(dg + static_cast<unsigned>(c * N), ad, bd, idesc, (t >= G || e > 0) ? 1u : 0u);
                 }
             };
@@ -1120,12 +1118,11 @@ __global__ void __launch_bounds__(kThreads, 1) contract_fused_kernel(const __gri
                     const unsigned long long bs = b_desc0 + ((static_cast<unsigned>(sb) * b_bytes) >> 4);
                     const unsigned bpiece = (32u * static_cast<unsigned>(N)) >> 4;
                     const unsigned dg = tmem + static_cast<unsigned>(t % G) * gcols;
-                    constexpr int pi[6] = {1, 0, 2, 0, 1, 0}, pjx[6] = {1, 2, 0, 1, 0, 0};
                     for (int c = w; c < P; c += kIssuers<P>) {
 #pragma unroll
                         for (int e = 0; e < 6; ++e) {
-                            const unsigned long long ad = as + static_cast<unsigned>(((pi[e] * P + c) * kATile) >> 4);
-                            const unsigned long long bd = bs + static_cast<unsigned>(pjx[e]) * bpiece;
+                            const unsigned long long ad = as + static_cast<unsigned>(((piece_a(e) * P + c) * kATile) >> 4);
+                            const unsigned long long bd = bs + static_cast<unsigned>(piece_b(e)) * bpiece;
                             tc_mma(dg + static_cast<unsigned>(c * N), ad, bd, idesc, (t >= G || e > 0) ? 1u : 0u);
                         }
                     }

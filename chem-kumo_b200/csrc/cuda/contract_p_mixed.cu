@@ -211,13 +211,12 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
                     const unsigned long long as = a_desc0 + ((static_cast<unsigned>(s) * L::a_bytes) >> 4);
                     const unsigned long long bs = b_desc0 + ((static_cast<unsigned>(s) * L::b_bytes) >> 4);
                     constexpr unsigned bpiece = (32u * kCols) >> 4;
-                    constexpr int pi[6] = {1, 0, 2, 0, 1, 0}, pj[6] = {1, 2, 0, 1, 0, 0};
 #pragma unroll
                     for (int c = 0; c < kPL; ++c) {
 #pragma unroll
                         for (int e = 0; e < 6; ++e) {
-                            const unsigned long long ad = as + static_cast<unsigned>(((pi[e] * kPL + c) * kATile) >> 4);
-                            const unsigned long long bd = bs + static_cast<unsigned>(pj[e]) * bpiece;
+                            const unsigned long long ad = as + static_cast<unsigned>(((piece_a(e) * kPL + c) * kATile) >> 4);
+                            const unsigned long long bd = bs + static_cast<unsigned>(piece_b(e)) * bpiece;
                             tc_mma(tmem + static_cast<unsigned>(c * kCols), ad, bd, idesc, (t > 0 || e > 0) ? 1u : 0u);
                         }
                     }

@@ -9,6 +9,13 @@ namespace kumo_dev {
 namespace {
 
 constexpr int kThreads = 256;
+
+// The six BF16 products a_i b_j (i + j <= 2) of one FP32 product, in the
+// order they are accumulated: the terms of order 2^-16, then 2^-8, then
+// a_0 b_0, so that the small terms meet a small partial sum.
+// Pieces (a_i, b_j) of product e: (1,1) (0,2) (2,0) (0,1) (1,0) (0,0).
+__host__ __device__ constexpr int piece_a(int e) { return e == 0 || e == 4 ? 1 : (e == 2 ? 2 : 0); }
+__host__ __device__ constexpr int piece_b(int e) { return e == 1 ? 2 : (e == 0 || e == 3 ? 1 : 0); }
 constexpr unsigned kATile = 4096;            // 128 points x 16 rows x 2 B
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s per wait
 

@@ -555,10 +555,11 @@ def test_fused_mixed_form_matches_two_kernel_form():
 @pytest.mark.parametrize("case", ["values", "gradient", "laplacian"])
 @pytest.mark.parametrize("name", ["o2.fchk.gz", "acrolein.fchk.gz"])
 def test_bulk_copy_contraction_equals_register_staged(name, case):
-    # The bulk-copy tensor-core contraction (rows fetched by cp.async.bulk
-    # into shared memory) and the register-staged one (KUMO_MIXED_BULK=0)
-    # split the same FP32 rows and issue the same MMAs in the same order: the
-    # results agree bit for bit, and both hold the mixed tolerance.
+    # The bulk-copy tensor-core contraction (rows fetched by tensor copies
+    # into shared memory, the default) and the register-staged one
+    # (KUMO_MIXED_BULK=0) split the same FP32 rows and accumulate the same
+    # products in the same order: the results agree bit for bit, and both
+    # hold the mixed tolerance.
     m, o = _pair(os.path.join(GOLDEN, name))
     pts = _box_points(o.atom_xyz.reshape(-1, 3), 5000, 33)
     comps = [D.Total, D.Alpha, D.Beta] if name == "o2.fchk.gz" else [D.Total]
