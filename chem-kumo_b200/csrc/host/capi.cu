@@ -8,6 +8,8 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <array>
+#include <mutex>
 #include <vector>
 
 #include "../cuda/esp.cuh"
@@ -155,42 +157,99 @@ Request to_request(const kumo_property* props, int n) {
     return r;
 }
 
+// A non-blocking stream per device for result copies that overlap the
+// evaluation (it waits only on events of the evaluation's stream).
+cudaStream_t copy_stream() {
+    static std::mutex mu;
+    static std::array<cudaStream_t, 64> streams{};
+    int dev = 0;
+    detail::check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= static_cast<int>(streams.size())) throw std::runtime_error("device index out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!streams[static_cast<std::size_t>(dev)])
+        detail::check_cuda(cudaStreamCreateWithFlags(&streams[static_cast<std::size_t>(dev)], cudaStreamNonBlocking),
+                           "cudaStreamCreateWithFlags (copies)");
+    return streams[static_cast<std::size_t>(dev)];
+}
+
+bool page_locked(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 // Evaluation into the caller's host arrays: device outputs from the
-// stream-ordered pool, the device evaluation, then one device-to-host copy per
-// property straight into the caller's array (no intermediate host copies;
-// with page-locked caller arrays the copies run at full link speed).
+// stream-ordered pool, the device evaluation, and device-to-host copies
+// straight into the caller's arrays (no intermediate host copies).  When
+// every output is page-locked, each finished range of points (the
+// evaluator's ready callback, after each wave of blocks) is copied on a
+// separate stream while the next wave runs; otherwise all results are copied
+// at the end.
 template <typename Launch>
 Backend evaluate_to_host(const Request& req, std::size_t n, double* const* outputs, Precision precision,
                          Launch&& launch) {
     const auto& props = req.properties();
-    std::vector<std::size_t> count(props.size());
+    std::vector<std::size_t> chans(props.size());
     std::size_t total = 0;
+    bool locked = true;
     for (std::size_t i = 0; i < props.size(); ++i) {
-        count[i] = property_channels(props[i].kind) * n;
-        total += count[i];
+        chans[i] = property_channels(props[i].kind);
+        total += chans[i] * n;
+        locked = locked && (n == 0 || page_locked(outputs[i]));
     }
     void* dev = nullptr;
     if (total) detail::check_cuda(cudaMallocAsync(&dev, sizeof(double) * total, nullptr), "cudaMallocAsync (outputs)");
-    struct Free {
-        void* p;
-        ~Free() {
-            if (p) cudaFreeAsync(p, nullptr);
+    cudaStream_t cs = locked && total ? copy_stream() : nullptr;
+    cudaEvent_t ev = nullptr;
+    if (cs) detail::check_cuda(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreateWithFlags");
+    // Declared after `dev`: on every exit the copies end before the buffer is freed.
+    struct Release {
+        void* dev;
+        cudaStream_t cs;
+        cudaEvent_t ev;
+        ~Release() {
+            if (cs) cudaStreamSynchronize(cs);
+            if (ev) cudaEventDestroy(ev);
+            if (dev) cudaFreeAsync(dev, nullptr);
         }
-    } guard{dev};
+    } guard{dev, cs, ev};
     std::vector<double*> dptr(props.size());
     std::size_t off = 0;
     for (std::size_t i = 0; i < props.size(); ++i) {
         dptr[i] = static_cast<double*>(dev) + off;
-        off += count[i];
+        off += chans[i] * n;
     }
     if (total)
         detail::check_cuda(cudaMemsetAsync(dev, 0, sizeof(double) * total, nullptr), "cudaMemsetAsync (outputs)");
-    const Backend used = launch(dptr.data());
-    for (std::size_t i = 0; i < props.size(); ++i)
-        if (count[i])
-            detail::check_cuda(cudaMemcpyAsync(outputs[i], dptr[i], sizeof(double) * count[i], cudaMemcpyDeviceToHost,
-                                               nullptr),
-                               "cudaMemcpyAsync (results)");
+    std::size_t copied = 0;
+    // Points [copied, done) of every channel, on the copy stream once the
+    // evaluation's launches enqueued so far have run.
+    auto copy_range = [&](std::size_t done) {
+        if (!cs || done <= copied) return;
+        detail::check_cuda(cudaEventRecord(ev, nullptr), "cudaEventRecord");
+        detail::check_cuda(cudaStreamWaitEvent(cs, ev, 0), "cudaStreamWaitEvent");
+        for (std::size_t i = 0; i < props.size(); ++i)
+            for (std::size_t c = 0; c < chans[i]; ++c)
+                detail::check_cuda(cudaMemcpyAsync(outputs[i] + c * n + copied, dptr[i] + c * n + copied,
+                                                   sizeof(double) * (done - copied), cudaMemcpyDeviceToHost, cs),
+                                   "cudaMemcpyAsync (results)");
+        copied = done;
+    };
+    const Evaluator::ReadyCallback ready = [&](std::size_t done) { copy_range(done); };
+    const Backend used = launch(dptr.data(), cs ? ready : Evaluator::ReadyCallback{});
+    if (cs) {
+        copy_range(n);
+        detail::check_cuda(cudaStreamSynchronize(cs), "cudaStreamSynchronize (results)");
+    } else {
+        for (std::size_t i = 0; i < props.size(); ++i)
+            if (chans[i] * n)
+                detail::check_cuda(cudaMemcpyAsync(outputs[i], dptr[i], sizeof(double) * chans[i] * n,
+                                                   cudaMemcpyDeviceToHost, nullptr),
+                                   "cudaMemcpyAsync (results)");
+    }
     detail::check_cuda(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize (results)");
     if (precision == Precision::Mixed && kumo_dev::take_pipeline_status() != 0)
         throw std::runtime_error("mixed-precision contraction: a tensor-core pipeline wait timed out");
@@ -370,7 +429,9 @@ int kumo_evaluate_grid(const kumo_molecule* m, const kumo_options* opt, const ku
         ev.validate(req);
         if (!outputs && nprops > 0) throw std::invalid_argument("null outputs");
         const Backend b = evaluate_to_host(req, n, outputs, o.precision,
-                                           [&](double* const* d) { return ev.evaluate_device(g, req, d, nullptr); });
+                                           [&](double* const* d, const Evaluator::ReadyCallback& ready) {
+                                               return ev.evaluate_device(g, req, d, nullptr, ready);
+                                           });
         if (backend_used) *backend_used = static_cast<int>(b);
     });
 }
@@ -398,9 +459,10 @@ int kumo_evaluate_points(const kumo_molecule* m, const kumo_options* opt, const 
         if (n)
             detail::check_cuda(cudaMemcpyAsync(dpts, points, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, nullptr),
                                "cudaMemcpyAsync (points)");
-        const Backend b = evaluate_to_host(req, n, outputs, o.precision, [&](double* const* d) {
-            return ev.evaluate_device(Points{static_cast<const double*>(dpts), n}, req, d, nullptr);
-        });
+        const Backend b =
+            evaluate_to_host(req, n, outputs, o.precision, [&](double* const* d, const Evaluator::ReadyCallback& ready) {
+                return ev.evaluate_device(Points{static_cast<const double*>(dpts), n}, req, d, nullptr, ready);
+            });
         if (backend_used) *backend_used = static_cast<int>(b);
     });
 }

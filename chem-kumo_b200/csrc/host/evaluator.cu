@@ -181,8 +181,9 @@ public:
 
     Backend backend() const { return backend_; }
 
-    void execute(const std::vector<std::pair<Property, double*>>& outs) {
+    void execute(const std::vector<std::pair<Property, double*>>& outs, const ReadyCallback& ready = {}) {
         outs_ = outs;
+        ready_ = &ready;
         if (n_ == 0) return;
         keep_pool_memory();
         dev_ = &mol_.device();
@@ -229,6 +230,9 @@ public:
 
 private:
     void report(std::size_t done_in_pass) {
+        // With one pass, every output of points [0, done) is final once the
+        // launches enqueued so far have run.
+        if (ready_ && *ready_ && passes_ == 1) (*ready_)(std::min(n_, completed_ + done_in_pass));
         if (!opt_.progress) return;
         check_cuda(cudaStreamSynchronize(stream_), "cudaStreamSynchronize (progress)");
         opt_.progress(completed_ + done_in_pass, passes_ * n_);
@@ -781,6 +785,7 @@ private:
     kumo_dev::PointSource src_{};
     std::vector<std::pair<Property, double*>> outs_;
     std::size_t passes_ = 0, completed_ = 0;
+    const ReadyCallback* ready_ = nullptr;
     detail::OrbitalEnergyNeeds oe_needs_;
     std::string oe_what_;
 };
@@ -884,21 +889,22 @@ Results Evaluator::evaluate(Points points, const Request& request) const {
 
 void Evaluator::validate(const Request& request) const { Run run(*this, nullptr, nullptr, 0, request, nullptr); }
 
-Backend Evaluator::evaluate_device(const Grid& grid, const Request& request, double* const* outputs, void* stream) const {
+Backend Evaluator::evaluate_device(const Grid& grid, const Request& request, double* const* outputs, void* stream,
+                                   const ReadyCallback& ready) const {
     const std::size_t n = detail::validated_point_count(grid);
     Run run(*this, &grid, nullptr, n, request, static_cast<cudaStream_t>(stream));
     std::vector<std::pair<Property, double*>> outs;
     for (std::size_t i = 0; i < request.properties().size(); ++i) outs.emplace_back(request.properties()[i], outputs[i]);
-    run.execute(outs);
+    run.execute(outs, ready);
     return run.backend();
 }
 
-Backend Evaluator::evaluate_device(Points device_points, const Request& request, double* const* outputs,
-                                   void* stream) const {
+Backend Evaluator::evaluate_device(Points device_points, const Request& request, double* const* outputs, void* stream,
+                                   const ReadyCallback& ready) const {
     Run run(*this, nullptr, device_points.data, device_points.count, request, static_cast<cudaStream_t>(stream));
     std::vector<std::pair<Property, double*>> outs;
     for (std::size_t i = 0; i < request.properties().size(); ++i) outs.emplace_back(request.properties()[i], outputs[i]);
-    run.execute(outs);
+    run.execute(outs, ready);
     return run.backend();
 }
 

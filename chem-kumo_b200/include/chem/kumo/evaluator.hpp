@@ -5,6 +5,7 @@
 #include "chem/kumo/density.hpp"
 
 #include <cstddef>
+#include <functional>
 #include <map>
 #include <span>
 #include <vector>
@@ -196,17 +197,24 @@ public:
     [[nodiscard]] Results evaluate(Points points, const Request& request) const;
     [[nodiscard]] Field field(const Grid& grid, Property property) const;
 
+    /// Called by evaluate_device, without synchronizing, each time the work
+    /// that completes points [0, done) of every output has been enqueued on
+    /// the stream (one pass over the points writes all outputs; requests that
+    /// need several passes report only the end).
+    using ReadyCallback = std::function<void(std::size_t done)>;
+
     /// Device-resident form: outputs[i] points to property_channels(kind) x N
     /// device doubles (component-major) for the i-th property of `request`,
     /// written on `stream` (a cudaStream_t); returns the backend used.  The
     /// points of evaluate_device(Points) are a device array.
-    Backend evaluate_device(const Grid& grid, const Request& request, double* const* outputs, void* stream) const;
+    Backend evaluate_device(const Grid& grid, const Request& request, double* const* outputs, void* stream,
+                            const ReadyCallback& ready = {}) const;
     /// The request checks evaluate() makes before any device work (backend
     /// eligibility, orbital indices, block size, potential tolerance); throws
     /// the same exceptions.
     void validate(const Request& request) const;
-    Backend evaluate_device(Points device_points, const Request& request, double* const* outputs,
-                            void* stream) const;
+    Backend evaluate_device(Points device_points, const Request& request, double* const* outputs, void* stream,
+                            const ReadyCallback& ready = {}) const;
 
 private:
     class Run;

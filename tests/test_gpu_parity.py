@@ -479,6 +479,42 @@ def test_mixed_tensor_core_several_mo_passes(synth_cache):
         assert scaled_error(a, r) <= 1e-6, (p, scaled_error(a, r))
 
 
+@pytest.mark.parametrize("precision", ["Mixed", "FP64"])
+def test_streamed_result_copies_match(precision):
+    # Page-locked outputs: each wave's finished points are copied while the
+    # next wave runs (a small scratch budget forces many waves).  The values
+    # equal those of pageable outputs (copied once at the end), for a
+    # one-pass request and for a request with a second (ESP) pass.
+    import torch
+    m = K.Molecule.from_fchk(os.path.join(GOLDEN, "acrolein.fchk.gz"))
+    grid = m.grid_around(2.0, 0.3)
+    prec = getattr(K.Precision, precision)
+    for props in ([K.density(P.Density), K.density(P.Gradient), K.density(P.Tau), K.density(P.Elf)],
+                  [K.density(P.Density), K.density(P.ElectrostaticPotential)]):
+        os.environ["KUMO_SCRATCH_MB"] = "8"
+        try:
+            ev = K.Evaluator(m, precision=prec)
+            paged, _ = ev.evaluate_grid(grid, props)
+            pinned = [torch.empty((K.channels(p.kind), grid.npoints), dtype=torch.float64, pin_memory=True).numpy()
+                      for p in props]
+            for o in pinned:
+                o.fill(np.nan)
+            ev.evaluate_grid(grid, props, out=pinned)
+            pts = grid.points()[::3]
+            ppts = [torch.empty((K.channels(p.kind), len(pts)), dtype=torch.float64, pin_memory=True).numpy()
+                    for p in props]
+            ev.evaluate_points(pts, props, out=ppts)
+            ref_pts, _ = ev.evaluate_points(pts, props)
+        finally:
+            del os.environ["KUMO_SCRATCH_MB"]
+        whole, _ = K.Evaluator(m, precision=prec).evaluate_grid(grid, props)
+        for a, b, c in zip(paged, pinned, whole):
+            assert np.array_equal(a, b)
+            assert np.array_equal(a, c)
+        for a, b in zip(ppts, ref_pts):
+            assert np.array_equal(a, b)
+
+
 def test_host_api_writes_into_caller_arrays():
     # Host-output calls copy each property from the device straight into the
     # caller's arrays; page-locked arrays reused across calls give the same
