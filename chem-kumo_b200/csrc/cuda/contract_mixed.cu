@@ -664,11 +664,13 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                     const int k = t * 16 + kh * 8 + k8;
                     float4 ra[P][2];
                     if (k < nk) {
-                        const unsigned char* fs = f_st + u * L::f_bytes;
+                        const unsigned fs = smem_u32(f_st + u * L::f_bytes);
 #pragma unroll
                         for (int c = 0; c < P; ++c) {
-                            const float4 x0 = *reinterpret_cast<const float4*>(fs + c * kBulkRowBytes + f_off);
-                            const float4 x1 = *reinterpret_cast<const float4*>(fs + c * kBulkRowBytes + (f_off ^ 16u));
+                            // Half hf first: the quarter-warp's two loads each touch
+                            // eight different bank groups.
+                            const float4 x0 = lds128(fs + c * kBulkRowBytes + f_off);
+                            const float4 x1 = lds128(fs + c * kBulkRowBytes + (f_off ^ 16u));
                             ra[c][0] = hf ? x1 : x0;
                             ra[c][1] = hf ? x0 : x1;
                         }

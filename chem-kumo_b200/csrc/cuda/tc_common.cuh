@@ -45,16 +45,34 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
     return ok != 0;
 }
 
-// Waits until the phase with the given parity has completed; false if that
-// did not happen within kWaitNs.
+// As mbar_try_wait, but the thread may be suspended until the phase
+// completes or about `hint_ns` nanoseconds pass, instead of returning at once
+// (a waiting warp then does not poll the barrier through the shared-memory
+// port).
+__device__ __forceinline__ bool mbar_try_wait_suspend(unsigned long long* bar, unsigned parity, unsigned hint_ns) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
 // One arrival (release semantics) on an mbarrier, without waiting.
 __device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
     asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
+
+// Waits until the phase with the given parity has completed; false if that
+// did not happen within kWaitNs.
+constexpr unsigned kSuspendNs = 20000;
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
-    while (!mbar_try_wait(bar, parity))
+    while (!mbar_try_wait_suspend(bar, parity, kSuspendNs))
         if (global_ns() - t0 > kWaitNs) return false;
     return true;
 }
@@ -142,6 +160,15 @@ __device__ __forceinline__ void tma_load_4d(unsigned saddr, const void* map, int
         "[%6];" ::"r"(saddr),
         "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(bar))
         : "memory");
+}
+
+// 16-byte shared-memory load at a fixed address (the compiler may not fold a
+// later select of the result into the address, which would change the banks
+// the warp's lanes touch).
+__device__ __forceinline__ float4 lds128(unsigned saddr) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(saddr) : "memory");
+    return v;
 }
 
 __device__ __forceinline__ void cp_async16(unsigned saddr, const void* gmem, bool valid) {
