@@ -264,6 +264,24 @@ def esp_bench(K, synth, fchk_dir: str, oracle_pts: int = 32):
     sout = torch.empty(len(surf), dtype=torch.float64, device="cuda")
     ms_surf = timed(lambda: ev.evaluate_points_device(dpts.data_ptr(), len(surf), [esp], [sout.data_ptr()],
                                                       stream.cuda_stream))
+    # Mixed form (FP64 Boys values and nuclear term, FP32 Hermite recursion
+    # and compensated pair sums) on the same cube and surface, against FP64.
+    evm = K.Evaluator(m, precision=K.Precision.Mixed)
+    outm = torch.empty_like(out)
+    soutm = torch.empty_like(sout)
+    evm.evaluate_grid_device(K.Grid(origin, steps, (8, 8, 8)), [esp], [outm.data_ptr()], stream.cuda_stream)
+    ms_cube_m = timed(lambda: evm.evaluate_grid_device(grid, [esp], [outm.data_ptr()], stream.cuda_stream))
+    ms_surf_m = timed(lambda: evm.evaluate_points_device(dpts.data_ptr(), len(surf), [esp], [soutm.data_ptr()],
+                                                         stream.cuda_stream))
+
+    def scaled(a, r):
+        return float((a - r).abs().max() / max(1.0, float(r.abs().max())))
+
+    mixed = {"cube_ms": ms_cube_m, "cube_pair_points_per_s": n * pairs / (ms_cube_m * 1e-3),
+             "surface_ms": ms_surf_m, "surface_pair_points_per_s": len(surf) * pairs / (ms_surf_m * 1e-3),
+             "speedup_vs_fp64_cube": ms_cube / ms_cube_m, "speedup_vs_fp64_surface": ms_surf / ms_surf_m,
+             "scaled_err_vs_fp64_cube": scaled(outm, out), "scaled_err_vs_fp64_surface": scaled(soutm, sout),
+             "max_rel_err_vs_fp64_surface": float(((soutm - sout).abs() / sout.abs().clamp_min(1e-300)).max())}
     # Accuracy on a sample against the CPU oracle, and the oracle's own rate.
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
@@ -282,6 +300,7 @@ def esp_bench(K, synth, fchk_dir: str, oracle_pts: int = 32):
                         "build_s": surface_build_s, "ms": ms_surf,
                         "pair_points_per_s": len(surf) * pairs / (ms_surf * 1e-3)},
             "scaled_err_vs_oracle": float(np.max(np.abs(got - ref)) / max(1.0, float(np.max(np.abs(ref))))),
+            "mixed": mixed,
             "cpu_oracle": {"pair_points_per_s": oracle_pts * pairs / cpu_s, "cores": O.lib().ko_max_threads(),
                            "sample": f"{oracle_pts} surface points, {cpu_s:.1f} s"}}
 

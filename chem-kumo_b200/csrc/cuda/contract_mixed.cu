@@ -540,7 +540,13 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
     nk = block_row_order(scr.rowmax ? scr.rowmax + static_cast<size_t>(blk) * scr.row_stride * 4 : nullptr, nk,
                          prm.threshold, perm, bucket_start, keys, sorted, static_cast<int>(cap));
     for (int k = tid; producer && k < nk; k += kThreads) aoidx[k] = static_cast<std::uint16_t>(kept[sorted ? perm[k] : k]);
-    const int ntiles = (nk + 15) / 16;
+    // The last nx rows of the K order (the largest block maxima) are added in
+    // FP64 in the epilogue instead of on the tensor cores: the truncation of
+    // each MMA's FP32 sum is relative to its largest product, so taking the
+    // largest products out of the MMAs lowers the error of every output.
+    const int nx = prm.exact_rows < nk ? prm.exact_rows : nk;
+    const int nkt = nk - nx;
+    const int ntiles = (nkt + 15) / 16;
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -586,7 +592,7 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                     const int rh = static_cast<int>(rest2 & 1u), piece = static_cast<int>(rest2 >> 1);
                     const int k = t * 16 + rh * 8 + r8;
                     const int col = n0 + ng * 8;
-                    const bool ok = k < nk && col < ch.ldn;
+                    const bool ok = k < nkt && col < ch.ldn;
                     const int ao = ok ? static_cast<int>(aoidx[k]) : 0;
                     const std::uint16_t* src =
                         ch.cs + (ok ? piece * ch.piece_stride + static_cast<long long>(ao) * ch.ldn + col : 0);
@@ -629,7 +635,7 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
             } else if (loader) {
                 for (int t = 0; t < ntiles; ++t, ++gtile) {
                     const int u = static_cast<int>(gtile % F);
-                    const int nv = nk - t * 16 < 16 ? nk - t * 16 : 16;
+                    const int nv = nkt - t * 16 < 16 ? nkt - t * 16 : 16;
                     bool ok = true;
                     if (lane == 0) {
                         // The stage's previous rows (step gtile - F) have been read.
@@ -663,7 +669,7 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                     }
                     const int k = t * 16 + kh * 8 + k8;
                     float4 ra[P][2];
-                    if (k < nk) {
+                    if (k < nkt) {
                         const unsigned fs = smem_u32(f_st + u * L::f_bytes);
 #pragma unroll
                         for (int c = 0; c < P; ++c) {
@@ -708,14 +714,14 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                     }
                 }
             }
-            if (ntiles == 0) continue;
+            if (ntiles == 0 && nx == 0) continue;
             // A role's timeout becomes every thread's before the pass ends.
             if (__syncthreads_or(failed)) {
                 failed = true;
                 break;
             }
             const long long last = gtile - 1;
-            if (!mbar_wait(&a_empty[last % S], static_cast<unsigned>((last / S) & 1))) failed = true;
+            if (ntiles > 0 && !mbar_wait(&a_empty[last % S], static_cast<unsigned>((last / S) & 1))) failed = true;
             if (__syncthreads_or(failed)) {
                 failed = true;
                 break;
@@ -744,6 +750,24 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                         reg_fence<MG>(v[c]);
 #pragma unroll
                         for (int u = 0; u < MG; ++u) x[c][u] += static_cast<double>(__uint_as_float(v[c][u]));
+                    }
+                }
+                // The exact rows: FP32 AO values times FP64 coefficients,
+                // accumulated in FP64 (rows padded to a multiple of 4 MOs,
+                // so the MG = 4 columns read stay inside the row).
+                for (int kx = nkt; kx < nk; ++kx) {
+                    const int slot = sorted ? static_cast<int>(perm[kx]) : kx;
+                    const float* prow = scr.panels +
+                                        (static_cast<size_t>(blk) * P * scr.row_stride + slot) * kBlockPoints + point;
+                    const double* crow = ch.c64 + static_cast<long long>(aoidx[kx]) * ch.ld64 + n0 + i0;
+                    double cv[MG];
+#pragma unroll
+                    for (int u = 0; u < MG; ++u) cv[u] = crow[u];
+#pragma unroll
+                    for (int c = 0; c < P; ++c) {
+                        const double f = static_cast<double>(prow[static_cast<size_t>(c) * scr.row_stride * kBlockPoints]);
+#pragma unroll
+                        for (int u = 0; u < MG; ++u) x[c][u] += f * cv[u];
                     }
                 }
                 fold<P, MG>(x, q, i_hi - i0);

@@ -7,6 +7,7 @@
 #include <numbers>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 
 #include "../host/device_state.hpp"
 #include "chem/kumo/density.hpp"
@@ -358,16 +359,17 @@ __device__ __forceinline__ void boys_top(const double* table, double T, double (
 // One level of the Hermite recursion: R^(n) from R^(n+1) in place, entries
 // K = NT-1 down to 1 of the first `live` (each entry reads lower-index entries
 // of the level above, which a descending sweep has not overwritten yet).
-template <int K, int NT>
-__device__ __forceinline__ void hermite_level(double (&R)[NT], int live, double pcx, double pcy, double pcz) {
+// R is double in the FP64 form and float in the mixed one.
+template <int K, int NT, typename R_t>
+__device__ __forceinline__ void hermite_level(R_t (&R)[NT], int live, R_t pcx, R_t pcy, R_t pcz) {
     if constexpr (K >= 1) {
         if (K < live) {
             constexpr int ax = kHermite.axis[K];
             constexpr int one = kHermite.one[K];
             constexpr int two = kHermite.two[K];
-            constexpr double f = static_cast<double>(kHermite.factor[K]);
-            const double X = ax == 0 ? pcx : (ax == 1 ? pcy : pcz);
-            double v = X * R[one];
+            constexpr R_t f = static_cast<R_t>(kHermite.factor[K]);
+            const R_t X = ax == 0 ? pcx : (ax == 1 ? pcy : pcz);
+            R_t v = X * R[one];
             if constexpr (two >= 0) v += f * R[two];
             R[K] = v;
         }
@@ -381,14 +383,23 @@ __device__ __forceinline__ void hermite_level(double (&R)[NT], int live, double 
 // coefficients (contiguous, in pair order) are staged in shared memory in
 // batches by the whole CTA with coalesced loads, so the per-pair loop reads
 // them with broadcast shared loads instead of dependent global ones.
-template <int L>
+//
+// MIXED = false: FP64 throughout (src/electrostatic_potential.cpp:231-348).
+// MIXED = true: the Boys values F_0..F_L(T), their (-2p)^n scaling and the
+// point-to-centre vector stay FP64; the Hermite recursion, the dot with the
+// coefficients and the sum over the chunk's pairs are FP32, the sum
+// compensated (Kahan) so that its rounding does not grow with the chunk's
+// length.  The nuclear term and the subtraction of the partial sums stay
+// FP64 (esp_reduce_kernel).
+template <int L, bool MIXED>
 __global__ void __launch_bounds__(128) esp_order_kernel(const __grid_constant__ EspParams prm, long long first,
                                                        long long count, long long chunk, int slot0, double* part,
                                                        long long ld) {
+    using R_t = std::conditional_t<MIXED, float, double>;
     constexpr int NT = hermite_count(L);
     constexpr int BATCH = (2048 / NT) < 128 ? (2048 / NT) : 128;
     __shared__ double s_p[BATCH], s_q[BATCH][3];
-    __shared__ double s_c[BATCH * NT];
+    __shared__ R_t s_c[BATCH * NT];
     const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     const bool valid = q < prm.src.count;
     double x = 0.0, y = 0.0, z = 0.0;
@@ -396,7 +407,7 @@ __global__ void __launch_bounds__(128) esp_order_kernel(const __grid_constant__ 
     const EspView& e = prm.esp;
     const long long i0 = first + static_cast<long long>(blockIdx.y) * chunk;
     const long long i1 = min(first + count, i0 + chunk);
-    double sum = 0.0;
+    R_t sum = 0, comp = 0;
     for (long long b0 = i0; b0 < i1; b0 += BATCH) {
         const int nb = static_cast<int>(min(static_cast<long long>(BATCH), i1 - b0));
         __syncthreads();  // the previous batch is no longer read
@@ -408,7 +419,7 @@ __global__ void __launch_bounds__(128) esp_order_kernel(const __grid_constant__ 
             s_q[t][2] = pr.qz;
         }
         const double* cbase = e.coef + e.pairs[b0].first;
-        for (int t = threadIdx.x; t < nb * NT; t += blockDim.x) s_c[t] = cbase[t];
+        for (int t = threadIdx.x; t < nb * NT; t += blockDim.x) s_c[t] = static_cast<R_t>(cbase[t]);
         __syncthreads();
         for (int ib = 0; ib < nb; ++ib) {
             const double pcx = s_q[ib][0] - x, pcy = s_q[ib][1] - y, pcz = s_q[ib][2] - z;
@@ -421,20 +432,32 @@ __global__ void __launch_bounds__(128) esp_order_kernel(const __grid_constant__ 
                 power *= -2.0 * pp;
                 F[k] *= power;
             }
-            double R[NT];
+            const R_t rx = static_cast<R_t>(pcx), ry = static_cast<R_t>(pcy), rz = static_cast<R_t>(pcz);
+            R_t R[NT];
 #pragma unroll
             for (int n = L; n >= 0; --n) {
-                hermite_level<NT - 1, NT>(R, hermite_count(L - n), pcx, pcy, pcz);
-                R[0] = F[n];
+                hermite_level<NT - 1, NT>(R, hermite_count(L - n), rx, ry, rz);
+                R[0] = static_cast<R_t>(F[n]);
             }
-            const double* c = s_c + ib * NT;
-            double s = 0.0;
+            const R_t* c = s_c + ib * NT;
+            R_t s = 0;
 #pragma unroll
             for (int k = 0; k < NT; ++k) s += c[k] * R[k];
-            sum += s;
+            if constexpr (MIXED) {
+                const R_t yk = s - comp;
+                const R_t t = sum + yk;
+                comp = (t - sum) - yk;
+                sum = t;
+            } else {
+                sum += s;
+            }
         }
     }
-    if (valid) part[static_cast<long long>(slot0 + blockIdx.y) * ld + q] = sum;
+    if (valid) {
+        double total = static_cast<double>(sum);
+        if constexpr (MIXED) total -= static_cast<double>(comp);
+        part[static_cast<long long>(slot0 + blockIdx.y) * ld + q] = total;
+    }
 }
 
 // out = nuclear term - the partial sums in slot order.
@@ -461,11 +484,16 @@ __global__ void __launch_bounds__(128) esp_reduce_kernel(const __grid_constant__
 template <int L>
 void launch_order(const EspParams& p, long long first, long long count, long long chunk, int chunks, int slot0,
                   double* part, long long ld, unsigned tiles, cudaStream_t stream) {
-    esp_order_kernel<L><<<dim3(tiles, static_cast<unsigned>(chunks)), 128, 0, stream>>>(p, first, count, chunk, slot0,
+    if (p.mixed) {
+        esp_order_kernel<L, true><<<dim3(tiles, static_cast<unsigned>(chunks)), 128, 0, stream>>>(
+            p, first, count, chunk, slot0, part, ld);
+        return;
+    }
+    esp_order_kernel<L, false><<<dim3(tiles, static_cast<unsigned>(chunks)), 128, 0, stream>>>(p, first, count, chunk, slot0,
                                                                                        part, ld);
 }
 
-void launch_esp_f64(const EspParams& p, cudaStream_t stream) {
+void launch_esp(const EspParams& p, cudaStream_t stream) {
     using chem::kumo::detail::check_cuda;
     const long long n = p.src.count;
     if (n <= 0) return;

@@ -54,6 +54,9 @@ struct EspParams {
     PointSource src;
     double* out = nullptr;
     long long out_base = 0;
+    // Mixed form: FP32 Hermite recursion, coefficient dot and pair sums;
+    // FP64 Boys values, scaling and nuclear-minus-electronic difference.
+    bool mixed = false;
 };
 
 /// Host setup of the pairs and the Boys table, uploaded to the device.
@@ -80,8 +83,9 @@ void boys_host(const double* table, double T, int n, double* out);
 
 /// Exact potential at the points of p.src: one launch per pair order over
 /// (128-point tiles x pair chunks) writing partial sums to stream-ordered
-/// scratch, then a fixed-order reduction with the nuclear term.
-void launch_esp_f64(const EspParams& p, cudaStream_t stream);
+/// scratch, then a fixed-order FP64 reduction with the nuclear term.  FP64
+/// throughout, or the mixed form when p.mixed is set.
+void launch_esp(const EspParams& p, cudaStream_t stream);
 /// F_m(T) for an array of T on the device (test seam of the Boys kernel).
 void launch_boys_f64(const double* table, const double* t, long long n, int nvalues, double* out, cudaStream_t stream);
 

@@ -19,6 +19,8 @@ struct MoChannelTC {
     int ldn = 0;                        // multiple of 16, >= nocc
     int nocc = 0;
     int role = 0;  // 1 alpha, 2 beta
+    const double* c64 = nullptr;  // FP64 coefficients [nao][ld64] (rows padded to a multiple of 4 MOs)
+    int ld64 = 0;
 };
 
 struct ContractMixedParams {
@@ -38,6 +40,10 @@ struct ContractMixedParams {
     float threshold = 0.0f;      // screening threshold on the rows' block maxima
     FieldSpec spec;
     unsigned* status = nullptr;  // set nonzero if a pipeline wait ran out
+    // Rows at the end of each block's K order (largest block maxima) that the
+    // bulk-copy kernel adds in FP64 with ch[].c64 instead of on the tensor
+    // cores (0: all rows on the tensor cores).
+    int exact_rows = 0;
 };
 
 // AO-P form (density_derivatives_shared): Y = P[kept, kept] Phi[kept, 0..3]

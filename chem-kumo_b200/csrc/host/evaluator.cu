@@ -44,6 +44,16 @@ namespace {
 
 using detail::check_cuda;
 
+// Rows per block that the mixed AO-MO contraction adds in FP64 rather than
+// on the tensor cores (KUMO_MIXED_EXACT_ROWS, default 0).
+int mixed_exact_rows() {
+    static const int v = [] {
+        const char* e = std::getenv("KUMO_MIXED_EXACT_ROWS");
+        return e ? std::max(0, std::atoi(e)) : 0;
+    }();
+    return v;
+}
+
 bool uses_point_path(const detail::ComponentNeeds& c, Backend b, bool grid) {
     return c.derivatives() || ((b == Backend::AO_MO || !grid) && c.density);
 }
@@ -470,7 +480,7 @@ private:
             const bool beta = ch[i].role == 2;
             const int ldn = beta ? dev_->ldn_beta : dev_->ldn_alpha;
             cp.ch[i] = {beta ? dev_->cs_beta : dev_->cs_alpha, static_cast<long long>(nao) * ldn, ldn, ch[i].nocc,
-                        ch[i].role};
+                        ch[i].role, beta ? dev_->ct_beta : dev_->ct_alpha, beta ? dev_->ldc_beta : dev_->ldc_alpha};
             nocc16 = std::max(nocc16, (ch[i].nocc + 15) / 16 * 16);
         }
         kumo_dev::mixed_columns(npanel, nocc16, cp.ncols, cp.groups, cp.tmem_cols);
@@ -479,6 +489,7 @@ private:
         cp.beta_is_alpha = bia;
         cp.ao_order = ao_order;
         cp.spec = spec;
+        cp.exact_rows = mixed_exact_rows();
         for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
             const int nb = static_cast<int>(std::min<std::size_t>(W, nblocks - b0));
             bp.first_point = static_cast<long long>(b0 * bs);
@@ -754,16 +765,18 @@ private:
         double* out = nullptr;
         for (const auto& [key, ptr] : outs_)
             if (key.kind == PropertyKind::ElectrostaticPotential) out = ptr;
-        // Every primitive pair is evaluated exactly, so the result meets any
-        // potential_tolerance >= 0 (src/electrostatic_potential.cpp:501-521
+        // Every primitive pair is evaluated exactly, so in FP64 the result
+        // meets any potential_tolerance >= 0 (src/electrostatic_potential.cpp:501-521
         // bounds the far-field error by the tolerance; here it is rounding).
+        // The mixed form's error is its FP32 rounding, whatever the tolerance.
         kumo_dev::EspDevice& esp = esp_state();
         kumo_dev::EspParams ep{};
         ep.esp = esp.view();
         ep.src = src_;
         ep.out = out;
+        ep.mixed = opt_.precision == Precision::Mixed;
         const int tok = detail::profile_begin(detail::kProfEsp, stream_);
-        kumo_dev::launch_esp_f64(ep, stream_);
+        kumo_dev::launch_esp(ep, stream_);
         detail::profile_end(tok, stream_);
         detail::profile_count(detail::kProfEsp, nullptr, 0, 0.0, static_cast<double>(n_) * esp.pair_count(), 0.0, 0.0,
                               stream_);

@@ -379,6 +379,34 @@ def test_esp_with_tolerance_within_bound(tol):
     assert scaled_error(got[0][0], ref) <= 1e-12
 
 
+def test_esp_mixed_vs_fp64():
+    # Mixed form of the potential: FP64 Boys values and nuclear term, FP32
+    # Hermite recursion and compensated FP32 pair sums.  Against the FP64 form
+    # on a grid around acrolein and on water's and O2's Multiwfn points, and
+    # against the Multiwfn values at the reference test's tolerance.
+    esp = [K.density(P.ElectrostaticPotential)]
+    m = K.Molecule.from_fchk(os.path.join(GOLDEN, "acrolein.fchk.gz"))
+    grid = m.grid_around(2.0, 0.3)
+    f64, _ = K.Evaluator(m).evaluate_grid(grid, esp)
+    mix, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_grid(grid, esp)
+    err = scaled_error(mix[0][0], f64[0][0])
+    print("esp mixed acrolein grid scaled error", err)
+    assert err <= 1e-6, err
+    for name in ["h2o_esp", "o2_esp"]:
+        g = np.load(os.path.join(GOLDEN, f"multiwfn_{name}.npz"))
+        m = K.Molecule.from_fchk(os.path.join(GOLDEN, str(g["fchk"])))
+        pts = golden_points(g)
+        f64, _ = K.Evaluator(m).evaluate_points(pts, esp)
+        mix, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_points(pts, esp)
+        err = scaled_error(mix[0][0], f64[0][0])
+        print("esp mixed", name, "scaled error", err)
+        assert err <= 1e-6, (name, err)
+        d = np.min(np.linalg.norm(pts[:, None, :] - m.atoms()[2][None], axis=2), axis=1)
+        keep = d >= 1e-3
+        ratio = np.abs(mix[0][0] - g["values"])[keep] / (2e-5 * np.abs(g["values"][keep]) + 1e-7)
+        assert ratio.max() <= 1.0, name
+
+
 def test_boys_device_matches_oracle():
     t = np.concatenate([np.linspace(0.0, 45.0, 2001), [1e-9, 39.999999, 40.0, 200.0, 1e4]])
     got = K.boys(t, 13)
