@@ -391,7 +391,7 @@ def test_esp_mixed_vs_fp64():
     mix, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_grid(grid, esp)
     err = scaled_error(mix[0][0], f64[0][0])
     print("esp mixed acrolein grid scaled error", err)
-    assert err <= 1e-6, err
+    assert err <= 1e-7, err
     for name in ["h2o_esp", "o2_esp"]:
         g = np.load(os.path.join(GOLDEN, f"multiwfn_{name}.npz"))
         m = K.Molecule.from_fchk(os.path.join(GOLDEN, str(g["fchk"])))
@@ -400,10 +400,12 @@ def test_esp_mixed_vs_fp64():
         mix, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_points(pts, esp)
         err = scaled_error(mix[0][0], f64[0][0])
         print("esp mixed", name, "scaled error", err)
-        assert err <= 1e-6, (name, err)
+        assert err <= 1e-7, (name, err)
+        # The Multiwfn comparison on the points the FP64 test uses.
+        pts, ref, got = pts[:1500], g["values"][:1500], mix[0][0][:1500]
         d = np.min(np.linalg.norm(pts[:, None, :] - m.atoms()[2][None], axis=2), axis=1)
         keep = d >= 1e-3
-        ratio = np.abs(mix[0][0] - g["values"])[keep] / (2e-5 * np.abs(g["values"][keep]) + 1e-7)
+        ratio = np.abs(got - ref)[keep] / (2e-5 * np.abs(ref[keep]) + 1e-7)
         assert ratio.max() <= 1.0, name
 
 
