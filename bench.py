@@ -264,8 +264,10 @@ def esp_bench(K, synth, fchk_dir: str, oracle_pts: int = 32):
     sout = torch.empty(len(surf), dtype=torch.float64, device="cuda")
     ms_surf = timed(lambda: ev.evaluate_points_device(dpts.data_ptr(), len(surf), [esp], [sout.data_ptr()],
                                                       stream.cuda_stream))
-    # Mixed form (FP64 Boys values and nuclear term, FP32 Hermite recursion
-    # and compensated pair sums) on the same cube and surface, against FP64.
+    # Opt-in mixed form (FP64 Boys values and nuclear term, FP32 Hermite
+    # recursion and compensated pair sums) on the same cube and surface,
+    # against FP64.
+    os.environ["KUMO_ESP_MIXED"] = "1"
     evm = K.Evaluator(m, precision=K.Precision.Mixed)
     outm = torch.empty_like(out)
     soutm = torch.empty_like(sout)
@@ -274,10 +276,12 @@ def esp_bench(K, synth, fchk_dir: str, oracle_pts: int = 32):
     ms_surf_m = timed(lambda: evm.evaluate_points_device(dpts.data_ptr(), len(surf), [esp], [soutm.data_ptr()],
                                                          stream.cuda_stream))
 
+    del os.environ["KUMO_ESP_MIXED"]
+
     def scaled(a, r):
         return float((a - r).abs().max() / max(1.0, float(r.abs().max())))
 
-    mixed = {"cube_ms": ms_cube_m, "cube_pair_points_per_s": n * pairs / (ms_cube_m * 1e-3),
+    mixed = {"opt_in": "KUMO_ESP_MIXED=1", "cube_ms": ms_cube_m, "cube_pair_points_per_s": n * pairs / (ms_cube_m * 1e-3),
              "surface_ms": ms_surf_m, "surface_pair_points_per_s": len(surf) * pairs / (ms_surf_m * 1e-3),
              "speedup_vs_fp64_cube": ms_cube / ms_cube_m, "speedup_vs_fp64_surface": ms_surf / ms_surf_m,
              "scaled_err_vs_fp64_cube": scaled(outm, out), "scaled_err_vs_fp64_surface": scaled(soutm, sout),

@@ -45,13 +45,21 @@ namespace {
 using detail::check_cuda;
 
 // Rows per block that the mixed AO-MO contraction adds in FP64 rather than
-// on the tensor cores (KUMO_MIXED_EXACT_ROWS, default 0).
+// on the tensor cores (KUMO_MIXED_EXACT_ROWS, read at each evaluation;
+// default 0).  16 rows take rho and grad rho of a 740-AO molecule from about
+// 1.8e-7 to 7e-8 (scaled, vs FP64) for about 60% more time.
 int mixed_exact_rows() {
-    static const int v = [] {
-        const char* e = std::getenv("KUMO_MIXED_EXACT_ROWS");
-        return e ? std::max(0, std::atoi(e)) : 0;
-    }();
-    return v;
+    const char* e = std::getenv("KUMO_MIXED_EXACT_ROWS");
+    return e ? std::max(0, std::atoi(e)) : 0;
+}
+
+// The mixed form of the potential (FP32 Hermite sums) is opt-in
+// (KUMO_ESP_MIXED=1, read at each evaluation): on a 1260-AO molecule it was
+// 1.07x faster than FP64 with 9e-4 scaled error on its density isosurface, so
+// by default Precision::Mixed evaluates the potential in FP64.
+bool esp_mixed_opt_in() {
+    const char* e = std::getenv("KUMO_ESP_MIXED");
+    return e != nullptr && e[0] == '1';
 }
 
 bool uses_point_path(const detail::ComponentNeeds& c, Backend b, bool grid) {
@@ -768,13 +776,14 @@ private:
         // Every primitive pair is evaluated exactly, so in FP64 the result
         // meets any potential_tolerance >= 0 (src/electrostatic_potential.cpp:501-521
         // bounds the far-field error by the tolerance; here it is rounding).
-        // The mixed form's error is its FP32 rounding, whatever the tolerance.
+        // The opt-in mixed form's error is its FP32 rounding, whatever the
+        // tolerance.
         kumo_dev::EspDevice& esp = esp_state();
         kumo_dev::EspParams ep{};
         ep.esp = esp.view();
         ep.src = src_;
         ep.out = out;
-        ep.mixed = opt_.precision == Precision::Mixed;
+        ep.mixed = opt_.precision == Precision::Mixed && esp_mixed_opt_in();
         const int tok = detail::profile_begin(detail::kProfEsp, stream_);
         kumo_dev::launch_esp(ep, stream_);
         detail::profile_end(tok, stream_);

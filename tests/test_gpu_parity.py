@@ -379,7 +379,7 @@ def test_esp_with_tolerance_within_bound(tol):
     assert scaled_error(got[0][0], ref) <= 1e-12
 
 
-def test_esp_mixed_vs_fp64():
+def test_esp_mixed_vs_fp64(monkeypatch):
     # Mixed form of the potential: FP64 Boys values and nuclear term, FP32
     # Hermite recursion and compensated FP32 pair sums.  Against the FP64 form
     # (which the other tests hold to the oracle and to Multiwfn) on a grid
@@ -391,6 +391,11 @@ def test_esp_mixed_vs_fp64():
     m = K.Molecule.from_fchk(os.path.join(GOLDEN, "acrolein.fchk.gz"))
     grid = m.grid_around(2.0, 0.3)
     f64, _ = K.Evaluator(m).evaluate_grid(grid, esp)
+    # Without the opt-in, Precision::Mixed evaluates the potential in FP64.
+    monkeypatch.delenv("KUMO_ESP_MIXED", raising=False)
+    same, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_grid(grid, esp)
+    assert np.array_equal(same[0][0], f64[0][0])
+    monkeypatch.setenv("KUMO_ESP_MIXED", "1")
     mix, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_grid(grid, esp)
     err = scaled_error(mix[0][0], f64[0][0])
     print("esp mixed acrolein grid scaled error", err)
@@ -404,6 +409,28 @@ def test_esp_mixed_vs_fp64():
         err = scaled_error(mix[0][0], f64[0][0])
         print("esp mixed", name, "scaled error", err)
         assert err <= 1e-7, (name, err)
+
+
+@pytest.mark.parametrize("rows", [16, 100000])
+def test_mixed_exact_rows(monkeypatch, rows):
+    # The mixed AO-MO contraction with the last `rows` rows of each block's K
+    # order added in FP64 (100000: every row, so no tensor-core step runs and
+    # only the FP32 AO values separate the result from FP64).
+    m = K.Molecule.from_fchk(os.path.join(GOLDEN, "acrolein.fchk.gz"))
+    _, _, xyz = m.atoms()
+    rng = np.random.default_rng(3)
+    pts = np.concatenate([xyz + rng.normal(0.0, 0.05, xyz.shape),
+                          rng.uniform(xyz.min(0) - 2.0, xyz.max(0) + 2.0, (4000, 3))])
+    props = [K.density(k, c) for k, c in FIELDS]
+    f64, _ = K.Evaluator(m, backend=K.Backend.AO_MO).evaluate_points(pts, props)
+    monkeypatch.setenv("KUMO_MIXED_EXACT_ROWS", str(rows))
+    mix, _ = K.Evaluator(m, backend=K.Backend.AO_MO, precision=K.Precision.Mixed).evaluate_points(pts, props)
+    monkeypatch.delenv("KUMO_MIXED_EXACT_ROWS")
+    for p, a, r in zip(props[:4], mix[:4], f64[:4]):
+        assert np.all(np.isfinite(a)), p
+        print("exact rows", rows, p, scaled_error(a, r))
+        assert scaled_error(a, r) <= 1e-6, (p, scaled_error(a, r))
+    assert scaled_error(mix[4], f64[4]) <= 1e-5
 
 
 def test_boys_device_matches_oracle():
