@@ -544,7 +544,13 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
     // FP64 in the epilogue instead of on the tensor cores: the truncation of
     // each MMA's FP32 sum is relative to its largest product, so taking the
     // largest products out of the MMAs lowers the error of every output.
-    const int nx = prm.exact_rows < nk ? prm.exact_rows : nk;
+    // At most as many rows as the idle stages hold during the epilogue: AO
+    // values in the AO stages (2 * 3 * P * 4096 bytes = 48 rows of P * 512),
+    // coefficients in the coefficient stages (SB * 96 * N bytes = 12 * SB rows
+    // of N doubles).
+    constexpr int kExactCap = 12 * SB < 48 ? 12 * SB : 48;
+    int nx = prm.exact_rows < nk ? prm.exact_rows : nk;
+    if (nx > kExactCap) nx = kExactCap;
     const int nkt = nk - nx;
     const int ntiles = (nkt + 15) / 16;
     tc_fence_before();
@@ -727,6 +733,30 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                 break;
             }
             tc_fence_after();
+            // Stage the exact rows in the stages no MMA reads any more: AO
+            // values [row][panel][point] (FP32) and this pass's coefficient
+            // columns [row][column] (FP64, zero past the padded row).
+            float* xs_phi = reinterpret_cast<float*>(a_st);
+            double* xs_c = reinterpret_cast<double*>(b_st);
+            if (nx > 0) {
+                for (int v = tid; v < nx * P * 32; v += kBulkThreads) {
+                    const int r = v / (P * 32), rem = v - r * (P * 32), c = rem >> 5, q4 = rem & 31;
+                    const int slot = sorted ? static_cast<int>(perm[nkt + r]) : nkt + r;
+                    const float4 f = *reinterpret_cast<const float4*>(
+                        scr.panels + ((static_cast<size_t>(blk) * P + c) * scr.row_stride + slot) * kBlockPoints + q4 * 4);
+                    *reinterpret_cast<float4*>(xs_phi + (r * P + c) * kBlockPoints + q4 * 4) = f;
+                }
+                const int half_n = N / 2;
+                for (int v = tid; v < nx * half_n; v += kBulkThreads) {
+                    const int r = v / half_n, j = v - r * half_n;
+                    const int col = n0 + 2 * j;
+                    double2 cv = make_double2(0.0, 0.0);
+                    if (col < ch.ld64)
+                        cv = *reinterpret_cast<const double2*>(ch.c64 + static_cast<long long>(aoidx[nkt + r]) * ch.ld64 + col);
+                    *reinterpret_cast<double2*>(xs_c + r * N + 2 * j) = cv;
+                }
+                __syncthreads();
+            }
             const int nvalid = ch.nocc - n0 < N ? ch.nocc - n0 : N;
             // Warps 8 and 9 (half 2) read no accumulators.
             const int i_lo = half * (N / 2), i_hi = min(nvalid, (half + 1) * (N / 2));
@@ -753,19 +783,15 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                     }
                 }
                 // The exact rows: FP32 AO values times FP64 coefficients,
-                // accumulated in FP64 (rows padded to a multiple of 4 MOs,
-                // so the MG = 4 columns read stay inside the row).
-                for (int kx = nkt; kx < nk; ++kx) {
-                    const int slot = sorted ? static_cast<int>(perm[kx]) : kx;
-                    const float* prow = scr.panels +
-                                        (static_cast<size_t>(blk) * P * scr.row_stride + slot) * kBlockPoints + point;
-                    const double* crow = ch.c64 + static_cast<long long>(aoidx[kx]) * ch.ld64 + n0 + i0;
+                // accumulated in FP64, from the staged copies.
+                for (int r = 0; r < nx; ++r) {
+                    const double* crow = xs_c + r * N + i0;
                     double cv[MG];
 #pragma unroll
                     for (int u = 0; u < MG; ++u) cv[u] = crow[u];
 #pragma unroll
                     for (int c = 0; c < P; ++c) {
-                        const double f = static_cast<double>(prow[static_cast<size_t>(c) * scr.row_stride * kBlockPoints]);
+                        const double f = static_cast<double>(xs_phi[(r * P + c) * kBlockPoints + point]);
 #pragma unroll
                         for (int u = 0; u < MG; ++u) x[c][u] += f * cv[u];
                     }
