@@ -46,11 +46,12 @@ using detail::check_cuda;
 
 // Rows per block that the mixed AO-MO contraction adds in FP64 rather than
 // on the tensor cores (KUMO_MIXED_EXACT_ROWS, read at each evaluation;
-// default 0).  16 rows take rho and grad rho of a 740-AO molecule from about
-// 1.8e-7 to 7e-8 (scaled, vs FP64) for about 60% more time.
+// default 16, 0 turns it off).  On a 740-AO molecule 16 rows take rho and
+// grad rho from about 1.8e-7 to 7e-8 (scaled, vs FP64) and every other field
+// down a little, for about 18% more time per step.
 int mixed_exact_rows() {
     const char* e = std::getenv("KUMO_MIXED_EXACT_ROWS");
-    return e ? std::max(0, std::atoi(e)) : 0;
+    return e ? std::max(0, std::atoi(e)) : 16;
 }
 
 // The mixed form of the potential (FP32 Hermite sums) is opt-in

@@ -411,11 +411,11 @@ def test_esp_mixed_vs_fp64(monkeypatch):
         assert err <= 1e-7, (name, err)
 
 
-@pytest.mark.parametrize("rows", [16, 100000])
+@pytest.mark.parametrize("rows", [0, 16, 100000])
 def test_mixed_exact_rows(monkeypatch, rows):
     # The mixed AO-MO contraction with the last `rows` rows of each block's K
-    # order added in FP64 (100000: every row, so no tensor-core step runs and
-    # only the FP32 AO values separate the result from FP64).
+    # order added in FP64 (0: every row on the tensor cores; 16: the default;
+    # 100000: as many as the kernel's staging holds).
     m = K.Molecule.from_fchk(os.path.join(GOLDEN, "acrolein.fchk.gz"))
     _, _, xyz = m.atoms()
     rng = np.random.default_rng(3)
