@@ -644,16 +644,19 @@ def test_fused_mixed_form_matches_two_kernel_form():
 
 @pytest.mark.parametrize("case", ["values", "gradient", "laplacian"])
 @pytest.mark.parametrize("name", ["o2.fchk.gz", "acrolein.fchk.gz"])
-def test_bulk_copy_contraction_equals_register_staged(name, case):
+def test_bulk_copy_contraction_equals_register_staged(name, case, monkeypatch):
     # The bulk-copy tensor-core contraction (rows fetched by tensor copies
     # into shared memory, the default) and the register-staged one
     # (KUMO_MIXED_BULK=0) split the same FP32 rows and accumulate the same
-    # products in the same order: the results agree bit for bit, and both
-    # hold the mixed tolerance.
+    # products in the same order when every row goes through the tensor cores
+    # (KUMO_MIXED_EXACT_ROWS=0): the results agree bit for bit, and both hold
+    # the mixed tolerance, as does the default bulk form with its exact rows.
     m, o = _pair(os.path.join(GOLDEN, name))
     pts = _box_points(o.atom_xyz.reshape(-1, 3), 5000, 33)
     comps = [D.Total, D.Alpha, D.Beta] if name == "o2.fchk.gz" else [D.Total]
     props = [K.density(k, c) for k in MIXED_CASES[case] for c in comps]
+    default, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_points(pts, props)
+    monkeypatch.setenv("KUMO_MIXED_EXACT_ROWS", "0")
     bulk, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_points(pts, props)
     os.environ["KUMO_MIXED_BULK"] = "0"
     try:
@@ -661,9 +664,10 @@ def test_bulk_copy_contraction_equals_register_staged(name, case):
     finally:
         del os.environ["KUMO_MIXED_BULK"]
     ref, _ = K.Evaluator(m).evaluate_points(pts, props)
-    for p, a, b, r in zip(props, bulk, staged, ref):
+    for p, a, b, r, d in zip(props, bulk, staged, ref, default):
         assert np.array_equal(a, b), p
         assert scaled_error(a, r) <= (1e-5 if p.kind == P.Elf else 1e-6), p
+        assert scaled_error(d, r) <= (1e-5 if p.kind == P.Elf else 1e-6), p
 
 
 def test_sharded_grid_equals_whole_grid():
