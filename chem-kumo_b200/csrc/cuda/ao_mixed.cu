@@ -52,25 +52,32 @@ __global__ void __launch_bounds__(kBlockPoints, (P == 10 || MAXL >= 4) ? 6 : 8) 
         const bool inside = valid && r2d <= o.w;
         float* dst = pan + static_cast<size_t>(row) * kBlockPoints;
         if (__any_sync(0xffffffffu, inside)) {
-            float R0 = 0.0f, R1 = 0.0f, R2 = 0.0f;
+            // Radial sums in FP64 of the FP32 products u e (a and a^2 times
+            // them are exact in FP64), and the Laplacian's radial factor
+            // q = (2l+3) R1' + r^2 R2', whose terms partly cancel, formed in
+            // FP64: each factor is rounded to FP32 once.
+            double R0 = 0.0, R1 = 0.0, R2 = 0.0;
             if (inside) {
                 for (int p = 0; p < nprim; ++p) {
                     const MixPrim pr = prm.prims[inf.y + p];
-                    const float ue = pr.u * exp_neg(pr.al2, r2d);
+                    const double ue = static_cast<double>(pr.u * exp_neg(pr.al2, r2d));
+                    const double a = static_cast<double>(pr.alpha);
                     R0 += ue;
-                    R1 += ue * pr.alpha;
-                    R2 += ue * pr.alpha * pr.alpha;
+                    R1 += ue * a;
+                    R2 += ue * (a * a);
                 }
             }
             const float x = static_cast<float>(dx), y = static_cast<float>(dy), z = static_cast<float>(dz);
             const float r2 = static_cast<float>(r2d);
-            const float R1p = -2.0f * R1, R2p = 4.0f * R2;
+            const float R1p = static_cast<float>(-2.0 * R1), R2p = static_cast<float>(4.0 * R2);
+            const float q = static_cast<float>(static_cast<double>(2 * l + 3) * (-2.0 * R1) + r2d * (4.0 * R2));
             float* rm = rmx + static_cast<size_t>(row) * 4;
             switch (l | (pure ? 16 : 0)) {
 #define KUMO_MIXED(LL, PP)                                                                                   \
     case (LL) | ((PP) ? 16 : 0):                                                                             \
         if constexpr (LL <= MAXL)                                                                            \
-            mixed_shell<(LL <= MAXL ? LL : 0), PP, P>(prm, x, y, z, r2, R0, R1p, R2p, dst, pstride, rm, lane); \
+            mixed_shell<(LL <= MAXL ? LL : 0), PP, P>(prm, x, y, z, r2, static_cast<float>(R0), R1p, R2p, q, dst, \
+                                                      pstride, rm, lane);                                   \
         break;
                 KUMO_MIXED(0, false) KUMO_MIXED(1, false) KUMO_MIXED(2, false) KUMO_MIXED(3, false)
                 KUMO_MIXED(4, false) KUMO_MIXED(2, true) KUMO_MIXED(3, true) KUMO_MIXED(4, true)

@@ -20,7 +20,8 @@ __device__ __forceinline__ float exp_neg(double al2, double r2) {
 
 template <int L, bool PURE, int P, bool ROWMAX = true>
 __device__ __forceinline__ void mixed_shell(const AoMixedParams& prm, float x, float y, float z, float r2, float R0,
-                                            float R1p, float R2p, float* dst, size_t pstride, float* rmax, int lane) {
+                                            float R1p, float R2p, float q, float* dst, size_t pstride, float* rmax,
+                                            int lane) {
     constexpr int NC = Cart<L>::NC;
     constexpr int NOUT = PURE ? 2 * L + 1 : NC;
     constexpr bool LAPM = P == 5 && !PURE;  // Cartesian Laplacian of the monomials
@@ -89,7 +90,7 @@ __device__ __forceinline__ void mixed_shell(const AoMixedParams& prm, float x, f
         }
     });
     const float r[3] = {x, y, z};
-    const float q = (float)(2 * L + 3) * R1p + r2 * R2p;
+    // q = (2L+3) R1' + r^2 R2' comes from the caller, formed in FP64.
 #pragma unroll
     for (int m = 0; m < NOUT; ++m) {
         float* d = dst + m * kBlockPoints;

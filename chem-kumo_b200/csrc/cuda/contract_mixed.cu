@@ -1081,8 +1081,9 @@ __global__ void __launch_bounds__(kThreads, 1) contract_fused_kernel(const __gri
 #define KUMO_FUSED(LL, PP)                                                                                          \
     case (LL) | ((PP) ? 16 : 0):                                                                                    \
         if constexpr (LL <= MAXL)                                                                                   \
-            mixed_shell<(LL <= MAXL ? LL : 0), PP, P, false>(ap, x, y, z, r2, R0, -2.0f * R1, 4.0f * R2, dst,      \
-                                                              pstride, nullptr, lane);                             \
+            mixed_shell<(LL <= MAXL ? LL : 0), PP, P, false>(ap, x, y, z, r2, R0, -2.0f * R1, 4.0f * R2,           \
+                                                              (float)(2 * LL + 3) * (-2.0f * R1) + r2 * (4.0f * R2),  \
+                                                              dst, pstride, nullptr, lane);                        \
         break;
                         KUMO_FUSED(0, false) KUMO_FUSED(1, false) KUMO_FUSED(2, false) KUMO_FUSED(3, false)
                         KUMO_FUSED(4, false) KUMO_FUSED(2, true) KUMO_FUSED(3, true) KUMO_FUSED(4, true)
