@@ -181,7 +181,16 @@ __global__ void __launch_bounds__(kCtaThreads<S>, 1) contract_mixed_kernel(const
     const bool have_idx = nk <= kSortCap && scr.row_stride <= 65535;
     if (have_idx)
         for (int k = tid; producer && k < nk; k += kThreads) aoidx[k] = static_cast<std::uint16_t>(kept[sorted ? perm[k] : k]);
-    const int ntiles = (nk + 15) / 16;
+    // The last nx rows of the K order (largest block maxima) are added in FP64
+    // in the epilogue, as in contract_bulk_kernel; at most what the idle
+    // stages hold (AO values: S * 3 * P * 4096 bytes = 24 * S rows of P * 512;
+    // coefficients: (S + 1) * 96 * N bytes = 12 * (S + 1) rows of N doubles),
+    // and only when the rows are in K order with their AO indices at hand.
+    constexpr int kExactCap = 24 * S < 12 * SB ? 24 * S : 12 * SB;
+    int nx = (sorted && have_idx) ? (prm.exact_rows < nk ? prm.exact_rows : nk) : 0;
+    if (nx > kExactCap) nx = kExactCap;
+    const int nkt = nk - nx;
+    const int ntiles = (nkt + 15) / 16;
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -219,7 +228,7 @@ __global__ void __launch_bounds__(kCtaThreads<S>, 1) contract_mixed_kernel(const
             float4 ra[P][2];
             auto load_a = [&](int t) {
                 const int k = t * 16 + kh * 8 + k8;
-                const bool ok = k < nk;
+                const bool ok = k < nkt;
                 const int row = ok ? (sorted ? perm[k] : k) : 0;
 #pragma unroll
                 for (int c = 0; c < P; ++c) {
@@ -246,7 +255,7 @@ __global__ void __launch_bounds__(kCtaThreads<S>, 1) contract_mixed_kernel(const
                     const int rh = static_cast<int>(rest2 & 1u), piece = static_cast<int>(rest2 >> 1);
                     const int k = t * 16 + rh * 8 + r8;
                     const int col = n0 + ng * 8;
-                    const bool ok = k < nk && col < ch.ldn;
+                    const bool ok = k < nkt && col < ch.ldn;
                     const int ao = ok ? (have_idx ? static_cast<int>(aoidx[k]) : kept[sorted ? perm[k] : k]) : 0;
                     const std::uint16_t* src =
                         ch.cs + (ok ? piece * ch.piece_stride + static_cast<long long>(ao) * ch.ldn + col : 0);
@@ -352,7 +361,7 @@ __global__ void __launch_bounds__(kCtaThreads<S>, 1) contract_mixed_kernel(const
                     if (t + 2 < ntiles) load_b(t + 2, static_cast<int>((gtile + 2) % SB));
                 }
             }
-            if (ntiles == 0) continue;
+            if (ntiles == 0 && nx == 0) continue;
             if constexpr (kSpec) {
                 // Producers' timeouts become every thread's before the pass ends.
                 if (__syncthreads_or(failed)) {
@@ -364,12 +373,36 @@ __global__ void __launch_bounds__(kCtaThreads<S>, 1) contract_mixed_kernel(const
             }
             // Accumulators of this pass complete once the last step's commit arrives.
             const long long last = gtile - 1;
-            if (!mbar_wait(&bar[last % S], static_cast<unsigned>((last / S) & 1))) failed = true;
+            if (ntiles > 0 && !mbar_wait(&bar[last % S], static_cast<unsigned>((last / S) & 1))) failed = true;
             if (__syncthreads_or(failed)) {
                 failed = true;
                 break;
             }
             tc_fence_after();
+            // Stage the exact rows in the stages no MMA reads any more: AO
+            // values [row][panel][point] (FP32) and this pass's coefficient
+            // columns [row][column] (FP64, zero past the padded row).
+            float* xs_phi = reinterpret_cast<float*>(a_st);
+            double* xs_c = reinterpret_cast<double*>(b_st);
+            if (nx > 0) {
+                for (int v = tid; v < nx * P * 32; v += static_cast<int>(blockDim.x)) {
+                    const int r = v / (P * 32), rem = v - r * (P * 32), c = rem >> 5, q4 = rem & 31;
+                    const int slot = perm[nkt + r];
+                    const float4 f = *reinterpret_cast<const float4*>(
+                        pbase + (static_cast<size_t>(c) * scr.row_stride + slot) * kBlockPoints + q4 * 4);
+                    *reinterpret_cast<float4*>(xs_phi + (r * P + c) * kBlockPoints + q4 * 4) = f;
+                }
+                const int half_n = N / 2;
+                for (int v = tid; v < nx * half_n; v += static_cast<int>(blockDim.x)) {
+                    const int r = v / half_n, j = v - r * half_n;
+                    const int col = n0 + 2 * j;
+                    double2 cv = make_double2(0.0, 0.0);
+                    if (col < ch.ld64)
+                        cv = *reinterpret_cast<const double2*>(ch.c64 + static_cast<long long>(aoidx[nkt + r]) * ch.ld64 + col);
+                    *reinterpret_cast<double2*>(xs_c + r * N + 2 * j) = cv;
+                }
+                __syncthreads();
+            }
             const int nvalid = ch.nocc - n0 < N ? ch.nocc - n0 : N;
             const int i_lo = half * (N / 2), i_hi = min(nvalid, (half + 1) * (N / 2));
             const unsigned lane_addr = tmem + (static_cast<unsigned>(quarter * 32) << 16);
@@ -394,6 +427,19 @@ __global__ void __launch_bounds__(kCtaThreads<S>, 1) contract_mixed_kernel(const
                         reg_fence<MG>(v[c]);
 #pragma unroll
                         for (int u = 0; u < MG; ++u) x[c][u] += static_cast<double>(__uint_as_float(v[c][u]));
+                    }
+                }
+                // The exact rows, from the staged copies, in FP64.
+                for (int r = 0; r < nx; ++r) {
+                    const double* crow = xs_c + r * N + i0;
+                    double cv[MG];
+#pragma unroll
+                    for (int u = 0; u < MG; ++u) cv[u] = crow[u];
+#pragma unroll
+                    for (int c = 0; c < P; ++c) {
+                        const double f = static_cast<double>(xs_phi[(r * P + c) * kBlockPoints + point]);
+#pragma unroll
+                        for (int u = 0; u < MG; ++u) x[c][u] += f * cv[u];
                     }
                 }
                 fold<P, MG>(x, q, i_hi - i0);

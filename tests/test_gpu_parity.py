@@ -422,10 +422,19 @@ def test_mixed_exact_rows(monkeypatch, rows):
     pts = np.concatenate([xyz + rng.normal(0.0, 0.05, xyz.shape),
                           rng.uniform(xyz.min(0) - 2.0, xyz.max(0) + 2.0, (4000, 3))])
     props = [K.density(k, c) for k, c in FIELDS]
+    # The Hessian request runs the register-staged kernel (ten panels).
+    hprops = [K.density(k) for k in (P.Density, P.Hessian, P.Laplacian)]
     f64, _ = K.Evaluator(m, backend=K.Backend.AO_MO).evaluate_points(pts, props)
+    hf64, _ = K.Evaluator(m, backend=K.Backend.AO_MO).evaluate_points(pts, hprops)
     monkeypatch.setenv("KUMO_MIXED_EXACT_ROWS", str(rows))
-    mix, _ = K.Evaluator(m, backend=K.Backend.AO_MO, precision=K.Precision.Mixed).evaluate_points(pts, props)
+    mixed = K.Evaluator(m, backend=K.Backend.AO_MO, precision=K.Precision.Mixed)
+    mix, _ = mixed.evaluate_points(pts, props)
+    hmix, _ = mixed.evaluate_points(pts, hprops)
     monkeypatch.delenv("KUMO_MIXED_EXACT_ROWS")
+    for p, a, r in zip(hprops, hmix, hf64):
+        assert np.all(np.isfinite(a)), p
+        print("exact rows", rows, "ten panels", p, scaled_error(a, r))
+        assert scaled_error(a, r) <= 1e-6, (p, scaled_error(a, r))
     # The default form (16 exact rows, FP64 radial sums in the AO kernel)
     # holds rho, grad rho, lap rho and tau to 1e-7 scaled.
     tol = 1e-7 if rows == 16 else 1e-6
