@@ -3,7 +3,9 @@
 #include <cstddef>
 #include <filesystem>
 #include <string>
-#include <unordered_map>
+#include <map>
+#include <string_view>
+#include <variant>
 #include <vector>
 
 namespace chem::kumo {
@@ -29,17 +31,12 @@ public:
 
 private:
     FormattedCheckpoint() = default;
-    void parse(std::istream& input, std::size_t logical_size, const std::string& name);
-    enum class Kind { IntegerScalar, RealScalar, IntegerArray, RealArray };
-    struct Record {
-        Kind kind{};
-        long long integer_scalar = 0;
-        double real_scalar = 0.0;
-        std::vector<long long> integer_array;
-        std::vector<double> real_array;
-    };
-    [[nodiscard]] const Record& record(const std::string& label) const;
-    std::unordered_map<std::string, Record> records_;
+    // One record: integer scalar, real scalar, integer array or real array.
+    using Value = std::variant<long long, double, std::vector<long long>, std::vector<double>>;
+    void load(std::string_view text, std::size_t logical_size, const std::string& name);
+    template <class T>
+    [[nodiscard]] const T& get(const std::string& label, const char* what) const;
+    std::map<std::string, Value, std::less<>> records_;
 };
 
 }  // namespace chem::kumo

@@ -215,3 +215,51 @@ def test_cube_values_match_printf_formatting(tmp_path):
             expect.append(line)
             line = ""
     assert body[:len(expect)] == expect
+
+
+def _o2_text():
+    import gzip
+    return gzip.decompress(open(os.path.join(GOLDEN, "o2.fchk.gz"), "rb").read()).decode()
+
+
+def _load_text(tmp_path, text, name="t.fchk"):
+    p = tmp_path / name
+    p.write_text(text)
+    return K.Molecule.from_fchk(str(p))
+
+
+def test_fchk_record_rules(tmp_path):
+    # Rules of chem-kumo's FormattedCheckpoint (src/fchk.cpp:111-186) that the
+    # reader must keep: Fortran D exponents read as E, an identical duplicate
+    # record is accepted, a conflicting one is rejected, values after the last
+    # array value on its line are rejected, a short array is "truncated", and
+    # an N=0 array takes the whole next line as its final line.
+    text = _o2_text()
+    base = _load_text(tmp_path, text, "base.fchk")
+    ref_blocks = base.blocks()
+    lines = text.split("\n")
+    i = next(k for k, l in enumerate(lines) if l.startswith("Primitive exponents"))
+    j = next(k for k in range(i + 1, len(lines)) if lines[k][:1].isalpha())
+    d_lines = lines[:i + 1] + [l.replace("E", "D") for l in lines[i + 1:j]] + lines[j:]
+    assert _load_text(tmp_path, "\n".join(d_lines), "d.fchk").blocks() == ref_blocks
+    dup = lines[:j] + lines[i:j] + lines[j:]
+    assert _load_text(tmp_path, "\n".join(dup), "dup.fchk").blocks() == ref_blocks
+    conflict = lines[:j] + [lines[i]] + [lines[i + 1].replace("E+", "E-", 1)] + lines[i + 2:j] + lines[j:]
+    with pytest.raises(K.KumoError, match="conflicting duplicate fchk record: Primitive exponents"):
+        _load_text(tmp_path, "\n".join(conflict), "conflict.fchk")
+    extra = list(lines)
+    extra[j - 1] = extra[j - 1] + "  1.0E+00"
+    with pytest.raises(K.KumoError, match="too many values on final array line in fchk: Primitive exponents"):
+        _load_text(tmp_path, "\n".join(extra), "extra.fchk")
+    short = list(lines)
+    n = int(lines[i].split()[-1])
+    short[i] = lines[i].replace(str(n), str(n + 1000))
+    with pytest.raises(K.KumoError, match="invalid real token|truncated array"):
+        _load_text(tmp_path, "\n".join(short), "short.fchk")
+    empty_then_header = lines[:2] + ["%-43sI   N=           0" % "Empty array"] + lines[2:]
+    with pytest.raises(K.KumoError, match="too many values on final array line in fchk: Empty array"):
+        _load_text(tmp_path, "\n".join(empty_then_header), "empty.fchk")
+    empty_then_blank = lines[:2] + ["%-43sI   N=           0" % "Empty array", ""] + lines[2:]
+    assert _load_text(tmp_path, "\n".join(empty_then_blank), "empty2.fchk").blocks() == ref_blocks
+    with pytest.raises(K.KumoError, match="missing its two-line header"):
+        _load_text(tmp_path, "only one line", "hdr.fchk")
