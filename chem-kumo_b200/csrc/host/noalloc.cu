@@ -98,12 +98,14 @@ void run(const kumo_molecule* m, const kumo_options* opt, const double* device_p
         throw std::invalid_argument("the no-allocation entry point supports block_size 1 to 128");
     if (!std::isfinite(thr) || thr < 0.0) throw std::invalid_argument("screening threshold must be finite and nonnegative");
     if (opt && opt->precision != 0) throw std::invalid_argument("the no-allocation entry point is FP64 only");
-    if (opt && opt->backend == 1) throw std::invalid_argument("the no-allocation entry point uses the AO_MO backend");
+    if (opt && opt->backend != 0 && opt->backend != 2)
+        throw std::invalid_argument("the no-allocation entry point takes backend AUTO or AO_MO");
     Request req;
     for (int i = 0; i < nprops; ++i) {
         if (props[i].kind < 0 || props[i].kind > static_cast<int>(PropertyKind::LolTsirelsonStash) || props[i].component < 0 ||
             props[i].component > 3)
             throw std::invalid_argument("unknown property");
+        if (!outputs[i]) throw std::invalid_argument("null output array for property " + std::to_string(i));
         const PropertyKind k = static_cast<PropertyKind>(props[i].kind);
         if (!point_path_kind(k))
             throw std::invalid_argument("the no-allocation entry point evaluates density properties only");

@@ -33,6 +33,30 @@ def block_range(npoints: int, rank: int, world: int, block: int = BLOCK) -> Tupl
     return first, end - first
 
 
+def slab_range(counts: Sequence[int], rank: int, world: int, block: int = BLOCK) -> Tuple[int, int]:
+    """Planes [i0, i1) of the grid's first (slowest) axis for this rank: the
+    planes split as evenly as whole planes allow, the first ``nx % world``
+    ranks one plane more.  A slab is a grid of its own, so each rank can
+    evaluate it as a grid (and the mixed form as compact tiles).  When a
+    plane holds a whole number of ``block``-point blocks (ny * nz % block ==
+    0) the slab boundaries fall on block boundaries of the whole grid."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("invalid rank or world size")
+    nx = int(counts[0])
+    base, extra = divmod(nx, world)
+    i0 = rank * base + min(rank, extra)
+    return i0, i0 + base + (1 if rank < extra else 0)
+
+
+def slab_grid(origin: Sequence[float], steps: np.ndarray, counts: Sequence[int], i0: int, i1: int):
+    """(origin, steps, counts) of planes i0 .. i1-1 as a grid of their own;
+    its points are those of the whole grid up to the rounding of the shifted
+    origin (origin + i0 * step of the first axis)."""
+    s = np.asarray(steps, dtype=float)
+    o = np.asarray(origin, dtype=float) + s[:, 0] * i0
+    return o, s, (i1 - i0, int(counts[1]), int(counts[2]))
+
+
 def grid_points(origin: Sequence[float], steps: np.ndarray, counts: Sequence[int], first: int, count: int) -> np.ndarray:
     """Points first .. first+count-1 of a grid (Field order, k fastest), (count, 3)."""
     ny, nz = int(counts[1]), int(counts[2])
@@ -48,10 +72,10 @@ def grid_points(origin: Sequence[float], steps: np.ndarray, counts: Sequence[int
 def gather_slices(local: List[np.ndarray], npoints: int, first: int, dist, rank: int, world: int,
                   dst: int = 0) -> List[np.ndarray]:
     """Host gather of each rank's slice (channels x count per property) into
-    full arrays on rank ``dst`` (an empty list elsewhere).  Uses
-    ``all_gather_object`` of (first, arrays), which every rank calls."""
-    parts = [None] * world
-    dist.all_gather_object(parts, (first, [np.ascontiguousarray(a) for a in local]))
+    full arrays on rank ``dst`` (an empty list elsewhere).  Every rank calls
+    ``gather_object`` with (first, arrays); only ``dst`` receives the slices."""
+    parts = [None] * world if rank == dst else None
+    dist.gather_object((first, [np.ascontiguousarray(a) for a in local]), parts, dst=dst)
     if rank != dst:
         return []
     out = [np.empty((a.shape[0], npoints)) for a in local]

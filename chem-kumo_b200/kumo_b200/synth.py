@@ -544,11 +544,21 @@ def read_fchk(path: str) -> Dict[str, object]:
         conv = int if kind == "I" else (lambda t: float(t.replace("D", "E").replace("d", "E")))
         if meta[1] == "N=":
             count = int(meta[2])
-            vals: List = []
-            while len(vals) < count:
-                vals.extend(conv(t) for t in lines[i].split())
+            # Collect the data lines (up to the next record header, which
+            # starts with a letter) and convert them in one numpy call.
+            first = i
+            while i < len(lines) and not lines[i][:1].isalpha():
                 i += 1
-            rec[label] = np.array(vals, dtype=np.int64 if kind == "I" else float)
+            text = "\n".join(lines[first:i])
+            if kind == "I":
+                rec[label] = np.array(text.split(), dtype=np.int64)
+            else:
+                if "D" in text or "d" in text:
+                    text = text.replace("D", "E").replace("d", "E")
+                vals = np.fromstring(text, dtype=float, sep=" ")
+                if vals.size != count:
+                    raise ValueError(f"malformed real array in FCHK: {label}")
+                rec[label] = vals
         else:
             rec[label] = conv(meta[1])
     return rec

@@ -68,3 +68,39 @@ def test_noalloc_needs_resident_molecule_and_density_properties():
     assert "device copy" in str(e.value)
     with pytest.raises(K.InvalidArgument):
         K.evaluate_points_noalloc(m, pts.data_ptr(), 4, [K.orbital(3)], [out.data_ptr()])
+
+
+def test_noalloc_unrestricted_two_channels():
+    # O2 (triplet, unrestricted): the alpha and beta channels take separate
+    # MO passes, and the spin-difference and beta densities come from both.
+    import torch
+
+    m = K.Molecule.from_fchk(os.path.join(GOLDEN, "o2.fchk.gz"))
+    _, _, xyz = m.atoms()
+    rng = np.random.default_rng(11)
+    pts = rng.uniform(xyz.min(0) - 2.5, xyz.max(0) + 2.5, (3000, 3))
+    P, D = K.PropertyKind, K.DensityComponent
+    props = [K.density(P.Density, D.Alpha), K.density(P.Density, D.Beta), K.density(P.Density, D.Difference),
+             K.density(P.Gradient, D.Total), K.density(P.Elf, D.Total), K.density(P.Laplacian, D.Beta)]
+    dpts = torch.tensor(pts.ravel(), dtype=torch.float64, device="cuda")
+    n = len(pts)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def outputs():
+        return [torch.full((K.channels(p.kind) * n,), float("nan"), dtype=torch.float64, device="cuda")
+                for p in props]
+
+    ref = outputs()
+    K.Evaluator(m, backend=K.Backend.AO_MO).evaluate_points_device(dpts.data_ptr(), n, props,
+                                                                   [o.data_ptr() for o in ref], stream)
+    torch.cuda.synchronize()
+    for _ in range(2):
+        got = outputs()
+        K.evaluate_points_noalloc(m, dpts.data_ptr(), n, props, [o.data_ptr() for o in got], stream)
+        torch.cuda.synchronize()
+        for p, a, r in zip(props, got, ref):
+            a, r = a.cpu().numpy(), r.cpu().numpy()
+            assert np.all(np.isfinite(a)), p
+            assert scaled_error(a, r) <= 1e-12, (p, scaled_error(a, r))
+    with pytest.raises(K.InvalidArgument):
+        K.evaluate_points_noalloc(m, dpts.data_ptr(), n, props, [o.data_ptr() for o in ref[:2]], stream)
