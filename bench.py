@@ -11,8 +11,11 @@ value: grid points/s of the mixed-precision form with the molecule resident
 and outputs left in HBM (device API), max over ranks; `fp64` holds the same
 for the FP64 form.  e2e: the same metric through the host C-ABI call
 (kumo_evaluate_grid, host output arrays, device-to-host copies inside the
-timed region).  Under torchrun each rank evaluates its own copy of the
-workload (independent requests, weak scaling, no collective on the data path).
+timed region).  Under torchrun the ranks split the one grid into slabs of
+whole planes (kumo_b200.shard.slab_range), each rank evaluating its slab as a
+grid of its own; no collective on the data path (strong scaling).  At one GPU
+the run adds the unrestricted-triplet workload (`triplet`), the
+electrostatic potential (`esp`) and the serving loop (`serve`).
 """
 from __future__ import annotations
 
@@ -119,7 +122,7 @@ def cpu_baseline(fchk: str, grid, nblocks_sample: int, threads: int = 0):
     t0 = time.perf_counter()
     o.evaluate(props, points=sample, threads=threads)
     dt = time.perf_counter() - t0
-    cores = O.lib().ko_max_threads()
+    cores = threads if threads > 0 else O.lib().ko_max_threads()
     return {"value": len(sample) / dt, "unit": "grid pts/s", "cores": cores, "kind": "port",
             "sample": f"{len(pick)} evenly spaced 128-point blocks ({len(sample)} points) of the 128^3 grid, "
                       f"{dt:.1f} s"}
@@ -155,6 +158,100 @@ def run_reference(args, rank: int) -> None:
                              "sample": info["sample"]},
             "e2e": {"value": value, "unit": "grid pts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def field_errors(torch, a, r, rho, kind_positive: bool):
+    """Errors of one field (channels x points, device tensors) against FP64:
+    `scaled` = max|a - r| / max(1, max|r|) (chem-kumo's
+    tests/density_screening_test.cpp:137-150), `pointwise` = max |a - r| /
+    max(1, |a|, |r|) (tests/test_support.hpp:68-76), and for fields that are
+    positive wherever rho > 1e-6 (rho, tau, ELF, RDG, the spin densities)
+    `rel` = max |a - r| / |r| over those points."""
+    d = (a - r).abs()
+    out = {"scaled": float(d.max() / max(1.0, float(r.abs().max()))),
+           "pointwise": float((d / torch.clamp(torch.maximum(a.abs(), r.abs()), min=1.0)).max())}
+    if kind_positive:
+        m = rho > 1e-6
+        out["rel"] = float((d[:, m] / r[:, m].abs().clamp_min(1e-300)).max()) if bool(m.any()) else 0.0
+    return out
+
+
+def triplet_bench(K, synth, d: str, grid_n: int = 0, steps: int = 1, peaks=None):
+    """Unrestricted-triplet workload: C60N20O20H100 (3,700 AOs, 381 alpha and
+    379 beta electrons, seed 2), alpha, beta and spin densities, RDG and
+    sign(lambda2) rho (the full AO Hessian) on its 192^3 grid at 0.17 bohr,
+    screening threshold 1e-10; FP64 and mixed forms of the AO-MO (AUTO's
+    choice) and AO-P backends, one warm-up and `steps` timed steps each, and
+    the mixed-vs-FP64 errors per field."""
+    import torch
+    fchk = synth.workload_fchk("triplet_3700", d)
+    m = K.Molecule.from_fchk(fchk)
+    _, _, xyz = m.atoms()
+    origin, st, counts = synth.workload_grid("triplet_3700", xyz)
+    if grid_n:
+        origin = xyz.mean(axis=0) - 0.5 * st[0, 0] * (grid_n - 1)
+        counts = (grid_n,) * 3
+    grid = K.Grid(origin, st, counts)
+    n = grid.npoints
+    P, D = K.PropertyKind, K.DensityComponent
+    props = [K.density(P.Density, D.Alpha), K.density(P.Density, D.Beta), K.density(P.Density, D.Difference),
+             K.density(P.ReducedGradient), K.density(P.SignLambda2Density)]
+    names = ["rho_alpha", "rho_beta", "spin", "rdg", "sign_lambda2_rho"]
+    positive = [True, True, False, True, False]
+    stream = torch.cuda.current_stream()
+    peaks = peaks or {}
+    res = {"workload": f"triplet_3700 (C60N20O20H100, 3700 AOs, 381/379 electrons) alpha/beta/spin density, "
+                       f"RDG, sign(lambda2)rho on {counts[0]}^3 @0.17 bohr, threshold 1e-10",
+           "points": n}
+    for backend in (K.Backend.AO_MO, K.Backend.AO_P):
+        outs = {}
+        for prec in (K.Precision.FP64, K.Precision.Mixed):
+            ev = K.Evaluator(m, backend=backend, threshold=1e-10, precision=prec)
+            out = torch.empty(5 * n, dtype=torch.float64, device="cuda")
+            ptrs = [out.data_ptr() + 8 * i * n for i in range(5)]
+            used = ev.evaluate_grid_device(grid, props, ptrs, stream.cuda_stream)  # warm-up
+            assert used == int(backend)
+            torch.cuda.synchronize()
+            K.profile_reset()
+            K.profile_enable(True)
+            ts = []
+            for _ in range(steps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                ev.evaluate_grid_device(grid, props, ptrs, stream.cuda_stream)
+                e1.record(stream)
+                ts.append((e0, e1))
+            torch.cuda.synchronize()
+            ms = float(np.mean([a.elapsed_time(b) for a, b in ts]))
+            prof = K.profile_read()
+            K.profile_enable(False)
+            kern = {k: {"launches": v["launches"], "ms": round(v["ms"], 3)} for k, v in prof.items() if v["launches"]}
+            ck = "contract_p" if backend == K.Backend.AO_P else (
+                "contract_mixed" if prec == K.Precision.Mixed else "contract_mo_f64")
+            entry = {"ms_per_step": ms, "pts_per_s": n / (ms * 1e-3), "kernels": kern}
+            c = prof.get(ck, {})
+            if c.get("launches"):
+                tf = c["flops"] / (c["ms"] * 1e-3) / 1e12
+                if prec == K.Precision.Mixed:
+                    peak, unit = peaks.get("bf16_tflops", 1590.0), "bf16 TFLOP/s (measured burst peak)"
+                else:
+                    peak, unit = 37.0, "FP64 TFLOP/s (nominal B200 FP64 peak)"
+                entry["roofline"] = {"kernel": ck, "achieved_tflops": tf, "peak": peak, "peak_unit": unit,
+                                     "frac": tf / peak,
+                                     "algorithmic": ("2 * m_kept^2 * 4 * 128 per block and density matrix"
+                                                     if backend == K.Backend.AO_P else
+                                                     "2 * 128 * 10 panels * m_kept * (n_alpha + n_beta) per block")}
+            res[f"{backend.name}_{prec.name}"] = entry
+            outs[prec] = out
+        f64, mix = outs[K.Precision.FP64], outs[K.Precision.Mixed]
+        rho = f64[:n] + f64[n:2 * n]
+        res[f"{backend.name}_mixed_vs_fp64"] = {
+            name: field_errors(torch, mix[i * n:(i + 1) * n].view(1, n), f64[i * n:(i + 1) * n].view(1, n), rho, pos)
+            for i, (name, pos) in enumerate(zip(names, positive))}
+        res[f"{backend.name}_mixed_over_fp64"] = (res[f"{backend.name}_FP64"]["ms_per_step"] /
+                                                  res[f"{backend.name}_Mixed"]["ms_per_step"])
+        del outs, f64, mix
+    return res
 
 
 def serve_bench(K, synth, precision: int, seconds: float, rate: float, pool, seed: int, graph_points: int = 65536,
@@ -373,6 +470,10 @@ def main() -> None:
     ap.add_argument("--esp-only", action="store_true", help="run the electrostatic-potential measurement only")
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="time one form only (small profiling cases)")
+    ap.add_argument("--no-triplet", action="store_true", help="skip the unrestricted-triplet workload")
+    ap.add_argument("--triplet-only", action="store_true", help="run the unrestricted-triplet workload only")
+    ap.add_argument("--triplet-grid-n", type=int, default=0, help="points per axis of the triplet grid (default 192)")
+    ap.add_argument("--triplet-steps", type=int, default=1, help="timed steps of each triplet variant")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -405,7 +506,12 @@ def main() -> None:
         spacing = steps[0, 0]
         origin = xyz.mean(axis=0) - 0.5 * spacing * (args.grid_n - 1)
         counts = (args.grid_n,) * 3
-    grid = K.Grid(origin, steps, counts)
+    from kumo_b200 import shard
+    n_total = int(np.prod(counts))
+    # One grid over the ranks: each rank evaluates its slab of whole planes.
+    i0, i1 = shard.slab_range(counts, rank, world)
+    s_origin, s_steps, s_counts = shard.slab_grid(origin, steps, counts, i0, i1)
+    grid = K.Grid(s_origin, s_steps, s_counts)
     n = grid.npoints
     props = _props(K)
     nchan = sum(K.channels(p.kind) for p in props)
@@ -435,14 +541,16 @@ def main() -> None:
         torch.cuda.synchronize()
         return [a.elapsed_time(b) for a, b in times]
 
-    from kumo_b200 import shard
-
     def max_over_ranks(x: float) -> float:
         return shard.max_over_ranks(x, dist, world, device="cuda")
 
     if args.esp_only:
         if rank == 0:
             print(json.dumps(esp_bench(K, synth, d)))
+        return
+    if args.triplet_only:
+        if rank == 0:
+            print(json.dumps(triplet_bench(K, synth, d, args.triplet_grid_n, args.triplet_steps, _peaks()[0])))
         return
     if args.serve_only:
         pool, _ = serving_pool(K, synth, args.serve_pool, args.serve_max_atoms)
@@ -482,15 +590,17 @@ def main() -> None:
     prof = K.profile_read()
     K.profile_enable(False)
     ms_mixed = max_over_ranks(float(np.mean(t_mixed)))
-    # Accuracy of the last mixed step against FP64 (scaled metric per field).
+    # Accuracy of the last mixed step against FP64, per field.
     acc = {}
     off = 0
     names = ["rho", "grad_rho", "lap_rho", "tau", "elf"]
-    for p, name in zip(props, names):
-        c = K.channels(p.kind) * n
-        a, r = out[off:off + c], ref[off:off + c]
-        acc[name] = float((a - r).abs().max() / max(1.0, float(r.abs().max())))
-        off += c
+    positive = [True, False, False, True, True]
+    rho_ref = ref[:n].view(1, n)
+    for p, name, pos in zip(props, names, positive):
+        c = K.channels(p.kind)
+        a, r = out[off:off + c * n].view(c, n), ref[off:off + c * n].view(c, n)
+        acc[name] = field_errors(torch, a, r, rho_ref[0], pos)
+        off += c * n
 
     if world > 1:
         dist.barrier()
@@ -511,9 +621,12 @@ def main() -> None:
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(float(np.median(e2e_times)) if e2e_times else float("nan"))
 
-    esp_line = None if args.no_esp else esp_bench(K, synth, d)
+    # The other workloads run at one GPU only (their own single-device measurements).
+    esp_line = None if (args.no_esp or world > 1) else esp_bench(K, synth, d)
+    triplet = None if (args.no_triplet or world > 1) else triplet_bench(K, synth, d, args.triplet_grid_n,
+                                                                          args.triplet_steps, _peaks()[0])
     serve = None
-    if args.serve_seconds > 0:
+    if args.serve_seconds > 0 and world == 1:
         pool, sizes = serving_pool(K, synth, args.serve_pool, args.serve_max_atoms)
         kw = dict(graph_points=args.serve_graph_points, scratch_gb=args.serve_scratch_gb)
         serve = {"config": {"arrivals": f"Poisson {args.serve_rate:g}/s for {args.serve_seconds:g} s (seeded)",
@@ -554,7 +667,7 @@ def main() -> None:
                    if v["launches"]}
         launches = sum(v["launches"] for v in prof.values())
         launches += 2 * prof["ao_build"]["launches"]  # kept-row counters of the profiler
-        value = world * n / (ms_mixed * 1e-3)
+        value = n_total / (ms_mixed * 1e-3)
         line = {
             "metric": METRIC,
             "value": value,
@@ -564,19 +677,21 @@ def main() -> None:
             "warmup": args.warmup,
             "ms_per_step": ms_mixed,
             "higher_is_better": True,
-            "scaling": "weak",
+            "scaling": "strong",
             "vs_baseline": None,
-            "dtype": "mixed: f32 AO values + f32 products, f64 reductions/fields",
+            "dtype": "mixed: f32 AO values and split-bf16 tensor-core products (f32 accumulation), "
+                     "f64 exact rows, reductions and fields",
             "data": "synthetic (seeded FCHK)",
             "config": {"workload": "organic_740 (C12N4O4H20, 740 AOs, 76 occ MOs) rho/grad/lap/tau/ELF on 128^3 @0.2 bohr",
-                       "points_per_gpu": n, "backend": "AO_MO", "block": 128, "threshold": 1e-12,
+                       "points": n_total, "points_rank0": n, "backend": "AO_MO", "block": 128,
+                       "threshold": 1e-12, "exact_rows": int(os.environ.get("KUMO_MIXED_EXACT_ROWS", "64")),
                        "l2": "256 MB buffer written between timed steps (untimed); AO scratch > L2",
-                       "parallelism": f"replicas x{world} (weak)"},
-            "fp64": {"value": world * n / (ms_f64 * 1e-3), "ms_per_step": ms_f64},
+                       "parallelism": f"slabs of whole planes x{world} (one grid, strong)"},
+            "fp64": {"value": n_total / (ms_f64 * 1e-3), "ms_per_step": ms_f64},
             "mixed_over_fp64": ms_f64 / ms_mixed,
-            "mixed_vs_fp64_scaled_error": acc,
-            "e2e": {"value": world * n / e2e_s, "unit": "grid pts/s", "h2d_bytes_per_step": 108,
-                    "d2h_bytes_per_step": nchan * n * 8},
+            "mixed_vs_fp64_error": acc,
+            "e2e": {"value": n_total / e2e_s, "unit": "grid pts/s", "h2d_bytes_per_step": 108,
+                    "d2h_bytes_per_step": nchan * n_total * 8},
             "roofline": roof,
             "kernels": kernels,
             "gpu_launches": launches,
@@ -586,8 +701,12 @@ def main() -> None:
             line["serve"] = serve
         if esp_line is not None:
             line["esp"] = esp_line
+        if triplet is not None:
+            line["triplet"] = triplet
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(fchk, grid, args.cpu_blocks)
+            whole = K.Grid(origin, steps, counts)
+            line["cpu_baseline"] = cpu_baseline(fchk, whole, args.cpu_blocks)
+            line["cpu_baseline_1_thread"] = cpu_baseline(fchk, whole, max(16, args.cpu_blocks // 32), threads=1)
         print(json.dumps(line))
     if world > 1:
         dist.barrier()

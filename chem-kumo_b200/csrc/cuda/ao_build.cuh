@@ -261,9 +261,9 @@ __global__ void __launch_bounds__(kBlockPoints, sizeof(T) == 8 ? 3 : 5) ao_build
     const int blk = blockIdx.x;
     if (blk >= prm.nblocks) return;
     const int j = threadIdx.x, warp = j >> 5, lane = j & 31;
-    const long long start = prm.first_point + (long long)blk * prm.block_size;
-    long long b = prm.src.count - start;
-    if (b > prm.block_size) b = prm.block_size;
+    long long start, b;
+    int sblock;
+    cta_points(prm.first_point, prm.block_size, prm.screen_block, prm.src.count, blk, start, b, sblock);
     const bool valid = j < b;
     double px = 0, py = 0, pz = 0;
     if (valid) point_at(prm.src, start + j, px, py, pz);
@@ -331,6 +331,15 @@ __global__ void __launch_bounds__(kBlockPoints, sizeof(T) == 8 ? 3 : 5) ao_build
             T mx = s_red[buf][0][m];
 #pragma unroll
             for (int w = 1; w < NW; ++w) mx = s_red[buf][w][m] > mx ? s_red[buf][w][m] : mx;
+            if (prm.mask_pass == 1) {
+                // Non-negative doubles order like their bit patterns.
+                if (j == 0 && mx > (T)0)
+                    atomicMax(reinterpret_cast<unsigned long long*>(prm.block_max) +
+                                  (size_t)sblock * B.nao + inf.w + m,
+                              static_cast<unsigned long long>(__double_as_longlong(static_cast<double>(mx))));
+                continue;
+            }
+            if (prm.mask_pass == 2) mx = (T)prm.block_max[(size_t)sblock * B.nao + inf.w + m];
             if (!(keep_all || mx > thr)) continue;
 #pragma unroll
             for (int c = 0; c < P; ++c)

@@ -26,7 +26,7 @@ __global__ void __launch_bounds__(kBlockPoints, (P == 10 || MAXL >= 4) ? 6 : 8) 
     const long long start = prm.first_point + static_cast<long long>(blk) * prm.block_size;
     long long bcount = prm.src.count - start;
     if (bcount > prm.block_size) bcount = prm.block_size;
-    const bool valid = j < bcount;
+    const bool valid = j < bcount && point_exists(prm.src, start + j);
     double px = 0, py = 0, pz = 0;
     if (valid) point_at(prm.src, start + j, px, py, pz);
 

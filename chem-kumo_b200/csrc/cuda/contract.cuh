@@ -23,7 +23,8 @@ struct MoChannel {
 struct ContractMoParams {
     AoScratch<double> scr;
     long long first_point = 0;
-    long long block_size = 128;
+    long long block_size = 128;   // points per CTA chunk (see cta_points)
+    long long screen_block = 0;   // points per screening block (0: block_size)
     long long count = 0;
     int nblocks = 0;
     int nchannels = 0;
@@ -58,7 +59,8 @@ struct OrbitalParams {
 struct ContractPParams {
     AoScratch<double> scr;
     long long first_point = 0;
-    long long block_size = 128;
+    long long block_size = 128;   // points per CTA chunk (see cta_points)
+    long long screen_block = 0;   // points per screening block (0: block_size)
     long long count = 0;
     int nblocks = 0;
     int nao = 0;
@@ -84,6 +86,7 @@ struct OrbitalEnergyParams {
     AoScratch<double> scr;  // values, threshold 0 (every AO of the shells reaching the block), AO order
     long long first_point = 0;
     long long block_size = 128;
+    long long screen_block = 0;  // unused: no screening (see cta_points)
     long long count = 0;
     int nblocks = 0;
     const double* w = nullptr;           // [nao][ldw]: the sets' columns, each set padded to 128-column chunks

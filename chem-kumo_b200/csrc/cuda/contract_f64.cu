@@ -103,9 +103,9 @@ __global__ void __launch_bounds__(256, 1) contract_mo_f64_kernel(const __grid_co
 
     const int blk = blockIdx.x >> 2;
     const int j0 = (blockIdx.x & 3) * 32;
-    const long long start = prm.first_point + (long long)blk * prm.block_size;
-    long long b = prm.count - start;
-    if (b > prm.block_size) b = prm.block_size;
+    long long start, b;
+    int sblock_unused;
+    cta_points(prm.first_point, prm.block_size, prm.screen_block, prm.count, blk, start, b, sblock_unused);
     if (j0 >= b) return;
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     const AoScratch<double>& scr = prm.scr;
@@ -251,9 +251,9 @@ __global__ void __launch_bounds__(256, 1) orbital_energy_f64_kernel(const __grid
 
     const int blk = blockIdx.x >> 2;
     const int j0 = (blockIdx.x & 3) * 32;
-    const long long start = prm.first_point + (long long)blk * prm.block_size;
-    long long b = prm.count - start;
-    if (b > prm.block_size) b = prm.block_size;
+    long long start, b;
+    int sblock_unused;
+    cta_points(prm.first_point, prm.block_size, prm.screen_block, prm.count, blk, start, b, sblock_unused);
     if (j0 >= b) return;
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     const AoScratch<double>& scr = prm.scr;
@@ -434,9 +434,9 @@ __global__ void __launch_bounds__(256, 1) contract_p_f64_kernel(const __grid_con
 
     const int blk = blockIdx.x >> 2;
     const int j0 = (blockIdx.x & 3) * 32;
-    const long long start = prm.first_point + (long long)blk * prm.block_size;
-    long long b = prm.count - start;
-    if (b > prm.block_size) b = prm.block_size;
+    long long start, b;
+    int sblock_unused;
+    cta_points(prm.first_point, prm.block_size, prm.screen_block, prm.count, blk, start, b, sblock_unused);
     if (j0 >= b) return;
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     const AoScratch<double>& scr = prm.scr;

@@ -175,6 +175,8 @@ __global__ void __launch_bounds__(kCtaThreads<S>, 1) contract_mixed_kernel(const
     bool sorted = false;
     nk = block_row_order(scr.rowmax ? scr.rowmax + static_cast<size_t>(blk) * scr.row_stride * 4 : nullptr, nk,
                          prm.threshold, perm, bucket_start, keys, sorted);
+    // The rows kept above the threshold (read back by the profiler).
+    if (threadIdx.x == 0) scr.nkept[blk] = nk;
     // AO index of each K row, in K order, so that the coefficient gathers
     // need no dependent global load (blocks of up to kSortCap rows and
     // bases below 65536 functions; others read the kept list).
@@ -498,6 +500,87 @@ __global__ void __launch_bounds__(kCtaThreads<S>, 1) contract_mixed_kernel(const
 }
 
 // ---------------------------------------------------------------------------
+// FP64 AO rows of the exact rows (the largest rows of a block, added in FP64
+// in the epilogue of the bulk-copy kernel).
+
+__device__ __forceinline__ double ipow(double x, int n) {
+    double r = 1.0;
+    for (int i = 0; i < n; ++i) r *= x;
+    return r;
+}
+
+// AO block (shell) holding AO `ao`: the last block whose first AO is <= ao.
+__device__ __forceinline__ int ao_block_of(const DevBasis& B, int ao) {
+    int lo = 0, hi = B.nblocks - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (B.info[mid].w <= ao)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// FP64 value, and for P >= 4 the gradient, for P == 5 the Laplacian, of AO
+// m of AO block s at offset (dx, dy, dz) from the block's centre, in closed
+// form: with R_n,k = sum_p W[k][p] a_p^n exp(-a_p r^2) and M_k the monomial of
+// Cartesian component k (Gaussian order), value = sum_k T[m][k] M_k R_0,k,
+// d/dx = sum_k T[m][k] (dM_k/dx R_0,k - 2 x M_k R_1,k) and Laplacian =
+// sum_k T[m][k] (lap(M_k) R_0,k + M_k (4 r^2 R_2,k - (4 l + 6) R_1,k)) (T the
+// identity for Cartesian blocks).  The same functions as the reference's
+// evaluate_derivatives_batch (src/basis_evaluator.cpp:512-643), rounded
+// differently; zero beyond the block's cutoff radius, as there.
+template <int P>
+__device__ void exact_ao(const DevBasis& B, const double (&pure)[3][135], int s, int m, double dx, double dy,
+                         double dz, double (&out)[P]) {
+#pragma unroll
+    for (int c = 0; c < P; ++c) out[c] = 0.0;
+    const double4 o = B.origin_r2[s];
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 > o.w) return;
+    const int4 inf = B.info[s];
+    const int l = inf.x & 0xff, nprim = inf.x >> 16;
+    const bool is_pure = ((inf.x >> 8) & 1) && l >= 2;
+    const int ncart = (l + 1) * (l + 2) / 2;
+    double e[kMaxPrim], al[kMaxPrim];
+    for (int q = 0; q < nprim; ++q) {
+        al[q] = B.exps[inf.y + q];
+        e[q] = exp(-al[q] * r2);
+    }
+    const double* W = B.weights + inf.z;
+    for (int k = 0; k < ncart; ++k) {
+        const double t = is_pure ? pure[l - 2][m * ncart + k] : (k == m ? 1.0 : 0.0);
+        if (t == 0.0) continue;
+        double R0 = 0.0, R1 = 0.0, R2 = 0.0;
+        for (int q = 0; q < nprim; ++q) {
+            const double we = W[k * nprim + q] * e[q];
+            R0 += we;
+            R1 += we * al[q];
+            R2 += we * (al[q] * al[q]);
+        }
+        const int a = cart_power(l, k, 0), b = cart_power(l, k, 1), c = cart_power(l, k, 2);
+        const double xa = ipow(dx, a), yb = ipow(dy, b), zc = ipow(dz, c);
+        const double M = xa * yb * zc;
+        out[0] += t * (M * R0);
+        if constexpr (P >= 4) {
+            const double mx = a ? a * ipow(dx, a - 1) * yb * zc : 0.0;
+            const double my = b ? b * xa * ipow(dy, b - 1) * zc : 0.0;
+            const double mz = c ? c * xa * yb * ipow(dz, c - 1) : 0.0;
+            out[1] += t * (mx * R0 - 2.0 * dx * M * R1);
+            out[2] += t * (my * R0 - 2.0 * dy * M * R1);
+            out[3] += t * (mz * R0 - 2.0 * dz * M * R1);
+        }
+        if constexpr (P == 5) {
+            const double lap = (a > 1 ? a * (a - 1) * ipow(dx, a - 2) * yb * zc : 0.0) +
+                               (b > 1 ? b * (b - 1) * xa * ipow(dy, b - 2) * zc : 0.0) +
+                               (c > 1 ? c * (c - 1) * xa * yb * ipow(dz, c - 2) : 0.0);
+            out[4] += t * (lap * R0 + M * (4.0 * r2 * R2 - (4.0 * l + 6.0) * R1));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Bulk-copy form (P = 1, 4, 5; two AO stages): a tenth warp fetches the FP32
 // rows of each K step into shared memory with the tensor-memory-access unit
 // (one tiled copy per kept row of a 4-D map [block][panel][row][point] with a
@@ -585,18 +668,23 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
     bool sorted = false;
     nk = block_row_order(scr.rowmax ? scr.rowmax + static_cast<size_t>(blk) * scr.row_stride * 4 : nullptr, nk,
                          prm.threshold, perm, bucket_start, keys, sorted, static_cast<int>(cap));
+    // The rows kept above the threshold (read back by the profiler).
+    if (threadIdx.x == 0) scr.nkept[blk] = nk;
     for (int k = tid; producer && k < nk; k += kThreads) aoidx[k] = static_cast<std::uint16_t>(kept[sorted ? perm[k] : k]);
     // The last nx rows of the K order (the largest block maxima) are added in
-    // FP64 in the epilogue instead of on the tensor cores: the truncation of
-    // each MMA's FP32 sum is relative to its largest product, so taking the
-    // largest products out of the MMAs lowers the error of every output.
-    // At most as many rows as the idle stages hold during the epilogue: AO
-    // values in the AO stages (2 * 3 * P * 4096 bytes = 48 rows of P * 512),
-    // coefficients in the coefficient stages (SB * 96 * N bytes = 12 * SB rows
-    // of N doubles).
-    constexpr int kExactCap = 12 * SB < 48 ? 12 * SB : 48;
+    // FP64 in the epilogue instead of on the tensor cores, with AO values
+    // computed there in FP64: the truncation of each MMA's FP32 sum is
+    // relative to its largest product and FP32 AO values carry 2^-24 relative
+    // errors, so taking the largest terms out of both lowers the error of
+    // every output.  The epilogue stages them in the idle stages (AO, row and
+    // coefficient stages, one contiguous region): the pass's coefficient
+    // columns [row][N] and the AO values [row][panel][point] of the points of
+    // one phase (128, 64 or 32 points: as many as fit).
+    const unsigned xs_bytes = 2u * L::a_bytes + F * L::f_bytes + SB * b_bytes;
+    auto xs_need = [&](int rows, int ph) { return 8u * static_cast<unsigned>(rows) * (N + P * ph + 1); };
     int nx = prm.exact_rows < nk ? prm.exact_rows : nk;
-    if (nx > kExactCap) nx = kExactCap;
+    while (nx > 0 && xs_need(nx, 32) > xs_bytes) --nx;
+    const int ph_points = xs_need(nx, 128) <= xs_bytes ? 128 : (xs_need(nx, 64) <= xs_bytes ? 64 : 32);
     const int nkt = nk - nx;
     const int ntiles = (nkt + 15) / 16;
     tc_fence_before();
@@ -779,19 +867,16 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                 break;
             }
             tc_fence_after();
-            // Stage the exact rows in the stages no MMA reads any more: AO
-            // values [row][panel][point] (FP32) and this pass's coefficient
-            // columns [row][column] (FP64, zero past the padded row).
-            float* xs_phi = reinterpret_cast<float*>(a_st);
-            double* xs_c = reinterpret_cast<double*>(b_st);
+            const int nvalid = ch.nocc - n0 < N ? ch.nocc - n0 : N;
+            // Warps 8 and 9 (half 2) read no accumulators.
+            const int i_lo = half * (N / 2), i_hi = min(nvalid, (half + 1) * (N / 2));
+            const unsigned lane_addr = tmem + (static_cast<unsigned>(quarter * 32) << 16);
+            const int ng = ntiles < G ? ntiles : G;
+            constexpr int MG = 4;
+            double* xs_c = reinterpret_cast<double*>(sm);
+            double* xs_phi = xs_c + nx * N;
+            int* xs_row = reinterpret_cast<int*>(xs_phi + nx * P * ph_points);
             if (nx > 0) {
-                for (int v = tid; v < nx * P * 32; v += kBulkThreads) {
-                    const int r = v / (P * 32), rem = v - r * (P * 32), c = rem >> 5, q4 = rem & 31;
-                    const int slot = sorted ? static_cast<int>(perm[nkt + r]) : nkt + r;
-                    const float4 f = *reinterpret_cast<const float4*>(
-                        scr.panels + ((static_cast<size_t>(blk) * P + c) * scr.row_stride + slot) * kBlockPoints + q4 * 4);
-                    *reinterpret_cast<float4*>(xs_phi + (r * P + c) * kBlockPoints + q4 * 4) = f;
-                }
                 const int half_n = N / 2;
                 for (int v = tid; v < nx * half_n; v += kBulkThreads) {
                     const int r = v / half_n, j = v - r * half_n;
@@ -801,48 +886,76 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                         cv = *reinterpret_cast<const double2*>(ch.c64 + static_cast<long long>(aoidx[nkt + r]) * ch.ld64 + col);
                     *reinterpret_cast<double2*>(xs_c + r * N + 2 * j) = cv;
                 }
+                for (int r = tid; r < nx; r += kBulkThreads) {
+                    const int ao = static_cast<int>(aoidx[nkt + r]);
+                    const int sh = ao_block_of(prm.basis, ao);
+                    xs_row[2 * r] = sh;
+                    xs_row[2 * r + 1] = ao - prm.basis.info[sh].w;
+                }
                 __syncthreads();
             }
-            const int nvalid = ch.nocc - n0 < N ? ch.nocc - n0 : N;
-            // Warps 8 and 9 (half 2) read no accumulators.
-            const int i_lo = half * (N / 2), i_hi = min(nvalid, (half + 1) * (N / 2));
-            const unsigned lane_addr = tmem + (static_cast<unsigned>(quarter * 32) << 16);
-            const int ng = ntiles < G ? ntiles : G;
-            constexpr int MG = 4;
-            for (int i0 = i_lo; i0 < i_hi; i0 += MG) {
-                double x[P][MG];
+            for (int ph0 = 0; ph0 < kBlockPoints; ph0 += ph_points) {
+                if (nx > 0) {
+                    // FP64 AO values of the exact rows at this phase's points.
+                    for (int v = tid; v < nx * ph_points; v += kBulkThreads) {
+                        const int r = v / ph_points, pp = v - r * ph_points;
+                        const long long e = start + ph0 + pp;
+                        double f[P];
+                        if (ph0 + pp < bcount && point_exists(prm.src, e)) {
+                            double x, y, z;
+                            point_at(prm.src, e, x, y, z);
+                            const int sh = xs_row[2 * r];
+                            const double4 o = prm.basis.origin_r2[sh];
+                            exact_ao<P>(prm.basis, prm.pure64, sh, xs_row[2 * r + 1], x - o.x, y - o.y, z - o.z, f);
+                        } else {
 #pragma unroll
-                for (int c = 0; c < P; ++c)
+                            for (int c = 0; c < P; ++c) f[c] = 0.0;
+                        }
 #pragma unroll
-                    for (int u = 0; u < MG; ++u) x[c][u] = 0.0;
-                for (int gi = 0; gi < ng; ++gi) {
-                    unsigned v[P][MG];
+                        for (int c = 0; c < P; ++c) xs_phi[(r * P + c) * ph_points + pp] = f[c];
+                    }
+                    __syncthreads();
+                }
+                if (point >= ph0 && point < ph0 + ph_points) {
+                    const int pq = point - ph0;
+                    for (int i0 = i_lo; i0 < i_hi; i0 += MG) {
+                        double x[P][MG];
 #pragma unroll
-                    for (int c = 0; c < P; ++c)
-                        tmem_ld<MG>(lane_addr + static_cast<unsigned>(gi) * gcols + static_cast<unsigned>(c * N + i0), v[c]);
-                    tmem_wait_ld();
+                        for (int c = 0; c < P; ++c)
 #pragma unroll
-                    for (int c = 0; c < P; ++c) {
-                        reg_fence<MG>(v[c]);
+                            for (int u = 0; u < MG; ++u) x[c][u] = 0.0;
+                        for (int gi = 0; gi < ng; ++gi) {
+                            unsigned v[P][MG];
 #pragma unroll
-                        for (int u = 0; u < MG; ++u) x[c][u] += static_cast<double>(__uint_as_float(v[c][u]));
+                            for (int c = 0; c < P; ++c)
+                                tmem_ld<MG>(lane_addr + static_cast<unsigned>(gi) * gcols + static_cast<unsigned>(c * N + i0),
+                                            v[c]);
+                            tmem_wait_ld();
+#pragma unroll
+                            for (int c = 0; c < P; ++c) {
+                                reg_fence<MG>(v[c]);
+#pragma unroll
+                                for (int u = 0; u < MG; ++u) x[c][u] += static_cast<double>(__uint_as_float(v[c][u]));
+                            }
+                        }
+                        // The exact rows: FP64 AO values times FP64 coefficients.
+                        for (int r = 0; r < nx; ++r) {
+                            const double* crow = xs_c + r * N + i0;
+                            double cv[MG];
+#pragma unroll
+                            for (int u = 0; u < MG; ++u) cv[u] = crow[u];
+#pragma unroll
+                            for (int c = 0; c < P; ++c) {
+                                const double f = xs_phi[(r * P + c) * ph_points + pq];
+#pragma unroll
+                                for (int u = 0; u < MG; ++u) x[c][u] += f * cv[u];
+                            }
+                        }
+                        fold<P, MG>(x, q, i_hi - i0);
                     }
                 }
-                // The exact rows: FP32 AO values times FP64 coefficients,
-                // accumulated in FP64, from the staged copies.
-                for (int r = 0; r < nx; ++r) {
-                    const double* crow = xs_c + r * N + i0;
-                    double cv[MG];
-#pragma unroll
-                    for (int u = 0; u < MG; ++u) cv[u] = crow[u];
-#pragma unroll
-                    for (int c = 0; c < P; ++c) {
-                        const double f = static_cast<double>(xs_phi[(r * P + c) * kBlockPoints + point]);
-#pragma unroll
-                        for (int u = 0; u < MG; ++u) x[c][u] += f * cv[u];
-                    }
-                }
-                fold<P, MG>(x, q, i_hi - i0);
+                // The next phase overwrites the staged AO values.
+                if (nx > 0) __syncthreads();
             }
             tc_fence_before();
             __syncthreads();
@@ -962,7 +1075,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_fused_kernel(const __gri
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     const int pj = tid & 127;          // this thread's point in the production
     const int phalf = tid >> 7;        // which alternate shells it builds
-    const bool pvalid = pj < bcount;
+    const bool pvalid = pj < bcount && point_exists(ap.src, start + pj);
     double px = 0.0, py = 0.0, pz = 0.0;
     if (pvalid) point_at(ap.src, start + pj, px, py, pz);
 

@@ -102,6 +102,8 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
     bool sorted = false;
     nk = block_row_order(scr.rowmax ? scr.rowmax + static_cast<size_t>(blk) * scr.row_stride * 4 : nullptr, nk,
                          prm.threshold, perm, bucket_start, keys, sorted);
+    // The rows kept above the threshold (read back by the profiler).
+    if (threadIdx.x == 0) scr.nkept[blk] = nk;
     const int ntiles = (nk + 15) / 16;
     tc_fence_before();
     __syncthreads();

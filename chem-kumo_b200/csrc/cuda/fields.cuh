@@ -5,6 +5,8 @@
 
 #include <cuda_runtime.h>
 
+#include "kumo_device.cuh"
+
 namespace kumo_dev {
 
 constexpr int kMaxProps = 40;
@@ -49,6 +51,7 @@ struct FieldSpec {
     long long stride = 0;       // points per output component array
     long long out_base = 0;     // global index of the point stored at out[0]
     OutProp props[kMaxProps];
+    GridTiles tiles;            // evaluation index -> grid index (see GridTiles)
 };
 
 __device__ __forceinline__ double fermi_constant() {
@@ -173,6 +176,7 @@ __device__ inline double dev_dori(const DevDD& d) {
 // store_block(), src/evaluator.cpp:248-353, for one point.  comp[c] is the
 // record of DensityComponent c (Total, Alpha, Beta, Difference).
 __device__ inline void store_point(const FieldSpec& spec, const DevDD* comp, long long q) {
+    if (spec.tiles.on && !tile_to_linear(spec.tiles, q, q)) return;  // tile padding
     const long long p = q - spec.out_base;
     const long long S = spec.stride;
     for (int i = 0; i < spec.nprops; ++i) {

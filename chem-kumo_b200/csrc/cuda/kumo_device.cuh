@@ -45,6 +45,21 @@ struct DevBasis {
     const float* weights_f = nullptr;
 };
 
+// Compact tiles of a grid.  With `on`, evaluation index e does not follow the
+// grid's linear order: block e / 128 is tile number e / 128 of ta x tb x tc
+// points (ta = 2^sa along i, tb = 2^sb along j, tc = 2^sc along k, product
+// 128), tiles numbered with k fastest and i slowest, and e % 128 numbers the
+// points inside the tile with k fastest.  Indices of a partial tile that fall
+// outside the grid are padding: no point, nothing stored.  The mixed form
+// evaluates grids this way, so that each 128-point block is a small box whose
+// largest AO rows dominate at all of its points.
+struct GridTiles {
+    int on = 0;
+    int sa = 0, sb = 0, sc = 0;
+    long long nx = 0, ny = 0, nz = 0;  // grid counts
+    long long tny = 0, tnz = 0;        // tiles along j and k
+};
+
 // Source of the evaluation points: a regular grid (generated in the kernel)
 // or an explicit 3 x N array (x, y, z per point).
 struct PointSource {
@@ -52,12 +67,65 @@ struct PointSource {
     double origin[3] = {0, 0, 0};
     double steps[9] = {0};           // column a = step vector of axis a
     long long ny = 1, nz = 1;
-    long long count = 0;
+    long long count = 0;             // evaluation indices (tiles * 128 when tiled)
+    GridTiles tiles;
 };
 
 #ifdef __CUDACC__
+// Linear grid index of evaluation index e of a tiled grid; false for padding.
+__device__ __forceinline__ bool tile_to_linear(const GridTiles& t, long long e, long long& q) {
+    const long long tile = e >> 7;
+    const int w = static_cast<int>(e & 127);
+    const long long tk = tile % t.tnz, rest = tile / t.tnz;
+    const long long tj = rest % t.tny, ti = rest / t.tny;
+    const int wk = w & ((1 << t.sc) - 1), wj = (w >> t.sc) & ((1 << t.sb) - 1), wi = w >> (t.sb + t.sc);
+    const long long i = (ti << t.sa) + wi, j = (tj << t.sb) + wj, k = (tk << t.sc) + wk;
+    if (i >= t.nx || j >= t.ny || k >= t.nz) return false;
+    q = (i * t.ny + j) * t.nz + k;
+    return true;
+}
+
+// Whether evaluation index q is a point (not past the end, not tile padding).
+__device__ __forceinline__ bool point_exists(const PointSource& s, long long q) {
+    if (q >= s.count) return false;
+    if (!s.tiles.on) return true;
+    long long lin;
+    return tile_to_linear(s.tiles, q, lin);
+}
+
+// Points of CTA `blk` of a wave whose first point is `first` (the start of a
+// screening block).  Screening blocks have `screen` points (0: `chunk`); a
+// CTA takes at most `chunk` (<= 128) points, so a larger screening block is
+// split into ceil(screen / chunk) chunks and CTA blk takes chunk
+// blk % chunks of screening block blk / chunks.  On return [start, start + n)
+// are the CTA's points (n <= 0 past the last point) and sblock is the
+// screening block's index in the wave.
+__device__ __forceinline__ void cta_points(long long first, long long chunk, long long screen, long long count, int blk,
+                                           long long& start, long long& n, int& sblock) {
+    if (screen <= chunk) {
+        sblock = blk;
+        start = first + static_cast<long long>(blk) * chunk;
+        n = count - start < chunk ? count - start : chunk;
+        return;
+    }
+    const long long per = (screen + chunk - 1) / chunk;
+    const long long b = blk / per, c = blk - b * per;
+    sblock = static_cast<int>(b);
+    start = first + b * screen + c * chunk;
+    long long m = screen - c * chunk;
+    if (m > chunk) m = chunk;
+    if (m > count - start) m = count - start;
+    n = m;
+}
+
+// Coordinates of evaluation index q (a point: see point_exists).
 __device__ __forceinline__ void point_at(const PointSource& s, long long q, double& x, double& y,
                                          double& z) {
+    if (s.tiles.on) {
+        long long lin = 0;
+        (void)tile_to_linear(s.tiles, q, lin);
+        q = lin;
+    }
     if (s.points) {
         x = s.points[3 * q];
         y = s.points[3 * q + 1];
@@ -108,6 +176,16 @@ struct AoBuildParams {
     int keep_reaching = 0;
     AoScratch<T> out;
     T pure[3][135];                // Cartesian-to-pure matrices, l = 2..4, row-major
+    // Screening blocks larger than the `block_size` points of a CTA (see
+    // cta_points): screen_block points each (0: block_size).  Such a block
+    // is screened in two launches: mask_pass 1 stores nothing but raises
+    // block_max[sblock * nao + ao] to the largest |value| of each AO over the
+    // CTA's points (all panels of the AO order; block_max zeroed before);
+    // mask_pass 2 builds the panels and keeps the AOs whose block_max is
+    // above the threshold (src/ao_screening.hpp:35-50 over the whole block).
+    long long screen_block = 0;
+    int mask_pass = 0;
+    double* block_max = nullptr;
 };
 
 template <typename T>

@@ -42,8 +42,12 @@ struct ContractMixedParams {
     unsigned* status = nullptr;  // set nonzero if a pipeline wait ran out
     // Rows at the end of each block's K order (largest block maxima) that the
     // bulk-copy kernel adds in FP64 with ch[].c64 instead of on the tensor
-    // cores (0: all rows on the tensor cores).
+    // cores (0: all rows on the tensor cores), with their AO values computed
+    // in FP64 from the basis at the block's points.
     int exact_rows = 0;
+    PointSource src;        // the evaluation's points (for the exact rows)
+    DevBasis basis;         // FP64 exponents and weights (for the exact rows)
+    double pure64[3][135];  // Cartesian-to-pure matrices, l = 2..4, row-major
 };
 
 // AO-P form (density_derivatives_shared): Y = P[kept, kept] Phi[kept, 0..3]

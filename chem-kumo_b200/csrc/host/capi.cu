@@ -15,6 +15,7 @@
 #include "../cuda/esp.cuh"
 #include "../cuda/mixed.cuh"
 #include "grid_geometry.hpp"
+#include "chem/kumo/cube.hpp"
 #include "chem/kumo/evaluator.hpp"
 #include "chem/kumo/server.hpp"
 #include "chem/kumo/surface.hpp"
@@ -554,8 +555,8 @@ int kumo_screening_masks(const kumo_molecule* m, const kumo_grid* grid, long lon
                          double threshold, unsigned char* mask, char* err, size_t errlen) {
     return guarded(err, errlen, [&] {
         if (!m || !mask) throw std::invalid_argument("null argument");
-        if (block_size <= 0 || block_size > kumo_dev::kBlockPoints)
-            throw std::invalid_argument("block_size must be in [1, 128] for device screening masks");
+        if (block_size <= 0 || block_size > static_cast<long long>(max_block_size))
+            throw std::invalid_argument("evaluation block_size must be in [1, " + std::to_string(max_block_size) + "]");
         if (ao_order < 0 || ao_order > 2) throw std::invalid_argument("AO derivative order must be 0, 1 or 2");
         const Grid g = to_grid(grid);
         const long long n = static_cast<long long>(g.counts[0]) * g.counts[1] * g.counts[2];
@@ -569,6 +570,42 @@ int kumo_screening_masks(const kumo_molecule* m, const kumo_grid* grid, long lon
         src.nz = g.counts[2];
         src.count = n;
         const long long nblocks = (n + block_size - 1) / block_size;
+        if (block_size > kumo_dev::kBlockPoints) {
+            // Blocks above 128 points: the maximum of each AO over the whole
+            // block from chunks of 128 points (the AO build's first screening
+            // launch), compared with the threshold here.
+            const long long per = (block_size + kumo_dev::kBlockPoints - 1) / kumo_dev::kBlockPoints;
+            const long long ws = std::max<long long>(1, 256 / per);
+            DevBuf panels(sizeof(double) * static_cast<std::size_t>(npanel) * nao * kumo_dev::kBlockPoints * ws * per);
+            DevBuf kept(sizeof(int) * static_cast<std::size_t>(nao) * ws * per), nkept(sizeof(int) * ws * per);
+            DevBuf bmax(sizeof(double) * static_cast<std::size_t>(nao) * ws);
+            std::vector<double> hm(static_cast<std::size_t>(nao) * ws);
+            for (long long b0 = 0; b0 < nblocks; b0 += ws) {
+                const long long nb = std::min(ws, nblocks - b0);
+                kumo_dev::AoBuildParams<double> p{};
+                p.basis = d.basis;
+                p.src = src;
+                p.first_point = b0 * block_size;
+                p.block_size = kumo_dev::kBlockPoints;
+                p.screen_block = block_size;
+                p.nblocks = static_cast<int>(nb * per);
+                p.threshold = threshold;
+                p.out = {panels.as<double>(), kept.as<int>(), nkept.as<int>(), nao, npanel};
+                p.mask_pass = 1;
+                p.block_max = bmax.as<double>();
+                for (int l = 0; l < 3; ++l)
+                    for (int i = 0; i < 135; ++i) p.pure[l][i] = d.pure_d[l][i];
+                detail::check_cuda(cudaMemset(bmax.as<double>(), 0, sizeof(double) * nao * nb), "cudaMemset");
+                kumo_dev::launch_ao_build<double>(p, ao_order, npanel, nullptr);
+                detail::check_cuda(cudaGetLastError(), "ao_build launch");
+                detail::check_cuda(cudaMemcpy(hm.data(), bmax.as<double>(), sizeof(double) * nao * nb, cudaMemcpyDeviceToHost),
+                                   "cudaMemcpy");
+                for (long long b = 0; b < nb; ++b)
+                    for (int a = 0; a < nao; ++a)
+                        mask[(b0 + b) * nao + a] = (threshold == 0.0 || hm[static_cast<std::size_t>(b * nao + a)] > threshold) ? 1 : 0;
+            }
+            return;
+        }
         const int W = static_cast<int>(std::min<long long>(nblocks, 256));
         DevBuf panels(sizeof(double) * static_cast<std::size_t>(npanel) * nao * kumo_dev::kBlockPoints * W);
         DevBuf kept(sizeof(int) * static_cast<std::size_t>(nao) * W), nkept(sizeof(int) * W);
@@ -625,6 +662,73 @@ int kumo_write_cube(const char* path, const char* comment, const kumo_grid* grid
             f.write_orbital_cube(path, static_cast<std::size_t>(orbital_index), comment ? comment : "Molecular orbital amplitude");
         else
             f.write_cube(path, comment ? comment : "Electron density");
+    });
+}
+
+struct kumo_cube {
+    chem::kumo::CubeData data;
+};
+
+int kumo_read_cube(const char* path, kumo_cube** out, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!path || !out) throw std::invalid_argument("null argument");
+        *out = nullptr;
+        *out = new kumo_cube{read_cube(path)};
+    });
+}
+
+int kumo_cube_info(const kumo_cube* c, long long* natoms, kumo_grid* grid, int* angstrom) {
+    if (!c) return KUMO_INVALID_ARGUMENT;
+    const Grid& g = c->data.field.grid();
+    if (natoms) *natoms = static_cast<long long>(c->data.field.atoms().size());
+    if (grid) {
+        for (int k = 0; k < 3; ++k) grid->origin[k] = g.origin[k];
+        for (int i = 0; i < 9; ++i) grid->steps[i] = g.steps.m[static_cast<std::size_t>(i)];
+        for (int k = 0; k < 3; ++k) grid->counts[k] = g.counts[k];
+    }
+    if (angstrom) *angstrom = c->data.metadata.coordinates_in_angstrom ? 1 : 0;
+    return KUMO_OK;
+}
+
+int kumo_cube_data(const kumo_cube* c, int* z, double* charges, double* xyz, double* values, char* first_comment,
+                   size_t first_len, char* second_comment, size_t second_len) {
+    if (!c) return KUMO_INVALID_ARGUMENT;
+    const auto& atoms = c->data.field.atoms();
+    for (std::size_t i = 0; i < atoms.size(); ++i) {
+        if (z) z[i] = atoms[i].atomic_number;
+        if (charges) charges[i] = atoms[i].nuclear_charge;
+        if (xyz)
+            for (int k = 0; k < 3; ++k) xyz[3 * i + static_cast<std::size_t>(k)] = atoms[i].position[static_cast<std::size_t>(k)];
+    }
+    const auto& v = c->data.field.values();
+    if (values) std::memcpy(values, v.data(), sizeof(double) * v.size());
+    auto put_line = [](char* dst, size_t len, const std::string& src) {
+        if (!dst || !len) return;
+        const size_t n = std::min(len - 1, src.size());
+        std::memcpy(dst, src.data(), n);
+        dst[n] = '\0';
+    };
+    put_line(first_comment, first_len, c->data.metadata.first_comment);
+    put_line(second_comment, second_len, c->data.metadata.second_comment);
+    return KUMO_OK;
+}
+
+void kumo_cube_destroy(kumo_cube* c) { delete c; }
+
+int kumo_write_cube_data(const char* path, const char* first_comment, const char* second_comment, int angstrom,
+                         const kumo_grid* grid, long long natoms, const int* z, const double* charges, const double* xyz,
+                         const double* values, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!path || !grid || !values || natoms < 0 || (natoms > 0 && (!z || !charges || !xyz)))
+            throw std::invalid_argument("invalid cube arguments");
+        const Grid g = to_grid(grid);
+        std::vector<Atom> atoms;
+        atoms.reserve(static_cast<std::size_t>(natoms));
+        for (long long i = 0; i < natoms; ++i) atoms.push_back({z[i], charges[i], {xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]}});
+        const std::size_t n = static_cast<std::size_t>(g.counts[0]) * g.counts[1] * g.counts[2];
+        CubeData cube{Field(g, std::move(atoms), std::vector<double>(values, values + n)),
+                      {first_comment ? first_comment : "", second_comment ? second_comment : "", angstrom != 0}};
+        write_cube(cube, path);
     });
 }
 

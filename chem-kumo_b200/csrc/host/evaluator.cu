@@ -44,14 +44,14 @@ namespace {
 
 using detail::check_cuda;
 
-// Rows per block that the mixed AO-MO contraction adds in FP64 rather than
-// on the tensor cores (KUMO_MIXED_EXACT_ROWS, read at each evaluation;
-// default 16, 0 turns it off).  On a 740-AO molecule 16 rows take rho and
-// grad rho from about 1.8e-7 to 7e-8 (scaled, vs FP64) and every other field
-// down a little, for about 18% more time per step.
+// Rows per block that the mixed AO-MO contraction adds in FP64 (AO values
+// and products) rather than on the tensor cores (KUMO_MIXED_EXACT_ROWS, read
+// at each evaluation; default 64, 0 turns it off): the largest rows of each
+// block, whose FP32 rounding and truncated tensor-core sums would otherwise
+// set the error of the densities at the block's points.
 int mixed_exact_rows() {
     const char* e = std::getenv("KUMO_MIXED_EXACT_ROWS");
-    return e ? std::max(0, std::atoi(e)) : 16;
+    return e ? std::max(0, std::atoi(e)) : 64;
 }
 
 // The mixed form of the potential (FP32 Hermite sums) is opt-in
@@ -194,8 +194,6 @@ public:
                 if (p.orbital_index > c.cols()) throw std::out_of_range("MO index outside available coefficient range");
             }
         }
-        if (opt_.block_size > static_cast<std::size_t>(kumo_dev::kBlockPoints))
-            throw std::invalid_argument("the B200 evaluator supports block_size up to 128");
     }
 
     Backend backend() const { return backend_; }
@@ -257,10 +255,71 @@ private:
         opt_.progress(completed_ + done_in_pass, passes_ * n_);
     }
 
-    std::size_t block_size() const {
-        if (opt_.block_size > static_cast<std::size_t>(kumo_dev::kBlockPoints))
-            throw std::invalid_argument("the B200 evaluator supports block_size up to 128");
-        return opt_.block_size;
+    // Screening block of the FP64 passes (1 .. 65536 points, as the reference).
+    std::size_t block_size() const { return opt_.block_size; }
+    // Points per CTA of passes whose results do not depend on the block (no
+    // screening, or the mixed form): the screening block, at most 128.
+    std::size_t cta_block() const { return std::min<std::size_t>(opt_.block_size, kumo_dev::kBlockPoints); }
+
+    // FP64 screening passes: CTAs take chunks of at most 128 points of a
+    // screening block (kumo_dev::cta_points).
+    struct F64Blocks {
+        std::size_t screen = 128;  // points per screening block
+        std::size_t chunk = 128;   // points per CTA
+        std::size_t per = 1;       // CTAs per screening block
+        std::size_t nscreen = 0;   // screening blocks
+    };
+    F64Blocks f64_blocks() const {
+        F64Blocks b;
+        b.screen = block_size();
+        b.chunk = cta_block();
+        b.per = (b.screen + b.chunk - 1) / b.chunk;
+        b.nscreen = (n_ + b.screen - 1) / b.screen;
+        return b;
+    }
+
+    // CTAs of one wave for `per_cta` bytes of AO scratch each: whole
+    // screening blocks, at least one.
+    int f64_wave_ctas(const F64Blocks& fb, std::size_t per_cta) const {
+        const std::size_t w = static_cast<std::size_t>(wave_blocks(fb.nscreen * fb.per, per_cta));
+        return static_cast<int>(std::max<std::size_t>(w / fb.per, 1) * fb.per);
+    }
+
+    // Runs the waves of an FP64 screening pass: per wave the AO build (for
+    // screening blocks above 128 points first a launch that records each
+    // AO's maximum over the whole block, src/ao_screening.hpp:35-50, then the
+    // build that keeps rows by it) and `contract(first_point, ctas)`.
+    template <class Contract>
+    void f64_waves(const F64Blocks& fb, int W, kumo_dev::AoBuildParams<double>& bp, int ao_order, int npanel,
+                   Contract&& contract) {
+        const std::size_t ws = static_cast<std::size_t>(W) / fb.per;
+        const bool mask = fb.per > 1 && bp.threshold > 0.0;
+        const std::size_t nao = static_cast<std::size_t>(dev_->basis.nao);
+        DeviceAlloc bmax(mask ? sizeof(double) * ws * nao : 0, stream_);
+        bp.block_size = static_cast<long long>(fb.chunk);
+        bp.screen_block = static_cast<long long>(fb.screen);
+        for (std::size_t s0 = 0; s0 < fb.nscreen; s0 += ws) {
+            const std::size_t ns = std::min(ws, fb.nscreen - s0);
+            const int ctas = static_cast<int>(ns * fb.per);
+            bp.first_point = static_cast<long long>(s0 * fb.screen);
+            bp.nblocks = ctas;
+            if (mask) {
+                check_cuda(cudaMemsetAsync(bmax.as<double>(), 0, sizeof(double) * ns * nao, stream_),
+                           "cudaMemsetAsync (block maxima)");
+                bp.mask_pass = 1;
+                bp.block_max = bmax.as<double>();
+                kumo_dev::launch_ao_build<double>(bp, ao_order, npanel, stream_);
+                bp.mask_pass = 2;
+            }
+            const int tok = detail::profile_begin(detail::kProfAoBuild, stream_);
+            kumo_dev::launch_ao_build<double>(bp, ao_order, npanel, stream_);
+            detail::profile_end(tok, stream_);
+            count_ao_rows(bp.out.nkept, ctas);
+            contract(bp.first_point, ctas);
+            report(std::min(n_, (s0 + ns) * fb.screen));
+        }
+        bp.mask_pass = 0;
+        bp.block_max = nullptr;
     }
 
     // Blocks per wave for a scratch of `per_block` bytes per block.
@@ -327,17 +386,31 @@ private:
         completed_ += n_;
     }
 
+    // Rows written by one AO-build wave (counted right after its launch: the
+    // mixed contractions then overwrite nkept with the rows they keep).
+    void count_ao_rows(const int* nkept, int nb) const {
+        if (!detail::profiling_enabled()) return;
+        detail::profile_count(detail::kProfAoBuild, nkept, nb, 0.0, nb, 0.0, 0.0, stream_);
+    }
+
     // Algorithmic counters of one contraction wave: per kept AO row of a
-    // block, 2 * 128 points * panels * occupied MOs FLOPs (the dense product
-    // C_kept^T Phi_kept of every stored panel), and the AO panel bytes read.
+    // block (above the screening threshold), 2 * 128 points * panels *
+    // occupied MOs FLOPs (the dense product C_kept^T Phi_kept of every stored
+    // panel).
     void count_contraction(detail::ProfileKernel k, const int* nkept, int nb, int npanel, int nch, int nocc0,
-                           int nocc1, std::size_t elem) const {
+                           int nocc1) const {
         if (!detail::profiling_enabled()) return;
         const double mos = static_cast<double>(nocc0) + (nch > 1 ? nocc1 : 0);
         const double per_row = 2.0 * kumo_dev::kBlockPoints * npanel * mos;
-        detail::profile_count(detail::kProfAoBuild, nkept, nb, 0.0, nb, 0.0, 0.0, stream_);
-        (void)elem;
         detail::profile_count(k, nkept, nb, per_row, nb, 0.0, 0.0, stream_);
+    }
+
+    // AO-P contraction of a wave: per block and density matrix, the product
+    // P[kept, kept] Phi[kept, 4 panels], 2 * m^2 * 4 * 128 FLOPs.
+    void count_ao_p(const int* nkept, int nb, int nmatrices) const {
+        if (!detail::profiling_enabled()) return;
+        detail::profile_count_sq(detail::kProfContractP, nkept, nb, 2.0 * 4 * kumo_dev::kBlockPoints * nmatrices,
+                                 stream_);
     }
 
     // Occupied-MO channels needed by the AO-MO contraction
@@ -356,45 +429,109 @@ private:
         return nch;
     }
 
+    // Evaluation layout of a mixed-form pass (blocks of at most 128 points:
+    // a larger screening block only widens the FP64 form's kept sets, by
+    // rows below the threshold).  On a grid with 128-point (or larger)
+    // blocks the mixed form evaluates compact tiles (GridTiles) instead of
+    // runs of 128 points along k: the tile shape (powers of two, 128 points)
+    // leaves the fewest padding points, and among those spans the shortest
+    // diagonal.  The FP64 form keeps the reference's blocks, whose screening
+    // it reproduces bit for bit; the mixed form only has to agree with it to
+    // its tolerance, and a compact block lets its FP64 exact rows (the
+    // block's largest rows) cover the dominant terms of every point.
+    // KUMO_MIXED_TILES=0 keeps the linear blocks.
+    struct MixedLayout {
+        kumo_dev::PointSource src;
+        kumo_dev::GridTiles tiles;
+        std::size_t nblocks = 0;
+        long long count = 0;  // evaluation indices
+    };
+
+    MixedLayout mixed_layout() const {
+        MixedLayout L;
+        L.src = src_;
+        const std::size_t bs = cta_block();
+        const char* e = std::getenv("KUMO_MIXED_TILES");
+        const bool tiled = grid_ && bs == static_cast<std::size_t>(kumo_dev::kBlockPoints) && !(e && e[0] == '0');
+        if (!tiled) {
+            L.nblocks = (n_ + bs - 1) / bs;
+            L.count = static_cast<long long>(n_);
+            return L;
+        }
+        const long long n[3] = {static_cast<long long>(grid_->counts[0]), static_cast<long long>(grid_->counts[1]),
+                                static_cast<long long>(grid_->counts[2])};
+        double len[3];
+        for (int a = 0; a < 3; ++a) {
+            const double* c = &grid_->steps.m[static_cast<std::size_t>(3 * a)];
+            len[a] = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+        }
+        long long best_pad = -1;
+        double best_diag = 0.0;
+        kumo_dev::GridTiles t{};
+        for (int sa = 0; sa <= 7; ++sa)
+            for (int sb = 0; sa + sb <= 7; ++sb) {
+                const int sc = 7 - sa - sb;
+                const long long ta = (n[0] + (1ll << sa) - 1) >> sa, tb = (n[1] + (1ll << sb) - 1) >> sb,
+                                tc = (n[2] + (1ll << sc) - 1) >> sc;
+                const long long padded = ta * tb * tc * 128;
+                const double da = len[0] * double(1 << sa), db = len[1] * double(1 << sb), dc = len[2] * double(1 << sc);
+                const double diag = da * da + db * db + dc * dc;
+                if (best_pad < 0 || padded < best_pad || (padded == best_pad && diag < best_diag * (1.0 - 1e-12))) {
+                    best_pad = padded;
+                    best_diag = diag;
+                    t = {1, sa, sb, sc, n[0], n[1], n[2], tb, tc};
+                }
+            }
+        L.tiles = t;
+        L.src.tiles = t;
+        L.count = best_pad;
+        L.src.count = best_pad;
+        L.nblocks = static_cast<std::size_t>(best_pad / 128);
+        return L;
+    }
+
+    // Points of the grid whose results are final once the first `blocks`
+    // blocks of a pass have run (tiles run with i slowest, so finished tiles
+    // complete whole planes of the grid).
+    std::size_t done_points(const MixedLayout& L, std::size_t blocks) const {
+        const std::size_t bs = cta_block();
+        if (!L.tiles.on) return std::min(n_, blocks * bs);
+        const std::size_t per_slab = static_cast<std::size_t>(L.tiles.tny * L.tiles.tnz);
+        const std::size_t planes = (blocks / per_slab) << L.tiles.sa;
+        return std::min(n_, planes * static_cast<std::size_t>(L.tiles.ny * L.tiles.nz));
+    }
+
     void mo_pass_f64(int ao_order, int npanel, const std::array<bool, 4>& needed, const kumo_dev::FieldSpec& spec) {
-        const std::size_t bs = block_size();
-        const std::size_t nblocks = (n_ + bs - 1) / bs;
+        const F64Blocks fb = f64_blocks();
         const int nao = dev_->basis.nao;
         const int stride = nao;
-        const std::size_t per_block = sizeof(double) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints +
-                                      sizeof(int) * ((std::size_t)stride + 1);
-        const int W = wave_blocks(nblocks, per_block);
+        const std::size_t per_cta = sizeof(double) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints +
+                                    sizeof(int) * ((std::size_t)stride + 1);
+        const int W = f64_wave_ctas(fb, per_cta);
         DeviceAlloc panels(sizeof(double) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints * W, stream_);
         DeviceAlloc kept(sizeof(int) * (std::size_t)stride * W, stream_);
         DeviceAlloc nkept(sizeof(int) * (std::size_t)W, stream_);
         kumo_dev::AoBuildParams<double> bp = build_params<double>(opt_.screening_threshold);
-        bp.block_size = static_cast<long long>(bs);
         bp.out = {panels.as<double>(), kept.as<int>(), nkept.as<int>(), stride, npanel};
         kumo_dev::ContractMoParams cp{};
         cp.scr = bp.out;
-        cp.block_size = static_cast<long long>(bs);
+        cp.block_size = static_cast<long long>(fb.chunk);
+        cp.screen_block = static_cast<long long>(fb.screen);
         cp.count = static_cast<long long>(n_);
         bool bia = false;
         cp.nchannels = mo_channels(needed, cp.ch, bia, false);
         cp.beta_is_alpha = bia;
         cp.ao_order = ao_order;
         cp.spec = spec;
-        for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
-            const int nb = static_cast<int>(std::min<std::size_t>(W, nblocks - b0));
-            bp.first_point = static_cast<long long>(b0 * bs);
-            bp.nblocks = nb;
-            int tok = detail::profile_begin(detail::kProfAoBuild, stream_);
-            kumo_dev::launch_ao_build<double>(bp, ao_order, npanel, stream_);
-            detail::profile_end(tok, stream_);
-            cp.first_point = bp.first_point;
-            cp.nblocks = nb;
-            tok = detail::profile_begin(detail::kProfContractMo, stream_);
+        f64_waves(fb, W, bp, ao_order, npanel, [&](long long first, int ctas) {
+            cp.first_point = first;
+            cp.nblocks = ctas;
+            const int tok = detail::profile_begin(detail::kProfContractMo, stream_);
             kumo_dev::launch_contract_mo_f64(cp, npanel, stream_);
             detail::profile_end(tok, stream_);
-            count_contraction(detail::kProfContractMo, bp.out.nkept, nb, npanel, cp.nchannels, cp.ch[0].nocc,
-                              cp.nchannels > 1 ? cp.ch[1].nocc : 0, sizeof(double));
-            report(std::min(n_, (b0 + nb) * bs));
-        }
+            count_contraction(detail::kProfContractMo, bp.out.nkept, ctas, npanel, cp.nchannels, cp.ch[0].nocc,
+                              cp.nchannels > 1 ? cp.ch[1].nocc : 0);
+        });
     }
 
     // Fused mixed AO-MO pass: the AO rows are built inside the tensor-core
@@ -408,8 +545,9 @@ private:
         const char* e = std::getenv("KUMO_MIXED_FUSED");
         if (!e || std::string(e) != "1") return false;
         if (!kumo_dev::contract_fused_supported(npanel, dev_->basis.nblocks)) return false;
-        const std::size_t bs = block_size();
-        const std::size_t nblocks = (n_ + bs - 1) / bs;
+        const std::size_t bs = cta_block();
+        const MixedLayout lay = mixed_layout();
+        const std::size_t nblocks = lay.nblocks;
         const int nao = dev_->basis.nao;
         kumo_dev::ContractFusedParams cp{};
         bool bia = false;
@@ -429,15 +567,16 @@ private:
         if (builds > 2) return false;
         cp.ao.basis = dev_->basis;
         cp.ao.prims = dev_->mix_prims;
-        cp.ao.src = src_;
+        cp.ao.src = lay.src;
         cp.ao.block_size = static_cast<long long>(bs);
         std::memcpy(cp.ao.tpure, dev_->tpure_g, sizeof cp.ao.tpure);
         std::memcpy(cp.ao.gcart, dev_->gcart, sizeof cp.ao.gcart);
-        cp.count = static_cast<long long>(n_);
+        cp.count = lay.count;
         cp.status = kumo_dev::pipeline_status_word();
         cp.beta_is_alpha = bia;
         cp.ao_order = ao_order;
         cp.spec = spec;
+        cp.spec.tiles = lay.tiles;
         const int W = static_cast<int>(std::min<std::size_t>(nblocks, 1u << 16));
         DeviceAlloc nrows(sizeof(int) * static_cast<std::size_t>(W), stream_);
         cp.nrows = detail::profiling_enabled() ? nrows.as<int>() : nullptr;
@@ -450,16 +589,17 @@ private:
             detail::profile_end(tok, stream_);
             if (cp.nrows)
                 count_contraction(detail::kProfContractMixed, cp.nrows, nb, npanel, cp.nchannels, cp.ch[0].nocc,
-                                  cp.nchannels > 1 ? cp.ch[1].nocc : 0, sizeof(float));
-            report(std::min(n_, (b0 + nb) * bs));
+                                  cp.nchannels > 1 ? cp.ch[1].nocc : 0);
+            report(done_points(lay, b0 + nb));
         }
         return true;
     }
 
     void mo_pass_mixed(int ao_order, int npanel, const std::array<bool, 4>& needed, const kumo_dev::FieldSpec& spec) {
         if (mo_pass_fused(ao_order, npanel, needed, spec)) return;
-        const std::size_t bs = block_size();
-        const std::size_t nblocks = (n_ + bs - 1) / bs;
+        const std::size_t bs = cta_block();
+        const MixedLayout lay = mixed_layout();
+        const std::size_t nblocks = lay.nblocks;
         const int nao = dev_->basis.nao;
         const int stride = (nao + 7) / 8 * 8;
         const std::size_t per_block = sizeof(float) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints +
@@ -472,7 +612,7 @@ private:
         kumo_dev::AoMixedParams bp{};
         bp.basis = dev_->basis;
         bp.prims = dev_->mix_prims;
-        bp.src = src_;
+        bp.src = lay.src;
         bp.block_size = static_cast<long long>(bs);
         std::memcpy(bp.tpure, dev_->tpure_g, sizeof bp.tpure);
         std::memcpy(bp.gcart, dev_->gcart, sizeof bp.gcart);
@@ -480,7 +620,7 @@ private:
         kumo_dev::ContractMixedParams cp{};
         cp.scr = bp.out;
         cp.block_size = static_cast<long long>(bs);
-        cp.count = static_cast<long long>(n_);
+        cp.count = lay.count;
         bool bia = false;
         kumo_dev::MoChannel ch[2];
         cp.nchannels = mo_channels(needed, ch, bia, true);
@@ -498,7 +638,12 @@ private:
         cp.beta_is_alpha = bia;
         cp.ao_order = ao_order;
         cp.spec = spec;
+        cp.spec.tiles = lay.tiles;
         cp.exact_rows = mixed_exact_rows();
+        cp.src = lay.src;
+        cp.basis = dev_->basis;
+        for (int l = 0; l < 3; ++l)
+            for (int i = 0; i < 135; ++i) cp.pure64[l][i] = dev_->pure_d[l][i];
         for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
             const int nb = static_cast<int>(std::min<std::size_t>(W, nblocks - b0));
             bp.first_point = static_cast<long long>(b0 * bs);
@@ -506,22 +651,24 @@ private:
             int tok = detail::profile_begin(detail::kProfAoBuild, stream_);
             kumo_dev::launch_ao_mixed(bp, npanel, stream_);
             detail::profile_end(tok, stream_);
+            count_ao_rows(bp.out.nkept, nb);
             cp.first_point = bp.first_point;
             cp.nblocks = nb;
             tok = detail::profile_begin(detail::kProfContractMixed, stream_);
             kumo_dev::launch_contract_mixed(cp, npanel, stream_);
             detail::profile_end(tok, stream_);
             count_contraction(detail::kProfContractMixed, bp.out.nkept, nb, npanel, cp.nchannels, cp.ch[0].nocc,
-                              cp.nchannels > 1 ? cp.ch[1].nocc : 0, sizeof(float));
-            report(std::min(n_, (b0 + nb) * bs));
+                              cp.nchannels > 1 ? cp.ch[1].nocc : 0);
+            report(done_points(lay, b0 + nb));
         }
     }
 
     // Mixed AO-P form: FP32 AO rows (ao_mixed) and the tensor-core
     // Y = P[kept, kept] Phi contraction (density_derivatives_shared).
     void p_pass_mixed(int ao_order, int npanel, const std::array<bool, 4>& needed, const kumo_dev::FieldSpec& spec) {
-        const std::size_t bs = block_size();
-        const std::size_t nblocks = (n_ + bs - 1) / bs;
+        const std::size_t bs = cta_block();
+        const MixedLayout lay = mixed_layout();
+        const std::size_t nblocks = lay.nblocks;
         const int nao = dev_->basis.nao;
         const int stride = (nao + 7) / 8 * 8;
         const std::size_t per_block = sizeof(float) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints +
@@ -534,7 +681,7 @@ private:
         kumo_dev::AoMixedParams bp{};
         bp.basis = dev_->basis;
         bp.prims = dev_->mix_prims;
-        bp.src = src_;
+        bp.src = lay.src;
         bp.block_size = static_cast<long long>(bs);
         std::memcpy(bp.tpure, dev_->tpure_g, sizeof bp.tpure);
         std::memcpy(bp.gcart, dev_->gcart, sizeof bp.gcart);
@@ -542,7 +689,7 @@ private:
         kumo_dev::ContractPMixedParams cp{};
         cp.scr = bp.out;
         cp.block_size = static_cast<long long>(bs);
-        cp.count = static_cast<long long>(n_);
+        cp.count = lay.count;
         cp.nao = nao;
         cp.p_total_s = dev_->p_total_s;
         cp.p_spin_s = dev_->p_spin_s;
@@ -551,6 +698,7 @@ private:
         cp.ao_order = ao_order;
         cp.threshold = static_cast<float>(opt_.screening_threshold);
         cp.spec = spec;
+        cp.spec.tiles = lay.tiles;
         cp.status = kumo_dev::pipeline_status_word();
         for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
             const int nb = static_cast<int>(std::min<std::size_t>(W, nblocks - b0));
@@ -559,32 +707,33 @@ private:
             int tok = detail::profile_begin(detail::kProfAoBuild, stream_);
             kumo_dev::launch_ao_mixed(bp, npanel, stream_);
             detail::profile_end(tok, stream_);
+            count_ao_rows(bp.out.nkept, nb);
             cp.first_point = bp.first_point;
             cp.nblocks = nb;
             tok = detail::profile_begin(detail::kProfContractP, stream_);
             kumo_dev::launch_contract_p_mixed(cp, npanel, stream_);
             detail::profile_end(tok, stream_);
-            report(std::min(n_, (b0 + nb) * bs));
+            count_ao_p(bp.out.nkept, nb, (cp.total_needed ? 1 : 0) + (cp.spin_needed ? 1 : 0));
+            report(done_points(lay, b0 + nb));
         }
     }
 
     void p_pass_f64(int ao_order, int npanel, const std::array<bool, 4>& needed, const kumo_dev::FieldSpec& spec) {
-        const std::size_t bs = block_size();
-        const std::size_t nblocks = (n_ + bs - 1) / bs;
+        const F64Blocks fb = f64_blocks();
         const int nao = dev_->basis.nao;
         const int stride = nao;
-        const std::size_t per_block = sizeof(double) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints +
-                                      sizeof(int) * ((std::size_t)stride + 1);
-        const int W = wave_blocks(nblocks, per_block);
+        const std::size_t per_cta = sizeof(double) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints +
+                                    sizeof(int) * ((std::size_t)stride + 1);
+        const int W = f64_wave_ctas(fb, per_cta);
         DeviceAlloc panels(sizeof(double) * npanel * (std::size_t)stride * kumo_dev::kBlockPoints * W, stream_);
         DeviceAlloc kept(sizeof(int) * (std::size_t)stride * W, stream_);
         DeviceAlloc nkept(sizeof(int) * (std::size_t)W, stream_);
         kumo_dev::AoBuildParams<double> bp = build_params<double>(opt_.screening_threshold);
-        bp.block_size = static_cast<long long>(bs);
         bp.out = {panels.as<double>(), kept.as<int>(), nkept.as<int>(), stride, npanel};
         kumo_dev::ContractPParams cp{};
         cp.scr = bp.out;
-        cp.block_size = static_cast<long long>(bs);
+        cp.block_size = static_cast<long long>(fb.chunk);
+        cp.screen_block = static_cast<long long>(fb.screen);
         cp.count = static_cast<long long>(n_);
         cp.nao = nao;
         cp.total_needed = needed[0] || needed[1] || needed[2];
@@ -593,39 +742,32 @@ private:
         cp.p_spin = dev_->p_spin;
         cp.ao_order = ao_order;
         cp.spec = spec;
-        for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
-            const int nb = static_cast<int>(std::min<std::size_t>(W, nblocks - b0));
-            bp.first_point = static_cast<long long>(b0 * bs);
-            bp.nblocks = nb;
-            int tok = detail::profile_begin(detail::kProfAoBuild, stream_);
-            kumo_dev::launch_ao_build<double>(bp, ao_order, npanel, stream_);
-            detail::profile_end(tok, stream_);
-            cp.first_point = bp.first_point;
-            cp.nblocks = nb;
-            tok = detail::profile_begin(detail::kProfContractP, stream_);
+        f64_waves(fb, W, bp, ao_order, npanel, [&](long long first, int ctas) {
+            cp.first_point = first;
+            cp.nblocks = ctas;
+            const int tok = detail::profile_begin(detail::kProfContractP, stream_);
             kumo_dev::launch_contract_p_f64(cp, npanel, stream_);
             detail::profile_end(tok, stream_);
-            report(std::min(n_, (b0 + nb) * bs));
-        }
+            count_ao_p(bp.out.nkept, ctas, (cp.total_needed ? 1 : 0) + (cp.spin_needed ? 1 : 0));
+        });
     }
 
     // Molecule::densities_blocked for one component (src/density.cpp:366-444).
     void grid_density_pass(const Property& key, double* out) {
-        const std::size_t bs = block_size();
-        const std::size_t nblocks = (n_ + bs - 1) / bs;
+        const F64Blocks fb = f64_blocks();
         const int nao = dev_->basis.nao;
-        const std::size_t per_block =
+        const std::size_t per_cta =
             sizeof(double) * (std::size_t)nao * kumo_dev::kBlockPoints + sizeof(int) * ((std::size_t)nao + 1);
-        const int W = wave_blocks(nblocks, per_block);
+        const int W = f64_wave_ctas(fb, per_cta);
         DeviceAlloc panels(sizeof(double) * (std::size_t)nao * kumo_dev::kBlockPoints * W, stream_);
         DeviceAlloc kept(sizeof(int) * (std::size_t)nao * W, stream_);
         DeviceAlloc nkept(sizeof(int) * (std::size_t)W, stream_);
         kumo_dev::AoBuildParams<double> bp = build_params<double>(opt_.screening_threshold);
-        bp.block_size = static_cast<long long>(bs);
         bp.out = {panels.as<double>(), kept.as<int>(), nkept.as<int>(), nao, 1};
         kumo_dev::ContractPParams cp{};
         cp.scr = bp.out;
-        cp.block_size = static_cast<long long>(bs);
+        cp.block_size = static_cast<long long>(fb.chunk);
+        cp.screen_block = static_cast<long long>(fb.screen);
         cp.count = static_cast<long long>(n_);
         cp.nao = nao;
         cp.density_component = static_cast<int>(key.component);
@@ -635,16 +777,11 @@ private:
         cp.spec.stride = static_cast<long long>(n_);
         cp.spec.nprops = 1;
         cp.spec.props[0] = {static_cast<int>(key.kind), static_cast<int>(key.component), out};
-        for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
-            const int nb = static_cast<int>(std::min<std::size_t>(W, nblocks - b0));
-            bp.first_point = static_cast<long long>(b0 * bs);
-            bp.nblocks = nb;
-            kumo_dev::launch_ao_build<double>(bp, 0, 1, stream_);
-            cp.first_point = bp.first_point;
-            cp.nblocks = nb;
+        f64_waves(fb, W, bp, 0, 1, [&](long long first, int ctas) {
+            cp.first_point = first;
+            cp.nblocks = ctas;
             kumo_dev::launch_density_values_f64(cp, stream_);
-            report(std::min(n_, (b0 + nb) * bs));
-        }
+        });
         completed_ += n_;
     }
 
@@ -666,7 +803,7 @@ private:
             if (key.kind == PropertyKind::OrbitalHessian) order = 2;
         }
         if (sel.empty()) return;
-        const std::size_t bs = grid_path ? 128 : block_size();
+        const std::size_t bs = grid_path ? 128 : cta_block();  // no screening: any chunking gives the same values
         const std::size_t nblocks = (n_ + bs - 1) / bs;
         const int nao = dev_->basis.nao;
         // Values come from the value path (npanel 1); derivatives from the
@@ -716,7 +853,7 @@ private:
     // set sums over the scaled MO columns and the fields from them.
     void orbital_energy_pass() {
         const auto& st = dev_->orbital_energy_state(mol_, oe_needs_, oe_what_);
-        const std::size_t bs = block_size();
+        const std::size_t bs = cta_block();  // no screening: any chunking gives the same values
         const std::size_t nblocks = (n_ + bs - 1) / bs;
         const int nao = dev_->basis.nao;
         const std::size_t per_block =

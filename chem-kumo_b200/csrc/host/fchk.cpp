@@ -137,6 +137,15 @@ std::string inflate_file(const std::filesystem::path& path) {
         if (n == 0) break;
         out.append(chunk, static_cast<std::size_t>(n));
     }
+    // A member cut short (no CRC and length trailer) ends the reads early
+    // with a buffer error instead of a negative count.
+    int code = Z_OK;
+    const char* why = gzerror(g, &code);
+    if (code != Z_OK) {
+        const std::string m = why ? why : "gzip error";
+        gzclose(g);
+        fail("gzip decoding failed for formatted checkpoint: " + m);
+    }
     gzclose(g);
     return out;
 }

@@ -31,19 +31,29 @@ State& state() {
     return s;
 }
 
-__global__ void sum_kept(const int* nkept, int n, double flops_per_row, double* counters) {
-    __shared__ double s[256];
-    double v = 0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) v += nkept[i];
+// counters[0] += sum nkept; counters[1] += sum (flops_per_row nkept +
+// flops_per_row_sq nkept^2).
+__global__ void sum_kept(const int* nkept, int n, double flops_per_row, double flops_per_row_sq, double* counters) {
+    __shared__ double s[256], s2[256];
+    double v = 0, v2 = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double k = nkept[i];
+        v += k;
+        v2 += k * k;
+    }
     s[threadIdx.x] = v;
+    s2[threadIdx.x] = v2;
     __syncthreads();
     for (int o = 128; o > 0; o >>= 1) {
-        if (threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
+        if (threadIdx.x < o) {
+            s[threadIdx.x] += s[threadIdx.x + o];
+            s2[threadIdx.x] += s2[threadIdx.x + o];
+        }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
         counters[0] += s[0];
-        counters[1] += s[0] * flops_per_row;
+        counters[1] += s[0] * flops_per_row + s2[0] * flops_per_row_sq;
     }
 }
 
@@ -104,7 +114,13 @@ void profile_count(ProfileKernel k, const int* nkept, int n, double flops_per_ro
     s.units[k] += units;
     s.flops[k] += flops;
     s.bytes[k] += bytes;
-    if (nkept && n > 0) sum_kept<<<1, 256, 0, st>>>(nkept, n, flops_per_row, s.d_counters + 2 * k);
+    if (nkept && n > 0) sum_kept<<<1, 256, 0, st>>>(nkept, n, flops_per_row, 0.0, s.d_counters + 2 * k);
+}
+void profile_count_sq(ProfileKernel k, const int* nkept, int n, double flops_per_row_sq, cudaStream_t st) {
+    State& s = state();
+    if (!s.on) return;
+    std::lock_guard<std::mutex> l(s.mu);
+    if (nkept && n > 0) sum_kept<<<1, 256, 0, st>>>(nkept, n, 0.0, flops_per_row_sq, s.d_counters + 2 * k);
 }
 
 ProfileStats profile_read(ProfileKernel k) {
@@ -129,7 +145,7 @@ ProfileStats profile_read(ProfileKernel k) {
 }
 
 const char* profile_name(ProfileKernel k) {
-    static const char* names[kProfCount] = {"ao_build", "contract_mo_f64", "contract_mixed", "contract_p_f64",
+    static const char* names[kProfCount] = {"ao_build", "contract_mo_f64", "contract_mixed", "contract_p",
                                             "density_values_f64", "orbitals_f64", "esp_f64"};
     return names[k];
 }

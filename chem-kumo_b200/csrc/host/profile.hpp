@@ -22,6 +22,10 @@ void profile_end(int token, cudaStream_t s);
 // (blocks, points or point-pair interactions) and `flops` to its counters.
 void profile_count(ProfileKernel k, const int* nkept, int n, double flops_per_kept_row, double units,
                    double flops, double bytes, cudaStream_t s);
+// Adds sum(nkept[0..n)) to the kept-rows counter of kernel k and
+// flops_per_row_sq * sum(nkept^2) to its FLOPs (products with a kept x kept
+// block of a matrix).
+void profile_count_sq(ProfileKernel k, const int* nkept, int n, double flops_per_row_sq, cudaStream_t s);
 
 struct ProfileStats {
     int launches;

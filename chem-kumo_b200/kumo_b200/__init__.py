@@ -159,7 +159,8 @@ EXPORTS = [
     "kumo_server_reset_stats", "kumo_density_isosurface", "kumo_potential_surface", "kumo_ionization_energy_surface",
     "kumo_map_on_density_isosurface", "kumo_average_local_ionization_energy", "kumo_extract_isosurface",
     "kumo_surface_info", "kumo_surface_mesh", "kumo_surface_field", "kumo_surface_destroy",
-    "kumo_surface_statistics", "kumo_write_ply",
+    "kumo_surface_statistics", "kumo_write_ply", "kumo_read_cube", "kumo_cube_info", "kumo_cube_data",
+    "kumo_cube_destroy", "kumo_write_cube_data",
 ]
 
 
@@ -229,6 +230,13 @@ def lib():
         L.kumo_write_cube.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(_Grid), C.c_int, _I, _D, _D, _D,
                                       C.c_longlong, *eb]
         L.kumo_grid_around.argtypes = [C.c_void_p, C.c_double, C.c_double, C.POINTER(_Grid), *eb]
+        L.kumo_read_cube.argtypes = [C.c_char_p, C.POINTER(C.c_void_p), *eb]
+        L.kumo_cube_info.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(_Grid), _I]
+        L.kumo_cube_data.argtypes = [C.c_void_p, _I, _D, _D, _D, C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t]
+        L.kumo_cube_destroy.argtypes = [C.c_void_p]
+        L.kumo_cube_destroy.restype = None
+        L.kumo_write_cube_data.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.POINTER(_Grid),
+                                           C.c_longlong, _I, _D, _D, _D, *eb]
         L.kumo_profile_enable.argtypes = [C.c_int]
         L.kumo_set_device.argtypes = [C.c_int, *eb]
         L.kumo_evaluate_points_noalloc.argtypes = [C.c_void_p, C.POINTER(_Options), _D, C.c_longlong,
@@ -515,6 +523,8 @@ def evaluate_points_noalloc(molecule: Molecule, points_ptr: int, npoints: int, p
     call cudaMalloc.  The molecule must already have its device copy (any
     earlier evaluation of it on this device creates it); overlapping calls race
     on the library's fixed scratch array."""
+    if len(outputs) != len(props):
+        raise InvalidArgument(1, "one output array per property is required")
     ptrs = (_D * max(len(props), 1))(*[C.cast(C.c_void_p(int(o)), _D) for o in outputs])
     opt = _options(block_size, 0, threshold, 0.0, 0)
     e = _err()
@@ -541,6 +551,57 @@ def write_cube(path: str, grid: Grid, z, charges, xyz, values: np.ndarray, comme
     g = grid._c()
     _check(lib().kumo_write_cube(path.encode(), comment.encode(), C.byref(g), len(z), z.ctypes.data_as(_I), _dp(q),
                                  _dp(x), _dp(v), orbital_index, e, 512), e)
+
+
+@dataclass
+class CubeData:
+    """A scalar Cube dataset (chem::kumo::CubeData): grid and atoms in bohr,
+    values in Field order, the two comment lines and the header's unit."""
+    grid: "Grid"
+    atomic_numbers: np.ndarray
+    charges: np.ndarray
+    xyz: np.ndarray
+    values: np.ndarray
+    first_comment: str = ""
+    second_comment: str = ""
+    coordinates_in_angstrom: bool = False
+
+
+def read_cube(path: str) -> CubeData:
+    """kumo_read_cube: a scalar Cube file, plain or gzip (angstrom headers
+    converted to bohr); raises KumoError with the reader's message."""
+    L = lib()
+    h, e = C.c_void_p(), _err()
+    _check(L.kumo_read_cube(os.fsencode(path), C.byref(h), e, 512), e)
+    try:
+        na, g, ang = C.c_longlong(), _Grid(), C.c_int()
+        L.kumo_cube_info(h, C.byref(na), C.byref(g), C.byref(ang))
+        counts = tuple(int(c) for c in g.counts)
+        z = np.zeros(na.value, dtype=np.int32)
+        q = np.zeros(na.value)
+        xyz = np.zeros((na.value, 3))
+        vals = np.zeros(int(np.prod(counts)))
+        c1, c2 = C.create_string_buffer(1 << 16), C.create_string_buffer(1 << 16)
+        L.kumo_cube_data(h, z.ctypes.data_as(_I), _dp(q), _dp(xyz), _dp(vals), c1, len(c1), c2, len(c2))
+        steps = np.array(list(g.steps)).reshape(3, 3).T  # column a = step of axis a
+        grid = Grid(np.array(list(g.origin)), steps, counts)
+        return CubeData(grid, z, q, xyz, vals, c1.value.decode(errors="replace"), c2.value.decode(errors="replace"),
+                        bool(ang.value))
+    finally:
+        L.kumo_cube_destroy(h)
+
+
+def write_cube_data(path: str, cube: CubeData) -> None:
+    """kumo_write_cube_data: 13 significant digits, read_cube reproduces it."""
+    z = np.ascontiguousarray(cube.atomic_numbers, dtype=np.int32)
+    q = np.ascontiguousarray(cube.charges, dtype=float)
+    x = np.ascontiguousarray(cube.xyz, dtype=float).ravel()
+    v = np.ascontiguousarray(cube.values, dtype=float).ravel()
+    e = _err()
+    g = cube.grid._c()
+    _check(lib().kumo_write_cube_data(os.fsencode(path), cube.first_comment.encode(), cube.second_comment.encode(),
+                                      int(cube.coordinates_in_angstrom), C.byref(g), len(z), z.ctypes.data_as(_I),
+                                      _dp(q), _dp(x), _dp(v), e, 512), e)
 
 
 def set_device(device: int) -> None:

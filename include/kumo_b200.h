@@ -54,7 +54,7 @@ typedef struct {
 /* EvaluationOptions (include/chem/kumo/evaluator.hpp:406-441) plus the
  * arithmetic precision. */
 typedef struct {
-    long long block_size;       /* 1..128 on the device (default 128) */
+    long long block_size;       /* screening block, 1..65536 points (default 128) */
     int backend;
     double screening_threshold; /* default 1e-12 */
     double potential_tolerance; /* 0: exact electrostatic potential */
@@ -160,7 +160,10 @@ int kumo_evaluate_points_device(const kumo_molecule* m, const kumo_options* opt,
  * whose work overlaps on the GPU race: serialize them.  A molecule whose
  * scratch for one 128-point block exceeds the array is rejected with
  * KUMO_INVALID_ARGUMENT.  opt: block_size 1..128, backend AUTO or AO_MO,
- * precision FP64 (NULL for the defaults). */
+ * precision FP64 (NULL for the defaults); every outputs[i] must be non-null.
+ * The queued kernels read the molecule's device copy: do not evaluate the same
+ * molecule on another device (which replaces that copy) or destroy it while
+ * they may still run. */
 int kumo_evaluate_points_noalloc(const kumo_molecule* m, const kumo_options* opt,
                                  const double* device_points, long long npoints,
                                  const kumo_property* props, int nprops, double* const* outputs,
@@ -193,6 +196,28 @@ int kumo_esp_pair_count(const kumo_molecule* m, long long* count, char* err, siz
 int kumo_write_cube(const char* path, const char* comment, const kumo_grid* grid, int natoms,
                     const int* atomic_numbers, const double* charges, const double* xyz,
                     const double* values, long long orbital_index, char* err, size_t errlen);
+
+/* read_cube (include/chem/kumo/cube.hpp:32 of chem-kumo; src/cube.cpp:114-212):
+ * a scalar Cube file, plain or gzip, into a handle; angstrom headers are
+ * converted to bohr.  kumo_cube_info gives the atom count, the grid (bohr)
+ * and whether the header was in angstrom; kumo_cube_data copies the atoms
+ * (z, charges, xyz as natoms x 3), the values (Field order) and the two
+ * comment lines (truncated to their buffers, NUL-terminated); any output
+ * pointer may be NULL. */
+typedef struct kumo_cube kumo_cube;
+int kumo_read_cube(const char* path, kumo_cube** out, char* err, size_t errlen);
+int kumo_cube_info(const kumo_cube* c, long long* natoms, kumo_grid* grid, int* angstrom);
+int kumo_cube_data(const kumo_cube* c, int* atomic_numbers, double* charges, double* xyz, double* values,
+                   char* first_comment, size_t first_len, char* second_comment, size_t second_len);
+void kumo_cube_destroy(kumo_cube* c);
+/* write_cube(CubeData) (include/chem/kumo/cube.hpp:38; src/cube.cpp:215-251):
+ * 13 significant digits, the given comment lines and length unit (angstrom
+ * != 0: the header in angstrom, negative counts), so that kumo_read_cube
+ * reproduces the field to 13 digits.  Grid, atoms and values in bohr. */
+int kumo_write_cube_data(const char* path, const char* first_comment, const char* second_comment, int angstrom,
+                         const kumo_grid* grid, long long natoms, const int* atomic_numbers,
+                         const double* charges, const double* xyz, const double* values, char* err,
+                         size_t errlen);
 
 /* Grid::around / line / plane (include/chem/kumo/density.hpp:72-91). */
 int kumo_grid_around(const kumo_molecule* m, double margin, double spacing, kumo_grid* out,

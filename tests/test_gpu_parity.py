@@ -221,15 +221,41 @@ def test_unrestricted_triplet_mixed(synth_cache):
         assert np.abs(a - r).max() / scale <= 1e-6, p
 
 
-@pytest.mark.parametrize("block", [1, 7, 32, 37, 128])
-def test_block_sizes(block):
+@pytest.mark.parametrize("block", [1, 7, 32, 37, 128, 129, 200, 256, 1000, 65536])
+@pytest.mark.parametrize("backend", [K.Backend.AO_MO, K.Backend.AO_P])
+def test_block_sizes(block, backend):
+    # Screening blocks of any size of chem-kumo's EvaluationOptions::block_size
+    # (1..65536, include/chem/kumo/evaluator.hpp:411): above 128 points the
+    # device screens each block over all of its 128-point chunks.  The grid
+    # request takes the point path (rho, gradient, Laplacian) and, for AO-P,
+    # the grid path of the alpha density (src/density.cpp:366-444).
     m, o = _pair(os.path.join(GOLDEN, "acrolein.fchk.gz"))
     grid = m.grid_around(1.5, 0.6)
-    props = [K.density(P.Density), K.density(P.Gradient), K.density(P.Laplacian)]
+    props = [K.density(P.Density), K.density(P.Gradient), K.density(P.Laplacian), K.density(P.Density, D.Alpha)]
     tuples = [(int(p.kind), int(p.component), 0, 0) for p in props]
-    outs, _ = K.Evaluator(m, block_size=block).evaluate_grid(grid, props)
-    refs, _ = o.evaluate(tuples, grid=(grid.origin, grid.steps, grid.counts), block_size=block)
+    outs, used = K.Evaluator(m, block_size=block, backend=backend).evaluate_grid(grid, props)
+    refs, rused = o.evaluate(tuples, grid=(grid.origin, grid.steps, grid.counts), block_size=block,
+                             backend=int(backend))
+    assert used == rused == int(backend)
     _compare(outs, refs, 1e-12, props)
+    pts = grid.points()[::5]
+    outs, _ = K.Evaluator(m, block_size=block, backend=backend, threshold=1e-6).evaluate_points(pts, props)
+    refs, _ = o.evaluate(tuples, points=pts, block_size=block, backend=int(backend), threshold=1e-6)
+    _compare(outs, refs, 1e-12, props)
+
+
+@pytest.mark.parametrize("block,thr", [(200, 1e-12), (384, 1e-6), (1000, 1e-3), (300, 0.0)])
+def test_screening_masks_large_blocks(block, thr):
+    m, o = _pair(os.path.join(GOLDEN, "acrolein.fchk.gz"))
+    grid = m.grid_around(2.0, 0.45)
+    gm = m.screening_masks(grid, block, 2, thr)
+    pts = grid.points()
+    assert gm.shape[0] == (len(pts) + block - 1) // block
+    for b in range(gm.shape[0]):
+        blk = pts[b * block:(b + 1) * block]
+        mx = np.abs(o.ao_derivatives(blk, 2)).max(axis=(0, 2))
+        ref = np.ones(o.n, bool) if thr == 0.0 else mx > thr
+        assert np.array_equal(gm[b].astype(bool), ref), f"block {b}"
 
 
 def test_points_path_and_grid_agree():
