@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(kCtaThreads<S>, 1) contract_mixed_kernel(const
                         // Stage s holds step t once all producers arrived on
                         // full[s] for its (gtile / S)-th use.
                         if (lane == 0) {
-                            if (!mbar_wait(&full[s], static_cast<unsigned>((gtile / S) & 1))) failed = true;
+                            if (!mbar_wait(&full[s], static_cast<unsigned>((gtile / S) & 1), prm.wait_ns)) failed = true;
                             tc_fence_after();
 #pragma unroll
                             for (int c = 0; c < P; ++c) issue_panel(t, s, sb, c);
@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(kCtaThreads<S>, 1) contract_mixed_kernel(const
                         // Step t+1's AO stage and step t+2's coefficient stage
                         // were last read by the MMAs of step t+1-S.
                         const long long wv = gtile + 1 - S;
-                        if (wv >= 0 && !mbar_wait(&bar[wv % S], static_cast<unsigned>((wv / S) & 1))) failed = true;
+                        if (wv >= 0 && !mbar_wait(&bar[wv % S], static_cast<unsigned>((wv / S) & 1), prm.wait_ns)) failed = true;
                         if (t + 2 < ntiles) load_b(t + 2, static_cast<int>((gtile + 2) % SB));
                     }
                     continue;
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(kCtaThreads<S>, 1) contract_mixed_kernel(const
                 }
                 if (t + 1 < ntiles) {
                     const long long wv = gtile + 1 - S;
-                    if (wv >= 0 && !mbar_wait(&bar[wv % S], static_cast<unsigned>((wv / S) & 1))) failed = true;
+                    if (wv >= 0 && !mbar_wait(&bar[wv % S], static_cast<unsigned>((wv / S) & 1), prm.wait_ns)) failed = true;
                     if (t + 2 < ntiles) load_b(t + 2, static_cast<int>((gtile + 2) % SB));
                 }
             }
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(kCtaThreads<S>, 1) contract_mixed_kernel(const
             }
             // Accumulators of this pass complete once the last step's commit arrives.
             const long long last = gtile - 1;
-            if (ntiles > 0 && !mbar_wait(&bar[last % S], static_cast<unsigned>((last / S) & 1))) failed = true;
+            if (ntiles > 0 && !mbar_wait(&bar[last % S], static_cast<unsigned>((last / S) & 1), prm.wait_ns)) failed = true;
             if (__syncthreads_or(failed)) {
                 failed = true;
                 break;
@@ -759,7 +759,7 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                     const int sb = static_cast<int>(gtile % SB);
                     bool ok = true;
                     if (lane == 0) {
-                        ok = mbar_wait(&a_full[s], static_cast<unsigned>((gtile / S) & 1));
+                        ok = mbar_wait(&a_full[s], static_cast<unsigned>((gtile / S) & 1), prm.wait_ns);
                         if (ok) {
                             tc_fence_after();
 #pragma unroll
@@ -780,7 +780,7 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                     if (lane == 0) {
                         // The stage's previous rows (step gtile - F) have been read.
                         const long long prev = gtile - F;
-                        if (prev >= 0) ok = mbar_wait(&f_empty[u], static_cast<unsigned>((prev / F) & 1));
+                        if (prev >= 0) ok = mbar_wait(&f_empty[u], static_cast<unsigned>((prev / F) & 1), prm.wait_ns);
                         if (ok) mbar_arrive_expect_tx(&f_full[u], static_cast<unsigned>(nv * P) * (kBlockPoints * 4u));
                     }
                     if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) {
@@ -803,7 +803,7 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                     const int u = static_cast<int>(gtile % F);
                     // Stage s was released (MMAs of step gtile - S) at the end of
                     // the previous step; wait for this step's rows.
-                    if (!mbar_wait(&f_full[u], static_cast<unsigned>((gtile / F) & 1))) {
+                    if (!mbar_wait(&f_full[u], static_cast<unsigned>((gtile / F) & 1), prm.wait_ns)) {
                         failed = true;
                         break;
                     }
@@ -846,7 +846,7 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                         // Step t+1's AO stage and step t+SB-1's coefficient stage
                         // were last read by the MMAs of step gtile - 1.
                         const long long wv = gtile + 1 - S;
-                        if (wv >= 0 && !mbar_wait(&a_empty[wv % S], static_cast<unsigned>((wv / S) & 1))) {
+                        if (wv >= 0 && !mbar_wait(&a_empty[wv % S], static_cast<unsigned>((wv / S) & 1), prm.wait_ns)) {
                             failed = true;
                             break;
                         }
@@ -861,7 +861,7 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                 break;
             }
             const long long last = gtile - 1;
-            if (ntiles > 0 && !mbar_wait(&a_empty[last % S], static_cast<unsigned>((last / S) & 1))) failed = true;
+            if (ntiles > 0 && !mbar_wait(&a_empty[last % S], static_cast<unsigned>((last / S) & 1), prm.wait_ns)) failed = true;
             if (__syncthreads_or(failed)) {
                 failed = true;
                 break;
@@ -1342,13 +1342,13 @@ __global__ void __launch_bounds__(kThreads, 1) contract_fused_kernel(const __gri
                 }
                 if (t + 1 < ntiles) {
                     const long long wv = gtile + 1 - S;
-                    if (wv >= 0 && !mbar_wait(&bar[wv % S], static_cast<unsigned>((wv / S) & 1))) failed = true;
+                    if (wv >= 0 && !mbar_wait(&bar[wv % S], static_cast<unsigned>((wv / S) & 1), prm.wait_ns)) failed = true;
                     if (t + 2 < ntiles) load_b(t + 2, static_cast<int>((gtile + 2) % SB));
                 }
             }
             if (failed || ntiles == 0) continue;
             const long long last = gtile - 1;
-            if (!mbar_wait(&bar[last % S], static_cast<unsigned>((last / S) & 1))) failed = true;
+            if (!mbar_wait(&bar[last % S], static_cast<unsigned>((last / S) & 1), prm.wait_ns)) failed = true;
             if (__syncthreads_or(failed)) {
                 failed = true;
                 break;

@@ -226,13 +226,13 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
                 }
                 if (t + 1 < ntiles) {
                     const long long wt = gtile + 1 - S;
-                    if (wt >= 0 && !mbar_wait(&bar[wt % S], static_cast<unsigned>((wt / S) & 1))) failed = true;
+                    if (wt >= 0 && !mbar_wait(&bar[wt % S], static_cast<unsigned>((wt / S) & 1), prm.wait_ns)) failed = true;
                     load_b(t + 1, static_cast<int>((gtile + 1) % S));
                 }
             }
             if (failed || ntiles == 0) continue;
             const long long last = gtile - 1;
-            if (!mbar_wait(&bar[last % S], static_cast<unsigned>((last / S) & 1))) failed = true;
+            if (!mbar_wait(&bar[last % S], static_cast<unsigned>((last / S) & 1), prm.wait_ns)) failed = true;
             if (__syncthreads_or(failed)) {
                 failed = true;
                 break;

@@ -48,6 +48,9 @@ struct ContractMixedParams {
     PointSource src;        // the evaluation's points (for the exact rows)
     DevBasis basis;         // FP64 exponents and weights (for the exact rows)
     double pure64[3][135];  // Cartesian-to-pure matrices, l = 2..4, row-major
+    // Limit of each tensor-core pipeline wait in ns (0: one second); a wait
+    // that runs out sets *status and the CTA stores NaN for its points.
+    unsigned long long wait_ns = 0;
 };
 
 // AO-P form (density_derivatives_shared): Y = P[kept, kept] Phi[kept, 0..3]
@@ -67,6 +70,9 @@ struct ContractPMixedParams {
     float threshold = 0.0f;
     FieldSpec spec;
     unsigned* status = nullptr;
+    // Limit of each tensor-core pipeline wait in ns (0: one second); a wait
+    // that runs out sets *status and the CTA stores NaN for its points.
+    unsigned long long wait_ns = 0;
 };
 
 void launch_contract_p_mixed(const ContractPMixedParams& p, int npanel, cudaStream_t stream);
@@ -102,6 +108,9 @@ struct ContractFusedParams {
     FieldSpec spec;
     unsigned* status = nullptr;
     int* nrows = nullptr;  // optional: AO rows contracted per block (for the profiler)
+    // Limit of each tensor-core pipeline wait in ns (0: one second); a wait
+    // that runs out sets *status and the CTA stores NaN for its points.
+    unsigned long long wait_ns = 0;
 };
 
 bool contract_fused_supported(int npanel, int nshells);

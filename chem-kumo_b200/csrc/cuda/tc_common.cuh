@@ -67,13 +67,17 @@ __device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
 }
 
 // Waits until the phase with the given parity has completed; false if that
-// did not happen within kWaitNs.
+// did not happen within limit_ns (0: kWaitNs).  The pipeline waits take the
+// evaluation's limit (kernel parameter wait_ns); the waits that drain a
+// failed CTA's MMAs and copies before it frees tensor memory always take
+// kWaitNs.
 constexpr unsigned kSuspendNs = 20000;
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned long long limit_ns = 0) {
     if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long limit = limit_ns ? limit_ns : kWaitNs;
     const unsigned long long t0 = global_ns();
     while (!mbar_try_wait_suspend(bar, parity, kSuspendNs))
-        if (global_ns() - t0 > kWaitNs) return false;
+        if (global_ns() - t0 > limit) return false;
     return true;
 }
 

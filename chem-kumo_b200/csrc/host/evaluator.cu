@@ -58,6 +58,14 @@ int mixed_exact_rows() {
 // (KUMO_ESP_MIXED=1, read at each evaluation): on a 1260-AO molecule it was
 // 1.07x faster than FP64 with 9e-4 scaled error on its density isosurface, so
 // by default Precision::Mixed evaluates the potential in FP64.
+// Limit of the tensor-core pipeline waits (KUMO_PIPELINE_WAIT_NS, read at
+// each evaluation; 0 or unset: one second).  Tests shorten it to make the
+// waits run out and check that the failure is reported.
+unsigned long long pipeline_wait_ns() {
+    const char* e = std::getenv("KUMO_PIPELINE_WAIT_NS");
+    return e ? std::strtoull(e, nullptr, 10) : 0ull;
+}
+
 bool esp_mixed_opt_in() {
     const char* e = std::getenv("KUMO_ESP_MIXED");
     return e != nullptr && e[0] == '1';
@@ -451,37 +459,16 @@ private:
         MixedLayout L;
         L.src = src_;
         const std::size_t bs = cta_block();
-        const char* e = std::getenv("KUMO_MIXED_TILES");
-        const bool tiled = grid_ && bs == static_cast<std::size_t>(kumo_dev::kBlockPoints) && !(e && e[0] == '0');
+        const bool tiled = grid_ && detail::mixed_grid_tiles(opt_.block_size);
         if (!tiled) {
             L.nblocks = (n_ + bs - 1) / bs;
             L.count = static_cast<long long>(n_);
             return L;
         }
-        const long long n[3] = {static_cast<long long>(grid_->counts[0]), static_cast<long long>(grid_->counts[1]),
-                                static_cast<long long>(grid_->counts[2])};
-        double len[3];
-        for (int a = 0; a < 3; ++a) {
-            const double* c = &grid_->steps.m[static_cast<std::size_t>(3 * a)];
-            len[a] = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
-        }
-        long long best_pad = -1;
-        double best_diag = 0.0;
-        kumo_dev::GridTiles t{};
-        for (int sa = 0; sa <= 7; ++sa)
-            for (int sb = 0; sa + sb <= 7; ++sb) {
-                const int sc = 7 - sa - sb;
-                const long long ta = (n[0] + (1ll << sa) - 1) >> sa, tb = (n[1] + (1ll << sb) - 1) >> sb,
-                                tc = (n[2] + (1ll << sc) - 1) >> sc;
-                const long long padded = ta * tb * tc * 128;
-                const double da = len[0] * double(1 << sa), db = len[1] * double(1 << sb), dc = len[2] * double(1 << sc);
-                const double diag = da * da + db * db + dc * dc;
-                if (best_pad < 0 || padded < best_pad || (padded == best_pad && diag < best_diag * (1.0 - 1e-12))) {
-                    best_pad = padded;
-                    best_diag = diag;
-                    t = {1, sa, sb, sc, n[0], n[1], n[2], tb, tc};
-                }
-            }
+        const detail::TileShape ts = detail::choose_tiles(*grid_);
+        const kumo_dev::GridTiles t{1,           ts.sa,       ts.sb,   ts.sc, grid_->counts[0], grid_->counts[1],
+                                    grid_->counts[2], ts.tny, ts.tnz};
+        const long long best_pad = ts.padded();
         L.tiles = t;
         L.src.tiles = t;
         L.count = best_pad;
@@ -573,6 +560,7 @@ private:
         std::memcpy(cp.ao.gcart, dev_->gcart, sizeof cp.ao.gcart);
         cp.count = lay.count;
         cp.status = kumo_dev::pipeline_status_word();
+        cp.wait_ns = pipeline_wait_ns();
         cp.beta_is_alpha = bia;
         cp.ao_order = ao_order;
         cp.spec = spec;
@@ -634,6 +622,7 @@ private:
         }
         kumo_dev::mixed_columns(npanel, nocc16, cp.ncols, cp.groups, cp.tmem_cols);
         cp.status = kumo_dev::pipeline_status_word();
+        cp.wait_ns = pipeline_wait_ns();
         cp.threshold = static_cast<float>(opt_.screening_threshold);
         cp.beta_is_alpha = bia;
         cp.ao_order = ao_order;
@@ -700,6 +689,7 @@ private:
         cp.spec = spec;
         cp.spec.tiles = lay.tiles;
         cp.status = kumo_dev::pipeline_status_word();
+        cp.wait_ns = pipeline_wait_ns();
         for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
             const int nb = static_cast<int>(std::min<std::size_t>(W, nblocks - b0));
             bp.first_point = static_cast<long long>(b0 * bs);

