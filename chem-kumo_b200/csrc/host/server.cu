@@ -136,6 +136,7 @@ struct Server::Impl {
         double* pstage = nullptr;         // direct path: page-locked points
         std::size_t pstage_bytes = 0;
         std::size_t row = 0;              // row length of the staged results (bucket or n)
+        bool high_priority = false;       // stream from free_streams_hi
     };
     std::deque<Pending> queue;
     std::deque<Active> finished;  // handed to the completion thread
@@ -146,7 +147,12 @@ struct Server::Impl {
 
     // Scheduler-owned state.
     std::vector<Active> active;
-    std::vector<cudaStream_t> free_streams;
+    // Streams of small requests (at most graph_points points) take the
+    // device's highest priority, those of larger requests its lowest: a
+    // small request's blocks are scheduled as soon as SMs free up, instead of
+    // after every queued block of a large cube.
+    std::vector<cudaStream_t> free_streams, free_streams_hi;
+    int prio_low = 0, prio_high = 0;
     std::vector<cudaEvent_t> free_events;
     std::map<std::string, std::vector<std::unique_ptr<GraphEntry>>> graphs;
     std::map<std::string, int> seen;  // small-request keys met so far (a graph is captured on the second)
@@ -301,18 +307,22 @@ void Server::Impl::fail(std::uint64_t ticket, const std::string& what, clock_typ
 
 void Server::Impl::launch(Pending&& p) {
     Active a;
-    if (free_streams.empty()) {
+    const bool small = p.n_eval <= opt.graph_points;
+    auto& pool = small ? free_streams_hi : free_streams;
+    if (pool.empty()) {
         cudaStream_t s;
-        check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
-        free_streams.push_back(s);
+        check_cuda(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, small ? prio_high : prio_low),
+                   "cudaStreamCreateWithPriority");
+        pool.push_back(s);
     }
     if (free_events.empty()) {
         cudaEvent_t e;
         check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
         free_events.push_back(e);
     }
-    a.stream = free_streams.back();
-    free_streams.pop_back();
+    a.stream = pool.back();
+    pool.pop_back();
+    a.high_priority = small;
     a.event = free_events.back();
     free_events.pop_back();
     const Molecule& mol = *p.req.molecule;
@@ -400,7 +410,7 @@ void Server::Impl::launch(Pending&& p) {
         if (a.entry) a.entry->busy = false;
         if (a.stage) free_stage.emplace(stage_class(a.stage_bytes), a.stage);
         if (a.pstage) free_stage.emplace(stage_class(a.pstage_bytes), a.pstage);
-        free_streams.push_back(a.stream);
+        (a.high_priority ? free_streams_hi : free_streams).push_back(a.stream);
         free_events.push_back(a.event);
         active_bytes -= p.footprint;
         fail(p.ticket, ex.what(), p.t_submit);
@@ -412,6 +422,7 @@ void Server::Impl::launch(Pending&& p) {
 
 void Server::Impl::run_scheduler() {
     check_cuda(cudaSetDevice(opt.device), "cudaSetDevice");
+    check_cuda(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high), "cudaDeviceGetStreamPriorityRange");
     detail::prepare_device_for_capture();
     for (;;) {
         bool progressed = false;
@@ -425,7 +436,7 @@ void Server::Impl::run_scheduler() {
             Active a = std::move(active[i]);
             active.erase(active.begin() + static_cast<std::ptrdiff_t>(i));
             active_bytes -= a.p.footprint;
-            free_streams.push_back(a.stream);
+            (a.high_priority ? free_streams_hi : free_streams).push_back(a.stream);
             free_events.push_back(a.event);
             progressed = true;
             if (a.pstage) {
@@ -586,6 +597,7 @@ Server::~Server() {
         if (!m.in_arena(p)) cudaFreeHost(p);
     if (m.arena) cudaFreeHost(m.arena);
     for (auto s : m.free_streams) cudaStreamDestroy(s);
+    for (auto s : m.free_streams_hi) cudaStreamDestroy(s);
     for (auto e : m.free_events) cudaEventDestroy(e);
 }
 
