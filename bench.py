@@ -694,6 +694,7 @@ def main() -> None:
                     "d2h_bytes_per_step": nchan * n_total * 8},
             "roofline": roof,
             "kernels": kernels,
+            "tile_tuning": K.tile_tuning_report().strip().splitlines(),
             "gpu_launches": launches,
             "clocks": clk,
         }

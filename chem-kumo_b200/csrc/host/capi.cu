@@ -22,6 +22,10 @@
 #include "device_state.hpp"
 #include "profile.hpp"
 
+namespace chem::kumo::detail {
+std::string tile_tuning_report();  // evaluator.cu
+}
+
 struct kumo_molecule {
     chem::kumo::Molecule mol;
 };
@@ -663,6 +667,21 @@ int kumo_write_cube(const char* path, const char* comment, const kumo_grid* grid
         else
             f.write_cube(path, comment ? comment : "Electron density");
     });
+}
+
+long long kumo_tile_tuning_report(char* buf, size_t len) {
+    std::string r;
+    try {
+        r = chem::kumo::detail::tile_tuning_report();
+    } catch (...) {
+        return -1;
+    }
+    if (buf && len) {
+        const size_t n = std::min(len - 1, r.size());
+        std::memcpy(buf, r.data(), n);
+        buf[n] = '\0';
+    }
+    return static_cast<long long>(r.size());
 }
 
 struct kumo_cube {

@@ -8,6 +8,7 @@
 // The field each property comes from follows src/evaluator.cpp:79-111.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -135,6 +136,70 @@ void keep_pool_memory() {
         check_cuda(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep),
                    "cudaMemPoolSetAttribute");
     });
+}
+
+// ---------------------------------------------------------------------------
+// Tile-shape autotuner of the mixed form.  For grids of more than
+// kTuneMinPoints points (KUMO_TILE_AUTOTUNE=0 turns it off) the tile shape is
+// chosen by measurement: per molecule, backend, stored panels, exact-row count
+// and grid step lengths, each compact candidate shape (see tile_candidates) is
+// timed on a probe: the request's point-path properties on a sub-grid of at
+// most 32 points per axis around the grid's centre, once untimed and twice
+// timed with CUDA events, the faster time kept.  The ranking is cached; a
+// later grid takes the best-ranked candidate among the shapes with its own
+// fewest padding points.  Smaller grids (among them every grid the serving
+// loop replays from a graph) keep the default shape.
+constexpr std::size_t kTuneMinPoints = std::size_t(1) << 17;
+
+struct TileRank {
+    int sa, sb, sc;
+    double ms;  // probe time
+};
+
+struct TileTuner {
+    std::mutex mu;
+    std::map<std::string, std::vector<TileRank>> ranked;
+};
+
+TileTuner& tile_tuner() {
+    static TileTuner t;
+    return t;
+}
+
+// Shape forced on the probe evaluations of this thread (sa, sb, sc), or null.
+thread_local const int* t_forced_shape = nullptr;
+
+bool tile_autotune_enabled() {
+    const char* e = std::getenv("KUMO_TILE_AUTOTUNE");
+    return !(e && e[0] == '0');
+}
+
+detail::TileShape shape_on(const Grid& g, int sa, int sb, int sc) {
+    return {sa, sb, sc, (g.counts[0] + (1ll << sa) - 1) >> sa, (g.counts[1] + (1ll << sb) - 1) >> sb,
+            (g.counts[2] + (1ll << sc) - 1) >> sc};
+}
+
+// Candidate shapes for a grid: padding within 5% of the fewest and a
+// diagonal within twice the most compact's, the most compact first, at most 8.
+std::vector<detail::TileShape> tile_candidates(const Grid& g) {
+    double len[3];
+    for (int a = 0; a < 3; ++a)
+        len[a] = std::sqrt(g.steps(0, a) * g.steps(0, a) + g.steps(1, a) * g.steps(1, a) + g.steps(2, a) * g.steps(2, a));
+    const detail::TileShape best = detail::choose_tiles(g);
+    auto diag = [&](const detail::TileShape& t) {
+        const double da = len[0] * double(1 << t.sa), db = len[1] * double(1 << t.sb), dc = len[2] * double(1 << t.sc);
+        return da * da + db * db + dc * dc;
+    };
+    std::vector<std::pair<double, detail::TileShape>> c;
+    for (int sa = 0; sa <= 7; ++sa)
+        for (int sb = 0; sa + sb <= 7; ++sb) {
+            const detail::TileShape t = shape_on(g, sa, sb, 7 - sa - sb);
+            if (t.padded() <= best.padded() * 1.05 && diag(t) <= 2.0 * diag(best)) c.emplace_back(diag(t), t);
+        }
+    std::stable_sort(c.begin(), c.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+    std::vector<detail::TileShape> out;
+    for (std::size_t i = 0; i < c.size() && i < 8; ++i) out.push_back(c[i].second);
+    return out;
 }
 
 std::size_t scratch_budget() {
@@ -455,7 +520,105 @@ private:
         long long count = 0;  // evaluation indices
     };
 
-    MixedLayout mixed_layout() const {
+    // The tile shape of this run's grid: measured (see TileTuner) or, for
+    // small grids, under stream capture or with the tuner off, the default.
+    detail::TileShape tuned_shape(int npanel) const {
+        const detail::TileShape def = detail::choose_tiles(*grid_);
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        if (n_ <= kTuneMinPoints || !tile_autotune_enabled() ||
+            cudaStreamIsCapturing(stream_, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
+            return def;
+        char key[256];
+        double len[3];
+        for (int a = 0; a < 3; ++a)
+            len[a] = std::sqrt(grid_->steps(0, a) * grid_->steps(0, a) + grid_->steps(1, a) * grid_->steps(1, a) +
+                               grid_->steps(2, a) * grid_->steps(2, a));
+        std::snprintf(key, sizeof key, "%p|%d|%d|%d|%.6g,%.6g,%.6g", static_cast<const void*>(&mol_),
+                      static_cast<int>(backend_), npanel, mixed_exact_rows(), len[0], len[1], len[2]);
+        TileTuner& tt = tile_tuner();
+        std::vector<TileRank> rank;
+        {
+            std::lock_guard<std::mutex> lock(tt.mu);
+            auto it = tt.ranked.find(key);
+            if (it != tt.ranked.end()) rank = it->second;
+        }
+        const auto cands = tile_candidates(*grid_);
+        if (rank.empty()) {
+            rank = probe_shapes(cands);
+            std::lock_guard<std::mutex> lock(tt.mu);
+            tt.ranked[key] = rank;
+        }
+        for (const auto& r : rank)
+            for (const auto& c : cands)
+                if (c.sa == r.sa && c.sb == r.sb && c.sc == r.sc && c.padded() == def.padded()) return c;
+        return def;
+    }
+
+    // Times each candidate on the probe sub-grid; fastest first.
+    std::vector<TileRank> probe_shapes(const std::vector<detail::TileShape>& cands) const {
+        Grid sub = *grid_;
+        long long lo[3];
+        for (int a = 0; a < 3; ++a) {
+            const int n = std::min(grid_->counts[a], 32);
+            lo[a] = (grid_->counts[a] - n) / 2;
+            sub.counts[a] = n;
+        }
+        for (int r = 0; r < 3; ++r)
+            sub.origin[r] = grid_->origin[r] + ((grid_->steps(r, 0) * double(lo[0]) + grid_->steps(r, 1) * double(lo[1])) +
+                                                grid_->steps(r, 2) * double(lo[2]));
+        Request probe;
+        std::size_t chans = 0;
+        for (const auto& [key, ptr] : outs_)
+            if (from_point_path(key, backend_, true)) {
+                probe.add(key);
+                chans += property_channels(key.kind);
+            }
+        const std::size_t np = detail::validated_point_count(sub);
+        DeviceAlloc buf(sizeof(double) * std::max<std::size_t>(chans * np, 1), stream_);
+        std::vector<double*> outs;
+        std::size_t off = 0;
+        for (const auto& q : probe.properties()) {
+            outs.push_back(buf.as<double>() + off * np);
+            off += property_channels(q.kind);
+        }
+        EvaluationOptions o = opt_;
+        o.progress = {};
+        o.backend = backend_;
+        const Evaluator ev(mol_, o);
+        cudaEvent_t e0, e1;
+        check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
+        check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
+        std::vector<TileRank> rank;
+        for (const auto& c : cands) {
+            const int shape[3] = {c.sa, c.sb, c.sc};
+            t_forced_shape = shape;
+            double best = 1e300;
+            try {
+                for (int rep = 0; rep < 3; ++rep) {
+                    check_cuda(cudaEventRecord(e0, stream_), "cudaEventRecord");
+                    ev.evaluate_device(sub, probe, outs.data(), stream_);
+                    check_cuda(cudaEventRecord(e1, stream_), "cudaEventRecord");
+                    check_cuda(cudaEventSynchronize(e1), "cudaEventSynchronize (tile tuning)");
+                    float ms = 0.f;
+                    check_cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+                    if (rep > 0) best = std::min(best, static_cast<double>(ms));
+                }
+            } catch (...) {
+                t_forced_shape = nullptr;
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                throw;
+            }
+            t_forced_shape = nullptr;
+            rank.push_back({c.sa, c.sb, c.sc, best});
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        std::stable_sort(rank.begin(), rank.end(), [](const TileRank& x, const TileRank& y) { return x.ms < y.ms; });
+        return rank;
+    }
+
+    MixedLayout mixed_layout(int npanel) const {
         MixedLayout L;
         L.src = src_;
         const std::size_t bs = cta_block();
@@ -465,7 +628,8 @@ private:
             L.count = static_cast<long long>(n_);
             return L;
         }
-        const detail::TileShape ts = detail::choose_tiles(*grid_);
+        const detail::TileShape ts = t_forced_shape ? shape_on(*grid_, t_forced_shape[0], t_forced_shape[1], t_forced_shape[2])
+                                                    : tuned_shape(npanel);
         const kumo_dev::GridTiles t{1,           ts.sa,       ts.sb,   ts.sc, grid_->counts[0], grid_->counts[1],
                                     grid_->counts[2], ts.tny, ts.tnz};
         const long long best_pad = ts.padded();
@@ -533,7 +697,7 @@ private:
         if (!e || std::string(e) != "1") return false;
         if (!kumo_dev::contract_fused_supported(npanel, dev_->basis.nblocks)) return false;
         const std::size_t bs = cta_block();
-        const MixedLayout lay = mixed_layout();
+        const MixedLayout lay = mixed_layout(npanel);
         const std::size_t nblocks = lay.nblocks;
         const int nao = dev_->basis.nao;
         kumo_dev::ContractFusedParams cp{};
@@ -586,7 +750,7 @@ private:
     void mo_pass_mixed(int ao_order, int npanel, const std::array<bool, 4>& needed, const kumo_dev::FieldSpec& spec) {
         if (mo_pass_fused(ao_order, npanel, needed, spec)) return;
         const std::size_t bs = cta_block();
-        const MixedLayout lay = mixed_layout();
+        const MixedLayout lay = mixed_layout(npanel);
         const std::size_t nblocks = lay.nblocks;
         const int nao = dev_->basis.nao;
         const int stride = (nao + 7) / 8 * 8;
@@ -656,7 +820,7 @@ private:
     // Y = P[kept, kept] Phi contraction (density_derivatives_shared).
     void p_pass_mixed(int ao_order, int npanel, const std::array<bool, 4>& needed, const kumo_dev::FieldSpec& spec) {
         const std::size_t bs = cta_block();
-        const MixedLayout lay = mixed_layout();
+        const MixedLayout lay = mixed_layout(npanel);
         const std::size_t nblocks = lay.nblocks;
         const int nao = dev_->basis.nao;
         const int stride = (nao + 7) / 8 * 8;
@@ -1036,6 +1200,24 @@ Results Evaluator::evaluate(Points points, const Request& request) const {
     }
     return res;
 }
+
+namespace detail {
+std::string tile_tuning_report() {
+    TileTuner& tt = tile_tuner();
+    std::lock_guard<std::mutex> lock(tt.mu);
+    std::string out;
+    for (const auto& [key, rank] : tt.ranked) {
+        out += key;
+        for (const auto& r : rank) {
+            char b[64];
+            std::snprintf(b, sizeof b, " %dx%dx%d:%.4fms", 1 << r.sa, 1 << r.sb, 1 << r.sc, r.ms);
+            out += b;
+        }
+        out += '\n';
+    }
+    return out;
+}
+}  // namespace detail
 
 void Evaluator::validate(const Request& request) const { Run run(*this, nullptr, nullptr, 0, request, nullptr); }
 

@@ -160,7 +160,7 @@ EXPORTS = [
     "kumo_map_on_density_isosurface", "kumo_average_local_ionization_energy", "kumo_extract_isosurface",
     "kumo_surface_info", "kumo_surface_mesh", "kumo_surface_field", "kumo_surface_destroy",
     "kumo_surface_statistics", "kumo_write_ply", "kumo_read_cube", "kumo_cube_info", "kumo_cube_data",
-    "kumo_cube_destroy", "kumo_write_cube_data",
+    "kumo_cube_destroy", "kumo_write_cube_data", "kumo_tile_tuning_report",
 ]
 
 
@@ -231,6 +231,8 @@ def lib():
                                       C.c_longlong, *eb]
         L.kumo_grid_around.argtypes = [C.c_void_p, C.c_double, C.c_double, C.POINTER(_Grid), *eb]
         L.kumo_read_cube.argtypes = [C.c_char_p, C.POINTER(C.c_void_p), *eb]
+        L.kumo_tile_tuning_report.argtypes = [C.c_char_p, C.c_size_t]
+        L.kumo_tile_tuning_report.restype = C.c_longlong
         L.kumo_cube_info.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(_Grid), _I]
         L.kumo_cube_data.argtypes = [C.c_void_p, _I, _D, _D, _D, C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t]
         L.kumo_cube_destroy.argtypes = [C.c_void_p]
@@ -602,6 +604,15 @@ def write_cube_data(path: str, cube: CubeData) -> None:
     _check(lib().kumo_write_cube_data(os.fsencode(path), cube.first_comment.encode(), cube.second_comment.encode(),
                                       int(cube.coordinates_in_angstrom), C.byref(g), len(z), z.ctypes.data_as(_I),
                                       _dp(q), _dp(x), _dp(v), e, 512), e)
+
+
+def tile_tuning_report() -> str:
+    """The mixed form's measured tile shapes (kumo_tile_tuning_report)."""
+    L = lib()
+    n = L.kumo_tile_tuning_report(None, 0)
+    buf = C.create_string_buffer(max(int(n), 0) + 1)
+    L.kumo_tile_tuning_report(buf, len(buf))
+    return buf.value.decode()
 
 
 def set_device(device: int) -> None:

@@ -197,6 +197,13 @@ int kumo_write_cube(const char* path, const char* comment, const kumo_grid* grid
                     const int* atomic_numbers, const double* charges, const double* xyz,
                     const double* values, long long orbital_index, char* err, size_t errlen);
 
+/* No counterpart in the reference.  The mixed form's tile-shape autotuner:
+ * the shapes timed so far, one line per key (molecule, backend, panels,
+ * exact rows, grid step lengths) with the candidates fastest first as
+ * "AxBxC:time".  Copies at most len - 1 bytes and a NUL; returns the length
+ * of the whole report. */
+long long kumo_tile_tuning_report(char* buf, size_t len);
+
 /* read_cube (include/chem/kumo/cube.hpp:32 of chem-kumo; src/cube.cpp:114-212):
  * a scalar Cube file, plain or gzip, into a handle; angstrom headers are
  * converted to bohr.  kumo_cube_info gives the atom count, the grid (bohr)

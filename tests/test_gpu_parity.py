@@ -782,3 +782,28 @@ def test_mixed_accuracy_organic740_subgrid(synth_cache):
             assert e["rel"] <= 1e-7, (name, e)
         if name == "elf":
             assert e["scaled"] <= 1e-7, (name, e)
+
+
+def test_tile_autotuner_ranks_shapes_and_is_repeatable(monkeypatch):
+    # Grids above 131,072 points: the mixed form times the compact tile
+    # shapes on a probe sub-grid, keeps the ranking and evaluates with the
+    # fastest; the result agrees with the default shape to the mixed
+    # tolerance and repeats bit for bit.
+    m = K.Molecule.from_fchk(os.path.join(GOLDEN, "acrolein.fchk.gz"))
+    _, _, xyz = m.atoms()
+    n = 56
+    grid = K.Grid(xyz.mean(axis=0) - 0.5 * 0.2 * (n - 1), np.eye(3) * 0.2, (n, n, n))
+    props = [K.density(P.Density), K.density(P.Gradient), K.density(P.Laplacian), K.density(P.Tau)]
+    ev = K.Evaluator(m, precision=K.Precision.Mixed)
+    a, _ = ev.evaluate_grid(grid, props)
+    report = K.tile_tuning_report()
+    print(report)
+    line = [l for l in report.splitlines() if "|5|" in l]
+    assert line and len(line[-1].split()) >= 3  # key and at least two timed shapes
+    b, _ = ev.evaluate_grid(grid, props)
+    monkeypatch.setenv("KUMO_TILE_AUTOTUNE", "0")
+    c, _ = ev.evaluate_grid(grid, props)
+    f64, _ = K.Evaluator(m).evaluate_grid(grid, props)
+    for x, y, z, r in zip(a, b, c, f64):
+        assert np.array_equal(x, y)
+        assert scaled_error(x, r) <= 1e-7 and scaled_error(z, r) <= 1e-7

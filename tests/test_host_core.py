@@ -18,7 +18,7 @@ FCHKS = ["o2.fchk.gz", "h2o_b3lyp_def2tzvp.fchk.gz", "acrolein.fchk.gz"]
 
 def test_library_exports_every_declared_symbol():
     header = open(K.HEADER_PATH).read()
-    declared = set(re.findall(r"^\s*(?:int|void)\s+(kumo_\w+)\s*\(", header, flags=re.M))
+    declared = set(re.findall(r"^\s*(?:int|void|long long)\s+(kumo_\w+)\s*\(", header, flags=re.M))
     assert declared == set(K.EXPORTS)
     lib = K.lib()
     for name in declared:
