@@ -684,7 +684,7 @@ def main() -> None:
             "data": "synthetic (seeded FCHK)",
             "config": {"workload": "organic_740 (C12N4O4H20, 740 AOs, 76 occ MOs) rho/grad/lap/tau/ELF on 128^3 @0.2 bohr",
                        "points": n_total, "points_rank0": n, "backend": "AO_MO", "block": 128,
-                       "threshold": 1e-12, "exact_rows": int(os.environ.get("KUMO_MIXED_EXACT_ROWS", "64")),
+                       "threshold": 1e-12, "exact_rows": int(os.environ.get("KUMO_MIXED_EXACT_ROWS", "32")),
                        "l2": "256 MB buffer written between timed steps (untimed); AO scratch > L2",
                        "parallelism": f"slabs of whole planes x{world} (one grid, strong)"},
             "fp64": {"value": n_total / (ms_f64 * 1e-3), "ms_per_step": ms_f64},

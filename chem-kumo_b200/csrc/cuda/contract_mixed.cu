@@ -522,61 +522,145 @@ __device__ __forceinline__ int ao_block_of(const DevBasis& B, int ao) {
     return lo;
 }
 
-// FP64 value, and for P >= 4 the gradient, for P == 5 the Laplacian, of AO
-// m of AO block s at offset (dx, dy, dz) from the block's centre, in closed
-// form: with R_n,k = sum_p W[k][p] a_p^n exp(-a_p r^2) and M_k the monomial of
-// Cartesian component k (Gaussian order), value = sum_k T[m][k] M_k R_0,k,
-// d/dx = sum_k T[m][k] (dM_k/dx R_0,k - 2 x M_k R_1,k) and Laplacian =
-// sum_k T[m][k] (lap(M_k) R_0,k + M_k (4 r^2 R_2,k - (4 l + 6) R_1,k)) (T the
-// identity for Cartesian blocks).  The same functions as the reference's
+// FP64 AO values of the exact rows of one AO block (shell) s at one point,
+// offset (dx, dy, dz) from the shell's centre, in closed form: with
+// R_n,k = sum_p W[k][p] a_p^n exp(-a_p r^2) and M_k the monomial of Cartesian
+// component k (Gaussian order), value = sum_k T[m][k] M_k R_0,k,
+// d/dx = sum_k T[m][k] (dM_k/dx R_0,k - 2 x M_k R_1,k), and Laplacian =
+// sum_k T[m][k] (lap(M_k) R_0,k + M_k (4 r^2 R_2,k - (4 L + 6) R_1,k)) (T the
+// identity for Cartesian shells): the functions of the reference's
 // evaluate_derivatives_batch (src/basis_evaluator.cpp:512-643), rounded
-// differently; zero beyond the block's cutoff radius, as there.
-template <int P>
-__device__ void exact_ao(const DevBasis& B, const double (&pure)[3][135], int s, int m, double dx, double dy,
-                         double dz, double (&out)[P]) {
-#pragma unroll
-    for (int c = 0; c < P; ++c) out[c] = 0.0;
+// differently; zero beyond the shell's cutoff radius, as there.  The radial
+// sums are formed once per shell and point for all of the shell's rows
+// (rows[j] the staging row of component ms[j]); values for P = 1 (value),
+// 4 (+ gradient) or 5 (+ Laplacian) go to out[(row * P + c) * ld + col].
+template <int L, bool PURE, int P>
+__device__ void exact_shell(const DevBasis& B, const double (&pure)[3][135], int s, double dx, double dy, double dz,
+                            int nrows, const int* rows, const int* ms, double* out, int ld, int col) {
+    constexpr int NC = (L + 1) * (L + 2) / 2;
     const double4 o = B.origin_r2[s];
     const double r2 = dx * dx + dy * dy + dz * dz;
-    if (r2 > o.w) return;
+    if (r2 > o.w) {
+        for (int j = 0; j < nrows; ++j)
+#pragma unroll
+            for (int c = 0; c < P; ++c) out[(rows[j] * P + c) * ld + col] = 0.0;
+        return;
+    }
+    const int4 inf = B.info[s];
+    const int nprim = inf.x >> 16;
+    double R0[NC], R1[NC], R2[NC];
+#pragma unroll
+    for (int k = 0; k < NC; ++k) R0[k] = R1[k] = R2[k] = 0.0;
+    const double* W = B.weights + inf.z;
+    for (int q = 0; q < nprim; ++q) {
+        const double a = B.exps[inf.y + q];
+        const double e = exp(-a * r2);
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            const double we = W[k * nprim + q] * e;
+            R0[k] += we;
+            R1[k] += we * a;
+            R2[k] += we * (a * a);
+        }
+    }
+    for (int j = 0; j < nrows; ++j) {
+        const int m = ms[j];
+        double v[P];
+#pragma unroll
+        for (int c = 0; c < P; ++c) v[c] = 0.0;
+        static_for<NC>([&](auto kc) {
+            constexpr int k = decltype(kc)::value;
+            const double t = PURE ? pure[L - 2][m * NC + k] : (k == m ? 1.0 : 0.0);
+            if (t == 0.0) return;
+            constexpr int a = cart_power(L, k, 0), b = cart_power(L, k, 1), c = cart_power(L, k, 2);
+            const double xa = ipow(dx, a), yb = ipow(dy, b), zc = ipow(dz, c);
+            const double M = xa * yb * zc;
+            v[0] += t * (M * R0[k]);
+            if constexpr (P >= 4) {
+                const double mx = a ? a * ipow(dx, a - 1) * yb * zc : 0.0;
+                const double my = b ? b * xa * ipow(dy, b - 1) * zc : 0.0;
+                const double mz = c ? c * xa * yb * ipow(dz, c - 1) : 0.0;
+                v[1] += t * (mx * R0[k] - 2.0 * dx * M * R1[k]);
+                v[2] += t * (my * R0[k] - 2.0 * dy * M * R1[k]);
+                v[3] += t * (mz * R0[k] - 2.0 * dz * M * R1[k]);
+            }
+            if constexpr (P == 5) {
+                const double lap = (a > 1 ? a * (a - 1) * ipow(dx, a - 2) * yb * zc : 0.0) +
+                                   (b > 1 ? b * (b - 1) * xa * ipow(dy, b - 2) * zc : 0.0) +
+                                   (c > 1 ? c * (c - 1) * xa * yb * ipow(dz, c - 2) : 0.0);
+                v[4] += t * (lap * R0[k] + M * (4.0 * r2 * R2[k] - (4.0 * L + 6.0) * R1[k]));
+            }
+        });
+#pragma unroll
+        for (int c = 0; c < P; ++c) out[(rows[j] * P + c) * ld + col] = v[c];
+    }
+}
+
+// The same for any shell with runtime loops and the radial sums of one
+// Cartesian component at a time (exponentials recomputed per component):
+// for g shells, whose 15 components would not fit the registers.
+template <int P>
+__device__ void exact_shell_loops(const DevBasis& B, const double (&pure)[3][135], int s, double dx, double dy,
+                                  double dz, int nrows, const int* rows, const int* ms, double* out, int ld, int col) {
+    const double4 o = B.origin_r2[s];
+    const double r2 = dx * dx + dy * dy + dz * dz;
     const int4 inf = B.info[s];
     const int l = inf.x & 0xff, nprim = inf.x >> 16;
     const bool is_pure = ((inf.x >> 8) & 1) && l >= 2;
-    const int ncart = (l + 1) * (l + 2) / 2;
-    double e[kMaxPrim], al[kMaxPrim];
-    for (int q = 0; q < nprim; ++q) {
-        al[q] = B.exps[inf.y + q];
-        e[q] = exp(-al[q] * r2);
-    }
+    const int nc = (l + 1) * (l + 2) / 2;
     const double* W = B.weights + inf.z;
-    for (int k = 0; k < ncart; ++k) {
-        const double t = is_pure ? pure[l - 2][m * ncart + k] : (k == m ? 1.0 : 0.0);
-        if (t == 0.0) continue;
-        double R0 = 0.0, R1 = 0.0, R2 = 0.0;
-        for (int q = 0; q < nprim; ++q) {
-            const double we = W[k * nprim + q] * e[q];
-            R0 += we;
-            R1 += we * al[q];
-            R2 += we * (al[q] * al[q]);
+    for (int j = 0; j < nrows; ++j) {
+        const int m = ms[j];
+        double v[P];
+#pragma unroll
+        for (int c = 0; c < P; ++c) v[c] = 0.0;
+        if (!(r2 > o.w)) {
+            for (int k = 0; k < nc; ++k) {
+                const double t = is_pure ? pure[l - 2][m * nc + k] : (k == m ? 1.0 : 0.0);
+                if (t == 0.0) continue;
+                double R0 = 0.0, R1 = 0.0, R2 = 0.0;
+                for (int q = 0; q < nprim; ++q) {
+                    const double a = B.exps[inf.y + q];
+                    const double we = W[k * nprim + q] * exp(-a * r2);
+                    R0 += we;
+                    R1 += we * a;
+                    R2 += we * (a * a);
+                }
+                const int a = cart_power(l, k, 0), b = cart_power(l, k, 1), c = cart_power(l, k, 2);
+                const double xa = ipow(dx, a), yb = ipow(dy, b), zc = ipow(dz, c);
+                const double M = xa * yb * zc;
+                v[0] += t * (M * R0);
+                if constexpr (P >= 4) {
+                    v[1] += t * ((a ? a * ipow(dx, a - 1) * yb * zc : 0.0) * R0 - 2.0 * dx * M * R1);
+                    v[2] += t * ((b ? b * xa * ipow(dy, b - 1) * zc : 0.0) * R0 - 2.0 * dy * M * R1);
+                    v[3] += t * ((c ? c * xa * yb * ipow(dz, c - 1) : 0.0) * R0 - 2.0 * dz * M * R1);
+                }
+                if constexpr (P == 5) {
+                    const double lap = (a > 1 ? a * (a - 1) * ipow(dx, a - 2) * yb * zc : 0.0) +
+                                       (b > 1 ? b * (b - 1) * xa * ipow(dy, b - 2) * zc : 0.0) +
+                                       (c > 1 ? c * (c - 1) * xa * yb * ipow(dz, c - 2) : 0.0);
+                    v[4] += t * (lap * R0 + M * (4.0 * r2 * R2 - (4.0 * l + 6.0) * R1));
+                }
+            }
         }
-        const int a = cart_power(l, k, 0), b = cart_power(l, k, 1), c = cart_power(l, k, 2);
-        const double xa = ipow(dx, a), yb = ipow(dy, b), zc = ipow(dz, c);
-        const double M = xa * yb * zc;
-        out[0] += t * (M * R0);
-        if constexpr (P >= 4) {
-            const double mx = a ? a * ipow(dx, a - 1) * yb * zc : 0.0;
-            const double my = b ? b * xa * ipow(dy, b - 1) * zc : 0.0;
-            const double mz = c ? c * xa * yb * ipow(dz, c - 1) : 0.0;
-            out[1] += t * (mx * R0 - 2.0 * dx * M * R1);
-            out[2] += t * (my * R0 - 2.0 * dy * M * R1);
-            out[3] += t * (mz * R0 - 2.0 * dz * M * R1);
-        }
-        if constexpr (P == 5) {
-            const double lap = (a > 1 ? a * (a - 1) * ipow(dx, a - 2) * yb * zc : 0.0) +
-                               (b > 1 ? b * (b - 1) * xa * ipow(dy, b - 2) * zc : 0.0) +
-                               (c > 1 ? c * (c - 1) * xa * yb * ipow(dz, c - 2) : 0.0);
-            out[4] += t * (lap * R0 + M * (4.0 * r2 * R2 - (4.0 * l + 6.0) * R1));
-        }
+#pragma unroll
+        for (int c = 0; c < P; ++c) out[(rows[j] * P + c) * ld + col] = v[c];
+    }
+}
+
+template <int P>
+__device__ void exact_shell_any(const DevBasis& B, const double (&pure)[3][135], int s, double dx, double dy,
+                                double dz, int nrows, const int* rows, const int* ms, double* out, int ld, int col) {
+    const int4 inf = B.info[s];
+    const int l = inf.x & 0xff;
+    const bool pure_shell = ((inf.x >> 8) & 1) && l >= 2;
+    switch (l | (pure_shell ? 16 : 0)) {
+#define KUMO_EXACT(LL, PP) \
+    case (LL) | ((PP) ? 16 : 0): exact_shell<LL, PP, P>(B, pure, s, dx, dy, dz, nrows, rows, ms, out, ld, col); break;
+        KUMO_EXACT(0, false) KUMO_EXACT(1, false) KUMO_EXACT(2, false) KUMO_EXACT(3, false)
+        KUMO_EXACT(2, true) KUMO_EXACT(3, true)
+#undef KUMO_EXACT
+        default: exact_shell_loops<P>(B, pure, s, dx, dy, dz, nrows, rows, ms, out, ld, col); break;
     }
 }
 
@@ -681,7 +765,11 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
     // columns [row][N] and the AO values [row][panel][point] of the points of
     // one phase (128, 64 or 32 points: as many as fit).
     const unsigned xs_bytes = 2u * L::a_bytes + F * L::f_bytes + SB * b_bytes;
-    auto xs_need = [&](int rows, int ph) { return 8u * static_cast<unsigned>(rows) * (N + P * ph + 1); };
+    // Per exact row: its coefficients (N doubles), its AO values at the
+    // phase's points (P * ph doubles) and six ints of row and shell tables.
+    auto xs_need = [&](int rows, int ph) {
+        return 8u * static_cast<unsigned>(rows) * (N + P * ph) + 24u * static_cast<unsigned>(rows) + 16u;
+    };
     int nx = prm.exact_rows < nk ? prm.exact_rows : nk;
     while (nx > 0 && xs_need(nx, 32) > xs_bytes) --nx;
     const int ph_points = xs_need(nx, 128) <= xs_bytes ? 128 : (xs_need(nx, 64) <= xs_bytes ? 64 : 32);
@@ -875,7 +963,14 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
             constexpr int MG = 4;
             double* xs_c = reinterpret_cast<double*>(sm);
             double* xs_phi = xs_c + nx * N;
-            int* xs_row = reinterpret_cast<int*>(xs_phi + nx * P * ph_points);
+            // Row tables: shell and component of each exact row, the rows
+            // grouped by shell (grp_rows, group j spans grp_first[j] ..
+            // grp_first[j + 1]) and the groups' shells.
+            int* xs_shell = reinterpret_cast<int*>(xs_phi + nx * P * ph_points);
+            int* xs_m = xs_shell + nx;
+            int* grp_rows = xs_m + nx;
+            int* grp_m = grp_rows + nx;
+            int* grp_first = grp_m + nx;  // nx + 2 entries; [nx + 1] holds the group count
             if (nx > 0) {
                 const int half_n = N / 2;
                 for (int v = tid; v < nx * half_n; v += kBulkThreads) {
@@ -889,30 +984,49 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                 for (int r = tid; r < nx; r += kBulkThreads) {
                     const int ao = static_cast<int>(aoidx[nkt + r]);
                     const int sh = ao_block_of(prm.basis, ao);
-                    xs_row[2 * r] = sh;
-                    xs_row[2 * r + 1] = ao - prm.basis.info[sh].w;
+                    xs_shell[r] = sh;
+                    xs_m[r] = ao - prm.basis.info[sh].w;
+                }
+                __syncthreads();
+                // Rows in (shell, row) order.
+                for (int r = tid; r < nx; r += kBulkThreads) {
+                    const int sh = xs_shell[r];
+                    int pos = 0;
+                    for (int q = 0; q < nx; ++q) pos += (xs_shell[q] < sh || (xs_shell[q] == sh && q < r)) ? 1 : 0;
+                    grp_rows[pos] = r;
+                    grp_m[pos] = xs_m[r];
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    int ng = 0;
+                    for (int j = 0; j < nx; ++j)
+                        if (j == 0 || xs_shell[grp_rows[j]] != xs_shell[grp_rows[j - 1]]) grp_first[ng++] = j;
+                    grp_first[ng] = nx;
+                    grp_first[nx + 1] = ng;
                 }
                 __syncthreads();
             }
+            const int ngrp = nx > 0 ? grp_first[nx + 1] : 0;
             for (int ph0 = 0; ph0 < kBlockPoints; ph0 += ph_points) {
                 if (nx > 0) {
-                    // FP64 AO values of the exact rows at this phase's points.
-                    for (int v = tid; v < nx * ph_points; v += kBulkThreads) {
-                        const int r = v / ph_points, pp = v - r * ph_points;
+                    // FP64 AO values of the exact rows at this phase's points,
+                    // one (shell, point) per thread.
+                    for (int v = tid; v < ngrp * ph_points; v += kBulkThreads) {
+                        const int g = v / ph_points, pp = v - g * ph_points;
+                        const int j0 = grp_first[g], nr = grp_first[g + 1] - j0;
+                        const int sh = xs_shell[grp_rows[j0]];
                         const long long e = start + ph0 + pp;
-                        double f[P];
                         if (ph0 + pp < bcount && point_exists(prm.src, e)) {
                             double x, y, z;
                             point_at(prm.src, e, x, y, z);
-                            const int sh = xs_row[2 * r];
                             const double4 o = prm.basis.origin_r2[sh];
-                            exact_ao<P>(prm.basis, prm.pure64, sh, xs_row[2 * r + 1], x - o.x, y - o.y, z - o.z, f);
+                            exact_shell_any<P>(prm.basis, prm.pure64, sh, x - o.x, y - o.y, z - o.z, nr, grp_rows + j0,
+                                               grp_m + j0, xs_phi, ph_points, pp);
                         } else {
+                            for (int j = 0; j < nr; ++j)
 #pragma unroll
-                            for (int c = 0; c < P; ++c) f[c] = 0.0;
+                                for (int c = 0; c < P; ++c) xs_phi[(grp_rows[j0 + j] * P + c) * ph_points + pp] = 0.0;
                         }
-#pragma unroll
-                        for (int c = 0; c < P; ++c) xs_phi[(r * P + c) * ph_points + pp] = f[c];
                     }
                     __syncthreads();
                 }

@@ -75,8 +75,10 @@ constexpr unsigned kSuspendNs = 20000;
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned long long limit_ns = 0) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long limit = limit_ns ? limit_ns : kWaitNs;
+    // A suspended try_wait may sleep up to its hint: never longer than the limit.
+    const unsigned hint = limit < kSuspendNs ? static_cast<unsigned>(limit) : kSuspendNs;
     const unsigned long long t0 = global_ns();
-    while (!mbar_try_wait_suspend(bar, parity, kSuspendNs))
+    while (!mbar_try_wait_suspend(bar, parity, hint))
         if (global_ns() - t0 > limit) return false;
     return true;
 }

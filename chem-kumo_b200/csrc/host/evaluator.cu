@@ -47,12 +47,12 @@ using detail::check_cuda;
 
 // Rows per block that the mixed AO-MO contraction adds in FP64 (AO values
 // and products) rather than on the tensor cores (KUMO_MIXED_EXACT_ROWS, read
-// at each evaluation; default 64, 0 turns it off): the largest rows of each
+// at each evaluation; default 32, 0 turns it off): the largest rows of each
 // block, whose FP32 rounding and truncated tensor-core sums would otherwise
 // set the error of the densities at the block's points.
 int mixed_exact_rows() {
     const char* e = std::getenv("KUMO_MIXED_EXACT_ROWS");
-    return e ? std::max(0, std::atoi(e)) : 64;
+    return e ? std::max(0, std::atoi(e)) : 32;
 }
 
 // The mixed form of the potential (FP32 Hermite sums) is opt-in
