@@ -535,7 +535,7 @@ __device__ __forceinline__ int ao_block_of(const DevBasis& B, int ao) {
 // (rows[j] the staging row of component ms[j]); values for P = 1 (value),
 // 4 (+ gradient) or 5 (+ Laplacian) go to out[(row * P + c) * ld + col].
 template <int L, bool PURE, int P>
-__device__ void exact_shell(const DevBasis& B, const double (&pure)[3][135], int s, double dx, double dy, double dz,
+__device__ void exact_shell(const DevBasis& B, const double* pure, int s, double dx, double dy, double dz,
                             int nrows, const int* rows, const int* ms, double* out, int ld, int col) {
     constexpr int NC = (L + 1) * (L + 2) / 2;
     const double4 o = B.origin_r2[s];
@@ -570,7 +570,7 @@ __device__ void exact_shell(const DevBasis& B, const double (&pure)[3][135], int
         for (int c = 0; c < P; ++c) v[c] = 0.0;
         static_for<NC>([&](auto kc) {
             constexpr int k = decltype(kc)::value;
-            const double t = PURE ? pure[L - 2][m * NC + k] : (k == m ? 1.0 : 0.0);
+            const double t = PURE ? pure[(L - 2) * 135 + m * NC + k] : (k == m ? 1.0 : 0.0);
             if (t == 0.0) return;
             constexpr int a = cart_power(L, k, 0), b = cart_power(L, k, 1), c = cart_power(L, k, 2);
             const double xa = ipow(dx, a), yb = ipow(dy, b), zc = ipow(dz, c);
@@ -600,7 +600,7 @@ __device__ void exact_shell(const DevBasis& B, const double (&pure)[3][135], int
 // Cartesian component at a time (exponentials recomputed per component):
 // for g shells, whose 15 components would not fit the registers.
 template <int P>
-__device__ void exact_shell_loops(const DevBasis& B, const double (&pure)[3][135], int s, double dx, double dy,
+__device__ void exact_shell_loops(const DevBasis& B, const double* pure, int s, double dx, double dy,
                                   double dz, int nrows, const int* rows, const int* ms, double* out, int ld, int col) {
     const double4 o = B.origin_r2[s];
     const double r2 = dx * dx + dy * dy + dz * dz;
@@ -616,7 +616,7 @@ __device__ void exact_shell_loops(const DevBasis& B, const double (&pure)[3][135
         for (int c = 0; c < P; ++c) v[c] = 0.0;
         if (!(r2 > o.w)) {
             for (int k = 0; k < nc; ++k) {
-                const double t = is_pure ? pure[l - 2][m * nc + k] : (k == m ? 1.0 : 0.0);
+                const double t = is_pure ? pure[(l - 2) * 135 + m * nc + k] : (k == m ? 1.0 : 0.0);
                 if (t == 0.0) continue;
                 double R0 = 0.0, R1 = 0.0, R2 = 0.0;
                 for (int q = 0; q < nprim; ++q) {
@@ -649,7 +649,7 @@ __device__ void exact_shell_loops(const DevBasis& B, const double (&pure)[3][135
 }
 
 template <int P>
-__device__ void exact_shell_any(const DevBasis& B, const double (&pure)[3][135], int s, double dx, double dy,
+__device__ void exact_shell_any(const DevBasis& B, const double* pure, int s, double dx, double dy,
                                 double dz, int nrows, const int* rows, const int* ms, double* out, int ld, int col) {
     const int4 inf = B.info[s];
     const int l = inf.x & 0xff;

@@ -47,7 +47,7 @@ struct ContractMixedParams {
     int exact_rows = 0;
     PointSource src;        // the evaluation's points (for the exact rows)
     DevBasis basis;         // FP64 exponents and weights (for the exact rows)
-    double pure64[3][135];  // Cartesian-to-pure matrices, l = 2..4, row-major
+    const double* pure64 = nullptr;  // device: Cartesian-to-pure matrices, l = 2..4, [3][135] row-major
     // Limit of each tensor-core pipeline wait in ns (0: one second); a wait
     // that runs out sets *status and the CTA stores NaN for its points.
     unsigned long long wait_ns = 0;

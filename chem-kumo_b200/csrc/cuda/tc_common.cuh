@@ -75,10 +75,11 @@ constexpr unsigned kSuspendNs = 20000;
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned long long limit_ns = 0) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long limit = limit_ns ? limit_ns : kWaitNs;
-    // A suspended try_wait may sleep up to its hint: never longer than the limit.
-    const unsigned hint = limit < kSuspendNs ? static_cast<unsigned>(limit) : kSuspendNs;
+    // A limit below the suspend hint (finer than the global timer resolves)
+    // allows one suspended attempt of at most that long.
+    if (limit < kSuspendNs) return mbar_try_wait_suspend(bar, parity, static_cast<unsigned>(limit));
     const unsigned long long t0 = global_ns();
-    while (!mbar_try_wait_suspend(bar, parity, hint))
+    while (!mbar_try_wait_suspend(bar, parity, kSuspendNs))
         if (global_ns() - t0 > limit) return false;
     return true;
 }

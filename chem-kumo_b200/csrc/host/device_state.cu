@@ -130,6 +130,7 @@ DeviceMolecule::DeviceMolecule(const Molecule& m) {
                     throw std::logic_error("Cartesian-to-pure pattern mismatch");
             }
     }
+    pure_dev = upload(&pure_d[0][0], 3 * 135);
     const Matrix pt = m.density_matrix(DensityComponent::Total);
     const Matrix ps = m.density_matrix(DensityComponent::Difference);
     p_total = upload(pt.data(), pt.size());

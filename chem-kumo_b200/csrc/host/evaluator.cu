@@ -180,7 +180,8 @@ detail::TileShape shape_on(const Grid& g, int sa, int sb, int sc) {
 }
 
 // Candidate shapes for a grid: padding within 5% of the fewest and a
-// diagonal within twice the most compact's, the most compact first, at most 8.
+// diagonal within 1.25 times the most compact's (the compact shapes, whose
+// accuracy is the same), the most compact first, at most 8.
 std::vector<detail::TileShape> tile_candidates(const Grid& g) {
     double len[3];
     for (int a = 0; a < 3; ++a)
@@ -194,7 +195,7 @@ std::vector<detail::TileShape> tile_candidates(const Grid& g) {
     for (int sa = 0; sa <= 7; ++sa)
         for (int sb = 0; sa + sb <= 7; ++sb) {
             const detail::TileShape t = shape_on(g, sa, sb, 7 - sa - sb);
-            if (t.padded() <= best.padded() * 1.05 && diag(t) <= 2.0 * diag(best)) c.emplace_back(diag(t), t);
+            if (t.padded() <= best.padded() * 1.05 && diag(t) <= 1.25 * diag(best)) c.emplace_back(diag(t), t);
         }
     std::stable_sort(c.begin(), c.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
     std::vector<detail::TileShape> out;
@@ -795,8 +796,7 @@ private:
         cp.exact_rows = mixed_exact_rows();
         cp.src = lay.src;
         cp.basis = dev_->basis;
-        for (int l = 0; l < 3; ++l)
-            for (int i = 0; i < 135; ++i) cp.pure64[l][i] = dev_->pure_d[l][i];
+        cp.pure64 = dev_->pure_dev;
         for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
             const int nb = static_cast<int>(std::min<std::size_t>(W, nblocks - b0));
             bp.first_point = static_cast<long long>(b0 * bs);

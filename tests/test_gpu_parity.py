@@ -730,7 +730,8 @@ def test_mixed_grid_tiles_padding(monkeypatch, counts):
     # The mixed form evaluates grids as compact tiles of 128 points (shapes
     # chosen per grid: cubes, planes, lines); partial tiles at the edges are
     # padding.  Against the FP64 form and against the same form on runs of
-    # 128 points along k (KUMO_MIXED_TILES=0).
+    # 128 points along k (KUMO_MIXED_TILES=0).  A line's tiles are as long as
+    # runs of 128 points, so it gets the tolerance of linear blocks.
     m = K.Molecule.from_fchk(os.path.join(GOLDEN, "acrolein.fchk.gz"))
     _, _, xyz = m.atoms()
     c = xyz.mean(axis=0)
@@ -744,12 +745,14 @@ def test_mixed_grid_tiles_padding(monkeypatch, counts):
     monkeypatch.setenv("KUMO_MIXED_TILES", "0")
     linear, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_grid(grid, props)
     dense = f64[0][0] > 1e-6  # ELF, a ratio, is compared where the density is not negligible
+    compact = sorted(counts)[1] > 1  # tiles extend over at least two axes
     for p, t, l, r in zip(props, tiled, linear, f64):
         assert np.all(np.isfinite(t)), p
         if p.kind == P.Elf:
             t, l, r = t[:, dense], l[:, dense], r[:, dense]
-        assert scaled_error(t, r) <= 1e-7, (p, scaled_error(t, r))
-        assert scaled_error(l, r) <= (1e-5 if p.kind == P.Elf else 1e-6), (p, scaled_error(l, r))
+        loose = 1e-5 if p.kind == P.Elf else 1e-6
+        assert scaled_error(t, r) <= (1e-7 if compact else loose), (p, scaled_error(t, r))
+        assert scaled_error(l, r) <= loose, (p, scaled_error(l, r))
 
 
 def _field_errors(a, r, rho, positive):
