@@ -648,8 +648,15 @@ def main() -> None:
         if kern.startswith("contract"):
             achieved = st["flops"] / (st["ms"] * 1e-3) / 1e12
             peak = peaks["bf16_tflops"]
+            # DRAM bytes per launch: the ncu capture of contract_bulk_kernel on the
+            # 48^3 case read and wrote 1.210 GB for the 437,070 AO rows the AO
+            # kernel wrote (2,769 B per row); scaled by the rows written per launch.
+            ao = prof.get("ao_build", {})
+            rows_per_launch = ao["kept_rows"] / ao["launches"] if ao.get("launches") else 0.0
             roof = {"bound": "tensor", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": achieved / peak, "traffic": None,
+                    "frac": achieved / peak, "traffic": 2769.0 * rows_per_launch,
+                    "traffic_source": "ncu dram__bytes_read+write of contract_bulk_kernel, 48^3 capture, "
+                                      "per AO row written, scaled to this launch's rows",
                     "peak_source": f"{peak_kind} bf16_tflops (burst)",
                     "algorithmic": "2 * 128 points * 5 panels * 76 MOs per AO row of a block",
                     "issued_tflops": 6 * achieved,
@@ -684,7 +691,7 @@ def main() -> None:
             "data": "synthetic (seeded FCHK)",
             "config": {"workload": "organic_740 (C12N4O4H20, 740 AOs, 76 occ MOs) rho/grad/lap/tau/ELF on 128^3 @0.2 bohr",
                        "points": n_total, "points_rank0": n, "backend": "AO_MO", "block": 128,
-                       "threshold": 1e-12, "exact_rows": int(os.environ.get("KUMO_MIXED_EXACT_ROWS", "32")),
+                       "threshold": 1e-12, "exact_rows": int(os.environ.get("KUMO_MIXED_EXACT_ROWS", "38")),
                        "l2": "256 MB buffer written between timed steps (untimed); AO scratch > L2",
                        "parallelism": f"slabs of whole planes x{world} (one grid, strong)"},
             "fp64": {"value": n_total / (ms_f64 * 1e-3), "ms_per_step": ms_f64},

@@ -47,12 +47,12 @@ using detail::check_cuda;
 
 // Rows per block that the mixed AO-MO contraction adds in FP64 (AO values
 // and products) rather than on the tensor cores (KUMO_MIXED_EXACT_ROWS, read
-// at each evaluation; default 32, 0 turns it off): the largest rows of each
+// at each evaluation; default 38, 0 turns it off): the largest rows of each
 // block, whose FP32 rounding and truncated tensor-core sums would otherwise
 // set the error of the densities at the block's points.
 int mixed_exact_rows() {
     const char* e = std::getenv("KUMO_MIXED_EXACT_ROWS");
-    return e ? std::max(0, std::atoi(e)) : 32;
+    return e ? std::max(0, std::atoi(e)) : 38;
 }
 
 // The mixed form of the potential (FP32 Hermite sums) is opt-in
@@ -168,6 +168,9 @@ TileTuner& tile_tuner() {
 
 // Shape forced on the probe evaluations of this thread (sa, sb, sc), or null.
 thread_local const int* t_forced_shape = nullptr;
+// Whether evaluations on this thread may run probes (the serving loop's
+// scheduler thread may not: it only takes rankings already measured).
+thread_local bool t_probe_tiles = true;
 
 bool tile_autotune_enabled() {
     const char* e = std::getenv("KUMO_TILE_AUTOTUNE");
@@ -544,6 +547,7 @@ private:
             if (it != tt.ranked.end()) rank = it->second;
         }
         const auto cands = tile_candidates(*grid_);
+        if (rank.empty() && !t_probe_tiles) return def;
         if (rank.empty()) {
             rank = probe_shapes(cands);
             std::lock_guard<std::mutex> lock(tt.mu);
@@ -1202,6 +1206,8 @@ Results Evaluator::evaluate(Points points, const Request& request) const {
 }
 
 namespace detail {
+void set_tile_probing(bool on) { t_probe_tiles = on; }
+
 std::string tile_tuning_report() {
     TileTuner& tt = tile_tuner();
     std::lock_guard<std::mutex> lock(tt.mu);

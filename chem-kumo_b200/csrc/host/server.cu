@@ -38,6 +38,7 @@ namespace chem::kumo {
 
 namespace detail {
 void prepare_device_for_capture();
+void set_tile_probing(bool on);
 }
 
 namespace {
@@ -423,6 +424,9 @@ void Server::Impl::launch(Pending&& p) {
 void Server::Impl::run_scheduler() {
     check_cuda(cudaSetDevice(opt.device), "cudaSetDevice");
     check_cuda(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high), "cudaDeviceGetStreamPriorityRange");
+    // No synchronous tile-shape probes on this thread (they would hold up
+    // admission); grids take a shape already measured, or the default.
+    detail::set_tile_probing(false);
     detail::prepare_device_for_capture();
     for (;;) {
         bool progressed = false;

@@ -15,23 +15,29 @@ import pytest
 from conftest import GOLDEN
 
 import kumo_b200 as K
+from kumo_b200 import synth
 
 pytestmark = pytest.mark.gpu
 
 P = K.PropertyKind
 
+# The register-staged and AO-P kernels wait only on their own MMAs, which on
+# a small molecule are done before the wait starts: those cases use the
+# 740-AO molecule, whose longer K loops keep waits pending.
 CASES = {
-    "bulk_gradient": (K.Backend.AO_MO, [P.Density, P.Gradient, P.Tau, P.Elf]),
-    "bulk_laplacian": (K.Backend.AO_MO, [P.Density, P.Gradient, P.Laplacian, P.Tau]),
-    "register_staged_hessian": (K.Backend.AO_MO, [P.Density, P.Hessian]),
-    "ao_p": (K.Backend.AO_P, [P.Density, P.Gradient, P.Laplacian]),
+    "bulk_gradient": (K.Backend.AO_MO, [P.Density, P.Gradient, P.Tau, P.Elf], "acrolein"),
+    "bulk_laplacian": (K.Backend.AO_MO, [P.Density, P.Gradient, P.Laplacian, P.Tau], "acrolein"),
+    "register_staged_hessian": (K.Backend.AO_MO, [P.Density, P.Hessian], "organic_740"),
+    "ao_p": (K.Backend.AO_P, [P.Density, P.Gradient, P.Laplacian], "organic_740"),
 }
 
 
 @pytest.mark.parametrize("case", list(CASES))
-def test_pipeline_wait_timeout_is_reported_and_recovers(monkeypatch, case):
-    backend, kinds = CASES[case]
-    m = K.Molecule.from_fchk(os.path.join(GOLDEN, "acrolein.fchk.gz"))
+def test_pipeline_wait_timeout_is_reported_and_recovers(monkeypatch, synth_cache, case):
+    backend, kinds, name = CASES[case]
+    path = (os.path.join(GOLDEN, "acrolein.fchk.gz") if name == "acrolein"
+            else synth.workload_fchk(name, synth_cache))
+    m = K.Molecule.from_fchk(path)
     _, _, xyz = m.atoms()
     rng = np.random.default_rng(17)
     pts = rng.uniform(xyz.min(0) - 2.0, xyz.max(0) + 2.0, (3000, 3))
