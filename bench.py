@@ -162,13 +162,14 @@ def run_reference(args, rank: int) -> None:
 
 def field_errors(torch, a, r, rho, kind_positive: bool):
     """Errors of one field (channels x points, device tensors) against FP64:
-    `scaled` = max|a - r| / max(1, max|r|) (chem-kumo's
+    `abs` = max |a - r|, `scaled` = max|a - r| / max(1, max|r|) (chem-kumo's
     tests/density_screening_test.cpp:137-150), `pointwise` = max |a - r| /
     max(1, |a|, |r|) (tests/test_support.hpp:68-76), and for fields that are
     positive wherever rho > 1e-6 (rho, tau, ELF, RDG, the spin densities)
     `rel` = max |a - r| / |r| over those points."""
     d = (a - r).abs()
-    out = {"scaled": float(d.max() / max(1.0, float(r.abs().max()))),
+    out = {"abs": float(d.max()),
+           "scaled": float(d.max() / max(1.0, float(r.abs().max()))),
            "pointwise": float((d / torch.clamp(torch.maximum(a.abs(), r.abs()), min=1.0)).max())}
     if kind_positive:
         m = rho > 1e-6

@@ -960,7 +960,11 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
             const int i_lo = half * (N / 2), i_hi = min(nvalid, (half + 1) * (N / 2));
             const unsigned lane_addr = tmem + (static_cast<unsigned>(quarter * 32) << 16);
             const int ng = ntiles < G ? ntiles : G;
-            constexpr int MG = 4;
+            // Eight MO columns per register block: each exact row's P AO
+            // values are read once from shared memory for 8 P FP64 products
+            // (with four columns the shared-memory reads, not the FP64 pipe,
+            // set the epilogue's rate).
+            constexpr int MG = 8;
             double* xs_c = reinterpret_cast<double*>(sm);
             double* xs_phi = xs_c + nx * N;
             // Row tables: shell and component of each exact row, the rows
@@ -1054,10 +1058,15 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                         }
                         // The exact rows: FP64 AO values times FP64 coefficients.
                         for (int r = 0; r < nx; ++r) {
-                            const double* crow = xs_c + r * N + i0;
+                            // 64-byte aligned: N and i0 are multiples of 8.
+                            const double2* crow = reinterpret_cast<const double2*>(xs_c + r * N + i0);
                             double cv[MG];
 #pragma unroll
-                            for (int u = 0; u < MG; ++u) cv[u] = crow[u];
+                            for (int u = 0; u < MG / 2; ++u) {
+                                const double2 c2 = crow[u];
+                                cv[2 * u] = c2.x;
+                                cv[2 * u + 1] = c2.y;
+                            }
 #pragma unroll
                             for (int c = 0; c < P; ++c) {
                                 const double f = xs_phi[(r * P + c) * ph_points + pq];

@@ -66,6 +66,19 @@ __device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
     asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// Whether the phase has completed, without waiting.
+__device__ __forceinline__ bool mbar_test_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 // Waits until the phase with the given parity has completed; false if that
 // did not happen within limit_ns (0: kWaitNs).  The pipeline waits take the
 // evaluation's limit (kernel parameter wait_ns); the waits that drain a
@@ -73,11 +86,12 @@ __device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
 // kWaitNs.
 constexpr unsigned kSuspendNs = 20000;
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned long long limit_ns = 0) {
-    if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long limit = limit_ns ? limit_ns : kWaitNs;
     // A limit below the suspend hint (finer than the global timer resolves)
-    // allows one suspended attempt of at most that long.
-    if (limit < kSuspendNs) return mbar_try_wait_suspend(bar, parity, static_cast<unsigned>(limit));
+    // allows no waiting at all: try_wait may itself block for a
+    // system-dependent time, test_wait never does.
+    if (limit < kSuspendNs) return mbar_test_wait(bar, parity);
+    if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     while (!mbar_try_wait_suspend(bar, parity, kSuspendNs))
         if (global_ns() - t0 > limit) return false;
