@@ -39,10 +39,22 @@ __global__ void __launch_bounds__(kBlockPoints, (P == 10 || MAXL >= 4) ? 6 : 8) 
     int* kept = out.kept + static_cast<size_t>(blk) * out.row_stride;
     float* rmx = out.rowmax + static_cast<size_t>(blk) * out.row_stride * 4 + warp;
     int row = 0;
+    // The next listed block's centre and table entry are loaded one iteration
+    // ahead (read-only tables), so their latency overlaps this block's work.
+    double4 o_next = make_double4(0.0, 0.0, 0.0, -1.0);
+    int4 inf_next = make_int4(0, 0, 0, 0);
+    if (nlist > 0) {
+        o_next = B.origin_r2[s_list[0]];
+        inf_next = B.info[s_list[0]];
+    }
     for (int it = 0; it < nlist; ++it) {
-        const int s = s_list[it];
-        const double4 o = B.origin_r2[s];
-        const int4 inf = B.info[s];
+        const double4 o = o_next;
+        const int4 inf = inf_next;
+        if (it + 1 < nlist) {
+            const int sn = s_list[it + 1];
+            o_next = B.origin_r2[sn];
+            inf_next = B.info[sn];
+        }
         const int l = inf.x & 0xff;
         const bool pure = (inf.x >> 8) & 1;
         const int nprim = inf.x >> 16;

@@ -10,12 +10,16 @@ namespace kumo_dev {
 namespace {
 
 // exp(-a r^2) given al2 = a log2(e): FP64 argument reduction t = n - f with
-// |f| <= 1/2, FP32 2^f, exact scaling by 2^-n; 0 below the FP32 range.
+// |f| <= 1/2, FP32 2^f, scaling by 2^-n as two products by normal powers of
+// two (2^-h, h = n/2, exact; then 2^-(n-h), the only rounding, which also
+// gives the subnormal results exactly as ldexpf does); 0 below the FP32 range.
 __device__ __forceinline__ float exp_neg(double al2, double r2) {
     const double t = al2 * r2;
     if (!(t < 149.0)) return 0.0f;
     const double n = rint(t);
-    return ldexpf(exp2f(static_cast<float>(n - t)), -static_cast<int>(n));
+    const int ni = static_cast<int>(n), h = ni >> 1;
+    const float s1 = __int_as_float((127 - h) << 23), s2 = __int_as_float((127 - (ni - h)) << 23);
+    return (exp2f(static_cast<float>(n - t)) * s1) * s2;
 }
 
 template <int L, bool PURE, int P, bool ROWMAX = true>
@@ -122,7 +126,9 @@ __device__ __forceinline__ void mixed_shell(const AoMixedParams& prm, float x, f
             }
         }
         if constexpr (ROWMAX) {
-            mx = warp_max(mx);
+            // Non-negative floats order like their bit patterns: one warp
+            // reduction instruction.
+            mx = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(mx)));
             if (lane == 0) rmax[m * 4] = mx;
         }
     }

@@ -509,158 +509,208 @@ __device__ __forceinline__ double ipow(double x, int n) {
     return r;
 }
 
-// AO block (shell) holding AO `ao`: the last block whose first AO is <= ao.
-__device__ __forceinline__ int ao_block_of(const DevBasis& B, int ao) {
-    int lo = 0, hi = B.nblocks - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (B.info[mid].w <= ao)
-            lo = mid;
-        else
-            hi = mid - 1;
+// FP64 normalisation tables of the exact rows (the same for every basis;
+// upload_exact_tables copies them once per device): g_k of each Cartesian
+// component in Gaussian order, 1/g of the first component of each order, and
+// T[m][k] g_k of the Cartesian-to-pure transforms of l = 2..4 (row-major m, k).
+__constant__ double c_exact_g[kMaxL + 1][15];
+__constant__ double c_exact_ig0[kMaxL + 1];
+__constant__ double c_exact_tg[3][135];
+
+// Radial sums of the factorised weights W[k][p] = u_p g_k at squared distance
+// r2: S_n = sum_p u_p a_p^n exp(-a_p r2), n = 0, 1, 2, with u_p = W[0][p] / g_0
+// (one FP64 exponential per primitive for all components of the shell).
+__device__ __forceinline__ void exact_radial(const DevBasis& B, int4 inf, int l, double r2, double& S0, double& S1,
+                                             double& S2) {
+    const int nprim = inf.x >> 16;
+    const double* W0 = B.weights + inf.z;
+    const double* A = B.exps + inf.y;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll 4
+    for (int q = 0; q < nprim; ++q) {
+        const double a = A[q];
+        const double we = W0[q] * exp(-a * r2);
+        s0 += we;
+        s1 += we * a;
+        s2 += we * (a * a);
     }
-    return lo;
+    const double ig0 = c_exact_ig0[l];
+    S0 = s0 * ig0;
+    S1 = s1 * ig0;
+    S2 = s2 * ig0;
 }
 
 // FP64 AO values of the exact rows of one AO block (shell) s at one point,
-// offset (dx, dy, dz) from the shell's centre, in closed form: with
-// R_n,k = sum_p W[k][p] a_p^n exp(-a_p r^2) and M_k the monomial of Cartesian
-// component k (Gaussian order), value = sum_k T[m][k] M_k R_0,k,
-// d/dx = sum_k T[m][k] (dM_k/dx R_0,k - 2 x M_k R_1,k), and Laplacian =
-// sum_k T[m][k] (lap(M_k) R_0,k + M_k (4 r^2 R_2,k - (4 L + 6) R_1,k)) (T the
-// identity for Cartesian shells): the functions of the reference's
-// evaluate_derivatives_batch (src/basis_evaluator.cpp:512-643), rounded
-// differently; zero beyond the shell's cutoff radius, as there.  The radial
-// sums are formed once per shell and point for all of the shell's rows
-// (rows[j] the staging row of component ms[j]); values for P = 1 (value),
-// 4 (+ gradient) or 5 (+ Laplacian) go to out[(row * P + c) * ld + col].
+// offset (dx, dy, dz) from the shell's centre.  With R0 = S_0, R1' = -2 S_1,
+// R2' = 4 S_2 and the polynomial P_m = sum_k T[m][k] g_k M_k of output m (M_k
+// the monomial of Cartesian component k; T the identity for Cartesian
+// shells): value P_m R0, d/dx_i dP_m/dx_i R0 + x_i P_m R1', Laplacian
+// lap(P_m) R0 + P_m ((2L+3) R1' + r^2 R2') (lap(P_m) = 0 for solid
+// harmonics) -- the functions of the reference's evaluate_derivatives_batch
+// (src/basis_evaluator.cpp:512-643), rounded differently; zero beyond the
+// shell's cutoff radius, as there.  Bit m of `mask` marks an exact output m;
+// its staging row is slots[number of mask bits below m].  Values for P = 1
+// (value), 4 (+ gradient) or 5 (+ Laplacian) go to out[(row * P + c) * ld +
+// col].  The zero entries of the pure transforms are skipped at compile time.
 template <int L, bool PURE, int P>
-__device__ void exact_shell(const DevBasis& B, const double* pure, int s, double dx, double dy, double dz,
-                            int nrows, const int* rows, const int* ms, double* out, int ld, int col) {
+__device__ void exact_shell(const DevBasis& B, double4 o, int4 inf, double dx, double dy, double dz, unsigned mask,
+                            const int* slots, double* out, int ld, int col) {
     constexpr int NC = (L + 1) * (L + 2) / 2;
-    const double4 o = B.origin_r2[s];
+    constexpr int NOUT = PURE ? 2 * L + 1 : NC;
     const double r2 = dx * dx + dy * dy + dz * dz;
+    auto row_of = [&](int m) { return slots[__popc(mask & ((1u << m) - 1u))]; };
     if (r2 > o.w) {
-        for (int j = 0; j < nrows; ++j)
+        static_for<NOUT>([&](auto mc) {
+            constexpr int m = decltype(mc)::value;
+            if ((mask >> m) & 1u) {
+                const int r = row_of(m);
 #pragma unroll
-            for (int c = 0; c < P; ++c) out[(rows[j] * P + c) * ld + col] = 0.0;
-        return;
-    }
-    const int4 inf = B.info[s];
-    const int nprim = inf.x >> 16;
-    double R0[NC], R1[NC], R2[NC];
-#pragma unroll
-    for (int k = 0; k < NC; ++k) R0[k] = R1[k] = R2[k] = 0.0;
-    const double* W = B.weights + inf.z;
-    for (int q = 0; q < nprim; ++q) {
-        const double a = B.exps[inf.y + q];
-        const double e = exp(-a * r2);
-#pragma unroll
-        for (int k = 0; k < NC; ++k) {
-            const double we = W[k * nprim + q] * e;
-            R0[k] += we;
-            R1[k] += we * a;
-            R2[k] += we * (a * a);
-        }
-    }
-    for (int j = 0; j < nrows; ++j) {
-        const int m = ms[j];
-        double v[P];
-#pragma unroll
-        for (int c = 0; c < P; ++c) v[c] = 0.0;
-        static_for<NC>([&](auto kc) {
-            constexpr int k = decltype(kc)::value;
-            const double t = PURE ? pure[(L - 2) * 135 + m * NC + k] : (k == m ? 1.0 : 0.0);
-            if (t == 0.0) return;
-            constexpr int a = cart_power(L, k, 0), b = cart_power(L, k, 1), c = cart_power(L, k, 2);
-            const double xa = ipow(dx, a), yb = ipow(dy, b), zc = ipow(dz, c);
-            const double M = xa * yb * zc;
-            v[0] += t * (M * R0[k]);
-            if constexpr (P >= 4) {
-                const double mx = a ? a * ipow(dx, a - 1) * yb * zc : 0.0;
-                const double my = b ? b * xa * ipow(dy, b - 1) * zc : 0.0;
-                const double mz = c ? c * xa * yb * ipow(dz, c - 1) : 0.0;
-                v[1] += t * (mx * R0[k] - 2.0 * dx * M * R1[k]);
-                v[2] += t * (my * R0[k] - 2.0 * dy * M * R1[k]);
-                v[3] += t * (mz * R0[k] - 2.0 * dz * M * R1[k]);
-            }
-            if constexpr (P == 5) {
-                const double lap = (a > 1 ? a * (a - 1) * ipow(dx, a - 2) * yb * zc : 0.0) +
-                                   (b > 1 ? b * (b - 1) * xa * ipow(dy, b - 2) * zc : 0.0) +
-                                   (c > 1 ? c * (c - 1) * xa * yb * ipow(dz, c - 2) : 0.0);
-                v[4] += t * (lap * R0[k] + M * (4.0 * r2 * R2[k] - (4.0 * L + 6.0) * R1[k]));
+                for (int c = 0; c < P; ++c) out[(r * P + c) * ld + col] = 0.0;
             }
         });
+        return;
+    }
+    double S0, S1, S2;
+    exact_radial(B, inf, L, r2, S0, S1, S2);
+    const double R1p = -2.0 * S1, R2p = 4.0 * S2;
+    const double qf = (2.0 * L + 3.0) * R1p + r2 * R2p;
+    double xp[L + 1], yp[L + 1], zp[L + 1];
+    xp[0] = yp[0] = zp[0] = 1.0;
 #pragma unroll
-        for (int c = 0; c < P; ++c) out[(rows[j] * P + c) * ld + col] = v[c];
+    for (int n = 1; n <= L; ++n) {
+        xp[n] = xp[n - 1] * dx;
+        yp[n] = yp[n - 1] * dy;
+        zp[n] = zp[n - 1] * dz;
+    }
+    const double d[3] = {dx, dy, dz};
+    if constexpr (PURE) {
+        double pm[NOUT], pg[3][NOUT];
+#pragma unroll
+        for (int m = 0; m < NOUT; ++m) pm[m] = pg[0][m] = pg[1][m] = pg[2][m] = 0.0;
+        static_for<NC>([&](auto kc) {
+            constexpr int k = decltype(kc)::value;
+            constexpr int a = cart_power(L, k, 0), b = cart_power(L, k, 1), c = cart_power(L, k, 2);
+            const double M = xp[a] * yp[b] * zp[c];
+            [[maybe_unused]] double Mi[3] = {0.0, 0.0, 0.0};
+            if constexpr (P >= 4) {
+                if constexpr (a > 0) Mi[0] = a * xp[a > 0 ? a - 1 : 0] * yp[b] * zp[c];
+                if constexpr (b > 0) Mi[1] = b * xp[a] * yp[b > 0 ? b - 1 : 0] * zp[c];
+                if constexpr (c > 0) Mi[2] = c * xp[a] * yp[b] * zp[c > 0 ? c - 1 : 0];
+            }
+            static_for<NOUT>([&](auto mc) {
+                constexpr int m = decltype(mc)::value;
+                if constexpr (solid_harmonic_nonzero(L, m, a, b)) {
+                    const double t = c_exact_tg[L - 2][m * NC + k];
+                    pm[m] += t * M;
+                    if constexpr (P >= 4)
+#pragma unroll
+                        for (int i = 0; i < 3; ++i) pg[i][m] += t * Mi[i];
+                }
+            });
+        });
+        static_for<NOUT>([&](auto mc) {
+            constexpr int m = decltype(mc)::value;
+            if ((mask >> m) & 1u) {
+                double* dst = out + static_cast<long long>(row_of(m)) * P * ld + col;
+                dst[0] = pm[m] * S0;
+                if constexpr (P >= 4)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) dst[(1 + i) * ld] = pg[i][m] * S0 + d[i] * pm[m] * R1p;
+                if constexpr (P == 5) dst[4 * ld] = pm[m] * qf;
+            }
+        });
+    } else {
+        static_for<NC>([&](auto kc) {
+            constexpr int k = decltype(kc)::value;
+            if ((mask >> k) & 1u) {
+                constexpr int a = cart_power(L, k, 0), b = cart_power(L, k, 1), c = cart_power(L, k, 2);
+                const double g = c_exact_g[L][k];
+                const double M = g * (xp[a] * yp[b] * zp[c]);
+                double* dst = out + static_cast<long long>(row_of(k)) * P * ld + col;
+                dst[0] = M * S0;
+                if constexpr (P >= 4) {
+                    const double mx = a > 0 ? g * (a * xp[a > 0 ? a - 1 : 0] * yp[b] * zp[c]) : 0.0;
+                    const double my = b > 0 ? g * (b * xp[a] * yp[b > 0 ? b - 1 : 0] * zp[c]) : 0.0;
+                    const double mz = c > 0 ? g * (c * xp[a] * yp[b] * zp[c > 0 ? c - 1 : 0]) : 0.0;
+                    dst[ld] = mx * S0 + dx * M * R1p;
+                    dst[2 * ld] = my * S0 + dy * M * R1p;
+                    dst[3 * ld] = mz * S0 + dz * M * R1p;
+                }
+                if constexpr (P == 5) {
+                    const double lap = (a > 1 ? a * (a - 1) * xp[a > 1 ? a - 2 : 0] * yp[b] * zp[c] : 0.0) +
+                                       (b > 1 ? b * (b - 1) * xp[a] * yp[b > 1 ? b - 2 : 0] * zp[c] : 0.0) +
+                                       (c > 1 ? c * (c - 1) * xp[a] * yp[b] * zp[c > 1 ? c - 2 : 0] : 0.0);
+                    dst[4 * ld] = g * lap * S0 + M * qf;
+                }
+            }
+        });
     }
 }
 
-// The same for any shell with runtime loops and the radial sums of one
-// Cartesian component at a time (exponentials recomputed per component):
-// for g shells, whose 15 components would not fit the registers.
+// The same with runtime loops over components and outputs (the radial sums
+// still formed once): g shells, whose templated form would not fit the
+// registers.
 template <int P>
-__device__ void exact_shell_loops(const DevBasis& B, const double* pure, int s, double dx, double dy,
-                                  double dz, int nrows, const int* rows, const int* ms, double* out, int ld, int col) {
-    const double4 o = B.origin_r2[s];
+__device__ void exact_shell_loops(const DevBasis& B, double4 o, int4 inf, double dx, double dy, double dz,
+                                  unsigned mask, const int* slots, double* out, int ld, int col) {
     const double r2 = dx * dx + dy * dy + dz * dz;
-    const int4 inf = B.info[s];
-    const int l = inf.x & 0xff, nprim = inf.x >> 16;
+    const int l = inf.x & 0xff;
     const bool is_pure = ((inf.x >> 8) & 1) && l >= 2;
-    const int nc = (l + 1) * (l + 2) / 2;
-    const double* W = B.weights + inf.z;
-    for (int j = 0; j < nrows; ++j) {
-        const int m = ms[j];
+    const int nc = (l + 1) * (l + 2) / 2, nout = is_pure ? 2 * l + 1 : nc;
+    const bool inside = !(r2 > o.w);
+    double S0 = 0.0, S1 = 0.0, S2 = 0.0;
+    if (inside) exact_radial(B, inf, l, r2, S0, S1, S2);
+    const double R1p = -2.0 * S1, R2p = 4.0 * S2;
+    const double qf = (2.0 * l + 3.0) * R1p + r2 * R2p;
+    for (int m = 0; m < nout; ++m) {
+        if (!((mask >> m) & 1u)) continue;
         double v[P];
 #pragma unroll
         for (int c = 0; c < P; ++c) v[c] = 0.0;
-        if (!(r2 > o.w)) {
+        if (inside) {
+            double pm = 0.0, pg[3] = {0.0, 0.0, 0.0}, pl = 0.0;
             for (int k = 0; k < nc; ++k) {
-                const double t = is_pure ? pure[(l - 2) * 135 + m * nc + k] : (k == m ? 1.0 : 0.0);
+                const double t = is_pure ? c_exact_tg[l - 2][m * nc + k] : (k == m ? c_exact_g[l][k] : 0.0);
                 if (t == 0.0) continue;
-                double R0 = 0.0, R1 = 0.0, R2 = 0.0;
-                for (int q = 0; q < nprim; ++q) {
-                    const double a = B.exps[inf.y + q];
-                    const double we = W[k * nprim + q] * exp(-a * r2);
-                    R0 += we;
-                    R1 += we * a;
-                    R2 += we * (a * a);
-                }
                 const int a = cart_power(l, k, 0), b = cart_power(l, k, 1), c = cart_power(l, k, 2);
                 const double xa = ipow(dx, a), yb = ipow(dy, b), zc = ipow(dz, c);
-                const double M = xa * yb * zc;
-                v[0] += t * (M * R0);
+                pm += t * (xa * yb * zc);
                 if constexpr (P >= 4) {
-                    v[1] += t * ((a ? a * ipow(dx, a - 1) * yb * zc : 0.0) * R0 - 2.0 * dx * M * R1);
-                    v[2] += t * ((b ? b * xa * ipow(dy, b - 1) * zc : 0.0) * R0 - 2.0 * dy * M * R1);
-                    v[3] += t * ((c ? c * xa * yb * ipow(dz, c - 1) : 0.0) * R0 - 2.0 * dz * M * R1);
+                    pg[0] += a ? t * (a * ipow(dx, a - 1) * yb * zc) : 0.0;
+                    pg[1] += b ? t * (b * xa * ipow(dy, b - 1) * zc) : 0.0;
+                    pg[2] += c ? t * (c * xa * yb * ipow(dz, c - 1)) : 0.0;
                 }
-                if constexpr (P == 5) {
-                    const double lap = (a > 1 ? a * (a - 1) * ipow(dx, a - 2) * yb * zc : 0.0) +
-                                       (b > 1 ? b * (b - 1) * xa * ipow(dy, b - 2) * zc : 0.0) +
-                                       (c > 1 ? c * (c - 1) * xa * yb * ipow(dz, c - 2) : 0.0);
-                    v[4] += t * (lap * R0 + M * (4.0 * r2 * R2 - (4.0 * l + 6.0) * R1));
-                }
+                if (P == 5 && !is_pure)
+                    pl += t * ((a > 1 ? a * (a - 1) * ipow(dx, a - 2) * yb * zc : 0.0) +
+                               (b > 1 ? b * (b - 1) * xa * ipow(dy, b - 2) * zc : 0.0) +
+                               (c > 1 ? c * (c - 1) * xa * yb * ipow(dz, c - 2) : 0.0));
             }
+            v[0] = pm * S0;
+            if constexpr (P >= 4) {
+                v[1] = pg[0] * S0 + dx * pm * R1p;
+                v[2] = pg[1] * S0 + dy * pm * R1p;
+                v[3] = pg[2] * S0 + dz * pm * R1p;
+            }
+            if constexpr (P == 5) v[4] = pl * S0 + pm * qf;
         }
+        const int r = slots[__popc(mask & ((1u << m) - 1u))];
 #pragma unroll
-        for (int c = 0; c < P; ++c) out[(rows[j] * P + c) * ld + col] = v[c];
+        for (int c = 0; c < P; ++c) out[(r * P + c) * ld + col] = v[c];
     }
 }
 
 template <int P>
-__device__ void exact_shell_any(const DevBasis& B, const double* pure, int s, double dx, double dy,
-                                double dz, int nrows, const int* rows, const int* ms, double* out, int ld, int col) {
-    const int4 inf = B.info[s];
+__device__ void exact_shell_any(const DevBasis& B, double4 o, int4 inf, double dx, double dy, double dz,
+                                unsigned mask, const int* slots, double* out, int ld, int col) {
     const int l = inf.x & 0xff;
     const bool pure_shell = ((inf.x >> 8) & 1) && l >= 2;
     switch (l | (pure_shell ? 16 : 0)) {
 #define KUMO_EXACT(LL, PP) \
-    case (LL) | ((PP) ? 16 : 0): exact_shell<LL, PP, P>(B, pure, s, dx, dy, dz, nrows, rows, ms, out, ld, col); break;
+    case (LL) | ((PP) ? 16 : 0): exact_shell<LL, PP, P>(B, o, inf, dx, dy, dz, mask, slots, out, ld, col); break;
         KUMO_EXACT(0, false) KUMO_EXACT(1, false) KUMO_EXACT(2, false) KUMO_EXACT(3, false)
         KUMO_EXACT(2, true) KUMO_EXACT(3, true)
 #undef KUMO_EXACT
-        default: exact_shell_loops<P>(B, pure, s, dx, dy, dz, nrows, rows, ms, out, ld, col); break;
+        default: exact_shell_loops<P>(B, o, inf, dx, dy, dz, mask, slots, out, ld, col); break;
     }
 }
 
@@ -766,9 +816,10 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
     // one phase (128, 64 or 32 points: as many as fit).
     const unsigned xs_bytes = 2u * L::a_bytes + F * L::f_bytes + SB * b_bytes;
     // Per exact row: its coefficients (N doubles), its AO values at the
-    // phase's points (P * ph doubles) and six ints of row and shell tables.
+    // phase's points (P * ph doubles), six ints of row tables and (for at most
+    // as many shell groups) a group's centre, table entry and row mask.
     auto xs_need = [&](int rows, int ph) {
-        return 8u * static_cast<unsigned>(rows) * (N + P * ph) + 24u * static_cast<unsigned>(rows) + 16u;
+        return 8u * static_cast<unsigned>(rows) * (N + P * ph) + 76u * static_cast<unsigned>(rows) + 16u;
     };
     int nx = prm.exact_rows < nk ? prm.exact_rows : nk;
     while (nx > 0 && xs_need(nx, 32) > xs_bytes) --nx;
@@ -970,7 +1021,12 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
             // Row tables: shell and component of each exact row, the rows
             // grouped by shell (grp_rows, group j spans grp_first[j] ..
             // grp_first[j + 1]) and the groups' shells.
-            int* xs_shell = reinterpret_cast<int*>(xs_phi + nx * P * ph_points);
+            // Per group: its shell's centre and table entry, and the mask of
+            // its exact components.
+            double4* xs_go = reinterpret_cast<double4*>(xs_phi + nx * P * ph_points);
+            int4* xs_gi = reinterpret_cast<int4*>(xs_go + nx);
+            unsigned* xs_gmask = reinterpret_cast<unsigned*>(xs_gi + nx);
+            int* xs_shell = reinterpret_cast<int*>(xs_gmask + nx);
             int* xs_m = xs_shell + nx;
             int* grp_rows = xs_m + nx;
             int* grp_m = grp_rows + nx;
@@ -986,50 +1042,72 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                     *reinterpret_cast<double2*>(xs_c + r * N + 2 * j) = cv;
                 }
                 for (int r = tid; r < nx; r += kBulkThreads) {
-                    const int ao = static_cast<int>(aoidx[nkt + r]);
-                    const int sh = ao_block_of(prm.basis, ao);
-                    xs_shell[r] = sh;
-                    xs_m[r] = ao - prm.basis.info[sh].w;
+                    const int bm = prm.basis.ao_block[aoidx[nkt + r]];
+                    xs_shell[r] = bm >> 5;
+                    xs_m[r] = bm & 31;
                 }
                 __syncthreads();
-                // Rows in (shell, row) order.
+                // Rows in (shell, component) order.
                 for (int r = tid; r < nx; r += kBulkThreads) {
-                    const int sh = xs_shell[r];
+                    const int sh = xs_shell[r], mr = xs_m[r];
                     int pos = 0;
-                    for (int q = 0; q < nx; ++q) pos += (xs_shell[q] < sh || (xs_shell[q] == sh && q < r)) ? 1 : 0;
+                    for (int q = 0; q < nx; ++q) pos += (xs_shell[q] < sh || (xs_shell[q] == sh && xs_m[q] < mr)) ? 1 : 0;
                     grp_rows[pos] = r;
                     grp_m[pos] = xs_m[r];
                 }
                 __syncthreads();
-                if (tid == 0) {
-                    int ng = 0;
-                    for (int j = 0; j < nx; ++j)
-                        if (j == 0 || xs_shell[grp_rows[j]] != xs_shell[grp_rows[j - 1]]) grp_first[ng++] = j;
-                    grp_first[ng] = nx;
-                    grp_first[nx + 1] = ng;
+                if (w == 0) {
+                    // Group starts (a new shell in the sorted rows), numbered by a
+                    // prefix count over the warp's ballots.
+                    int base = 0;
+                    for (int j0 = 0; j0 < nx; j0 += 32) {
+                        const int j = j0 + lane;
+                        const bool first = j < nx && (j == 0 || xs_shell[grp_rows[j]] != xs_shell[grp_rows[j - 1]]);
+                        const unsigned b = __ballot_sync(0xffffffffu, first);
+                        if (first) grp_first[base + __popc(b & ((1u << lane) - 1u))] = j;
+                        base += __popc(b);
+                    }
+                    if (lane == 0) {
+                        grp_first[base] = nx;
+                        grp_first[nx + 1] = base;
+                    }
+                }
+                __syncthreads();
+                for (int g = tid; g < grp_first[nx + 1]; g += kBulkThreads) {
+                    const int j0 = grp_first[g], j1 = grp_first[g + 1];
+                    const int sh = xs_shell[grp_rows[j0]];
+                    unsigned mask = 0;
+                    for (int j = j0; j < j1; ++j) mask |= 1u << grp_m[j];
+                    xs_go[g] = prm.basis.origin_r2[sh];
+                    xs_gi[g] = prm.basis.info[sh];
+                    xs_gmask[g] = mask;
                 }
                 __syncthreads();
             }
             const int ngrp = nx > 0 ? grp_first[nx + 1] : 0;
             for (int ph0 = 0; ph0 < kBlockPoints; ph0 += ph_points) {
                 if (nx > 0) {
-                    // FP64 AO values of the exact rows at this phase's points,
-                    // one (shell, point) per thread.
-                    for (int v = tid; v < ngrp * ph_points; v += kBulkThreads) {
-                        const int g = v / ph_points, pp = v - g * ph_points;
-                        const int j0 = grp_first[g], nr = grp_first[g + 1] - j0;
-                        const int sh = xs_shell[grp_rows[j0]];
+                    // FP64 AO values of the exact rows at this phase's points:
+                    // each producer thread keeps one point (ph_points divides
+                    // the 256 producers) and takes every (256 / ph_points)-th
+                    // shell group.
+                    if (producer) {
+                        const int pp = tid % ph_points;
                         const long long e = start + ph0 + pp;
-                        if (ph0 + pp < bcount && point_exists(prm.src, e)) {
-                            double x, y, z;
-                            point_at(prm.src, e, x, y, z);
-                            const double4 o = prm.basis.origin_r2[sh];
-                            exact_shell_any<P>(prm.basis, prm.pure64, sh, x - o.x, y - o.y, z - o.z, nr, grp_rows + j0,
-                                               grp_m + j0, xs_phi, ph_points, pp);
-                        } else {
-                            for (int j = 0; j < nr; ++j)
+                        const bool here = ph0 + pp < bcount && point_exists(prm.src, e);
+                        double x = 0.0, y = 0.0, z = 0.0;
+                        if (here) point_at(prm.src, e, x, y, z);
+                        for (int g = tid / ph_points; g < ngrp; g += kThreads / ph_points) {
+                            const int j0 = grp_first[g];
+                            if (here) {
+                                const double4 o = xs_go[g];
+                                exact_shell_any<P>(prm.basis, o, xs_gi[g], x - o.x, y - o.y, z - o.z, xs_gmask[g],
+                                                   grp_rows + j0, xs_phi, ph_points, pp);
+                            } else {
+                                for (int j = j0; j < grp_first[g + 1]; ++j)
 #pragma unroll
-                                for (int c = 0; c < P; ++c) xs_phi[(grp_rows[j0 + j] * P + c) * ph_points + pp] = 0.0;
+                                    for (int c = 0; c < P; ++c) xs_phi[(grp_rows[j] * P + c) * ph_points + pp] = 0.0;
+                            }
                         }
                     }
                     __syncthreads();
@@ -1687,6 +1765,15 @@ void launch_contract_fused(const ContractFusedParams& p, int npanel, cudaStream_
         case 4: fused_maxl<4>(p, stream); break;
         default: fused_maxl<5>(p, stream); break;
     }
+}
+
+void upload_exact_tables(const double (&g)[kMaxL + 1][15], const double (&tg)[3][135]) {
+    double ig0[kMaxL + 1];
+    for (int l = 0; l <= kMaxL; ++l) ig0[l] = 1.0 / g[l][0];
+    if (cudaMemcpyToSymbol(c_exact_g, g, sizeof(c_exact_g)) != cudaSuccess ||
+        cudaMemcpyToSymbol(c_exact_ig0, ig0, sizeof(c_exact_ig0)) != cudaSuccess ||
+        cudaMemcpyToSymbol(c_exact_tg, tg, sizeof(c_exact_tg)) != cudaSuccess)
+        throw std::runtime_error("CUDA error in cudaMemcpyToSymbol (exact-row tables)");
 }
 
 void launch_contract_mixed(const ContractMixedParams& p, int npanel, cudaStream_t stream) {

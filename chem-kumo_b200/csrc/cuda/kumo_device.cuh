@@ -43,6 +43,7 @@ struct DevBasis {
     const double* weights = nullptr;
     const float* exps_f = nullptr;
     const float* weights_f = nullptr;
+    const int* ao_block = nullptr;       // per AO: its block index * 32 + its component within the block
 };
 
 // Compact tiles of a grid.  With `on`, evaluation index e does not follow the

@@ -47,7 +47,6 @@ struct ContractMixedParams {
     int exact_rows = 0;
     PointSource src;        // the evaluation's points (for the exact rows)
     DevBasis basis;         // FP64 exponents and weights (for the exact rows)
-    const double* pure64 = nullptr;  // device: Cartesian-to-pure matrices, l = 2..4, [3][135] row-major
     // Limit of each tensor-core pipeline wait in ns (0: one second); a wait
     // that runs out sets *status and the CTA stores NaN for its points.
     unsigned long long wait_ns = 0;
@@ -87,6 +86,13 @@ unsigned* pipeline_status_word();
 unsigned take_pipeline_status();
 
 void launch_contract_mixed(const ContractMixedParams& p, int npanel, cudaStream_t stream);
+
+// Copies the FP64 normalisation tables of the exact rows to the current
+// device: g[l][k] (Cartesian component k of order l, Gaussian order) and
+// tg[l - 2][m * nc + k] = T[m][k] g[l][k] of the Cartesian-to-pure
+// transforms.  Synchronous; call outside stream capture, before the first
+// mixed contraction on the device.
+void upload_exact_tables(const double (&g)[kMaxL + 1][15], const double (&tg)[3][135]);
 
 // Fused form of the mixed AO-MO path: the FP32 AO rows of each K step are
 // computed in the contraction kernel itself (no panels in global memory).

@@ -2,10 +2,12 @@
 #include "device_state.hpp"
 
 #include "../cuda/esp.cuh"
+#include "../cuda/mixed.cuh"
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 namespace chem::kumo::detail {
 
@@ -101,11 +103,13 @@ DeviceMolecule::DeviceMolecule(const Molecule& m) {
         }
     }
     mix_prims = upload(mix.data(), mix.size());
+    double g64[kumo_dev::kMaxL + 1][15] = {};
     for (int l = 0; l <= kumo_dev::kMaxL; ++l) {
         const auto cart = gaussian_cartesian_order(l);
-        for (std::size_t k = 0; k < cart.size(); ++k)
-            gcart[l][k] = static_cast<float>(
-                1.0 / std::sqrt(odd_df(2 * cart[k].x - 1) * odd_df(2 * cart[k].y - 1) * odd_df(2 * cart[k].z - 1)));
+        for (std::size_t k = 0; k < cart.size(); ++k) {
+            g64[l][k] = 1.0 / std::sqrt(odd_df(2 * cart[k].x - 1) * odd_df(2 * cart[k].y - 1) * odd_df(2 * cart[k].z - 1));
+            gcart[l][k] = static_cast<float>(g64[l][k]);
+        }
     }
     basis.nblocks = static_cast<int>(blocks.size());
     basis.nao = static_cast<int>(n);
@@ -117,20 +121,36 @@ DeviceMolecule::DeviceMolecule(const Molecule& m) {
     basis.weights = upload(weights.data(), weights.size());
     basis.exps_f = upload(exps_f.data(), exps_f.size());
     basis.weights_f = upload(weights_f.data(), weights_f.size());
+    std::vector<int> ao_block(n);
+    for (std::size_t i = 0; i < blocks.size(); ++i)
+        for (std::size_t c = 0; c < blocks[i].count; ++c)
+            ao_block[blocks[i].offset + c] = static_cast<int>(i) * 32 + static_cast<int>(c);
+    basis.ao_block = upload(ao_block.data(), ao_block.size());
+    double tg64[3][135] = {};
     for (int l = 2; l <= kumo_dev::kMaxL; ++l) {
         const Matrix t = gaussian_cartesian_to_pure(l);
         for (std::size_t r = 0; r < t.rows(); ++r)
             for (std::size_t c = 0; c < t.cols(); ++c) {
                 pure_d[l - 2][r * t.cols() + c] = t(r, c);
                 pure_f[l - 2][r * t.cols() + c] = static_cast<float>(t(r, c));
-                tpure_g[l - 2][r * t.cols() + c] = static_cast<float>(t(r, c) * gcart[l][c]);
+                tg64[l - 2][r * t.cols() + c] = t(r, c) * g64[l][c];
+                tpure_g[l - 2][r * t.cols() + c] = static_cast<float>(tg64[l - 2][r * t.cols() + c]);
                 // The mixed AO kernel skips the entries this predicate calls zero.
                 const auto cart = gaussian_cartesian_order(l);
                 if (t(r, c) != 0.0 && !kumo_dev::solid_harmonic_nonzero(l, static_cast<int>(r), cart[c].x, cart[c].y))
                     throw std::logic_error("Cartesian-to-pure pattern mismatch");
             }
     }
-    pure_dev = upload(&pure_d[0][0], 3 * 135);
+    // The exact rows' FP64 tables are the same for every basis: once per device.
+    {
+        static std::mutex mu;
+        static bool done[64] = {};
+        std::lock_guard<std::mutex> lock(mu);
+        if (device < 0 || device >= 64 || !done[device]) {
+            kumo_dev::upload_exact_tables(g64, tg64);
+            if (device >= 0 && device < 64) done[device] = true;
+        }
+    }
     const Matrix pt = m.density_matrix(DensityComponent::Total);
     const Matrix ps = m.density_matrix(DensityComponent::Difference);
     p_total = upload(pt.data(), pt.size());

@@ -33,7 +33,6 @@ struct DeviceMolecule {
     kumo_dev::DevBasis basis;
     double pure_d[3][135] = {};
     float pure_f[3][135] = {};
-    double* pure_dev = nullptr;  // pure_d in HBM (read by the mixed contraction's exact rows)
     // Mixed-form AO build: per primitive a log2(e), a and the radial factor u
     // (weights = u_p g_k), T[m][k] g_k for pure blocks, g_k for Cartesian ones.
     kumo_dev::MixPrim* mix_prims = nullptr;

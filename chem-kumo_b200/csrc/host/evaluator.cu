@@ -800,7 +800,6 @@ private:
         cp.exact_rows = mixed_exact_rows();
         cp.src = lay.src;
         cp.basis = dev_->basis;
-        cp.pure64 = dev_->pure_dev;
         for (std::size_t b0 = 0; b0 < nblocks; b0 += static_cast<std::size_t>(W)) {
             const int nb = static_cast<int>(std::min<std::size_t>(W, nblocks - b0));
             bp.first_point = static_cast<long long>(b0 * bs);
