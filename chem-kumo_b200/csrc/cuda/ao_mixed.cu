@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(kBlockPoints, (P == 10 || MAXL >= 4) ? 6 : 8) 
                 for (int p = 0; p < nprim; ++p) {
                     const MixPrim pr = prm.prims[inf.y + p];
                     const double ue = static_cast<double>(pr.u * exp_neg(pr.al2, r2d));
-                    const double a = static_cast<double>(pr.alpha);
+                    const double a = pr.al2 * 0.6931471805599453;  // the exponent (ln 2 = 1 / log2 e)
                     R0 += ue;
                     R1 += ue * a;
                     R2 += ue * (a * a);

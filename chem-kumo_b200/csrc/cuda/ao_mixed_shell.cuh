@@ -16,8 +16,12 @@ namespace {
 __device__ __forceinline__ float exp_neg(double al2, double r2) {
     const double t = al2 * r2;
     if (!(t < 149.0)) return 0.0f;
-    const double n = rint(t);
-    const int ni = static_cast<int>(n), h = ni >> 1;
+    // n = rint(t) by adding and removing 1.5 * 2^52 (round to nearest even,
+    // as rint), its integer read from the low word: FP64 adds instead of a
+    // rounding and a conversion instruction.
+    const double tb = t + 6755399441055744.0;
+    const double n = tb - 6755399441055744.0;
+    const int ni = __double2loint(tb), h = ni >> 1;
     const float s1 = __int_as_float((127 - h) << 23), s2 = __int_as_float((127 - (ni - h)) << 23);
     return (exp2f(static_cast<float>(n - t)) * s1) * s2;
 }

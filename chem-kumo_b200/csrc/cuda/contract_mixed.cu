@@ -1134,7 +1134,10 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
                                 for (int u = 0; u < MG; ++u) x[c][u] += static_cast<double>(__uint_as_float(v[c][u]));
                             }
                         }
-                        // The exact rows: FP64 AO values times FP64 coefficients.
+                        // The exact rows: FP64 AO values times FP64 coefficients
+                        // (two rows per iteration, so that one row's loads overlap
+                        // the other's products).
+#pragma unroll 2
                         for (int r = 0; r < nx; ++r) {
                             // 64-byte aligned: N and i0 are multiples of 8.
                             const double2* crow = reinterpret_cast<const double2*>(xs_c + r * N + i0);
