@@ -1,9 +1,14 @@
 // Serving loop (see chem/kumo/server.hpp).
 //
-// Threads: the caller's (submit / wait), one scheduler thread that owns every
-// CUDA call of the server (admission, launches, completion polling), and one
-// completion thread that copies results from page-locked staging into the
-// caller's arrays, so that large copies never hold up admission.
+// Threads: the caller's (submit / wait); one scheduler thread that admits
+// requests; one launcher thread per active slot (ServerOptions::max_active),
+// each with its own streams and event, which issues an admitted request's
+// device work, waits for it and hands it on; and one completion thread that
+// copies results from page-locked staging into the caller's arrays, so that
+// large copies never hold up admission or launches.  Several host threads
+// issue launches at once, so the host time of one request's launches (tens of
+// kernels, allocations and copies for a large cube) does not hold up the
+// others.
 //
 // Admission: FIFO; the head request starts when a slot (stream) is free and
 // the footprint sum of the active requests plus the resident molecule copies
@@ -137,26 +142,26 @@ struct Server::Impl {
         double* pstage = nullptr;         // direct path: page-locked points
         std::size_t pstage_bytes = 0;
         std::size_t row = 0;              // row length of the staged results (bucket or n)
-        bool high_priority = false;       // stream from free_streams_hi
+        bool high_priority = false;       // on the launcher's high-priority stream
     };
-    std::deque<Pending> queue;
+    std::deque<Pending> queue;    // submitted, not admitted
+    std::deque<Pending> ready;    // admitted, waiting for a launcher
     std::deque<Active> finished;  // handed to the completion thread
-    std::vector<std::pair<std::size_t, double*>> returned_stage;  // staging back from the completion thread
-    bool stop_completer = false;
+    bool stop_launchers = false, stop_completer = false;
+    std::condition_variable cv_ready;
+    int inflight = 0;  // admitted and not yet handed to the completion thread
     std::unordered_map<std::uint64_t, Ticket> tickets;
     std::uint64_t next_ticket = 1;
 
-    // Scheduler-owned state.
-    std::vector<Active> active;
     // Streams of small requests (at most graph_points points) take the
     // device's highest priority, those of larger requests its lowest: a
     // small request's blocks are scheduled as soon as SMs free up, instead of
-    // after every queued block of a large cube.
-    std::vector<cudaStream_t> free_streams, free_streams_hi;
+    // after every queued block of a large cube.  Each launcher owns one of each.
     int prio_low = 0, prio_high = 0;
-    std::vector<cudaEvent_t> free_events;
+    std::mutex gmu;  // graphs, seen
     std::map<std::string, std::vector<std::unique_ptr<GraphEntry>>> graphs;
     std::map<std::string, int> seen;  // small-request keys met so far (a graph is captured on the second)
+    std::mutex smu;  // free_stage, arena_used
     std::multimap<std::size_t, double*> free_stage;  // page-locked staging by size
     // Page-locked arena, allocated once at start: staging buffers are carved
     // from it (page-locking on demand synchronises the device and stalls the
@@ -179,7 +184,7 @@ struct Server::Impl {
         const char* c = static_cast<const char*>(p);
         return arena && c >= arena && c < arena + arena_size;
     }
-    std::vector<const Molecule*> resident;
+    std::vector<const Molecule*> resident;  // guarded by mu
     std::size_t resident_bytes = 0, active_bytes = 0;
 
     // Statistics (guarded by mu).
@@ -190,12 +195,21 @@ struct Server::Impl {
     std::optional<clock_type::time_point> t_first, t_last;
 
     std::thread scheduler, completer;
+    std::vector<std::thread> launchers;
 
+    struct Lanes {  // one launcher's streams and completion event
+        cudaStream_t lo = nullptr, hi = nullptr;
+        cudaEvent_t event = nullptr;
+    };
     void run_scheduler();
+    void run_launcher();
     void run_completer();
-    void launch(Pending&& p);
+    // Issues p's device work on one of the lanes' streams and records the
+    // lanes' event after it; false (the ticket failed) if issuing threw.
+    bool launch(Pending& p, const Lanes& lanes, Active& a);
     GraphEntry* graph_for(const Pending& p, cudaStream_t stream);
     double* get_stage(std::size_t bytes);
+    void put_stage(std::size_t bytes, double* p);
     std::string key_of(const Pending& p) const;
     void fail(std::uint64_t ticket, const std::string& what, clock_type::time_point t0);
 };
@@ -220,8 +234,14 @@ std::size_t stage_class(std::size_t bytes) {
     return c;
 }
 
+void Server::Impl::put_stage(std::size_t bytes, double* p) {
+    std::lock_guard<std::mutex> lock(smu);
+    free_stage.emplace(stage_class(bytes), p);
+}
+
 double* Server::Impl::get_stage(std::size_t bytes) {
     const std::size_t cls = stage_class(bytes);
+    std::lock_guard<std::mutex> lock(smu);
     auto it = free_stage.find(cls);
     if (it != free_stage.end()) {
         double* p = it->second;
@@ -233,14 +253,18 @@ double* Server::Impl::get_stage(std::size_t bytes) {
 }
 
 GraphEntry* Server::Impl::graph_for(const Pending& p, cudaStream_t stream) {
-    auto& list = graphs[key_of(p)];
-    for (auto& e : list)
-        if (!e->busy) {
-            e->busy = true;
-            std::lock_guard<std::mutex> lock(mu);
-            ++st.graph_replays;
-            return e.get();
+    const std::string key = key_of(p);
+    {
+        std::lock_guard<std::mutex> glock(gmu);
+        for (auto& e : graphs[key]) {
+            bool idle = false;
+            if (e->busy.compare_exchange_strong(idle, true)) {
+                std::lock_guard<std::mutex> lock(mu);
+                ++st.graph_replays;
+                return e.get();
+            }
         }
+    }
     auto e = std::make_unique<GraphEntry>();
     e->bucket = round_bucket(p.n_eval);
     e->channels = p.channels;
@@ -252,12 +276,14 @@ GraphEntry* Server::Impl::graph_for(const Pending& p, cudaStream_t stream) {
     {
         const std::size_t pb = stage_class(sizeof(double) * 3 * e->bucket);
         const std::size_t ob = stage_class(sizeof(double) * std::max<std::size_t>(e->channels * e->bucket, 1));
+        std::unique_lock<std::mutex> slock(smu);
         if (arena && arena_used + pb + ob <= arena_size) {
             bool unused = false;
             e->h_points = pinned(pb, unused);
             e->h_out = pinned(ob, unused);
             e->own_host = false;
         } else {
+            slock.unlock();
             check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&e->h_points), pb, cudaHostAllocDefault),
                        "cudaHostAlloc (serving points)");
             check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&e->h_out), ob, cudaHostAllocDefault),
@@ -292,8 +318,10 @@ GraphEntry* Server::Impl::graph_for(const Pending& p, cudaStream_t stream) {
         std::lock_guard<std::mutex> lock(mu);
         ++st.graph_captures;
     }
-    list.push_back(std::move(e));
-    return list.back().get();
+    GraphEntry* got = e.get();
+    std::lock_guard<std::mutex> glock(gmu);
+    graphs[key].push_back(std::move(e));
+    return got;
 }
 
 void Server::Impl::fail(std::uint64_t ticket, const std::string& what, clock_type::time_point t0) {
@@ -306,38 +334,27 @@ void Server::Impl::fail(std::uint64_t ticket, const std::string& what, clock_typ
     cv_done.notify_all();
 }
 
-void Server::Impl::launch(Pending&& p) {
-    Active a;
+bool Server::Impl::launch(Pending& p, const Lanes& lanes, Active& a) {
     const bool small = p.n_eval <= opt.graph_points;
-    auto& pool = small ? free_streams_hi : free_streams;
-    if (pool.empty()) {
-        cudaStream_t s;
-        check_cuda(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, small ? prio_high : prio_low),
-                   "cudaStreamCreateWithPriority");
-        pool.push_back(s);
-    }
-    if (free_events.empty()) {
-        cudaEvent_t e;
-        check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
-        free_events.push_back(e);
-    }
-    a.stream = pool.back();
-    pool.pop_back();
+    a.stream = small ? lanes.hi : lanes.lo;
     a.high_priority = small;
-    a.event = free_events.back();
-    free_events.pop_back();
+    a.event = lanes.event;
     const Molecule& mol = *p.req.molecule;
     const auto& props = p.req.request.properties();
     try {
         if (!mol.device_if_resident()) {
             (void)mol.device();
-            resident.push_back(&mol);
-            resident_bytes += mol.device_bytes();
+            std::lock_guard<std::mutex> lock(mu);
+            if (std::find(resident.begin(), resident.end(), &mol) == resident.end()) {
+                resident.push_back(&mol);
+                resident_bytes += mol.device_bytes();
+            }
         }
         if (p.graph) {
             // A request shape met for the first time runs the regular path;
             // its graph is captured when the shape comes again.
             const std::string key = key_of(p);
+            std::lock_guard<std::mutex> glock(gmu);
             if (seen[key]++ == 0 && graphs.find(key) == graphs.end()) p.graph = false;
         }
         if (p.graph) {
@@ -354,6 +371,7 @@ void Server::Impl::launch(Pending&& p) {
                 }
             }
             GraphEntry* e = graph_for(p, a.stream);
+            a.entry = e;
             const std::size_t n = p.n_eval, b = e->bucket;
             std::memcpy(e->h_points, p.req.points.data(), sizeof(double) * 3 * n);
             for (std::size_t q = n; q < b; ++q) std::memcpy(e->h_points + 3 * q, e->h_points + 3 * (n - 1), 3 * sizeof(double));
@@ -363,7 +381,6 @@ void Server::Impl::launch(Pending&& p) {
             check_cuda(cudaMemcpyAsync(e->h_out, e->d_out, sizeof(double) * e->channels * b, cudaMemcpyDeviceToHost,
                                        a.stream),
                        "cudaMemcpyAsync (serving results)");
-            a.entry = e;
             a.row = b;
         } else {
             EvaluationOptions o = p.req.options;
@@ -409,90 +426,95 @@ void Server::Impl::launch(Pending&& p) {
         cudaStreamSynchronize(a.stream);
         cudaGetLastError();
         if (a.entry) a.entry->busy = false;
-        if (a.stage) free_stage.emplace(stage_class(a.stage_bytes), a.stage);
-        if (a.pstage) free_stage.emplace(stage_class(a.pstage_bytes), a.pstage);
-        (a.high_priority ? free_streams_hi : free_streams).push_back(a.stream);
-        free_events.push_back(a.event);
-        active_bytes -= p.footprint;
+        if (a.stage) put_stage(a.stage_bytes, a.stage);
+        if (a.pstage) put_stage(a.pstage_bytes, a.pstage);
+        a.entry = nullptr;
+        a.stage = a.pstage = nullptr;
         fail(p.ticket, ex.what(), p.t_submit);
-        return;
+        return false;
     }
-    a.p = std::move(p);
-    active.push_back(std::move(a));
+    return true;
 }
 
 void Server::Impl::run_scheduler() {
-    check_cuda(cudaSetDevice(opt.device), "cudaSetDevice");
-    check_cuda(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high), "cudaDeviceGetStreamPriorityRange");
-    // No synchronous tile-shape probes on this thread (they would hold up
-    // admission); grids take a shape already measured, or the default.
-    detail::set_tile_probing(false);
-    detail::prepare_device_for_capture();
+    check_cuda(cudaSetDevice(opt.device), "cudaSetDevice");  // device_if_resident compares devices
+    std::unique_lock<std::mutex> lock(mu);
     for (;;) {
-        bool progressed = false;
-        // Completed device work goes to the completion thread.
-        for (std::size_t i = 0; i < active.size();) {
-            const cudaError_t q = cudaEventQuery(active[i].event);
-            if (q == cudaErrorNotReady) {
-                ++i;
-                continue;
-            }
-            Active a = std::move(active[i]);
-            active.erase(active.begin() + static_cast<std::ptrdiff_t>(i));
-            active_bytes -= a.p.footprint;
-            (a.high_priority ? free_streams_hi : free_streams).push_back(a.stream);
-            free_events.push_back(a.event);
-            progressed = true;
+        // Admission, in arrival order: the head request starts when a slot is
+        // free and its footprint fits the budget beside the active requests.
+        while (!queue.empty() && inflight < opt.max_active) {
+            Pending& head = queue.front();
+            const bool resident_now = head.req.molecule->device_if_resident() != nullptr;
+            const std::size_t need = head.footprint + (resident_now ? 0 : molecule_bytes_estimate(*head.req.molecule));
+            if (inflight > 0 && resident_bytes + active_bytes + need > budget) break;
+            Pending p = std::move(head);
+            queue.pop_front();
+            active_bytes += p.footprint;
+            ++inflight;
+            queue_sum_ms += std::chrono::duration<double, std::milli>(clock_type::now() - p.t_submit).count();
+            ++admitted;
+            st.peak_bytes = std::max(st.peak_bytes, resident_bytes + active_bytes);
+            ready.push_back(std::move(p));
+            cv_ready.notify_one();
+        }
+        if (stop && queue.empty() && inflight == 0) break;
+        // Woken by submit and by every completion.
+        cv_work.wait(lock);
+    }
+}
+
+void Server::Impl::run_launcher() {
+    check_cuda(cudaSetDevice(opt.device), "cudaSetDevice");
+    // No synchronous tile-shape probes on the serving threads (they would
+    // hold up launches); grids take a shape already measured, or the default.
+    detail::set_tile_probing(false);
+    Lanes lanes;
+    check_cuda(cudaStreamCreateWithPriority(&lanes.lo, cudaStreamNonBlocking, prio_low), "cudaStreamCreateWithPriority");
+    check_cuda(cudaStreamCreateWithPriority(&lanes.hi, cudaStreamNonBlocking, prio_high), "cudaStreamCreateWithPriority");
+    // Blocking synchronisation: a launcher waiting for its request sleeps.
+    check_cuda(cudaEventCreateWithFlags(&lanes.event, cudaEventDisableTiming | cudaEventBlockingSync), "cudaEventCreate");
+    for (;;) {
+        Pending p;
+        {
+            std::unique_lock<std::mutex> lock(mu);
+            cv_ready.wait(lock, [&] { return stop_launchers || !ready.empty(); });
+            if (ready.empty()) break;
+            p = std::move(ready.front());
+            ready.pop_front();
+        }
+        const auto tl = clock_type::now();
+        Active a;
+        const bool ok = launch(p, lanes, a);
+        const double dt = std::chrono::duration<double>(clock_type::now() - tl).count();
+        cudaError_t q = cudaSuccess;
+        if (ok) {
+            q = cudaEventSynchronize(a.event);
             if (a.pstage) {
-                free_stage.emplace(stage_class(a.pstage_bytes), a.pstage);
+                put_stage(a.pstage_bytes, a.pstage);
                 a.pstage = nullptr;
             }
             if (q != cudaSuccess) {
                 cudaGetLastError();
                 if (a.entry) a.entry->busy = false;
-                if (a.stage) free_stage.emplace(stage_class(a.stage_bytes), a.stage);
-                fail(a.p.ticket, std::string("CUDA error: ") + cudaGetErrorString(q), a.p.t_submit);
-                continue;
+                if (a.stage) put_stage(a.stage_bytes, a.stage);
+                fail(p.ticket, std::string("CUDA error: ") + cudaGetErrorString(q), p.t_submit);
             }
-            std::lock_guard<std::mutex> lock(mu);
+        }
+        std::lock_guard<std::mutex> lock(mu);
+        st.launch_s += dt;
+        active_bytes -= p.footprint;
+        --inflight;
+        if (ok && q == cudaSuccess) {
+            a.p = std::move(p);
             finished.push_back(std::move(a));
-            cv_work.notify_all();
         }
-        {
-            std::unique_lock<std::mutex> lock(mu);
-            // Staging returned by the completion thread.
-            for (const auto& [bytes, ptr] : returned_stage) free_stage.emplace(bytes, ptr);
-            returned_stage.clear();
-            // Admission, in arrival order.
-            while (!queue.empty() && static_cast<int>(active.size()) < opt.max_active) {
-                Pending& head = queue.front();
-                const bool resident_now = head.req.molecule->device_if_resident() != nullptr;
-                const std::size_t need = head.footprint + (resident_now ? 0 : molecule_bytes_estimate(*head.req.molecule));
-                if (!active.empty() && resident_bytes + active_bytes + need > budget) break;
-                Pending p = std::move(head);
-                queue.pop_front();
-                lock.unlock();
-                active_bytes += p.footprint;
-                const auto tl = clock_type::now();
-                const double queued = std::chrono::duration<double, std::milli>(tl - p.t_submit).count();
-                launch(std::move(p));
-                const double dt = std::chrono::duration<double>(clock_type::now() - tl).count();
-                progressed = true;
-                lock.lock();
-                st.launch_s += dt;
-                queue_sum_ms += queued;
-                ++admitted;
-                st.peak_bytes = std::max(st.peak_bytes, resident_bytes + active_bytes);
-            }
-            if (stop && queue.empty() && active.empty()) break;
-            if (!progressed) {
-                if (active.empty())
-                    cv_work.wait_for(lock, std::chrono::milliseconds(50));
-                else
-                    cv_work.wait_for(lock, std::chrono::microseconds(100));
-            }
-        }
+        cv_work.notify_all();
     }
+    cudaStreamSynchronize(lanes.lo);
+    cudaStreamSynchronize(lanes.hi);
+    cudaStreamDestroy(lanes.lo);
+    cudaStreamDestroy(lanes.hi);
+    cudaEventDestroy(lanes.event);
 }
 
 void Server::Impl::run_completer() {
@@ -526,10 +548,10 @@ void Server::Impl::run_completer() {
             off += ch;
         }
         const auto now = clock_type::now();
+        if (a.entry) a.entry->busy = false;
+        if (a.stage) put_stage(a.stage_bytes, a.stage);
         std::lock_guard<std::mutex> lock(mu);
         st.copy_s += std::chrono::duration<double>(now - tc).count();
-        if (a.entry) a.entry->busy = false;
-        if (a.stage) returned_stage.emplace_back(stage_class(a.stage_bytes), a.stage);
         auto& t = tickets[a.p.ticket];
         t.done = true;
         t.latency_ms = std::chrono::duration<double, std::milli>(now - a.p.t_submit).count();
@@ -561,6 +583,31 @@ Server::Server(ServerOptions options) : impl_(std::make_unique<Impl>()) {
                    "cudaHostAlloc (staging arena)");
         m.arena_size = m.opt.staging_bytes;
     }
+    check_cuda(cudaDeviceGetStreamPriorityRange(&m.prio_low, &m.prio_high), "cudaDeviceGetStreamPriorityRange");
+    detail::prepare_device_for_capture();
+    for (int i = 0; i < m.opt.max_active; ++i)
+        m.launchers.emplace_back([&m] {
+            try {
+                m.run_launcher();
+            } catch (const std::exception& e) {
+                // This launcher cannot issue work: fail what it would take.
+                std::unique_lock<std::mutex> lock(m.mu);
+                for (;;) {
+                    m.cv_ready.wait(lock, [&] { return m.stop_launchers || !m.ready.empty(); });
+                    if (m.ready.empty()) return;
+                    Impl::Pending p = std::move(m.ready.front());
+                    m.ready.pop_front();
+                    auto& t = m.tickets[p.ticket];
+                    t.done = true;
+                    t.error = std::string("serving launcher stopped: ") + e.what();
+                    ++m.st.failed;
+                    m.active_bytes -= p.footprint;
+                    --m.inflight;
+                    m.cv_done.notify_all();
+                    m.cv_work.notify_all();
+                }
+            }
+        });
     m.scheduler = std::thread([&m] {
         try {
             m.run_scheduler();
@@ -588,6 +635,13 @@ Server::~Server() {
     if (m.scheduler.joinable()) m.scheduler.join();
     {
         std::lock_guard<std::mutex> lock(m.mu);
+        m.stop_launchers = true;
+        m.cv_ready.notify_all();
+    }
+    for (auto& t : m.launchers)
+        if (t.joinable()) t.join();
+    {
+        std::lock_guard<std::mutex> lock(m.mu);
         m.stop_completer = true;
         m.cv_work.notify_all();
     }
@@ -597,12 +651,7 @@ Server::~Server() {
     m.graphs.clear();
     for (auto& [b, p] : m.free_stage)
         if (!m.in_arena(p)) cudaFreeHost(p);
-    for (auto& [b, p] : m.returned_stage)
-        if (!m.in_arena(p)) cudaFreeHost(p);
     if (m.arena) cudaFreeHost(m.arena);
-    for (auto s : m.free_streams) cudaStreamDestroy(s);
-    for (auto s : m.free_streams_hi) cudaStreamDestroy(s);
-    for (auto e : m.free_events) cudaEventDestroy(e);
 }
 
 std::uint64_t Server::submit(ServeRequest r) {

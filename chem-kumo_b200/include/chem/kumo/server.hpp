@@ -4,7 +4,8 @@
 // admitted in arrival order while their device-memory footprint fits an HBM
 // budget and an active slot is free, and run concurrently, each on its own
 // CUDA stream, so that their kernels overlap on the device while later
-// requests arrive (continuous batching).  Small requests (up to
+// requests arrive (continuous batching); one host thread per active slot
+// issues its request's launches.  Small requests (up to
 // ServerOptions::graph_points points, grids converted to explicit points) whose
 // shape (molecule, options, properties, point bucket) has been met before are
 // replayed from a CUDA graph captured at the second meeting; the others run
@@ -33,7 +34,7 @@ struct ServerOptions {
     /// Device memory the active requests may hold together (molecule copies,
     /// scratch, inputs and outputs); 0 = 150 GB capped at 90% of free memory.
     std::size_t hbm_budget = 0;
-    int max_active = 8;                      ///< requests in flight (one stream each)
+    int max_active = 8;                      ///< requests in flight (one launcher thread and stream pair each)
     std::size_t graph_points = 65536;        ///< largest request replayed from a CUDA graph
     std::size_t request_scratch = 1ull << 30;  ///< AO scratch per request (sets its wave size)
     /// Page-locked host arena for staging results and points, allocated once
@@ -59,7 +60,7 @@ struct ServeStats {
     std::size_t graph_captures = 0, graph_replays = 0, direct_runs = 0;
     std::size_t peak_bytes = 0;           ///< largest admitted footprint sum
     std::size_t budget_bytes = 0;
-    double launch_s = 0;                  ///< scheduler host time spent issuing requests
+    double launch_s = 0;                  ///< host time spent issuing requests, summed over the launcher threads
     double copy_s = 0;                    ///< completion-thread time copying results
     double queue_ms = 0;                  ///< mean time from submit to admission
 };

