@@ -62,6 +62,10 @@ __device__ __forceinline__ T factor2(const T* xp, T a, T x) {
     return t1 - (T)2 * a * (T)(2 * M + 1) * xp[M] + (T)4 * a * a * x * x * xp[M];
 }
 
+// Largest angular momentum whose panels are summed primitives-outer (more
+// accumulators live at once; f and g shells would spill).
+constexpr int kPOuterMaxL = 2;
+
 // Panels of one shell for the thread's point into stage[(m * P + c) * 128 + j],
 // with maxabs[m] the largest |value| over the panels of the AO order.
 template <typename T, int L, bool PURE, int ORDER, int P, int NMAX>
@@ -119,7 +123,56 @@ __device__ __forceinline__ void shell_panels(const T (&pure)[3][135], const T* s
             for (int m = 0; m < NOUT; ++m)
 #pragma unroll
                 for (int c = 0; c < 4; ++c) acc[m][c] = (T)0;
-            static_for<NC>([&](auto kc) {
+            if constexpr (L <= kPOuterMaxL) {
+                // Primitives outer, components inner: the sums of every
+                // component advance together (independent chains), and each
+                // 1D factor is formed once per primitive and power.  Every
+                // sum still adds its primitives in order and every product
+                // is formed as in the components-outer form, so the values
+                // are the same bits.
+                T s[NC][4];
+#pragma unroll
+                for (int k = 0; k < NC; ++k)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) s[k][c] = (T)0;
+                for (int p = 0; p < nprim; ++p) {
+                    const T a = s_exps[p];
+                    const T rad = s_rad[p * kBlockPoints + j];
+                    T f1x[L + 1], f1y[L + 1], f1z[L + 1];
+                    static_for<L + 1>([&](auto nc) {
+                        constexpr int n = decltype(nc)::value;
+                        f1x[n] = factor1<T, n>(xp, a, rx);
+                        f1y[n] = factor1<T, n>(yp, a, ry);
+                        f1z[n] = factor1<T, n>(zp, a, rz);
+                    });
+                    static_for<NC>([&](auto kc) {
+                        constexpr int k = decltype(kc)::value;
+                        constexpr int px = cart_power(L, k, 0), py = cart_power(L, k, 1), pz = cart_power(L, k, 2);
+                        const T weight = s_w[k * nprim + p] * rad;
+                        const T fx0 = xp[px], fy0 = yp[py], fz0 = zp[pz];
+                        s[k][0] = s[k][0] + weight * fx0 * fy0 * fz0;
+                        s[k][1] = s[k][1] + weight * f1x[px] * fy0 * fz0;
+                        s[k][2] = s[k][2] + weight * fx0 * f1y[py] * fz0;
+                        s[k][3] = s[k][3] + weight * fx0 * fy0 * f1z[pz];
+                    });
+                }
+                static_for<NC>([&](auto kc) {
+                    constexpr int k = decltype(kc)::value;
+                    if constexpr (PURE) {
+#pragma unroll
+                        for (int m = 0; m < NOUT; ++m) {
+                            const T t = pure[TL][m * NC + k];
+                            if (t != (T)0) {
+#pragma unroll
+                                for (int c = 0; c < 4; ++c) acc[m][c] = acc[m][c] + t * s[k][c];
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) acc[k][c] = s[k][c];
+                    }
+                });
+            } else static_for<NC>([&](auto kc) {
                 constexpr int k = decltype(kc)::value;
                 constexpr int px = cart_power(L, k, 0), py = cart_power(L, k, 1), pz = cart_power(L, k, 2);
                 T s0 = 0, s1 = 0, s2 = 0, s3 = 0;
@@ -177,7 +230,62 @@ __device__ __forceinline__ void shell_panels(const T (&pure)[3][135], const T* s
                 for (int m = 0; m < NOUT; ++m)
 #pragma unroll
                     for (int c = 0; c < 3; ++c) acc[m][c] = (T)0;
-                static_for<NC>([&](auto kc) {
+                if constexpr (L <= kPOuterMaxL) {
+                    // Primitives outer, as for group 0 (same bits).
+                    T s[NC][3];
+#pragma unroll
+                    for (int k = 0; k < NC; ++k)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) s[k][c] = (T)0;
+                    for (int p = 0; p < nprim; ++p) {
+                        const T a = s_exps[p];
+                        const T rad = s_rad[p * kBlockPoints + j];
+                        T f1x[L + 1], f1y[L + 1], f1z[L + 1], f2a[L + 1], f2b[L + 1];
+                        static_for<L + 1>([&](auto nc) {
+                            constexpr int n = decltype(nc)::value;
+                            f1y[n] = factor1<T, n>(yp, a, ry);
+                            f1z[n] = factor1<T, n>(zp, a, rz);
+                            if constexpr (H == 0) {
+                                f1x[n] = factor1<T, n>(xp, a, rx);
+                                f2a[n] = factor2<T, n>(xp, a, rx);
+                            } else {
+                                f2a[n] = factor2<T, n>(yp, a, ry);
+                                f2b[n] = factor2<T, n>(zp, a, rz);
+                            }
+                        });
+                        static_for<NC>([&](auto kc) {
+                            constexpr int k = decltype(kc)::value;
+                            constexpr int px = cart_power(L, k, 0), py = cart_power(L, k, 1), pz = cart_power(L, k, 2);
+                            const T weight = s_w[k * nprim + p] * rad;
+                            const T fx0 = xp[px], fy0 = yp[py], fz0 = zp[pz];
+                            if constexpr (H == 0) {
+                                s[k][0] = s[k][0] + weight * f2a[px] * fy0 * fz0;
+                                s[k][1] = s[k][1] + weight * f1x[px] * f1y[py] * fz0;
+                                s[k][2] = s[k][2] + weight * f1x[px] * fy0 * f1z[pz];
+                            } else {
+                                s[k][0] = s[k][0] + weight * fx0 * f2a[py] * fz0;
+                                s[k][1] = s[k][1] + weight * fx0 * f1y[py] * f1z[pz];
+                                s[k][2] = s[k][2] + weight * fx0 * fy0 * f2b[pz];
+                            }
+                        });
+                    }
+                    static_for<NC>([&](auto kc) {
+                        constexpr int k = decltype(kc)::value;
+                        if constexpr (PURE) {
+#pragma unroll
+                            for (int m = 0; m < NOUT; ++m) {
+                                const T t = pure[TL][m * NC + k];
+                                if (t != (T)0) {
+#pragma unroll
+                                    for (int c = 0; c < 3; ++c) acc[m][c] = acc[m][c] + t * s[k][c];
+                                }
+                            }
+                        } else {
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) acc[k][c] = s[k][c];
+                        }
+                    });
+                } else static_for<NC>([&](auto kc) {
                     constexpr int k = decltype(kc)::value;
                     constexpr int px = cart_power(L, k, 0), py = cart_power(L, k, 1), pz = cart_power(L, k, 2);
                     T s[3] = {0, 0, 0};
