@@ -63,8 +63,10 @@ __device__ __forceinline__ T factor2(const T* xp, T a, T x) {
 }
 
 // Largest angular momentum whose panels are summed primitives-outer (more
-// accumulators live at once; f and g shells would spill).
-constexpr int kPOuterMaxL = 2;
+// accumulators live at once: f shells spill a few bytes and are still
+// faster that way, 104 -> 91 ms per FP64 step of the 740-AO workload; g
+// shells would spill far more).
+constexpr int kPOuterMaxL = 3;
 
 // Panels of one shell for the thread's point into stage[(m * P + c) * 128 + j],
 // with maxabs[m] the largest |value| over the panels of the AO order.

@@ -12,6 +12,7 @@
 // depend on scheduling.
 #include "func_attr.cuh"
 #include <cstdio>
+#include <initializer_list>
 
 #include "contract.cuh"
 
@@ -217,20 +218,48 @@ static void launch_mo(const ContractMoParams& p, cudaStream_t stream) {
     constexpr int MOC = 8 * MPT;
     constexpr int Q = NQ<P>::v;
     const size_t smem = sizeof(double) * (size_t)(2 * KT * P * 32 + 2 * KT * MOC + 2 * Q * 32);
-    static bool configured = false;
-    if (!configured) {
-        ensure_dynamic_smem(reinterpret_cast<const void*>(contract_mo_f64_kernel<P, MPT, KT>), (int)smem);
-        configured = true;
-    }
+    ensure_dynamic_smem(reinterpret_cast<const void*>(contract_mo_f64_kernel<P, MPT, KT>), (int)smem);
     contract_mo_f64_kernel<P, MPT, KT><<<p.nblocks * 4, 256, smem, stream>>>(p);
 }
 
+// MOs per warp and pass: the fewest passes the largest width allows, then the
+// narrowest listed width that covers the channel's occupied MOs in that many
+// passes (MO columns past the last occupied one are zero and cost as much as
+// real ones: 76 MOs in one pass of 8 x 16 columns would be 40% padding).
+static int mo_width(int nocc, std::initializer_list<int> widths) {
+    const int widest = *(widths.end() - 1);
+    const int passes = nocc > 0 ? (nocc + 8 * widest - 1) / (8 * widest) : 1;
+    const int need = (nocc + 8 * passes - 1) / (8 * passes);
+    for (int w : widths)
+        if (w >= need) return w;
+    return widest;
+}
+
+template <int P>
+static void launch_mo_width(const ContractMoParams& p, int width, cudaStream_t stream) {
+    switch (width) {
+        case 4: launch_mo<P, 4, 16>(p, stream); break;
+        case 8: launch_mo<P, 8, 16>(p, stream); break;
+        case 10: launch_mo<P, 10, 16>(p, stream); break;
+        case 12: launch_mo<P, 12, 16>(p, stream); break;
+        default: launch_mo<P, 16, 16>(p, stream); break;
+    }
+}
+
 void launch_contract_mo_f64(const ContractMoParams& p, int npanel, cudaStream_t stream) {
+    int nocc = 0;
+    for (int i = 0; i < p.nchannels; ++i) nocc = p.ch[i].nocc > nocc ? p.ch[i].nocc : nocc;
     switch (npanel) {
-        case 1: launch_mo<1, 16, 16>(p, stream); break;
-        case 4: launch_mo<4, 16, 16>(p, stream); break;
-        case 5: launch_mo<5, 16, 16>(p, stream); break;
-        case 10: launch_mo<10, 8, 8>(p, stream); break;
+        case 1: launch_mo_width<1>(p, mo_width(nocc, {4, 8, 10, 12, 16}), stream); break;
+        case 4: launch_mo_width<4>(p, mo_width(nocc, {4, 8, 10, 12, 16}), stream); break;
+        case 5: launch_mo_width<5>(p, mo_width(nocc, {4, 8, 10, 12, 16}), stream); break;
+        case 10:
+            switch (mo_width(nocc, {4, 6, 8})) {
+                case 4: launch_mo<10, 4, 8>(p, stream); break;
+                case 6: launch_mo<10, 6, 8>(p, stream); break;
+                default: launch_mo<10, 8, 8>(p, stream); break;
+            }
+            break;
         default: break;
     }
 }
