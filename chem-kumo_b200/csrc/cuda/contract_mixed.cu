@@ -800,10 +800,28 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
     }
     if (w == 0) tmem_alloc(tslot, static_cast<unsigned>(prm.tmem_cols));
     bool sorted = false;
+    const int nk_listed = nk;
     nk = block_row_order(scr.rowmax ? scr.rowmax + static_cast<size_t>(blk) * scr.row_stride * 4 : nullptr, nk,
                          prm.threshold, perm, bucket_start, keys, sorted, static_cast<int>(cap));
     // The rows kept above the threshold (read back by the profiler).
     if (threadIdx.x == 0) scr.nkept[blk] = nk;
+    // Rows that may be exact: those whose block maximum reaches exact_min
+    // (to the sort's power-of-two buckets); a block far from the nuclei, all
+    // of whose rows are small, keeps every row on the tensor cores.
+    int nbig = nk;
+    if (prm.exact_min > 0.0f && sorted) {
+        int emin = static_cast<int>((__float_as_uint(prm.exact_min) >> 23) & 0xffu) - 127 + kBuckets / 2;
+        emin = emin < 0 ? 0 : (emin >= kBuckets ? kBuckets - 1 : emin);
+        int* count = bucket_start + kBuckets + 2;  // spare slot of the sort's bucket array
+        if (tid == 0) *count = 0;
+        __syncthreads();
+        int mine = 0;
+        for (int k = tid; k < nk_listed; k += kBulkThreads) mine += (keys[k] != 0xffu && keys[k] >= emin) ? 1 : 0;
+        if (mine) atomicAdd(count, mine);
+        __syncthreads();
+        nbig = *count;
+        __syncthreads();
+    }
     for (int k = tid; producer && k < nk; k += kThreads) aoidx[k] = static_cast<std::uint16_t>(kept[sorted ? perm[k] : k]);
     // The last nx rows of the K order (the largest block maxima) are added in
     // FP64 in the epilogue instead of on the tensor cores, with AO values
@@ -821,7 +839,7 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
     auto xs_need = [&](int rows, int ph) {
         return 8u * static_cast<unsigned>(rows) * (N + P * ph) + 76u * static_cast<unsigned>(rows) + 16u;
     };
-    int nx = prm.exact_rows < nk ? prm.exact_rows : nk;
+    int nx = prm.exact_rows < nbig ? prm.exact_rows : nbig;
     while (nx > 0 && xs_need(nx, 32) > xs_bytes) --nx;
     const int ph_points = xs_need(nx, 128) <= xs_bytes ? 128 : (xs_need(nx, 64) <= xs_bytes ? 64 : 32);
     const int nkt = nk - nx;

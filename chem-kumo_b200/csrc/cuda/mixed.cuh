@@ -45,6 +45,9 @@ struct ContractMixedParams {
     // cores (0: all rows on the tensor cores), with their AO values computed
     // in FP64 from the basis at the block's points.
     int exact_rows = 0;
+    // Only rows whose block maximum reaches exact_min are taken exact (0: any
+    // row), so blocks whose rows are all small skip the FP64 epilogue.
+    float exact_min = 0.0f;
     PointSource src;        // the evaluation's points (for the exact rows)
     DevBasis basis;         // FP64 exponents and weights (for the exact rows)
     // Limit of each tensor-core pipeline wait in ns (0: one second); a wait
