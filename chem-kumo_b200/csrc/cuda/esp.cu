@@ -103,6 +103,14 @@ void boys_host(const double* table, double T, int n, double* out) {
     for (int m = top; m > 0; --m) out[m - 1] = (2.0 * T * out[m] + decay) / (2.0 * m - 1.0);
 }
 
+double hermite_sup(int t, int u, int v) {
+    const int n = t + u + v;
+    const double pi = std::numbers::pi;
+    return std::sqrt(pi) / (4.0 * pi * pi) * std::ldexp(1.0, n) * std::tgamma(0.5 * (n + 1)) * 2.0 *
+           std::tgamma(0.5 * (t + 1)) * std::tgamma(0.5 * (u + 1)) * std::tgamma(0.5 * (v + 1)) /
+           std::tgamma(0.5 * (n + 3));
+}
+
 EspDevice::EspDevice(const chem::kumo::Molecule& m, cudaStream_t stream) {
     using chem::kumo::detail::check_cuda;
     const auto& blocks = m.blocks();
@@ -203,6 +211,27 @@ EspDevice::EspDevice(const chem::kumo::Molecule& m, cudaStream_t stream) {
         }
         coef.swap(ordered);
     }
+    // Bound of each pair's contribution at any point: sum_k |c_k| p^(n_k/2)
+    // hermite_sup(alpha_k), the triples of order L being a prefix of those
+    // of order kEspMaxL.
+    {
+        const auto triples = hermite_triples(kEspMaxL);
+        std::vector<double> sup(triples.size());
+        std::vector<int> degree(triples.size());
+        for (std::size_t k = 0; k < triples.size(); ++k) {
+            sup[k] = hermite_sup(triples[k].t, triples[k].u, triples[k].v);
+            degree[k] = triples[k].t + triples[k].u + triples[k].v;
+        }
+        bound_.resize(pairs.size());
+        for (std::size_t i = 0; i < pairs.size(); ++i) {
+            const EspPair& pr = pairs[i];
+            const double sp = std::sqrt(pr.p);
+            double b = 0.0;
+            for (int k = 0; k < hermite_count(pr.order); ++k)
+                b += std::abs(coef[static_cast<std::size_t>(pr.first + k)]) * std::pow(sp, degree[k]) * sup[k];
+            bound_[i] = b;
+        }
+    }
     for (int L = 0; L <= kEspMaxL + 1; ++L)
         view_.order_first[L] = std::lower_bound(pairs.begin(), pairs.end(), L,
                                                 [](const EspPair& x, int v) { return x.order < v; }) -
@@ -246,6 +275,61 @@ EspDevice::EspDevice(const chem::kumo::Molecule& m, cudaStream_t stream) {
     view_.natoms = static_cast<int>(atoms.size());
     view_.recursion = static_cast<const int4*>(up(rec.data(), sizeof(int4) * rec.size()));
     check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize (potential setup)");
+    pairs_ = std::move(pairs);
+    coef_ = std::move(coef);
+}
+
+EspView EspDevice::view_for(double tolerance, cudaStream_t stream) {
+    using chem::kumo::detail::check_cuda;
+    if (!(tolerance > 0.0) || pairs_.empty()) return view_;
+    std::lock_guard<std::mutex> lock(views_mutex_);
+    const auto found = views_.find(tolerance);
+    if (found != views_.end()) return found->second;
+    // Drop the pairs of smallest bound while the dropped bounds sum to at most
+    // half the tolerance (the other half is left to rounding).
+    std::vector<std::size_t> order(pairs_.size());
+    for (std::size_t i = 0; i < order.size(); ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](std::size_t a, std::size_t b) { return bound_[a] < bound_[b]; });
+    std::vector<char> drop(pairs_.size(), 0);
+    double dropped = 0.0;
+    const double budget = 0.5 * tolerance;
+    for (const std::size_t i : order) {
+        if (dropped + bound_[i] > budget) break;
+        dropped += bound_[i];
+        drop[i] = 1;
+    }
+    std::vector<EspPair> kept;
+    std::vector<double> coef;
+    for (std::size_t i = 0; i < pairs_.size(); ++i) {
+        if (drop[i]) continue;
+        EspPair pr = pairs_[i];
+        const int nt = hermite_count(pr.order);
+        coef.insert(coef.end(), coef_.begin() + pr.first, coef_.begin() + pr.first + nt);
+        pr.first = static_cast<int>(coef.size()) - nt;
+        kept.push_back(pr);
+    }
+    EspView v = view_;
+    if (kept.size() != pairs_.size()) {
+        auto up = [&](const void* src, std::size_t bytes) {
+            void* d = nullptr;
+            check_cuda(cudaMalloc(&d, std::max<std::size_t>(bytes, 16)), "cudaMalloc (potential)");
+            allocs_.push_back(d);
+            bytes_ += std::max<std::size_t>(bytes, 16);
+            if (bytes)
+                check_cuda(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync (potential)");
+            return d;
+        };
+        v.pairs = static_cast<const EspPair*>(up(kept.data(), sizeof(EspPair) * kept.size()));
+        v.coef = static_cast<const double*>(up(coef.data(), sizeof(double) * coef.size()));
+        v.npairs = static_cast<long long>(kept.size());
+        for (int L = 0; L <= kEspMaxL + 1; ++L)
+            v.order_first[L] = std::lower_bound(kept.begin(), kept.end(), L,
+                                                [](const EspPair& x, int o) { return x.order < o; }) -
+                               kept.begin();
+        check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize (potential screening)");
+    }
+    views_.emplace(tolerance, v);
+    return v;
 }
 
 EspDevice::~EspDevice() {

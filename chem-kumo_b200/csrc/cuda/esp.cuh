@@ -8,6 +8,8 @@
 
 #include <cstddef>
 #include <vector>
+#include <mutex>
+#include <map>
 
 #include "kumo_device.cuh"
 
@@ -69,12 +71,38 @@ public:
     EspView view() const { return view_; }
     long long pair_count() const { return view_.npairs; }
     std::size_t device_bytes() const { return bytes_; }
+    /// The pairs to evaluate for a potential within `tolerance` of the exact
+    /// one: every pair for tolerance 0; otherwise the pairs left after
+    /// dropping, smallest bound first, those whose bounds sum to at most half
+    /// the tolerance (the bound of a pair holds at every point, so the
+    /// dropped pairs change no value by more than that).  Built on first use
+    /// per tolerance (synchronous copies on `stream`) and kept.
+    EspView view_for(double tolerance, cudaStream_t stream);
+    /// Bound of |sum_k c_k R_k(p, X)| over all X for each pair (in pair order).
+    const std::vector<double>& pair_bounds() const { return bound_; }
 
 private:
     EspView view_;
     std::vector<void*> allocs_;
     std::size_t bytes_ = 0;
+    // Host copies of the pairs (order-grouped) and coefficients, for the
+    // screened views.
+    std::vector<EspPair> pairs_;
+    std::vector<double> coef_;
+    std::vector<double> bound_;
+    std::mutex views_mutex_;
+    std::map<double, EspView> views_;
 };
+
+/// sup over Y of |d^(t,u,v) F_0(|Y|^2)| (F_0 the zeroth Boys function), from
+/// its Fourier form F_0(|Y|^2) = sqrt(pi) / (4 pi^2) int exp(-k^2 / 4) / k^2
+/// exp(i k.Y) d^3k: the derivative is bounded by the integral of
+/// |k_x^t k_y^u k_z^v| exp(-k^2 / 4) / k^2, which is
+/// sqrt(pi) / (4 pi^2) 2^n Gamma((n+1)/2) 2 Gamma((t+1)/2) Gamma((u+1)/2)
+/// Gamma((v+1)/2) / Gamma((n+3)/2), n = t + u + v (1 for n = 0, the value at
+/// Y = 0).  With R_tuv(p, X) = d^(t,u,v) F_0(p |X|^2) this gives
+/// |R_tuv(p, X)| <= p^(n/2) hermite_sup(t, u, v) for all X.
+double hermite_sup(int t, int u, int v);
 
 /// Boys table F_m(T_i), m < kBoysOrders, T_i = 0.05 i (src/boys_function.cpp:23-44).
 std::vector<double> boys_table_host();

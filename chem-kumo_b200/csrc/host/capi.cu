@@ -652,6 +652,16 @@ int kumo_esp_pair_count(const kumo_molecule* m, long long* count, char* err, siz
     });
 }
 
+int kumo_esp_pairs_evaluated(const kumo_molecule* m, double tolerance, long long* count, char* err, size_t errlen) {
+    return guarded(err, errlen, [&] {
+        if (!m || !count) throw std::invalid_argument("null argument");
+        if (!std::isfinite(tolerance) || tolerance < 0.0)
+            throw std::invalid_argument("potential tolerance must be finite and nonnegative");
+        auto& dev = m->mol.device();
+        *count = dev.esp_state(m->mol, nullptr).view_for(tolerance, nullptr).npairs;
+    });
+}
+
 int kumo_write_cube(const char* path, const char* comment, const kumo_grid* grid, int natoms, const int* z,
                     const double* charges, const double* xyz, const double* values, long long orbital_index, char* err,
                     size_t errlen) {

@@ -1082,21 +1082,21 @@ private:
         double* out = nullptr;
         for (const auto& [key, ptr] : outs_)
             if (key.kind == PropertyKind::ElectrostaticPotential) out = ptr;
-        // Every primitive pair is evaluated exactly, so in FP64 the result
-        // meets any potential_tolerance >= 0 (src/electrostatic_potential.cpp:501-521
-        // bounds the far-field error by the tolerance; here it is rounding).
-        // The opt-in mixed form's error is its FP32 rounding, whatever the
-        // tolerance.
+        // potential_tolerance as the reference's (src/electrostatic_potential.cpp:501-521:
+        // every value within the tolerance of the exact potential): the pairs
+        // whose bounds (valid at every point) sum to at most half of it are
+        // left out, the others are evaluated exactly.  The opt-in mixed
+        // form adds its FP32 rounding.
         kumo_dev::EspDevice& esp = esp_state();
         kumo_dev::EspParams ep{};
-        ep.esp = esp.view();
+        ep.esp = esp.view_for(opt_.potential_tolerance, stream_);
         ep.src = src_;
         ep.out = out;
         ep.mixed = opt_.precision == Precision::Mixed && esp_mixed_opt_in();
         const int tok = detail::profile_begin(detail::kProfEsp, stream_);
         kumo_dev::launch_esp(ep, stream_);
         detail::profile_end(tok, stream_);
-        detail::profile_count(detail::kProfEsp, nullptr, 0, 0.0, static_cast<double>(n_) * esp.pair_count(), 0.0, 0.0,
+        detail::profile_count(detail::kProfEsp, nullptr, 0, 0.0, static_cast<double>(n_) * ep.esp.npairs, 0.0, 0.0,
                               stream_);
         completed_ += n_;
         report(0);

@@ -152,7 +152,7 @@ EXPORTS = [
     "kumo_default_options", "kumo_molecule_from_fchk", "kumo_molecule_from_arrays", "kumo_molecule_destroy",
     "kumo_molecule_info_get", "kumo_molecule_atoms", "kumo_molecule_block", "kumo_evaluate_grid",
     "kumo_evaluate_points", "kumo_evaluate_grid_device", "kumo_evaluate_points_device", "kumo_ao_panels",
-    "kumo_screening_masks", "kumo_boys", "kumo_esp_pair_count", "kumo_write_cube", "kumo_grid_around",
+    "kumo_screening_masks", "kumo_boys", "kumo_esp_pair_count", "kumo_esp_pairs_evaluated", "kumo_write_cube", "kumo_grid_around",
     "kumo_profile_enable", "kumo_profile_reset", "kumo_profile_read", "kumo_set_device",
     "kumo_evaluate_points_noalloc", "kumo_server_create", "kumo_server_destroy", "kumo_server_submit_grid",
     "kumo_server_submit_points", "kumo_server_wait", "kumo_server_drain", "kumo_server_stats_get",
@@ -227,6 +227,7 @@ def lib():
                                            C.POINTER(C.c_ubyte), *eb]
         L.kumo_boys.argtypes = [_D, C.c_longlong, C.c_int, _D, *eb]
         L.kumo_esp_pair_count.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), *eb]
+        L.kumo_esp_pairs_evaluated.argtypes = [C.c_void_p, C.c_double, C.POINTER(C.c_longlong), *eb]
         L.kumo_write_cube.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(_Grid), C.c_int, _I, _D, _D, _D,
                                       C.c_longlong, *eb]
         L.kumo_grid_around.argtypes = [C.c_void_p, C.c_double, C.c_double, C.POINTER(_Grid), *eb]
@@ -450,6 +451,13 @@ class Molecule:
         c = C.c_longlong()
         e = _err()
         _check(lib().kumo_esp_pair_count(self._h, C.byref(c), e, 512), e)
+        return c.value
+
+    def esp_pairs_evaluated(self, tolerance: float) -> int:
+        """Primitive pairs evaluated for potential_tolerance `tolerance`."""
+        c = C.c_longlong()
+        e = _err()
+        _check(lib().kumo_esp_pairs_evaluated(self._h, float(tolerance), C.byref(c), e, 512), e)
         return c.value
 
 

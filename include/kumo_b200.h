@@ -191,6 +191,13 @@ int kumo_boys(const double* t, long long n, int nvalues, double* out, char* err,
  * (ElectrostaticPotential::primitive_pair_count, src/electrostatic_potential.hpp:61). */
 int kumo_esp_pair_count(const kumo_molecule* m, long long* count, char* err, size_t errlen);
 
+/* Primitive pairs the device evaluates for potential_tolerance `tolerance`
+ * (the role of ElectrostaticPotential::far_field_plan,
+ * src/electrostatic_potential.cpp:501-521): all of them for 0; otherwise those
+ * left after dropping the pairs whose bounds (|contribution| at any point)
+ * sum to at most tolerance / 2. */
+int kumo_esp_pairs_evaluated(const kumo_molecule* m, double tolerance, long long* count, char* err, size_t errlen);
+
 /* Field::write_cube / write_orbital_cube (include/chem/kumo/density.hpp:120-128;
  * src/cube.cpp:70-111); orbital_index 0 writes a density Cube. */
 int kumo_write_cube(const char* path, const char* comment, const kumo_grid* grid, int natoms,

@@ -133,3 +133,26 @@ def test_esp1260_exact_vs_oracle(synth_cache):
         errs[name] = scaled_error(got[0][0], ref)
         print("esp_1260", name, "scaled error", errs[name])
     assert max(errs.values()) <= 5e-11, errs
+
+
+@pytest.mark.parametrize("tol", [1e-8, 1e-6])
+def test_esp1260_tolerance_within_bound(synth_cache, tol):
+    # The potential with the tolerances of the ESP workload against the exact
+    # one (tolerance 0, itself held to the oracle above) at 1,000 cube and
+    # 1,000 isosurface points: every value within the tolerance.
+    path = synth.workload_fchk("esp_1260", synth_cache)
+    m = K.Molecule.from_fchk(path)
+    _, _, xyz = m.atoms()
+    origin, steps, counts = synth.workload_grid("esp_1260", xyz)
+    cube = K.Grid(origin, steps, counts).points()
+    cube = cube[np.linspace(0, len(cube) - 1, 1000).astype(int)]
+    surf = K.density_isosurface(m, 1e-3, 0.25).vertices
+    surf = surf[np.linspace(0, len(surf) - 1, 1000).astype(int)]
+    prop = [K.density(P.ElectrostaticPotential)]
+    for name, pts in (("cube", cube), ("surface", surf)):
+        exact, _ = K.Evaluator(m, potential_tolerance=0.0).evaluate_points(pts, prop)
+        got, _ = K.Evaluator(m, potential_tolerance=tol).evaluate_points(pts, prop)
+        err = float(np.max(np.abs(got[0][0] - exact[0][0])))
+        print("esp_1260", name, "tolerance", tol, "max error", err, "pairs", m.esp_pairs_evaluated(tol), "of",
+              m.esp_pair_count())
+        assert err <= tol, (name, err)
