@@ -641,10 +641,9 @@ def main() -> None:
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(float(np.median(e2e_times)) if e2e_times else float("nan"))
 
-    # The other workloads run at one GPU only (their own single-device measurements).
-    esp_line = None if (args.no_esp or world > 1) else esp_bench(K, synth, d)
-    triplet = None if (args.no_triplet or world > 1) else triplet_bench(K, synth, d, args.triplet_grid_n,
-                                                                          args.triplet_steps, _peaks()[0])
+    # The other workloads run at one GPU only (their own single-device
+    # measurements): the serving loop first, before the potential and triplet
+    # workloads leave GBs in the stream-ordered memory pool.
     serve = None
     if args.serve_seconds > 0 and world == 1:
         pool, sizes = serving_pool(K, synth, args.serve_pool, args.serve_max_atoms)
@@ -659,6 +658,9 @@ def main() -> None:
                                       21, **kw),
                  "fp64": serve_bench(K, synth, int(K.Precision.FP64), args.serve_seconds, args.serve_rate, pool,
                                      21, **kw)}
+    esp_line = None if (args.no_esp or world > 1) else esp_bench(K, synth, d)
+    triplet = None if (args.no_triplet or world > 1) else triplet_bench(K, synth, d, args.triplet_grid_n,
+                                                                          args.triplet_steps, _peaks()[0])
 
     if rank == 0:
         peaks, peak_kind = _peaks()

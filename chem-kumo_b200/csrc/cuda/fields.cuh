@@ -55,8 +55,9 @@ struct FieldSpec {
 };
 
 __device__ __forceinline__ double fermi_constant() {
-    // 0.3 (6 pi^2)^(2/3)
-    return 0.3 * pow(6.0 * 3.141592653589793 * 3.141592653589793, 2.0 / 3.0);
+    // 0.3 (6 pi^2)^(2/3) as the host's libm rounds it (a literal: the device
+    // pow of constant arguments is evaluated at run time, at every point).
+    return 4.557799872345596;
 }
 
 __device__ __forceinline__ double sq3(const double* g) { return g[0] * g[0] + g[1] * g[1] + g[2] * g[2]; }
@@ -113,7 +114,7 @@ __device__ inline double dev_gradient_expansion(const DevDD* const* ch, int n, b
 
 // reduced_gradient(), src/evaluator.cpp:145-154 (cap 100).
 __device__ inline double dev_reduced_gradient(const DevDD& d) {
-    const double scale = 2.0 * cbrt(3.0 * 3.141592653589793 * 3.141592653589793);
+    const double scale = 6.187335452560272;  // 2 cbrt(3 pi^2), as the host's libm rounds it
     if (!(d.value > 0.0)) return 100.0;
     const double den = scale * pow(d.value, 4.0 / 3.0);
     const double norm = sqrt(sq3(d.grad));

@@ -77,8 +77,21 @@ struct PointSource {
 __device__ __forceinline__ bool tile_to_linear(const GridTiles& t, long long e, long long& q) {
     const long long tile = e >> 7;
     const int w = static_cast<int>(e & 127);
-    const long long tk = tile % t.tnz, rest = tile / t.tnz;
-    const long long tj = rest % t.tny, ti = rest / t.tny;
+    long long tk, tj, ti;
+    if (tile < 0xffffffffll && t.tnz < 0xffffffffll && t.tny < 0xffffffffll) {
+        // 32-bit quotients (a fraction of the 64-bit division's instructions).
+        const unsigned u = static_cast<unsigned>(tile), nz = static_cast<unsigned>(t.tnz),
+                       ny = static_cast<unsigned>(t.tny);
+        const unsigned rest = u / nz;
+        tk = u - rest * nz;
+        ti = rest / ny;
+        tj = rest - static_cast<unsigned>(ti) * ny;
+    } else {
+        tk = tile % t.tnz;
+        const long long rest = tile / t.tnz;
+        tj = rest % t.tny;
+        ti = rest / t.tny;
+    }
     const int wk = w & ((1 << t.sc) - 1), wj = (w >> t.sc) & ((1 << t.sb) - 1), wi = w >> (t.sb + t.sc);
     const long long i = (ti << t.sa) + wi, j = (tj << t.sb) + wj, k = (tk << t.sc) + wk;
     if (i >= t.nx || j >= t.ny || k >= t.nz) return false;
@@ -134,9 +147,18 @@ __device__ __forceinline__ void point_at(const PointSource& s, long long q, doub
         return;
     }
     // src/grid_geometry.hpp:59-68: linear = (i * ny + j) * nz + k.
-    const long long i = q / (s.ny * s.nz);
-    const long long j = (q / s.nz) % s.ny;
-    const long long k = q % s.nz;
+    long long i, j, k;
+    if (q < 0xffffffffll && s.nz < 0xffffffffll && s.ny < 0xffffffffll) {
+        const unsigned u = static_cast<unsigned>(q), nz = static_cast<unsigned>(s.nz), ny = static_cast<unsigned>(s.ny);
+        const unsigned r = u / nz;
+        k = u - r * nz;
+        i = r / ny;
+        j = r - static_cast<unsigned>(i) * ny;
+    } else {
+        i = q / (s.ny * s.nz);
+        j = (q / s.nz) % s.ny;
+        k = q % s.nz;
+    }
     const double di = (double)i, dj = (double)j, dk = (double)k;
     x = __dadd_rn(s.origin[0], __dadd_rn(__dadd_rn(__dmul_rn(s.steps[0], di), __dmul_rn(s.steps[3], dj)),
                                          __dmul_rn(s.steps[6], dk)));

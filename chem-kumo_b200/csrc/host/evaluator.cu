@@ -219,12 +219,36 @@ std::vector<detail::TileShape> tile_candidates(const Grid& g) {
     return out;
 }
 
+// AO scratch of one wave (KUMO_SCRATCH_MB): by default a quarter of the
+// device memory free at the evaluation, between 4 and 32 GiB.  Molecules of
+// thousands of AOs need tens of MB per block (every AO row is reserved), so
+// a fixed 4 GiB left their waves at one or two hundred blocks, fewer than two
+// per SM.
 std::size_t scratch_budget() {
     if (const char* e = std::getenv("KUMO_SCRATCH_MB")) {
         const long long mb = std::atoll(e);
         if (mb > 0) return static_cast<std::size_t>(mb) << 20;
     }
-    return std::size_t(4) << 30;
+    std::size_t free_b = 0, total_b = 0;
+    const std::size_t lo = std::size_t(4) << 30, hi = std::size_t(32) << 30;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return lo;
+    }
+    return std::clamp(free_b / 4, lo, hi);
+}
+
+// SMs of the current device (cached per device).
+int sm_count() {
+    static int counts[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!counts[dev]) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+        counts[dev] = n;
+    }
+    return counts[dev];
 }
 
 }  // namespace
@@ -412,10 +436,15 @@ private:
         bp.block_max = nullptr;
     }
 
-    // Blocks per wave for a scratch of `per_block` bytes per block.
+    // Blocks per wave for a scratch of `per_block` bytes per block: as many as
+    // the scratch holds, but with the default scratch no more than an eighth
+    // of the blocks (down to 8 per SM), so that a large grid still has waves
+    // whose results the host-output calls copy while later waves compute.
     int wave_blocks(std::size_t total_blocks, std::size_t per_block) const {
         const std::size_t budget = opt_.scratch_bytes ? opt_.scratch_bytes : scratch_budget();
         std::size_t w = budget / std::max<std::size_t>(per_block, 1);
+        if (!opt_.scratch_bytes)
+            w = std::min(w, std::max<std::size_t>((total_blocks + 7) / 8, static_cast<std::size_t>(8 * sm_count())));
         w = std::max<std::size_t>(1, std::min(w, total_blocks));
         w = std::min<std::size_t>(w, kumo_dev::kMaxBlocksPerWave);
         return static_cast<int>(w);

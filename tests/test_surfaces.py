@@ -256,7 +256,12 @@ def test_potential_and_ionization_surfaces():
     es = K.electrostatic_potential_surface(m, 1e-3, 0.3, potential_tolerance=1e-8)
     assert np.array_equal(es.vertices, mesh.vertices) and np.array_equal(es.triangles, mesh.triangles)
     ref = O.OracleESP(o).evaluate(es.vertices)
-    assert scaled_error(es.values[0], ref) <= 1e-12
+    # potential_tolerance: every value within 1e-8 of the exact potential
+    # (pairs whose bounds sum to at most half of it are left out); with
+    # tolerance 0 the surface values are the exact ones to rounding.
+    assert np.max(np.abs(es.values[0] - ref)) <= 1e-8
+    exact = K.electrostatic_potential_surface(m, 1e-3, 0.3, potential_tolerance=0.0)
+    assert scaled_error(exact.values[0], ref) <= 1e-12
     st = K.surface_statistics(es.vertices, es.triangles, es.values[0])
     assert st == es.statistics[0] or all(
         (st[k] == es.statistics[0][k]) or (isinstance(st[k], float) and math.isnan(st[k]))
