@@ -671,12 +671,12 @@ def main() -> None:
             achieved = st["flops"] / (st["ms"] * 1e-3) / 1e12
             peak = peaks["bf16_tflops"]
             # DRAM bytes per launch: the ncu capture of contract_bulk_kernel on the
-            # 48^3 case read and wrote 1.210 GB for the 437,070 AO rows the AO
-            # kernel wrote (2,769 B per row); scaled by the rows written per launch.
+            # 48^3 case read and wrote 1.198 GB for the 437,070 AO rows the AO
+            # kernel wrote (2,741 B per row); scaled by the rows written per launch.
             ao = prof.get("ao_build", {})
             rows_per_launch = ao["kept_rows"] / ao["launches"] if ao.get("launches") else 0.0
             roof = {"bound": "tensor", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": achieved / peak, "traffic": 2769.0 * rows_per_launch,
+                    "frac": achieved / peak, "traffic": 2741.0 * rows_per_launch,
                     "traffic_source": "ncu dram__bytes_read+write of contract_bulk_kernel, 48^3 capture, "
                                       "per AO row written, scaled to this launch's rows",
                     "peak_source": f"{peak_kind} bf16_tflops (burst)",
