@@ -868,6 +868,8 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
 
     bool failed = false;
     long long gtile = 0;  // K steps of this thread's role so far (all passes)
+    // Records of the two spin channels (kept in local memory through the
+    // passes: in registers they would crowd the K loop's).
     DevDD chan_dd[2];
     dd_zero(chan_dd[0]);
     dd_zero(chan_dd[1]);
@@ -1216,23 +1218,19 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
         tmem_dealloc(tmem, static_cast<unsigned>(prm.tmem_cols));
     }
     if (half != 0 || point >= bcount) return;
-    DevDD comp[4];
     if (failed) {
         const double nan = __longlong_as_double(0x7ff8000000000000ll);
         DevDD d;
         d.value = d.lap = d.tau = nan;
         for (int i = 0; i < 3; ++i) d.grad[i] = d.tau_axes[i] = nan;
         for (int i = 0; i < 6; ++i) d.hess[i] = nan;
-        comp[0] = comp[1] = comp[2] = comp[3] = d;
-    } else {
-        DevDD alpha = chan_dd[0], beta = chan_dd[1];
-        if (prm.beta_is_alpha) beta = alpha;
-        comp[1] = alpha;
-        comp[2] = beta;
-        comp[0] = dd_combine(alpha, beta, 1.0, 1.0, false);
-        comp[3] = dd_combine(alpha, beta, -1.0, 1.0, false);
+        store_point(prm.spec, d, d, false, start + point);
+        return;
     }
-    store_point(prm.spec, comp, start + point);
+    // Total and Difference are formed where a property asks for them.
+    const DevDD alpha = chan_dd[0];
+    const DevDD beta = prm.beta_is_alpha ? chan_dd[0] : chan_dd[1];
+    store_point(prm.spec, alpha, beta, false, start + point);
 }
 
 // ---------------------------------------------------------------------------

@@ -63,7 +63,7 @@ __device__ __forceinline__ double fermi_constant() {
 __device__ __forceinline__ double sq3(const double* g) { return g[0] * g[0] + g[1] * g[1] + g[2] * g[2]; }
 
 // elf(), src/evaluator.cpp:127-140.
-__device__ inline double dev_elf(const DevDD* const* ch, int n) {
+__device__ __forceinline__ double dev_elf(const DevDD* const* ch, int n) {
     const double fermi = fermi_constant();
     double pauli = 0.0, uniform = 0.0;
     for (int i = 0; i < n; ++i) {
@@ -78,7 +78,7 @@ __device__ inline double dev_elf(const DevDD* const* ch, int n) {
 }
 
 // lol(), src/evaluator.cpp:168-179.
-__device__ inline double dev_lol(const DevDD* const* ch, int n) {
+__device__ __forceinline__ double dev_lol(const DevDD* const* ch, int n) {
     const double fermi = fermi_constant();
     double tau = 0.0, uniform = 0.0;
     for (int i = 0; i < n; ++i) {
@@ -91,7 +91,7 @@ __device__ inline double dev_lol(const DevDD* const* ch, int n) {
 }
 
 // gradient_expansion_locator(), src/evaluator.cpp:195-215.
-__device__ inline double dev_gradient_expansion(const DevDD* const* ch, int n, bool lol) {
+__device__ __forceinline__ double dev_gradient_expansion(const DevDD* const* ch, int n, bool lol) {
     const double fermi = fermi_constant();
     double uniform = 0.0, pauli = 0.0, kinetic = 0.0;
     for (int i = 0; i < n; ++i) {
@@ -174,9 +174,55 @@ __device__ inline double dev_dori(const DevDD& d) {
     return theta / (1.0 + theta);
 }
 
-// store_block(), src/evaluator.cpp:248-353, for one point.  comp[c] is the
-// record of DensityComponent c (Total, Alpha, Beta, Difference).
-__device__ inline void store_point(const FieldSpec& spec, const DevDD* comp, long long q) {
+// One property of one component record d (store_block's per-kind cases).
+__device__ __forceinline__ void store_one(int kind, const DevDD& d, double* out, long long p, long long S) {
+    const DevDD* one[1] = {&d};
+    switch (kind) {
+        case 0: out[p] = d.value; break;
+        case 1:
+            for (int a = 0; a < 3; ++a) out[a * S + p] = d.grad[a];
+            break;
+        case 2:
+            for (int h = 0; h < 6; ++h) out[h * S + p] = d.hess[h];
+            break;
+        case 3: out[p] = d.lap; break;
+        case 4: out[p] = d.tau; break;
+        case 6: out[p] = dev_elf(one, 1); break;
+        case 7: out[p] = dev_reduced_gradient(d); break;
+        case 8: out[p] = dev_lambda2(d.hess) < 0.0 ? -d.value : d.value; break;
+        case 10: out[p] = dev_lol(one, 1); break;
+        case 35: out[p] = dev_gradient_expansion(one, 1, false); break;
+        case 36: out[p] = dev_gradient_expansion(one, 1, true); break;
+        case 11: out[p] = dev_iri(d); break;
+        case 12: out[p] = dev_dori(d); break;
+        case 13: out[p] = d.tau - 0.25 * d.lap; break;
+        case 14: out[p] = 0.25 * d.lap - 2.0 * d.tau; break;
+        case 15: out[p] = 0.25 * d.lap - d.tau; break;
+        case 30:
+            for (int a = 0; a < 3; ++a) out[a * S + p] = d.tau_axes[a];
+            break;
+        case 31: {
+            const int diag[3] = {0, 3, 5};
+            for (int a = 0; a < 3; ++a) out[a * S + p] = d.tau_axes[a] - 0.25 * d.hess[diag[a]];
+            break;
+        }
+        case 32: out[p] = d.tau > 0.0 ? fabs(0.25 * d.lap - 2.0 * d.tau) / d.tau : 0.0; break;
+        case 33: out[p] = d.value > 0.0 ? (0.25 * d.lap - d.tau) / d.value : 0.0; break;
+        case 34: out[p] = d.value > 0.0 ? d.tau / d.value : 0.0; break;
+        case 17: out[p] = d.value > 0.0 ? -d.value * log(d.value) : 0.0; break;
+        case 18: out[p] = d.value > 0.0 ? sq3(d.grad) / d.value : 0.0; break;
+        default: break;
+    }
+}
+
+// store_block(), src/evaluator.cpp:248-353, for one point.  alpha and beta
+// are the records of DensityComponent Alpha and Beta; rec(c) gives the record
+// of Total (c = 0) or Difference (c = 3).  Each record is named in its own
+// branch (none is indexed at run time), so the caller's records can stay in
+// registers.
+template <typename Rec>
+__device__ __forceinline__ void store_point_records(const FieldSpec& spec, const DevDD& alpha, const DevDD& beta,
+                                                    Rec rec, long long q) {
     if (spec.tiles.on && !tile_to_linear(spec.tiles, q, q)) return;  // tile padding
     const long long p = q - spec.out_base;
     const long long S = spec.stride;
@@ -185,54 +231,36 @@ __device__ inline void store_point(const FieldSpec& spec, const DevDD* comp, lon
         const int cpt = spec.props[i].component;
         double* out = spec.props[i].out;
         if ((kind == 6 || kind == 10 || kind == 35 || kind == 36) && cpt == 0) {
-            const DevDD* ch[2] = {&comp[1], &comp[2]};
+            const DevDD* ch[2] = {&alpha, &beta};
             out[p] = kind == 6 ? dev_elf(ch, 2) : kind == 10 ? dev_lol(ch, 2) : dev_gradient_expansion(ch, 2, kind == 36);
             continue;
         }
         if (kind == 16) {
-            const double t = comp[0].value;
-            out[p] = t > 0.0 ? comp[3].value / t : 0.0;
+            const double t = rec(0).value;
+            out[p] = t > 0.0 ? rec(3).value / t : 0.0;
             continue;
         }
-        const DevDD& d = comp[cpt];
-        const DevDD* one[1] = {&d};
-        switch (kind) {
-            case 0: out[p] = d.value; break;
-            case 1:
-                for (int a = 0; a < 3; ++a) out[a * S + p] = d.grad[a];
-                break;
-            case 2:
-                for (int h = 0; h < 6; ++h) out[h * S + p] = d.hess[h];
-                break;
-            case 3: out[p] = d.lap; break;
-            case 4: out[p] = d.tau; break;
-            case 6: out[p] = dev_elf(one, 1); break;
-            case 7: out[p] = dev_reduced_gradient(d); break;
-            case 8: out[p] = dev_lambda2(d.hess) < 0.0 ? -d.value : d.value; break;
-            case 10: out[p] = dev_lol(one, 1); break;
-            case 35: out[p] = dev_gradient_expansion(one, 1, false); break;
-            case 36: out[p] = dev_gradient_expansion(one, 1, true); break;
-            case 11: out[p] = dev_iri(d); break;
-            case 12: out[p] = dev_dori(d); break;
-            case 13: out[p] = d.tau - 0.25 * d.lap; break;
-            case 14: out[p] = 0.25 * d.lap - 2.0 * d.tau; break;
-            case 15: out[p] = 0.25 * d.lap - d.tau; break;
-            case 30:
-                for (int a = 0; a < 3; ++a) out[a * S + p] = d.tau_axes[a];
-                break;
-            case 31: {
-                const int diag[3] = {0, 3, 5};
-                for (int a = 0; a < 3; ++a) out[a * S + p] = d.tau_axes[a] - 0.25 * d.hess[diag[a]];
-                break;
-            }
-            case 32: out[p] = d.tau > 0.0 ? fabs(0.25 * d.lap - 2.0 * d.tau) / d.tau : 0.0; break;
-            case 33: out[p] = d.value > 0.0 ? (0.25 * d.lap - d.tau) / d.value : 0.0; break;
-            case 34: out[p] = d.value > 0.0 ? d.tau / d.value : 0.0; break;
-            case 17: out[p] = d.value > 0.0 ? -d.value * log(d.value) : 0.0; break;
-            case 18: out[p] = d.value > 0.0 ? sq3(d.grad) / d.value : 0.0; break;
-            default: break;
+        switch (cpt) {
+            case 0: store_one(kind, rec(0), out, p, S); break;
+            case 1: store_one(kind, alpha, out, p, S); break;
+            case 2: store_one(kind, beta, out, p, S); break;
+            default: store_one(kind, rec(3), out, p, S); break;
         }
     }
+}
+
+// From the two channels' records: Total and Difference formed where a
+// property asks for them (combine(), src/density.cpp:50-60).
+__device__ __forceinline__ void store_point(const FieldSpec& spec, const DevDD& alpha, const DevDD& beta,
+                                            bool full_hessian, long long q) {
+    store_point_records(
+        spec, alpha, beta,
+        [&](int c) { return dd_combine(alpha, beta, c == 0 ? 1.0 : -1.0, 1.0, full_hessian); }, q);
+}
+
+// With comp[c] the record of DensityComponent c.
+__device__ inline void store_point(const FieldSpec& spec, const DevDD* comp, long long q) {
+    store_point_records(spec, comp[1], comp[2], [&](int c) { return comp[c]; }, q);
 }
 
 }  // namespace kumo_dev
