@@ -980,7 +980,13 @@ private:
         f64_waves(fb, W, bp, 0, 1, [&](long long first, int ctas) {
             cp.first_point = first;
             cp.nblocks = ctas;
+            const int tok = detail::profile_begin(detail::kProfContractP, stream_);
             kumo_dev::launch_density_values_f64(cp, stream_);
+            detail::profile_end(tok, stream_);
+            // 2 m^2 FLOPs per point (one panel, one density matrix).
+            if (detail::profiling_enabled())
+                detail::profile_count_sq(detail::kProfContractP, bp.out.nkept, ctas, 2.0 * kumo_dev::kBlockPoints,
+                                         stream_);
         });
         completed_ += n_;
     }
