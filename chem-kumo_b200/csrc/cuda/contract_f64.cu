@@ -193,7 +193,6 @@ __global__ void __launch_bounds__(256, 1) contract_mo_f64_kernel(const __grid_co
 
     if (w != 0 || j0 + lane >= b) return;
     double f[Q];
-    DevDD comp[4];
     DevDD alpha, beta;
     dd_zero(alpha);
     dd_zero(beta);
@@ -205,12 +204,7 @@ __global__ void __launch_bounds__(256, 1) contract_mo_f64_kernel(const __grid_co
             record_from_partials<P>(f, prm.ao_order, beta);
     }
     if (prm.beta_is_alpha) beta = alpha;
-    const bool full = P == 10 && prm.ao_order == 2;
-    comp[1] = alpha;
-    comp[2] = beta;
-    comp[0] = dd_combine(alpha, beta, 1.0, 1.0, full);
-    comp[3] = dd_combine(alpha, beta, -1.0, 1.0, full);
-    store_point(prm.spec, comp, start + j0 + lane);
+    store_point(prm.spec, alpha, beta, P == 10 && prm.ao_order == 2, start + j0 + lane);
 }
 
 template <int P, int MPT, int KT>
