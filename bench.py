@@ -239,7 +239,9 @@ def triplet_bench(K, synth, d: str, grid_n: int = 0, steps: int = 1, peaks=None)
                     peak, unit = 37.0, "FP64 TFLOP/s (nominal B200 FP64 peak)"
                 entry["roofline"] = {"kernel": ck, "achieved_tflops": tf, "peak": peak, "peak_unit": unit,
                                      "frac": tf / peak,
-                                     "algorithmic": ("2 * m_kept^2 * 4 * 128 per block and density matrix"
+                                     "algorithmic": ("2 * m_kept^2 * 128 * left panels per block and density "
+                                                     "matrix (4 panels; 1 for a matrix whose components need "
+                                                     "values only)"
                                                      if backend == K.Backend.AO_P else
                                                      "2 * 128 * 10 panels * m_kept * (n_alpha + n_beta) per block")}
             res[f"{backend.name}_{prec.name}"] = entry

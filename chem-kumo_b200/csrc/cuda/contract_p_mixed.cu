@@ -60,8 +60,9 @@ struct SmemP {
     static constexpr int Q = NQp<P>::v;
     static constexpr unsigned a_bytes = 3u * kPL * kATile;
     static constexpr unsigned b_bytes = 3u * 32u * kCols;
+    // perm and colord (u16), rowao (int) and keys (u8) per sortable row.
     static constexpr size_t total = kStages * (static_cast<size_t>(a_bytes) + b_bytes) + sizeof(double) * Q * 128 +
-                                    sizeof(int) * 2 * kCols + (sizeof(int) + 1) * kSortCap +
+                                    sizeof(int) * 2 * kCols + (2 * sizeof(std::uint16_t) + sizeof(int) + 1) * kSortCap +
                                     sizeof(int) * (kBuckets + 4) + 8 * kStages + 16;
 };
 
@@ -76,9 +77,11 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
     double* red = reinterpret_cast<double*>(b_st + S * L::b_bytes);
     int* colrow = reinterpret_cast<int*>(red + Q * 128);  // block row of each chunk column (-1: none)
     int* colao = colrow + kCols;                          // its AO index
-    int* perm = colao + kCols;
-    int* bucket_start = perm + kSortCap;
-    unsigned char* keys = reinterpret_cast<unsigned char*>(bucket_start + kBuckets + 4);
+    int* rowao = colao + kCols;                           // AO index of each K row (sorted blocks)
+    int* bucket_start = rowao + kSortCap;
+    std::uint16_t* perm = reinterpret_cast<std::uint16_t*>(bucket_start + kBuckets + 4);  // K order of the rows
+    std::uint16_t* colord = perm + kSortCap;  // the kept rows in AO order: the column order
+    unsigned char* keys = reinterpret_cast<unsigned char*>(colord + kSortCap);
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(keys + kSortCap);
     unsigned* tslot = reinterpret_cast<unsigned*>(bar + S);
 
@@ -100,10 +103,37 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
     }
     if (w == 0) tmem_alloc(tslot, 512u);
     bool sorted = false;
+    const int nrows = nk;
     nk = block_row_order(scr.rowmax ? scr.rowmax + static_cast<size_t>(blk) * scr.row_stride * 4 : nullptr, nk,
                          prm.threshold, perm, bucket_start, keys, sorted);
     // The rows kept above the threshold (read back by the profiler).
     if (threadIdx.x == 0) scr.nkept[blk] = nk;
+    if (sorted) {
+        // Columns k take the kept rows in AO order (runs of consecutive AOs,
+        // so that a row of P is read in contiguous pieces); the K rows keep
+        // the ascending-maximum order.  Each warp compacts one segment of the
+        // rows; the segments' counts give their offsets.
+        const int seg = (nrows + 8 * 32 - 1) / (8 * 32) * 32;
+        const int lo = w * seg, hi = min(nrows, lo + seg);
+        int cnt = 0;
+        for (int b = lo; b < hi; b += 32) {
+            const int k = b + lane;
+            cnt += __popc(__ballot_sync(0xffffffffu, k < hi && keys[k] != 0xffu));
+        }
+        __syncthreads();  // bucket_start is free again: the counts go there
+        if (lane == 0) bucket_start[w] = cnt;
+        __syncthreads();
+        int pos = 0;
+        for (int i = 0; i < w; ++i) pos += bucket_start[i];
+        for (int b = lo; b < hi; b += 32) {
+            const int k = b + lane;
+            const bool keep = k < hi && keys[k] != 0xffu;
+            const unsigned bal = __ballot_sync(0xffffffffu, keep);
+            if (keep) colord[pos + __popc(bal & ((1u << lane) - 1u))] = static_cast<std::uint16_t>(k);
+            pos += __popc(bal);
+        }
+        for (int k = tid; k < nk; k += kThreads) rowao[k] = kept[perm[k]];
+    }
     const int ntiles = (nk + 15) / 16;
     tc_fence_before();
     __syncthreads();
@@ -123,26 +153,27 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
     DevDD tot, spn;
     dd_zero(tot);
     dd_zero(spn);
-    const std::uint16_t* mats[2];
+    const uint2* mats[2];
     int roles[2], nmat = 0;
     if (prm.total_needed) {
-        mats[nmat] = prm.p_total_s;
+        mats[nmat] = reinterpret_cast<const uint2*>(prm.p_total_s);
         roles[nmat++] = 0;
     }
     if (prm.spin_needed) {
-        mats[nmat] = prm.p_spin_s;
+        mats[nmat] = reinterpret_cast<const uint2*>(prm.p_spin_s);
         roles[nmat++] = 3;
     }
-    const long long piece_stride = n * n;
 
     for (int mi = 0; mi < nmat && !failed; ++mi) {
-        const std::uint16_t* Pm = mats[mi];
+        const uint2* Pm = mats[mi];
+        // Left panels of this matrix: all four, or the value panel alone.
+        const int npl = (prm.value_only >> (roles[mi] == 0 ? 0 : 1)) & 1 ? 1 : kPL;
         double q[Q];
 #pragma unroll
         for (int i = 0; i < Q; ++i) q[i] = 0.0;
         for (int c0 = 0; c0 < nk && !failed; c0 += kCols) {
             for (int c = tid; c < kCols; c += kThreads) {
-                const int r = c0 + c < nk ? (sorted ? perm[c0 + c] : c0 + c) : -1;
+                const int r = c0 + c < nk ? (sorted ? colord[c0 + c] : c0 + c) : -1;
                 colrow[c] = r;
                 colao[c] = r >= 0 ? kept[r] : -1;
             }
@@ -154,6 +185,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
                 const int row = ok ? (sorted ? perm[k] : k) : 0;
 #pragma unroll
                 for (int c = 0; c < kPL; ++c) {
+                    if (c >= npl) break;
                     if (ok) {
                         const float4* src =
                             reinterpret_cast<const float4*>(pbase + static_cast<size_t>(c) * pstride +
@@ -165,27 +197,49 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
                     }
                 }
             };
-            // B tile of step t: P pieces at (kept row of K row j, kept column c),
-            // 3 pieces x 16 rows x 16 groups of 8 columns; unit v = ((piece*2 + jh)*16 + cg)*8 + j8.
+            // B tile of step t: the three BF16 pieces of P at (AO of K row j,
+            // AO of chunk column c), P stored [row][col] as 8-byte elements
+            // (pieces 0..2 and a zero).  Thread v gathers the 8 columns of
+            // group cg = v & 15 for K row j = v >> 4 (16 rows x 16 groups =
+            // kThreads) with 16-byte loads where they are 8 consecutive AOs,
+            // and writes one 16-byte line of each piece.
             auto load_b = [&](int t, int stage) {
                 unsigned char* bst = b_st + stage * L::b_bytes;
-                for (int v = tid; v < 3 * 16 * (kCols / 8); v += kThreads) {
-                    const int j8 = v & 7, cg = (v >> 3) & 15, jh = (v >> 7) & 1, piece = v >> 8;
-                    const int j = t * 16 + jh * 8 + j8;
-                    const int rao = j < nk ? kept[sorted ? perm[j] : j] : -1;
-                    unsigned short h[8];
+                const int cg = tid & 15, jr = tid >> 4, j = t * 16 + jr;
+                const int rao = j < nk ? (sorted ? rowao[j] : kept[j]) : -1;
+                uint2 e[8];
+                const int cao0 = colao[cg * 8];
+                bool run = rao >= 0 && cao0 >= 0;
+#pragma unroll
+                for (int u = 1; u < 8; ++u) run = run && colao[cg * 8 + u] == cao0 + u;
+                const long long at = static_cast<long long>(rao) * n + cao0;
+                if (run && (at & 1) == 0) {
+                    const uint4* src = reinterpret_cast<const uint4*>(Pm + at);
+#pragma unroll
+                    for (int h = 0; h < 4; ++h) {
+                        const uint4 q4 = __ldg(src + h);
+                        e[2 * h] = make_uint2(q4.x, q4.y);
+                        e[2 * h + 1] = make_uint2(q4.z, q4.w);
+                    }
+                } else {
 #pragma unroll
                     for (int u = 0; u < 8; ++u) {
                         const int cao = colao[cg * 8 + u];
-                        h[u] = (rao >= 0 && cao >= 0) ? Pm[piece * piece_stride + static_cast<long long>(rao) * n + cao]
-                                                      : static_cast<unsigned short>(0);
+                        e[u] = (rao >= 0 && cao >= 0) ? __ldg(Pm + static_cast<long long>(rao) * n + cao) : make_uint2(0u, 0u);
                     }
-                    const uint4 val = make_uint4(h[0] | (static_cast<unsigned>(h[1]) << 16),
-                                                 h[2] | (static_cast<unsigned>(h[3]) << 16),
-                                                 h[4] | (static_cast<unsigned>(h[5]) << 16),
-                                                 h[6] | (static_cast<unsigned>(h[7]) << 16));
-                    *reinterpret_cast<uint4*>(bst + piece * 32 * kCols + cg * 128 + jh * (kCols * 16) + j8 * 16) = val;
                 }
+                unsigned w0[4], w1[4], w2[4];
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    const uint2 a = e[2 * h], b = e[2 * h + 1];
+                    w0[h] = (a.x & 0xffffu) | (b.x << 16);
+                    w1[h] = (a.x >> 16) | (b.x & 0xffff0000u);
+                    w2[h] = (a.y & 0xffffu) | (b.y << 16);
+                }
+                unsigned char* dst = bst + cg * 128 + (jr >> 3) * (kCols * 16) + (jr & 7) * 16;
+                *reinterpret_cast<uint4*>(dst) = make_uint4(w0[0], w0[1], w0[2], w0[3]);
+                *reinterpret_cast<uint4*>(dst + 32 * kCols) = make_uint4(w1[0], w1[1], w1[2], w1[3]);
+                *reinterpret_cast<uint4*>(dst + 64 * kCols) = make_uint4(w2[0], w2[1], w2[2], w2[3]);
             };
             if (ntiles > 0) {
                 load_a(0);
@@ -196,6 +250,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
                 unsigned char* ast = a_st + s * L::a_bytes;
 #pragma unroll
                 for (int c = 0; c < kPL; ++c) {
+                    if (c >= npl) break;
                     uint4 p0, p1, p2;
                     split8(ra[c][0], ra[c][1], p0, p1, p2);
                     *reinterpret_cast<uint4*>(ast + (0 * kPL + c) * kATile + a_off) = p0;
@@ -215,6 +270,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
                     constexpr unsigned bpiece = (32u * kCols) >> 4;
 #pragma unroll
                     for (int c = 0; c < kPL; ++c) {
+                        if (c >= npl) break;
 #pragma unroll
                         for (int e = 0; e < 6; ++e) {
                             const unsigned long long ad = as + static_cast<unsigned>(((piece_a(e) * kPL + c) * kATile) >> 4);
@@ -241,7 +297,21 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
             // Fold: columns [half*64, half*64 + 64) of the chunk, 4 at a time.
             const unsigned lane_addr = tmem + (static_cast<unsigned>(quarter * 32) << 16);
             const int c_hi = min(nk - c0, (half + 1) * (kCols / 2));
-            for (int i0 = half * (kCols / 2); i0 < c_hi; i0 += 4) {
+            if (npl == 1) {
+                for (int i0 = half * (kCols / 2); i0 < c_hi; i0 += 8) {
+                    unsigned v[8];
+                    tmem_ld<8>(lane_addr + static_cast<unsigned>(i0), v);
+                    tmem_wait_ld();
+                    reg_fence<8>(v);
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        if (i0 + u >= c_hi) break;
+                        const float* row = pbase + static_cast<size_t>(colrow[i0 + u]) * kBlockPoints + point;
+                        q[0] += static_cast<double>(row[0]) * static_cast<double>(__uint_as_float(v[u]));
+                    }
+                }
+            }
+            for (int i0 = half * (kCols / 2); npl != 1 && i0 < c_hi; i0 += 4) {
                 unsigned v[kPL][4];
 #pragma unroll
                 for (int c = 0; c < kPL; ++c) tmem_ld<4>(lane_addr + static_cast<unsigned>(c * kCols + i0), v[c]);
@@ -287,7 +357,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
         if (half == 0) {
 #pragma unroll
             for (int i = 0; i < Q; ++i) q[i] += red[i * 128 + point];
-            record_p<P>(q, prm.ao_order, roles[mi] == 0 ? tot : spn);
+            record_p<P>(q, npl == 1 ? 0 : prm.ao_order, roles[mi] == 0 ? tot : spn);
         }
         __syncthreads();
     }

@@ -64,11 +64,14 @@ struct ContractPMixedParams {
     long long count = 0;
     int nblocks = 0;
     int nao = 0;
-    const std::uint16_t* p_total_s = nullptr;  // [3][nao][nao] BF16 pieces of P_total
+    const std::uint16_t* p_total_s = nullptr;  // [nao][nao][4]: BF16 pieces 0..2 of P_total and a zero
     const std::uint16_t* p_spin_s = nullptr;   // same for P_spin
     int total_needed = 0;
     int spin_needed = 0;
     int ao_order = 2;
+    // Bit 0 (P_total) and bit 1 (P_spin): that matrix's components need
+    // values only, so only Y_0 = Phi_0 P is formed and folded.
+    int value_only = 0;
     float threshold = 0.0f;
     FieldSpec spec;
     unsigned* status = nullptr;

@@ -155,13 +155,13 @@ DeviceMolecule::DeviceMolecule(const Molecule& m) {
     const Matrix ps = m.density_matrix(DensityComponent::Difference);
     p_total = upload(pt.data(), pt.size());
     auto split_matrix = [&](const Matrix& m) {
-        std::vector<std::uint16_t> pieces(3 * n * n);
+        std::vector<std::uint16_t> pieces(4 * n * n, 0);
         for (std::size_t r = 0; r < n; ++r)
             for (std::size_t c = 0; c < n; ++c) {
                 double rest = m(r, c);
                 for (int k = 0; k < 3; ++k) {
                     const std::uint16_t h = bf16_bits(rest);
-                    pieces[(static_cast<std::size_t>(k) * n + r) * n + c] = h;
+                    pieces[(r * n + c) * 4 + static_cast<std::size_t>(k)] = h;
                     rest -= bf16_value(h);
                 }
             }

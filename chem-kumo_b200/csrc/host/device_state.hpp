@@ -48,8 +48,8 @@ struct DeviceMolecule {
     // Occupied MOs of the mixed form as three BF16 pieces (c = c0 + c1 + c2,
     // each the BF16 rounding of what the previous pieces leave), stored
     // [piece][AO][MO] with rows of ldn MOs (a multiple of 16, zero padded).
-    // P_total and P_spin as three BF16 pieces [piece][row][col] for the mixed
-    // AO-P form.
+    // P_total and P_spin for the mixed AO-P form: each element as its three
+    // BF16 pieces and a zero, [row][col][4] (one 8-byte load per element).
     std::uint16_t* p_total_s = nullptr;
     std::uint16_t* p_spin_s = nullptr;
     std::uint16_t* cs_alpha = nullptr;

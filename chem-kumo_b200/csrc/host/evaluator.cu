@@ -85,16 +85,28 @@ bool esp_mixed_opt_in() {
     return e != nullptr && e[0] == '1';
 }
 
-bool uses_point_path(const detail::ComponentNeeds& c, Backend b, bool grid) {
-    return c.derivatives() || ((b == Backend::AO_MO || !grid) && c.density);
+// Which pass computes each requested property.  Grid-path orbital amplitudes
+// follow src/orbitals.cpp:66-102.  AO-P densities on a grid take the
+// reference's blocked grid path (src/density.cpp:366-444) in the FP64 form;
+// the mixed form computes them in its tensor-core point pass, where one
+// contraction per density matrix serves every component.
+struct Route {
+    Backend backend = Backend::AO_P;
+    bool grid = false;
+    bool mixed = false;
+    bool grid_densities() const { return grid && backend == Backend::AO_P && !mixed; }
+};
+
+bool uses_point_path(const detail::ComponentNeeds& c, const Route& r) {
+    return c.derivatives() || (!r.grid_densities() && c.density);
 }
 
-bool on_grid_path(const Property& p, Backend b, bool grid) {
-    return grid && (p.kind == PropertyKind::Orbital || (p.kind == PropertyKind::Density && b == Backend::AO_P));
+bool on_grid_path(const Property& p, const Route& r) {
+    return r.grid && (p.kind == PropertyKind::Orbital || (p.kind == PropertyKind::Density && r.grid_densities()));
 }
 
-bool from_point_path(const Property& p, Backend b, bool grid) {
-    return !on_grid_path(p, b, grid) && !detail::is_orbital_kind(p.kind) &&
+bool from_point_path(const Property& p, const Route& r) {
+    return !on_grid_path(p, r) && !detail::is_orbital_kind(p.kind) &&
            p.kind != PropertyKind::ElectrostaticPotential && !detail::is_orbital_energy_kind(p.kind);
 }
 
@@ -328,9 +340,9 @@ public:
         } else {
             src_.points = points_;
         }
-        const bool grid = grid_ != nullptr;
+        const Route rt = route();
         bool point_path = false;
-        for (const auto& c : plan_.c) point_path |= uses_point_path(c, backend_, grid);
+        for (const auto& c : plan_.c) point_path |= uses_point_path(c, rt);
         // Progress over all passes, src/evaluator.cpp:599-607.
         passes_ = (point_path ? 1 : 0) + (plan_.needs_esp() ? 1 : 0) + (plan_.orbital_energies ? 1 : 0);
         bool orbital_pass = false;
@@ -338,11 +350,11 @@ public:
         std::size_t grid_densities = 0;
         for (const auto& [key, ptr] : outs_) {
             if (detail::is_orbital_kind(key.kind)) {
-                if (on_grid_path(key, backend_, grid))
+                if (on_grid_path(key, rt))
                     grid_orbitals[key.channel == SpinChannel::Beta ? 1 : 0] = true;
                 else
                     orbital_pass = true;
-            } else if (on_grid_path(key, backend_, grid)) {
+            } else if (on_grid_path(key, rt)) {
                 ++grid_densities;
             }
         }
@@ -353,7 +365,7 @@ public:
         if (plan_.orbital_energies) orbital_energy_pass();
         if (orbital_pass) orbital_pass_run(false);
         for (const auto& [key, ptr] : outs_)
-            if (on_grid_path(key, backend_, grid) && key.kind == PropertyKind::Density) grid_density_pass(key, ptr);
+            if (on_grid_path(key, rt) && key.kind == PropertyKind::Density) grid_density_pass(key, ptr);
         for (int ch = 0; ch < 2; ++ch)
             if (grid_orbitals[ch]) orbital_pass_run(true, ch);
         check_cuda(cudaGetLastError(), "kernel launch");
@@ -462,12 +474,14 @@ private:
         return p;
     }
 
-    kumo_dev::FieldSpec field_spec(bool (*select)(const Property&, Backend, bool)) const {
+    Route route() const { return {backend_, grid_ != nullptr, opt_.precision == Precision::Mixed}; }
+
+    kumo_dev::FieldSpec field_spec(bool (*select)(const Property&, const Route&)) const {
         kumo_dev::FieldSpec spec{};
         spec.stride = static_cast<long long>(n_);
         spec.out_base = 0;
         for (const auto& [key, ptr] : outs_) {
-            if (!select(key, backend_, grid_ != nullptr)) continue;
+            if (!select(key, route())) continue;
             if (spec.nprops == kumo_dev::kMaxProps) throw std::invalid_argument("too many properties in one request");
             spec.props[spec.nprops++] = {static_cast<int>(key.kind), static_cast<int>(key.component), ptr};
         }
@@ -477,11 +491,12 @@ private:
     void point_pass() {
         const bool grid = grid_ != nullptr;
         std::array<bool, 4> needed{};
-        for (int c = 0; c < 4; ++c) needed[c] = uses_point_path(plan_.c[c], backend_, grid);
+        const Route rt = route();
+        for (int c = 0; c < 4; ++c) needed[c] = uses_point_path(plan_.c[c], rt);
         const int ao_order = grid ? plan_.max_order : std::max(1, plan_.max_order);
         bool full = false;
         for (const auto& [key, ptr] : outs_)
-            if (from_point_path(key, backend_, grid) && needs_full_hessian(key.kind)) full = true;
+            if (from_point_path(key, rt) && needs_full_hessian(key.kind)) full = true;
         int npanel;
         if (ao_order <= 0)
             npanel = kumo_dev::kPanelsValue;
@@ -526,10 +541,11 @@ private:
 
     // AO-P contraction of a wave: per block and density matrix, the product
     // P[kept, kept] Phi[kept, 4 panels], 2 * m^2 * 4 * 128 FLOPs.
-    void count_ao_p(const int* nkept, int nb, int nmatrices) const {
+    // npanels: left panels summed over the density matrices contracted (4 per
+    // matrix, 1 for a matrix whose components need values only).
+    void count_ao_p(const int* nkept, int nb, int npanels) const {
         if (!detail::profiling_enabled()) return;
-        detail::profile_count_sq(detail::kProfContractP, nkept, nb, 2.0 * 4 * kumo_dev::kBlockPoints * nmatrices,
-                                 stream_);
+        detail::profile_count_sq(detail::kProfContractP, nkept, nb, 2.0 * kumo_dev::kBlockPoints * npanels, stream_);
     }
 
     // Occupied-MO channels needed by the AO-MO contraction
@@ -616,7 +632,7 @@ private:
         Request probe;
         std::size_t chans = 0;
         for (const auto& [key, ptr] : outs_)
-            if (from_point_path(key, backend_, true)) {
+            if (from_point_path(key, route())) {
                 probe.add(key);
                 chans += property_channels(key.kind);
             }
@@ -895,6 +911,17 @@ private:
         cp.total_needed = needed[0] || needed[1] || needed[2];
         cp.spin_needed = needed[3] || needed[1] || needed[2];
         cp.ao_order = ao_order;
+        // A density matrix whose components need values only (the alpha, beta
+        // and spin densities beside a Total-only RDG, say) is contracted with
+        // the value panel alone.
+        int order_total = -1, order_spin = -1;
+        for (int c = 0; c < 4; ++c) {
+            if (!needed[c]) continue;
+            const int o = std::max(0, plan_.c[c].ao_order());
+            if (c != 3) order_total = std::max(order_total, o);
+            if (c != 0) order_spin = std::max(order_spin, o);
+        }
+        cp.value_only = (order_total == 0 ? 1 : 0) | (order_spin == 0 ? 2 : 0);
         cp.threshold = static_cast<float>(opt_.screening_threshold);
         cp.spec = spec;
         cp.spec.tiles = lay.tiles;
@@ -913,7 +940,8 @@ private:
             tok = detail::profile_begin(detail::kProfContractP, stream_);
             kumo_dev::launch_contract_p_mixed(cp, npanel, stream_);
             detail::profile_end(tok, stream_);
-            count_ao_p(bp.out.nkept, nb, (cp.total_needed ? 1 : 0) + (cp.spin_needed ? 1 : 0));
+            count_ao_p(bp.out.nkept, nb,
+                       (cp.total_needed ? (cp.value_only & 1 ? 1 : 4) : 0) + (cp.spin_needed ? (cp.value_only & 2 ? 1 : 4) : 0));
             report(done_points(lay, b0 + nb));
         }
     }
@@ -948,7 +976,7 @@ private:
             const int tok = detail::profile_begin(detail::kProfContractP, stream_);
             kumo_dev::launch_contract_p_f64(cp, npanel, stream_);
             detail::profile_end(tok, stream_);
-            count_ao_p(bp.out.nkept, ctas, (cp.total_needed ? 1 : 0) + (cp.spin_needed ? 1 : 0));
+            count_ao_p(bp.out.nkept, ctas, 4 * ((cp.total_needed ? 1 : 0) + (cp.spin_needed ? 1 : 0)));
         });
     }
 
@@ -1001,7 +1029,7 @@ private:
         int order = 0;
         for (const auto& [key, ptr] : outs_) {
             if (!detail::is_orbital_kind(key.kind)) continue;
-            const bool gp = on_grid_path(key, backend_, grid);
+            const bool gp = on_grid_path(key, route());
             if (gp != grid_path) continue;
             if (grid_path && static_cast<int>(key.channel) != channel) continue;
             sel.emplace_back(key, ptr);

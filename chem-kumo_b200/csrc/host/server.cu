@@ -62,7 +62,9 @@ std::size_t molecule_bytes_estimate(const Molecule& m) {
     const std::size_t n = m.basis_size();
     const std::size_t nmo = m.orbital_count(SpinChannel::Alpha) + (m.unrestricted() ? m.orbital_count(SpinChannel::Beta) : 0);
     const std::size_t occ = m.occupied_count(SpinChannel::Alpha) + m.occupied_count(SpinChannel::Beta) + 32;
-    return 2 * n * n * 8 + n * nmo * 8 + n * occ * (8 + 6) + (std::size_t(4) << 20);
+    // P_total and P_spin in FP64 and as 8-byte BF16 piece elements, all MO
+    // coefficients, the occupied MOs in FP64 and as pieces, and the tables.
+    return 2 * n * n * (8 + 8) + n * nmo * 8 + n * occ * (8 + 6) + (std::size_t(4) << 20);
 }
 
 // Grid points in the device's arithmetic (point_at: origin + ((s_a i + s_b j) + s_c k)).

@@ -554,6 +554,32 @@ def test_mixed_tensor_core_ao_p(name, case):
         assert np.abs(a - r).max() / scale <= 1e-6, (p, np.abs(a - r).max() / scale)
 
 
+@pytest.mark.parametrize("with_hessian", [False, True])
+def test_mixed_ao_p_grid_densities(with_hessian):
+    # On a grid the FP64 AO-P form takes each density on the blocked grid path;
+    # the mixed form computes them in its tensor-core point pass (values-only
+    # products for a matrix whose components need no derivatives).
+    m = K.Molecule.from_fchk(os.path.join(GOLDEN, "o2.fchk.gz"))
+    grid = m.grid_around(2.0, 0.25)
+    props = [K.density(P.Density, c) for c in (D.Alpha, D.Beta, D.Difference, D.Total)]
+    if with_hessian:
+        props += [K.density(P.ReducedGradient), K.density(P.SignLambda2Density)]
+    f64, used = K.Evaluator(m, backend=K.Backend.AO_P).evaluate_grid(grid, props)
+    mix, used_m = K.Evaluator(m, backend=K.Backend.AO_P, precision=K.Precision.Mixed).evaluate_grid(grid, props)
+    assert used == used_m == int(K.Backend.AO_P)
+    rho = np.asarray(f64[3]).ravel()
+    for p, a, r in zip(props, mix, f64):
+        a, r = np.asarray(a).ravel(), np.asarray(r).ravel()
+        assert np.all(np.isfinite(a)), p
+        if p.kind == P.ReducedGradient:
+            # RDG = |grad rho| / rho^(4/3): compared where rho > 1e-6.
+            sel = rho > 1e-6
+            assert np.abs(a[sel] - r[sel]).max() / np.abs(r[sel]).max() <= 1e-5, p
+            continue
+        scale = max(1.0, np.abs(rho).max())
+        assert np.abs(a - r).max() / scale <= 1e-6, (p, np.abs(a - r).max() / scale)
+
+
 def test_mixed_tensor_core_ao_p_many_column_chunks(synth_cache):
     # 740 AOs: about six 128-column chunks of Y per block.
     m = K.Molecule.from_fchk(synth.workload_fchk("organic_740", synth_cache))
