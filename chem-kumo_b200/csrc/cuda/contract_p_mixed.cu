@@ -202,12 +202,13 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
             // (pieces 0..2 and a zero).  Thread v gathers the 8 columns of
             // group cg = v & 15 for K row j = v >> 4 (16 rows x 16 groups =
             // kThreads) with 16-byte loads where they are 8 consecutive AOs,
-            // and writes one 16-byte line of each piece.
-            auto load_b = [&](int t, int stage) {
-                unsigned char* bst = b_st + stage * L::b_bytes;
-                const int cg = tid & 15, jr = tid >> 4, j = t * 16 + jr;
+            // and writes one 16-byte line of each piece.  The loads of step t + 1
+            // are issued before the MMAs of step t and stored after them.
+            uint2 eb[8];
+            const int cg = tid & 15, jr = tid >> 4;
+            auto fetch_b = [&](int t) {
+                const int j = t * 16 + jr;
                 const int rao = j < nk ? (sorted ? rowao[j] : kept[j]) : -1;
-                uint2 e[8];
                 const int cao0 = colao[cg * 8];
                 bool run = rao >= 0 && cao0 >= 0;
 #pragma unroll
@@ -218,20 +219,23 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
 #pragma unroll
                     for (int h = 0; h < 4; ++h) {
                         const uint4 q4 = __ldg(src + h);
-                        e[2 * h] = make_uint2(q4.x, q4.y);
-                        e[2 * h + 1] = make_uint2(q4.z, q4.w);
+                        eb[2 * h] = make_uint2(q4.x, q4.y);
+                        eb[2 * h + 1] = make_uint2(q4.z, q4.w);
                     }
                 } else {
 #pragma unroll
                     for (int u = 0; u < 8; ++u) {
                         const int cao = colao[cg * 8 + u];
-                        e[u] = (rao >= 0 && cao >= 0) ? __ldg(Pm + static_cast<long long>(rao) * n + cao) : make_uint2(0u, 0u);
+                        eb[u] = (rao >= 0 && cao >= 0) ? __ldg(Pm + static_cast<long long>(rao) * n + cao) : make_uint2(0u, 0u);
                     }
                 }
+            };
+            auto store_b = [&](int stage) {
+                unsigned char* bst = b_st + stage * L::b_bytes;
                 unsigned w0[4], w1[4], w2[4];
 #pragma unroll
                 for (int h = 0; h < 4; ++h) {
-                    const uint2 a = e[2 * h], b = e[2 * h + 1];
+                    const uint2 a = eb[2 * h], b = eb[2 * h + 1];
                     w0[h] = (a.x & 0xffffu) | (b.x << 16);
                     w1[h] = (a.x >> 16) | (b.x & 0xffff0000u);
                     w2[h] = (a.y & 0xffffu) | (b.y << 16);
@@ -243,7 +247,7 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
             };
             if (ntiles > 0) {
                 load_a(0);
-                load_b(0, static_cast<int>(gtile % S));
+                fetch_b(0);
             }
             for (int t = 0; t < ntiles; ++t, ++gtile) {
                 const int s = static_cast<int>(gtile % S);
@@ -257,7 +261,11 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
                     *reinterpret_cast<uint4*>(ast + (1 * kPL + c) * kATile + a_off) = p1;
                     *reinterpret_cast<uint4*>(ast + (2 * kPL + c) * kATile + a_off) = p2;
                 }
-                if (t + 1 < ntiles) load_a(t + 1);
+                store_b(s);
+                if (t + 1 < ntiles) {
+                    load_a(t + 1);
+                    fetch_b(t + 1);
+                }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 if (__syncthreads_or(failed)) {
                     failed = true;
@@ -283,7 +291,6 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
                 if (t + 1 < ntiles) {
                     const long long wt = gtile + 1 - S;
                     if (wt >= 0 && !mbar_wait(&bar[wt % S], static_cast<unsigned>((wt / S) & 1), prm.wait_ns)) failed = true;
-                    load_b(t + 1, static_cast<int>((gtile + 1) % S));
                 }
             }
             if (failed || ntiles == 0) continue;
@@ -294,55 +301,91 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
                 break;
             }
             tc_fence_after();
-            // Fold: columns [half*64, half*64 + 64) of the chunk, 4 at a time.
+            // Fold: columns [half*64, half*64 + 64) of the chunk.
             const unsigned lane_addr = tmem + (static_cast<unsigned>(quarter * 32) << 16);
             const int c_hi = min(nk - c0, (half + 1) * (kCols / 2));
+            // The panel values of a group's columns are loaded one group
+            // ahead, so that their latency overlaps the previous group's
+            // products.
+            const int i_lo = half * (kCols / 2);
             if (npl == 1) {
-                for (int i0 = half * (kCols / 2); i0 < c_hi; i0 += 8) {
+                float rv[2][8];
+                auto rows8 = [&](float (&r)[8], int i0) {
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+                        r[u] = i0 + u < c_hi ? pbase[static_cast<size_t>(colrow[i0 + u]) * kBlockPoints + point] : 0.0f;
+                };
+                auto fold8 = [&](const float (&r)[8], int i0) {
                     unsigned v[8];
                     tmem_ld<8>(lane_addr + static_cast<unsigned>(i0), v);
                     tmem_wait_ld();
                     reg_fence<8>(v);
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) {
-                        if (i0 + u >= c_hi) break;
-                        const float* row = pbase + static_cast<size_t>(colrow[i0 + u]) * kBlockPoints + point;
-                        q[0] += static_cast<double>(row[0]) * static_cast<double>(__uint_as_float(v[u]));
+                    for (int u = 0; u < 8; ++u)
+                        if (i0 + u < c_hi) q[0] += static_cast<double>(r[u]) * static_cast<double>(__uint_as_float(v[u]));
+                };
+                if (i_lo < c_hi) rows8(rv[0], i_lo);
+                for (int i0 = i_lo; i0 < c_hi; i0 += 16) {
+                    if (i0 + 8 < c_hi) rows8(rv[1], i0 + 8);
+                    fold8(rv[0], i0);
+                    if (i0 + 8 < c_hi) {
+                        if (i0 + 16 < c_hi) rows8(rv[0], i0 + 16);
+                        fold8(rv[1], i0 + 8);
                     }
                 }
-            }
-            for (int i0 = half * (kCols / 2); npl != 1 && i0 < c_hi; i0 += 4) {
-                unsigned v[kPL][4];
+            } else {
+                // Panel values of CG columns, r[u][c] of panel c (all P
+                // panels); two columns at a time with the Hessian panels.
+                constexpr int CG = P == 10 ? 2 : 4;
+                float rv[2][CG][P];
+                auto rows4 = [&](float (&r)[CG][P], int i0) {
 #pragma unroll
-                for (int c = 0; c < kPL; ++c) tmem_ld<4>(lane_addr + static_cast<unsigned>(c * kCols + i0), v[c]);
-                tmem_wait_ld();
+                    for (int u = 0; u < CG; ++u) {
+                        const bool ok = i0 + u < c_hi;
+                        const float* row = pbase + static_cast<size_t>(ok ? colrow[i0 + u] : 0) * kBlockPoints + point;
 #pragma unroll
-                for (int c = 0; c < kPL; ++c) reg_fence<4>(v[c]);
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    if (i0 + u >= c_hi) break;
-                    const int r = colrow[i0 + u];
-                    const float* row = pbase + static_cast<size_t>(r) * kBlockPoints + point;
-                    double y[kPL];
-#pragma unroll
-                    for (int c = 0; c < kPL; ++c) y[c] = static_cast<double>(__uint_as_float(v[c][u]));
-                    const double f0 = row[0];
-                    q[0] += f0 * y[0];
-                    double fa[3];
-#pragma unroll
-                    for (int a = 0; a < 3; ++a) {
-                        fa[a] = row[(1 + a) * pstride];
-                        q[1 + a] += fa[a] * y[0];
-                        q[4 + a] += fa[a] * y[1 + a];
+                        for (int c = 0; c < P; ++c) r[u][c] = ok ? row[c * pstride] : 0.0f;
                     }
-                    if constexpr (P == 5) q[7] += static_cast<double>(row[4 * pstride]) * y[0];
-                    if constexpr (P == 10) {
-                        constexpr int pa[6] = {0, 0, 0, 1, 1, 2}, pc[6] = {0, 1, 2, 1, 2, 2};
+                };
+                auto fold4 = [&](const float (&r)[CG][P], int i0) {
+                    unsigned v[kPL][CG];
 #pragma unroll
-                        for (int h = 0; h < 6; ++h) {
-                            q[7 + h] += static_cast<double>(row[(4 + h) * pstride]) * y[0];
-                            q[13 + h] += fa[pa[h]] * y[1 + pc[h]];
+                    for (int c = 0; c < kPL; ++c) tmem_ld<CG>(lane_addr + static_cast<unsigned>(c * kCols + i0), v[c]);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int c = 0; c < kPL; ++c) reg_fence<CG>(v[c]);
+#pragma unroll
+                    for (int u = 0; u < CG; ++u) {
+                        if (i0 + u >= c_hi) break;
+                        double y[kPL];
+#pragma unroll
+                        for (int c = 0; c < kPL; ++c) y[c] = static_cast<double>(__uint_as_float(v[c][u]));
+                        q[0] += static_cast<double>(r[u][0]) * y[0];
+                        double fa[3];
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            fa[a] = r[u][1 + a];
+                            q[1 + a] += fa[a] * y[0];
+                            q[4 + a] += fa[a] * y[1 + a];
                         }
+                        if constexpr (P == 5) q[7] += static_cast<double>(r[u][4]) * y[0];
+                        if constexpr (P == 10) {
+                            constexpr int pa[6] = {0, 0, 0, 1, 1, 2}, pc[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+                            for (int h = 0; h < 6; ++h) {
+                                q[7 + h] += static_cast<double>(r[u][4 + h]) * y[0];
+                                q[13 + h] += fa[pa[h]] * y[1 + pc[h]];
+                            }
+                        }
+                    }
+                };
+                if (i_lo < c_hi) rows4(rv[0], i_lo);
+                for (int i0 = i_lo; i0 < c_hi; i0 += 2 * CG) {
+                    if (i0 + CG < c_hi) rows4(rv[1], i0 + CG);
+                    fold4(rv[0], i0);
+                    if (i0 + CG < c_hi) {
+                        if (i0 + 2 * CG < c_hi) rows4(rv[0], i0 + 2 * CG);
+                        fold4(rv[1], i0 + CG);
                     }
                 }
             }

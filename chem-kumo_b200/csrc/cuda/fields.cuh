@@ -124,8 +124,10 @@ __device__ inline double dev_reduced_gradient(const DevDD& d) {
 
 // Middle eigenvalue of the symmetric 3x3 Hessian by cyclic Jacobi rotations
 // (the sign decides sign(lambda2) rho, src/evaluator.cpp:158-161).
-__device__ inline double dev_lambda2(const double* h6) {
-    double a[3][3] = {{h6[0], h6[1], h6[2]}, {h6[1], h6[3], h6[4]}, {h6[2], h6[4], h6[5]}};
+// Hessian entries xx, xy, xz, yy, yz, zz by value: the caller's record then
+// need not live in memory.
+static __device__ __noinline__ double dev_lambda2(double xx, double xy, double xz, double yy, double yz, double zz) {
+    double a[3][3] = {{xx, xy, xz}, {xy, yy, yz}, {xz, yz, zz}};
     for (int sweep = 0; sweep < 64; ++sweep) {
         const double off = fabs(a[0][1]) + fabs(a[0][2]) + fabs(a[1][2]);
         if (off == 0.0) break;
@@ -151,6 +153,35 @@ __device__ inline double dev_lambda2(const double* h6) {
     if ((e0 >= e1 && e0 <= e2) || (e0 <= e1 && e0 >= e2)) return e0;
     if ((e1 >= e0 && e1 <= e2) || (e1 <= e0 && e1 >= e2)) return e1;
     return e2;
+}
+
+// Whether lambda2 < 0 (lambda2 == 0 counts as positive).  The eigenvalues
+// l1 <= l2 <= l3 are the roots of det(x I - H); with e1 = l1 + l2 + l3,
+// e2 = l1 l2 + l1 l3 + l2 l3 and e3 = l1 l2 l3, l2 < 0 exactly when at least
+// two eigenvalues are negative: for e3 < 0 when all three are (e1 < 0 and
+// e2 > 0), for e3 > 0 unless all three are positive (e1 > 0 and e2 > 0).
+// Where e1, e2 and e3 all stand clear of zero (|e_k| > 1e-8 |H|_F^k, far
+// above their rounding errors) the signs are exact and |l2| > 1e-8 |H|_F,
+// so the answer is the Jacobi eigenvalue's sign; elsewhere the Jacobi
+// eigenvalue decides.  H is first scaled by a power of two (exactly) to
+// entries of magnitude below 2, so that no product under- or overflows.
+__device__ __forceinline__ bool dev_lambda2_negative(const double* h6) {
+    double m = 0.0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) m = fmax(m, fabs(h6[i]));
+    // (A NaN entry makes the e_k NaN, and the margins then fail.)
+    if (!(m > 0.0) || !isfinite(m)) return dev_lambda2(h6[0], h6[1], h6[2], h6[3], h6[4], h6[5]) < 0.0;
+    const int ex = ilogb(m);
+    const double a = ldexp(h6[0], -ex), b = ldexp(h6[1], -ex), c = ldexp(h6[2], -ex);
+    const double d = ldexp(h6[3], -ex), e = ldexp(h6[4], -ex), f = ldexp(h6[5], -ex);
+    const double e1 = a + d + f;
+    const double e2 = (a * d - b * b) + (a * f - c * c) + (d * f - e * e);
+    const double e3 = a * (d * f - e * e) - b * (b * f - c * e) + c * (b * e - c * d);
+    const double s2 = (a * a + d * d + f * f) + 2.0 * ((b * b + c * c) + e * e);
+    const double k2 = 1e-16;  // (1e-8)^2
+    if (e1 * e1 > k2 * s2 && e2 * e2 > k2 * s2 * s2 && e3 * e3 > k2 * s2 * s2 * s2)
+        return e3 < 0.0 ? (e1 < 0.0 && e2 > 0.0) : !(e1 > 0.0 && e2 > 0.0);
+    return dev_lambda2(h6[0], h6[1], h6[2], h6[3], h6[4], h6[5]) < 0.0;
 }
 
 __device__ inline double dev_iri(const DevDD& d) {
@@ -189,7 +220,7 @@ __device__ __forceinline__ void store_one(int kind, const DevDD& d, double* out,
         case 4: out[p] = d.tau; break;
         case 6: out[p] = dev_elf(one, 1); break;
         case 7: out[p] = dev_reduced_gradient(d); break;
-        case 8: out[p] = dev_lambda2(d.hess) < 0.0 ? -d.value : d.value; break;
+        case 8: out[p] = dev_lambda2_negative(d.hess) ? -d.value : d.value; break;
         case 10: out[p] = dev_lol(one, 1); break;
         case 35: out[p] = dev_gradient_expansion(one, 1, false); break;
         case 36: out[p] = dev_gradient_expansion(one, 1, true); break;

@@ -143,10 +143,12 @@ __device__ __forceinline__ unsigned instr_desc(int n) {
            (static_cast<unsigned>(128 >> 4) << 24);
 }
 
-// MG (8 or 4) consecutive FP32 columns of the warp's 32 lanes.
+// MG (8, 4 or 2) consecutive FP32 columns of the warp's 32 lanes.
 template <int MG>
 __device__ __forceinline__ void tmem_ld(unsigned taddr, unsigned (&r)[MG]) {
-    if constexpr (MG == 8) {
+    if constexpr (MG == 2) {
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(taddr));
+    } else if constexpr (MG == 8) {
         asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
                      : "r"(taddr));
@@ -160,7 +162,9 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 // Orders later uses of r after the preceding wait::ld.
 template <int MG>
 __device__ __forceinline__ void reg_fence(unsigned (&r)[MG]) {
-    if constexpr (MG == 8)
+    if constexpr (MG == 2)
+        asm volatile("" : "+r"(r[0]), "+r"(r[1]));
+    else if constexpr (MG == 8)
         asm volatile("" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]));
     else
         asm volatile("" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]));
