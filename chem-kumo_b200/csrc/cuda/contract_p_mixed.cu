@@ -179,6 +179,8 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
             }
             __syncthreads();
             float4 ra[kPL][2];
+            // Panel rows of step t into registers (read again for every
+            // column chunk and density matrix: default caching).
             auto load_a = [&](int t) {
                 const int k = t * 16 + kh * 8 + k8;
                 const bool ok = k < nk;
@@ -190,8 +192,8 @@ __global__ void __launch_bounds__(kThreads, 1) contract_p_mixed_kernel(const __g
                         const float4* src =
                             reinterpret_cast<const float4*>(pbase + static_cast<size_t>(c) * pstride +
                                                             static_cast<size_t>(row) * kBlockPoints + g * 8);
-                        ra[c][0] = __ldcs(src);
-                        ra[c][1] = __ldcs(src + 1);
+                        ra[c][0] = __ldg(src);
+                        ra[c][1] = __ldg(src + 1);
                     } else {
                         ra[c][0] = ra[c][1] = make_float4(0.f, 0.f, 0.f, 0.f);
                     }
