@@ -154,21 +154,6 @@ DeviceMolecule::DeviceMolecule(const Molecule& m) {
     const Matrix pt = m.density_matrix(DensityComponent::Total);
     const Matrix ps = m.density_matrix(DensityComponent::Difference);
     p_total = upload(pt.data(), pt.size());
-    auto split_matrix = [&](const Matrix& m) {
-        std::vector<std::uint16_t> pieces(4 * n * n, 0);
-        for (std::size_t r = 0; r < n; ++r)
-            for (std::size_t c = 0; c < n; ++c) {
-                double rest = m(r, c);
-                for (int k = 0; k < 3; ++k) {
-                    const std::uint16_t h = bf16_bits(rest);
-                    pieces[(r * n + c) * 4 + static_cast<std::size_t>(k)] = h;
-                    rest -= bf16_value(h);
-                }
-            }
-        return upload(pieces.data(), pieces.size());
-    };
-    p_total_s = split_matrix(pt);
-    p_spin_s = split_matrix(ps);
     p_spin = upload(ps.data(), ps.size());
     unrestricted = m.unrestricted();
     const Matrix& ca = m.mo_coefficients(SpinChannel::Alpha);
@@ -205,6 +190,28 @@ DeviceMolecule::DeviceMolecule(const Molecule& m) {
         transpose_occ(ca, nocc_alpha, ldc_alpha, ct_alpha, ldn_alpha, cs_alpha);
         transpose_occ(unrestricted ? cb : ca, nocc_beta, ldc_beta, ct_beta, ldn_beta, cs_beta);
     }
+}
+
+void DeviceMolecule::ensure_p_pieces(const Molecule& m) {
+    std::lock_guard<std::mutex> lock(esp_mutex);
+    if (p_total_s) return;
+    const std::size_t n = m.basis_size();
+    auto split_matrix = [&](const Matrix& a) {
+        std::vector<std::uint16_t> pieces(4 * n * n, 0);
+        for (std::size_t r = 0; r < n; ++r)
+            for (std::size_t c = 0; c < n; ++c) {
+                double rest = a(r, c);
+                for (int k = 0; k < 3; ++k) {
+                    const std::uint16_t h = bf16_bits(rest);
+                    pieces[(r * n + c) * 4 + static_cast<std::size_t>(k)] = h;
+                    rest -= bf16_value(h);
+                }
+            }
+        return upload(pieces.data(), pieces.size());
+    };
+    std::uint16_t* spin = split_matrix(m.density_matrix(DensityComponent::Difference));
+    p_spin_s = spin;
+    p_total_s = split_matrix(m.density_matrix(DensityComponent::Total));
 }
 
 kumo_dev::EspDevice& DeviceMolecule::esp_state(const Molecule& m, cudaStream_t stream) {

@@ -50,8 +50,11 @@ struct DeviceMolecule {
     // [piece][AO][MO] with rows of ldn MOs (a multiple of 16, zero padded).
     // P_total and P_spin for the mixed AO-P form: each element as its three
     // BF16 pieces and a zero, [row][col][4] (one 8-byte load per element).
+    // Built on first use by ensure_p_pieces (the AO-MO form never reads them,
+    // and splitting a large P costs the host far more than a launch).
     std::uint16_t* p_total_s = nullptr;
     std::uint16_t* p_spin_s = nullptr;
+    void ensure_p_pieces(const Molecule& m);
     std::uint16_t* cs_alpha = nullptr;
     std::uint16_t* cs_beta = nullptr;
     int ldn_alpha = 0, ldn_beta = 0;
@@ -66,7 +69,7 @@ struct DeviceMolecule {
     // Primitive pairs of the electrostatic potential, built on first use and
     // kept with the molecule (their host set-up costs far more than a launch).
     std::unique_ptr<kumo_dev::EspDevice> esp;
-    std::mutex esp_mutex;
+    std::mutex esp_mutex;  // guards every state built on first use
     kumo_dev::EspDevice& esp_state(const Molecule& m, cudaStream_t stream);
     // Scaled MO columns of the orbital-energy sums, one entry per set of
     // needs met so far, built on first use and kept with the molecule.

@@ -906,6 +906,7 @@ private:
         cp.block_size = static_cast<long long>(bs);
         cp.count = lay.count;
         cp.nao = nao;
+        dev_->ensure_p_pieces(mol_);
         cp.p_total_s = dev_->p_total_s;
         cp.p_spin_s = dev_->p_spin_s;
         cp.total_needed = needed[0] || needed[1] || needed[2];
