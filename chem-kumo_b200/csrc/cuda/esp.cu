@@ -3,10 +3,13 @@
 #include "esp.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <exception>
 #include <numbers>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <type_traits>
 
 #include "../host/device_state.hpp"
@@ -120,10 +123,17 @@ EspDevice::EspDevice(const chem::kumo::Molecule& m, cudaStream_t stream) {
     const chem::kumo::Matrix P = m.density_matrix(chem::kumo::DensityComponent::Total);
     std::vector<chem::kumo::Matrix> transforms(kMaxL + 1);
     for (int l = 2; l <= kMaxL; ++l) transforms[static_cast<std::size_t>(l)] = chem::kumo::gaussian_cartesian_to_pure(l);
-    std::vector<EspPair> pairs;
-    std::vector<double> coef;
-    std::vector<double> cart, left, pc;
-    for (std::size_t a = 0; a < blocks.size(); ++a) {
+    // The pairs of each first block a are built independently (host threads
+    // take blocks a from a shared counter) and joined in the order of a, so
+    // the pair list is the same as one thread's.
+    struct Part {
+        std::vector<EspPair> pairs;
+        std::vector<double> coef;
+    };
+    std::vector<Part> parts(blocks.size());
+    auto build_a = [&](std::size_t a, std::vector<double>& cart, std::vector<double>& left, std::vector<double>& pc) {
+        std::vector<EspPair>& pairs = parts[a].pairs;
+        std::vector<double>& coef = parts[a].coef;
         const auto& A = blocks[a];
         for (std::size_t bb = a; bb < blocks.size(); ++bb) {
             const auto& B = blocks[bb];
@@ -193,6 +203,38 @@ EspDevice::EspDevice(const chem::kumo::Molecule& m, cudaStream_t stream) {
                     for (double x : pc) coef.push_back(scale * x);
                 }
         }
+    };
+    {
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const std::size_t nthreads = blocks.size() < 64 ? 1 : std::min<std::size_t>(hw, 32);
+        std::atomic<std::size_t> next{0};
+        std::vector<std::exception_ptr> errors(nthreads);
+        auto worker = [&](std::size_t t) {
+            try {
+                std::vector<double> cart, left, pc;
+                for (std::size_t a = next++; a < blocks.size(); a = next++) build_a(a, cart, left, pc);
+            } catch (...) {
+                errors[t] = std::current_exception();
+                next = blocks.size();
+            }
+        };
+        std::vector<std::thread> pool;
+        for (std::size_t t = 1; t < nthreads; ++t) pool.emplace_back(worker, t);
+        worker(0);
+        for (auto& th : pool) th.join();
+        for (const auto& e : errors)
+            if (e) std::rethrow_exception(e);
+    }
+    std::vector<EspPair> pairs;
+    std::vector<double> coef;
+    for (auto& part : parts) {
+        const int base = static_cast<int>(coef.size());
+        for (EspPair pr : part.pairs) {
+            pr.first += base;
+            pairs.push_back(pr);
+        }
+        coef.insert(coef.end(), part.coef.begin(), part.coef.end());
+        part = Part{};
     }
     // Pairs grouped by order (stable), so that each launch of the device
     // kernel handles one order with its recursion unrolled.
