@@ -73,6 +73,7 @@ struct ContractPMixedParams {
     // values only, so only Y_0 = Phi_0 P is formed and folded.
     int value_only = 0;
     float threshold = 0.0f;
+    int sort_cap = 0;  // rows the row-order arrays hold (set at launch)
     FieldSpec spec;
     unsigned* status = nullptr;
     // Limit of each tensor-core pipeline wait in ns (0: one second); a wait

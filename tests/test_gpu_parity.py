@@ -554,16 +554,21 @@ def test_mixed_tensor_core_ao_p(name, case):
         assert np.abs(a - r).max() / scale <= 1e-6, (p, np.abs(a - r).max() / scale)
 
 
-@pytest.mark.parametrize("with_hessian", [False, True])
-def test_mixed_ao_p_grid_densities(with_hessian):
+@pytest.mark.parametrize("extra", ["none", "hessian", "spin_gradient"])
+def test_mixed_ao_p_grid_densities(extra):
     # On a grid the FP64 AO-P form takes each density on the blocked grid path;
-    # the mixed form computes them in its tensor-core point pass (values-only
-    # products for a matrix whose components need no derivatives).
+    # the mixed form computes them in its tensor-core point pass.  A density
+    # matrix whose components need no derivatives is contracted with the value
+    # panel only, in the same pass as the other matrix: values only for both
+    # ("none"), four panels of P_total with P_spin's values ("hessian"), and
+    # four panels of P_spin with P_total's values ("spin_gradient").
     m = K.Molecule.from_fchk(os.path.join(GOLDEN, "o2.fchk.gz"))
     grid = m.grid_around(2.0, 0.25)
     props = [K.density(P.Density, c) for c in (D.Alpha, D.Beta, D.Difference, D.Total)]
-    if with_hessian:
+    if extra == "hessian":
         props += [K.density(P.ReducedGradient), K.density(P.SignLambda2Density)]
+    elif extra == "spin_gradient":
+        props += [K.density(P.Gradient, D.Difference), K.density(P.Tau, D.Difference)]
     f64, used = K.Evaluator(m, backend=K.Backend.AO_P).evaluate_grid(grid, props)
     mix, used_m = K.Evaluator(m, backend=K.Backend.AO_P, precision=K.Precision.Mixed).evaluate_grid(grid, props)
     assert used == used_m == int(K.Backend.AO_P)
