@@ -149,6 +149,13 @@ private:
 // memory back to the driver and the next evaluation maps it again, which
 // blocks the host for tens to hundreds of milliseconds per call; keep it
 // cached instead (once per device).
+//
+// The pool may also hand an allocation on one stream memory whose free is
+// still queued on another stream, making the first stream wait for all the
+// work queued before that free.  Evaluations issued concurrently on separate
+// streams (the serving loop's slots) would then wait for one another: a small
+// request for a large one that happened to free a block first.  That reuse is
+// turned off; memory freed by work that has completed is still reused.
 void keep_pool_memory() {
     static std::once_flag flags[64];
     int dev = 0;
@@ -159,6 +166,9 @@ void keep_pool_memory() {
         check_cuda(cudaDeviceGetDefaultMemPool(&pool, dev), "cudaDeviceGetDefaultMemPool");
         unsigned long long keep = ~0ull;
         check_cuda(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep),
+                   "cudaMemPoolSetAttribute");
+        int no_wait = 0;
+        check_cuda(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no_wait),
                    "cudaMemPoolSetAttribute");
     });
 }
