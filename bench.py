@@ -308,7 +308,7 @@ def _serve_arrivals(K, srv, precision: int, seconds: float, rate: float, pool, s
 
 
 def serve_bench(K, synth, precision: int, seconds: float, rate: float, pool, seed: int, graph_points: int = 65536,
-                scratch_gb: float = 2.0, warmup_s: float = 5.0):
+                scratch_gb: float = 2.0, warmup_s: float = 0.0):
     """Serving loop under the serving workload: Poisson arrivals at `rate`
     requests/s for `seconds`, each request one type drawn uniformly (cube of
     40^3..160^3 points at 0.2 bohr, 200x200 plane at 0.2 bohr, 1000-point line,
@@ -318,12 +318,11 @@ def serve_bench(K, synth, precision: int, seconds: float, rate: float, pool, see
     until the results are in the caller's arrays; the run ends when every
     request is done.
 
-    Before the measured window, `warmup_s` seconds of the same arrivals (another
-    seed) run through a server of their own and are not counted: the first
-    launch of each kernel in a process loads it (CUDA's lazy module loading,
-    which holds up every issuing thread) and the stream-ordered memory pool
-    grows to the serving footprint, one-time costs of a server process that
-    would otherwise sit in the measured latencies."""
+    With `warmup_s` > 0, that many seconds of the same arrivals (another seed)
+    run first through a server of their own and are not counted, so that the
+    stream-ordered memory pool has grown to the serving footprint (the server
+    itself loads every kernel of the library when it is created).  The default
+    measures a cold server."""
     kw = dict(max_active=8, graph_points=graph_points, request_scratch_bytes=scratch_gb * 2**30)
     if warmup_s > 0:
         warm = K.Server(**kw)
@@ -504,7 +503,7 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--grid-n", type=int, default=0, help="points per axis (default: the workload's 128)")
     ap.add_argument("--serve-seconds", type=float, default=5.0, help="arrival window of the serving run (0: skip)")
-    ap.add_argument("--serve-warmup", type=float, default=5.0,
+    ap.add_argument("--serve-warmup", type=float, default=0.0,
                     help="seconds of uncounted arrivals (own server, other seed) before the measured window")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="mean arrivals per second")
     ap.add_argument("--serve-pool", type=int, default=32, help="molecules in the serving pool")
@@ -680,9 +679,10 @@ def main() -> None:
                                          f"{args.serve_scratch_gb:g} GiB AO scratch per request",
                             "graphs": f"requests <= {args.serve_graph_points} points replay CUDA graphs "
                                       "from the second time their shape is met",
-                            "warmup": f"{args.serve_warmup:g} s of the same arrivals (other seed) through a "
-                                      "server of their own before the measured window, not counted "
-                                      "(loads each kernel once, grows the memory pool)"},
+                            "warmup": (f"{args.serve_warmup:g} s of the same arrivals (other seed) through a "
+                                       "server of their own before the measured window, not counted"
+                                       if args.serve_warmup > 0 else
+                                       "none (the server loads every kernel of the library when created)")},
                  "mixed": serve_bench(K, synth, int(K.Precision.Mixed), args.serve_seconds, args.serve_rate, pool,
                                       21, **kw),
                  "fp64": serve_bench(K, synth, int(K.Precision.FP64), args.serve_seconds, args.serve_rate, pool,

@@ -9,6 +9,7 @@ template <int ORDER, int P, int MAXL>
 static void launch(const AoBuildParams<double>& p, cudaStream_t stream) {
     const size_t smem = sizeof(double) * ((size_t)p.basis.max_count * P * kBlockPoints + (size_t)kMaxPrim * kBlockPoints) +
                         sizeof(int) * (size_t)p.basis.nblocks;
+    KUMO_REGISTER_KERNEL(ao_build_kernel<double, ORDER, P, MAXL>);
     ensure_dynamic_smem(reinterpret_cast<const void*>(ao_build_kernel<double, ORDER, P, MAXL>), (int)smem);
     ao_build_kernel<double, ORDER, P, MAXL><<<p.nblocks, kBlockPoints, smem, stream>>>(p);
 }

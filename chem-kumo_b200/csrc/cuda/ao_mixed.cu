@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(kBlockPoints, (P == 10 || MAXL >= 4) ? 6 : 8) 
 
 template <int P, int MAXL>
 void launch(const AoMixedParams& p, cudaStream_t stream) {
+    KUMO_REGISTER_KERNEL(ao_mixed_kernel<P, MAXL>);
     const size_t smem = sizeof(int) * static_cast<size_t>(p.basis.nblocks > 0 ? p.basis.nblocks : 1);
     if (smem > 48 * 1024)
         ensure_dynamic_smem(reinterpret_cast<const void*>(ao_mixed_kernel<P, MAXL>), static_cast<int>(smem));

@@ -212,6 +212,7 @@ static void launch_mo(const ContractMoParams& p, cudaStream_t stream) {
     constexpr int MOC = 8 * MPT;
     constexpr int Q = NQ<P>::v;
     const size_t smem = sizeof(double) * (size_t)(2 * KT * P * 32 + 2 * KT * MOC + 2 * Q * 32);
+    KUMO_REGISTER_KERNEL(contract_mo_f64_kernel<P, MPT, KT>);
     ensure_dynamic_smem(reinterpret_cast<const void*>(contract_mo_f64_kernel<P, MPT, KT>), (int)smem);
     contract_mo_f64_kernel<P, MPT, KT><<<p.nblocks * 4, 256, smem, stream>>>(p);
 }
@@ -399,6 +400,7 @@ __global__ void __launch_bounds__(256, 1) orbital_energy_f64_kernel(const __grid
 void launch_orbital_energy_f64(const OrbitalEnergyParams& p, cudaStream_t stream) {
     constexpr int KT = 16;
     const size_t smem = sizeof(double) * (size_t)(2 * KT * 32 + 2 * KT * 128 + 8 * 2 * kOrbitalEnergySets * 32);
+    KUMO_REGISTER_KERNEL(orbital_energy_f64_kernel<KT>);
     ensure_dynamic_smem(reinterpret_cast<const void*>(orbital_energy_f64_kernel<KT>), (int)smem);
     orbital_energy_f64_kernel<KT><<<p.nblocks * 4, 256, smem, stream>>>(p);
 }
@@ -431,6 +433,7 @@ __global__ void __launch_bounds__(128) orbitals_f64_kernel(const __grid_constant
 }
 
 void launch_orbitals_f64(const OrbitalParams& p, cudaStream_t stream) {
+    KUMO_REGISTER_KERNEL(orbitals_f64_kernel);
     orbitals_f64_kernel<<<p.nblocks, 128, 0, stream>>>(p);
 }
 
@@ -631,6 +634,7 @@ static void launch_p(const ContractPParams& p, cudaStream_t stream) {
     constexpr int Q = NQ<P>::v;
     const size_t smem = sizeof(double) * (size_t)(2 * KT * NY * 32 + 2 * KT * RC + 2 * Q * 32) + sizeof(int) * RC;
     static_assert(8 * Q * 32 <= 2 * KT * NY * 32 || VALUES, "reduction buffer must fit the tile buffers");
+    KUMO_REGISTER_KERNEL(contract_p_f64_kernel<P, VALUES, RPT, KT>);
     ensure_dynamic_smem(reinterpret_cast<const void*>(contract_p_f64_kernel<P, VALUES, RPT, KT>), (int)smem);
     contract_p_f64_kernel<P, VALUES, RPT, KT><<<p.nblocks * 4, 256, smem, stream>>>(p);
 }

@@ -1655,6 +1655,7 @@ void launch_fused(const ContractFusedParams& p, cudaStream_t stream) {
     constexpr size_t kMaxSmem = 227u * 1024u;
     if (FusedSmem<P, S>::total(p.ncols) > kMaxSmem)
         throw std::invalid_argument("fused tensor-core contraction: stages exceed shared memory");
+    KUMO_REGISTER_KERNEL(contract_fused_kernel<P, S, MAXL>);
     ensure_dynamic_smem(reinterpret_cast<const void*>(contract_fused_kernel<P, S, MAXL>), static_cast<int>(kMaxSmem));
     contract_fused_kernel<P, S, MAXL><<<p.ao.nblocks, kThreads, kMaxSmem, stream>>>(p);
 }
@@ -1706,6 +1707,7 @@ bool launch_bulk(const ContractMixedParams& p, cudaStream_t stream) {
         return false;
     CUtensorMap map;
     if (!panel_row_map(p, P, map)) return false;
+    KUMO_REGISTER_KERNEL(contract_bulk_kernel<P, F, SB>);
     ensure_dynamic_smem(reinterpret_cast<const void*>(contract_bulk_kernel<P, F, SB>), static_cast<int>(kMaxSmem));
     contract_bulk_kernel<P, F, SB><<<p.nblocks, kBulkThreads, kMaxSmem, stream>>>(p, map);
     return true;
@@ -1732,6 +1734,7 @@ void launch(const ContractMixedParams& p, cudaStream_t stream) {
     constexpr size_t kMaxSmem = 227u * 1024u;
     if (Smem<P, S>::total(p.ncols) > kMaxSmem) throw std::invalid_argument("tensor-core contraction: stages exceed shared memory");
     const size_t smem = kMaxSmem;
+    KUMO_REGISTER_KERNEL(contract_mixed_kernel<P, S>);
     ensure_dynamic_smem(reinterpret_cast<const void*>(contract_mixed_kernel<P, S>), static_cast<int>(smem));
     contract_mixed_kernel<P, S><<<p.nblocks, kCtaThreads<S>, smem, stream>>>(p);
 }

@@ -508,6 +508,7 @@ void launch(const ContractPMixedParams& p, cudaStream_t stream) {
     ContractPMixedParams q = p;
     q.sort_cap = static_cast<int>(std::min<unsigned>(SmemP<P>::cap16(p.scr.row_stride), kSortCap));
     const size_t smem = SmemP<P>::total(static_cast<unsigned>(q.sort_cap));
+    KUMO_REGISTER_KERNEL(contract_p_mixed_kernel<P>);
     ensure_dynamic_smem(reinterpret_cast<const void*>(contract_p_mixed_kernel<P>), static_cast<int>(kMaxSmem));
     contract_p_mixed_kernel<P><<<p.nblocks, kThreads, smem, stream>>>(q);
 }

@@ -1,6 +1,7 @@
 // Electrostatic potential: host setup of the primitive pairs and the FP64
 // device kernel; see esp.cuh.
 #include "esp.cuh"
+#include "func_attr.cuh"
 
 #include <algorithm>
 #include <atomic>
@@ -610,6 +611,8 @@ __global__ void __launch_bounds__(128) esp_reduce_kernel(const __grid_constant__
 template <int L>
 void launch_order(const EspParams& p, long long first, long long count, long long chunk, int chunks, int slot0,
                   double* part, long long ld, unsigned tiles, cudaStream_t stream) {
+    KUMO_REGISTER_KERNEL(esp_order_kernel<L, true>);
+    KUMO_REGISTER_KERNEL(esp_order_kernel<L, false>);
     if (p.mixed) {
         esp_order_kernel<L, true><<<dim3(tiles, static_cast<unsigned>(chunks)), 128, 0, stream>>>(
             p, first, count, chunk, slot0, part, ld);
@@ -665,6 +668,7 @@ void launch_esp(const EspParams& p, cudaStream_t stream) {
         }
         slot += nc;
     }
+    KUMO_REGISTER_KERNEL(esp_reduce_kernel);
     esp_reduce_kernel<<<tiles, 128, 0, stream>>>(p, part, nslots, ld);
     if (part) cudaFreeAsync(part, stream);
 }
@@ -678,6 +682,7 @@ __global__ void boys_kernel(const double* table, const double* t, long long n, i
 }
 
 void launch_boys_f64(const double* table, const double* t, long long n, int nvalues, double* out, cudaStream_t stream) {
+    KUMO_REGISTER_KERNEL(boys_kernel);
     if (n <= 0) return;
     boys_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(table, t, n, nvalues, out);
 }

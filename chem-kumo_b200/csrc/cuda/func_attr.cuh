@@ -6,8 +6,31 @@
 #include <map>
 #include <mutex>
 #include <utility>
+#include <vector>
 
 namespace kumo_dev {
+
+// Every kernel instantiation the library launches, listed while the library
+// loads: a launch site names its kernel with KUMO_REGISTER_KERNEL, whose
+// class-template static member adds the kernel to the list during static
+// initialisation, before any launch.  preload_kernels() asks CUDA for each
+// listed kernel's attributes once per device, which loads it; otherwise CUDA
+// loads a kernel at its first launch, and every host thread launching
+// meanwhile waits.  Defined in csrc/host/evaluator.cu.
+std::vector<const void*>& kernel_registry();
+void preload_kernels();
+
+inline bool register_kernel(const void* func) {
+    kernel_registry().push_back(func);
+    return true;
+}
+
+template <auto Func>
+struct KernelEntry {
+    static inline const bool registered = register_kernel(reinterpret_cast<const void*>(Func));
+};
+
+#define KUMO_REGISTER_KERNEL(...) (void)::kumo_dev::KernelEntry<&__VA_ARGS__>::registered
 
 // Raises a kernel's dynamic shared-memory limit once per device (again only
 // for a larger size).  Setting a function attribute while launches of that

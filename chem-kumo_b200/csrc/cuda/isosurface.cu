@@ -18,6 +18,7 @@
 #include <stdexcept>
 #include <string>
 
+#include "func_attr.cuh"
 #include "isosurface.cuh"
 
 namespace kumo_dev {
@@ -265,6 +266,7 @@ bool iso_reaches_boundary(const IsoGrid& g, const double* samples, double iso, c
     int* hit = nullptr;
     check(cudaMallocAsync(reinterpret_cast<void**>(&hit), sizeof(int), stream), "cudaMallocAsync (isosurface)");
     check(cudaMemsetAsync(hit, 0, sizeof(int), stream), "cudaMemsetAsync (isosurface)");
+    KUMO_REGISTER_KERNEL(boundary_kernel);
     boundary_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, stream>>>(g, samples, iso, n, hit);
     int h = 0;
     check(cudaMemcpyAsync(&h, hit, sizeof(int), cudaMemcpyDeviceToHost, stream), "cudaMemcpyAsync (isosurface)");
@@ -291,6 +293,8 @@ void iso_polygonize(const IsoGrid& g, const double* samples, double iso, std::ve
     int* vbase = bases;
     int* pbase = bases + n;
     const unsigned blocks = static_cast<unsigned>((ncells + 127) / 128);
+    KUMO_REGISTER_KERNEL(count_kernel);
+    KUMO_REGISTER_KERNEL(emit_kernel);
     count_kernel<<<blocks, 128, 0, stream>>>(g, samples, iso, ncells, vcount, pcount);
     check(cudaGetLastError(), "isosurface count kernel");
     size_t tmp_bytes = 0;

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../cuda/esp.cuh"
+#include "../cuda/func_attr.cuh"
 #include "../cuda/mixed.cuh"
 #include "grid_geometry.hpp"
 #include "chem/kumo/cube.hpp"
@@ -305,6 +306,12 @@ void kumo_default_options(kumo_options* opt) {
 int kumo_set_device(int device, char* err, size_t errlen) {
     return guarded(err, errlen, [&] { detail::check_cuda(cudaSetDevice(device), "cudaSetDevice"); });
 }
+
+int kumo_preload_kernels(char* err, size_t errlen) {
+    return guarded(err, errlen, [&] { kumo_dev::preload_kernels(); });
+}
+
+int kumo_registered_kernels(void) { return static_cast<int>(kumo_dev::kernel_registry().size()); }
 
 int kumo_molecule_from_fchk(const char* path, kumo_molecule** out, char* err, size_t errlen) {
     return guarded(err, errlen, [&] {

@@ -20,6 +20,7 @@
 
 #include "../cuda/contract.cuh"
 #include "../cuda/esp.cuh"
+#include "../cuda/func_attr.cuh"
 #include "../cuda/mixed.cuh"
 #include "chem/kumo/evaluator.hpp"
 #include "device_state.hpp"
@@ -275,12 +276,43 @@ int sm_count() {
 
 }  // namespace
 
+}  // namespace chem::kumo
+
+namespace kumo_dev {
+
+std::vector<const void*>& kernel_registry() {
+    static std::vector<const void*> kernels;
+    return kernels;
+}
+
+// Loads every listed kernel on the current device, once per device: asking
+// for a kernel's attributes makes CUDA load it.
+void preload_kernels() {
+    static std::once_flag flags[64];
+    int dev = 0;
+    chem::kumo::detail::check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= 64) return;
+    std::call_once(flags[dev], [] {
+        for (const void* f : kernel_registry()) {
+            cudaFuncAttributes a;
+            chem::kumo::detail::check_cuda(cudaFuncGetAttributes(&a, f), "cudaFuncGetAttributes (kernel preload)");
+        }
+    });
+}
+
+}  // namespace kumo_dev
+
+namespace chem::kumo {
+
 namespace detail {
 // Once-per-device set-up that must not run inside a CUDA stream capture: the
-// pool's release threshold and the tensor-core status word's address.
+// pool's settings, the tensor-core status word's address and every kernel of
+// the library loaded (a serving loop's threads would otherwise wait while
+// CUDA loads each kernel at its first launch).
 void prepare_device_for_capture() {
     keep_pool_memory();
     (void)kumo_dev::pipeline_status_word();
+    kumo_dev::preload_kernels();
 }
 }  // namespace detail
 

@@ -17,6 +17,10 @@
 // its wave size), plus the molecule's device copy when it is not resident yet
 // (molecule copies then stay resident).
 //
+// Creating a server loads every kernel of the library on its device
+// (kumo_dev::preload_kernels), so that no launcher waits while CUDA loads a
+// kernel at its first launch.
+//
 // Graph path (requests of at most graph_points points): the points are padded
 // to a power-of-two bucket (>= 128) by repeating the last point, which leaves
 // the last block's bounding box and screening unchanged; one CUDA graph per

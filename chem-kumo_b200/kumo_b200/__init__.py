@@ -154,6 +154,7 @@ EXPORTS = [
     "kumo_evaluate_points", "kumo_evaluate_grid_device", "kumo_evaluate_points_device", "kumo_ao_panels",
     "kumo_screening_masks", "kumo_boys", "kumo_esp_pair_count", "kumo_esp_pairs_evaluated", "kumo_write_cube", "kumo_grid_around",
     "kumo_profile_enable", "kumo_profile_reset", "kumo_profile_read", "kumo_set_device",
+    "kumo_preload_kernels", "kumo_registered_kernels",
     "kumo_evaluate_points_noalloc", "kumo_server_create", "kumo_server_destroy", "kumo_server_submit_grid",
     "kumo_server_submit_points", "kumo_server_wait", "kumo_server_drain", "kumo_server_stats_get",
     "kumo_server_reset_stats", "kumo_density_isosurface", "kumo_potential_surface", "kumo_ionization_energy_surface",
@@ -242,6 +243,8 @@ def lib():
                                            C.c_longlong, _I, _D, _D, _D, *eb]
         L.kumo_profile_enable.argtypes = [C.c_int]
         L.kumo_set_device.argtypes = [C.c_int, *eb]
+        L.kumo_preload_kernels.argtypes = [*eb]
+        L.kumo_registered_kernels.argtypes = []
         L.kumo_evaluate_points_noalloc.argtypes = [C.c_void_p, C.POINTER(_Options), _D, C.c_longlong,
                                                    C.POINTER(_Property), C.c_int, C.POINTER(_D), C.c_void_p, *eb]
         L.kumo_profile_read.argtypes = [C.POINTER(_ProfileEntry), C.c_int]
@@ -626,6 +629,18 @@ def tile_tuning_report() -> str:
 def set_device(device: int) -> None:
     e = _err()
     _check(lib().kumo_set_device(int(device), e, 512), e)
+
+
+def preload_kernels() -> None:
+    """Load every kernel of the library on the current device now (once per
+    device); CUDA otherwise loads each kernel at its first launch."""
+    e = _err()
+    _check(lib().kumo_preload_kernels(e, 512), e)
+
+
+def registered_kernels() -> int:
+    """Kernel instantiations the library lists for preloading (no GPU needed)."""
+    return int(lib().kumo_registered_kernels())
 
 
 def profile_enable(on: bool = True) -> None:

@@ -91,6 +91,15 @@ void kumo_default_options(kumo_options* opt);
  * GPU; no counterpart in the CPU-only reference). */
 int kumo_set_device(int device, char* err, size_t errlen);
 
+/* Load every kernel of this library on the current device now, once per
+ * device (no counterpart in the CPU-only reference).  CUDA otherwise loads
+ * each kernel at its first launch, and every host thread launching meanwhile
+ * waits; latency-sensitive callers make this call before taking traffic
+ * (kumo_server_create makes it).  kumo_registered_kernels returns how many
+ * kernel instantiations the library lists (available without a GPU). */
+int kumo_preload_kernels(char* err, size_t errlen);
+int kumo_registered_kernels(void);
+
 /* Molecule::from_fchk (include/chem/kumo/density.hpp:218; src/molecule.cpp:153-180). */
 int kumo_molecule_from_fchk(const char* path, kumo_molecule** out, char* err, size_t errlen);
 

@@ -25,6 +25,14 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(lib, name), name
 
 
+def test_kernels_listed_for_preloading_at_load():
+    # Every launch site lists its kernel while the library loads, so the
+    # preload (kumo_preload_kernels, run by kumo_server_create) covers each
+    # instantiation: AO builds, both contractions of each form, orbitals,
+    # potential orders, isosurface.
+    assert K.registered_kernels() >= 60
+
+
 @pytest.mark.parametrize("name", FCHKS)
 def test_molecule_matches_oracle(name):
     path = os.path.join(GOLDEN, name)
