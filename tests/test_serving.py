@@ -119,6 +119,23 @@ def test_serving_admission_under_small_budget():
     srv.close()
 
 
+@pytest.mark.gpu
+def test_kernel_preload_then_evaluation():
+    # Loading every listed kernel succeeds (each name resolves to a kernel of
+    # this device's code), a second call does nothing, and evaluations after
+    # it give the same bits as before.
+    m = K.Molecule.from_fchk(os.path.join(GOLDEN, "acrolein.fchk.gz"))
+    grid = m.grid_around(3.0, 0.3)
+    ev = K.Evaluator(m, precision=K.Precision.Mixed)
+    before = ev.evaluate_grid(grid, FIELDS)[0]
+    assert K.registered_kernels() >= 60
+    K.preload_kernels()
+    K.preload_kernels()
+    after = ev.evaluate_grid(grid, FIELDS)[0]
+    for a, b in zip(after, before):
+        assert np.array_equal(a, b)
+
+
 def test_serving_rejects_bad_requests_before_device_work():
     # Validation happens at submit, with the evaluator's exception types; no
     # GPU is needed to see it (creating the server needs one, so this only
