@@ -467,10 +467,13 @@ def test_mixed_exact_rows(monkeypatch, rows):
     for p, a, r in zip(hprops, hmix, hf64):
         assert np.all(np.isfinite(a)), p
         print("exact rows", rows, "ten panels", p, scaled_error(a, r))
-        assert scaled_error(a, r) <= 1e-6, (p, scaled_error(a, r))
-    # The default form (16 exact rows, FP64 radial sums in the AO kernel)
-    # holds rho, grad rho, lap rho and tau to 1e-7 scaled.
-    tol = 1e-7 if rows == 16 else 1e-6
+        # FP32 exact rows in the ten-panel kernel (measured 7.6e-8, 1.3e-7
+        # with none).
+        assert scaled_error(a, r) <= 3e-7, (p, scaled_error(a, r))
+    # FP64 exact rows: 16 hold rho, grad rho, lap rho and tau to 1.6e-9
+    # scaled (measured), every row exact gives the FP64 path's values
+    # (8.5e-16), none leaves the tensor cores' 1.6e-7.
+    tol = {0: 5e-7, 16: 1e-8}.get(rows, 1e-12)
     for p, a, r in zip(props[:4], mix[:4], f64[:4]):
         assert np.all(np.isfinite(a)), p
         print("exact rows", rows, p, scaled_error(a, r))
@@ -493,7 +496,11 @@ def test_mixed_precision_water(water28):
     f64, _ = K.Evaluator(m).evaluate_grid(grid, props)
     mix, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_grid(grid, props)
     for p, a, r in zip(props[:4], mix[:4], f64[:4]):
-        assert scaled_error(a, r) <= 1e-6, (p, scaled_error(a, r))
+        print("water mixed", p, scaled_error(a, r))
+        # Every row of this 28-AO molecule that reaches the exact-row floor
+        # is taken in FP64 (measured 2e-15).
+        assert scaled_error(a, r) <= 1e-10, (p, scaled_error(a, r))
+    print("water mixed ELF", scaled_error(mix[4], f64[4]))
     assert scaled_error(mix[4], f64[4]) <= 1e-5
 
 
@@ -521,11 +528,14 @@ def test_mixed_tensor_core_panels_and_components(name, case):
     total = {p.kind: r for p, r in zip(props, f64) if p.component == D.Total}
     for p, a, r in zip(props, mix, f64):
         assert np.all(np.isfinite(a)), p
-        tol = 1e-5 if p.kind == P.Elf else 1e-6
+        # Measured at most 5.7e-8 (ELF 3.8e-7) over every panel count and
+        # component.
+        tol = 2e-6 if p.kind == P.Elf else 1e-7
         # alpha - beta cancels: its FP32-level error follows the channels'
         # scale, so it is measured against the total of the same kind.
         scale = max(1.0, np.abs(total[p.kind]).max()) if p.component == D.Difference else max(1.0, np.abs(r).max())
         err = np.abs(a - r).max() / scale
+        print("panels", name, case, p, err)
         assert err <= tol, (p, err)
 
 
@@ -548,10 +558,13 @@ def test_mixed_tensor_core_ao_p(name, case):
             # Y = sum_j phi_j P_jk sums many cancelling density-matrix entries,
             # and D = tau - |grad rho|^2 / 8 rho of ELF cancels again: the
             # mixed AO-P form holds ELF to 1e-4 (the AO-MO form to 1e-5).
+            print("aop", name, case, p, "abs", np.abs(a - r).max())
             assert np.abs(a - r).max() <= 1e-4, (p, np.abs(a - r).max())
             continue
         scale = max(1.0, np.abs(total[p.kind]).max()) if p.component == D.Difference else max(1.0, np.abs(r).max())
-        assert np.abs(a - r).max() / scale <= 1e-6, (p, np.abs(a - r).max() / scale)
+        print("aop", name, case, p, np.abs(a - r).max() / scale)
+        # Measured at most 9.4e-8 (no exact rows in the AO-P form).
+        assert np.abs(a - r).max() / scale <= 2e-7, (p, np.abs(a - r).max() / scale)
 
 
 @pytest.mark.parametrize("extra", ["none", "hessian", "spin_gradient"])
