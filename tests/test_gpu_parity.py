@@ -592,10 +592,12 @@ def test_mixed_ao_p_grid_densities(extra):
         if p.kind == P.ReducedGradient:
             # RDG = |grad rho| / rho^(4/3): compared where rho > 1e-6.
             sel = rho > 1e-6
-            assert np.abs(a[sel] - r[sel]).max() / np.abs(r[sel]).max() <= 1e-5, p
+            print("gridaop", extra, p, "rdg", np.abs(a[sel] - r[sel]).max() / np.abs(r[sel]).max())
+            assert np.abs(a[sel] - r[sel]).max() / np.abs(r[sel]).max() <= 5e-7, p  # measured 7.8e-8
             continue
         scale = max(1.0, np.abs(rho).max())
-        assert np.abs(a - r).max() / scale <= 1e-6, (p, np.abs(a - r).max() / scale)
+        print("gridaop", extra, p, np.abs(a - r).max() / scale)
+        assert np.abs(a - r).max() / scale <= 2e-7, (p, np.abs(a - r).max() / scale)  # measured 9.4e-8
 
 
 def test_mixed_tensor_core_ao_p_many_column_chunks(synth_cache):
@@ -606,7 +608,8 @@ def test_mixed_tensor_core_ao_p_many_column_chunks(synth_cache):
     f64, _ = K.Evaluator(m, backend=K.Backend.AO_P).evaluate_points(pts, props)
     mix, _ = K.Evaluator(m, backend=K.Backend.AO_P, precision=K.Precision.Mixed).evaluate_points(pts, props)
     for p, a, r in zip(props, mix, f64):
-        assert scaled_error(a, r) <= 1e-6, (p, scaled_error(a, r))
+        print("chunks", p, scaled_error(a, r))
+        assert scaled_error(a, r) <= 5e-7, (p, scaled_error(a, r))  # measured 2.4e-7
 
 
 def test_mixed_tensor_core_several_mo_passes(synth_cache):
@@ -619,6 +622,8 @@ def test_mixed_tensor_core_several_mo_passes(synth_cache):
     f64, _ = K.Evaluator(m).evaluate_points(pts, props)
     mix, _ = K.Evaluator(m, precision=K.Precision.Mixed).evaluate_points(pts, props)
     for p, a, r in zip(props, mix, f64):
+        print("mopasses", p, scaled_error(a, r))
+        # FP32 exact rows in the ten-panel kernel: measured 4.6e-7.
         assert scaled_error(a, r) <= 1e-6, (p, scaled_error(a, r))
 
 
@@ -755,8 +760,11 @@ def test_bulk_copy_contraction_equals_register_staged(name, case, monkeypatch):
     ref, _ = K.Evaluator(m).evaluate_points(pts, props)
     for p, a, b, r, d in zip(props, bulk, staged, ref, default):
         assert np.array_equal(a, b), p
-        assert scaled_error(a, r) <= (1e-5 if p.kind == P.Elf else 1e-6), p
-        assert scaled_error(d, r) <= (1e-5 if p.kind == P.Elf else 1e-6), p
+        print("bulk", name, case, p, scaled_error(a, r), scaled_error(d, r))
+        # Measured: every row on the tensor cores 1.9e-7 (ELF 6.8e-7); the
+        # default exact rows 4e-10 (ELF 5.1e-7).
+        assert scaled_error(a, r) <= (2e-6 if p.kind == P.Elf else 5e-7), p
+        assert scaled_error(d, r) <= (2e-6 if p.kind == P.Elf else 1e-8), p
 
 
 def test_sharded_grid_equals_whole_grid():
